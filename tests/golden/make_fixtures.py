@@ -1,0 +1,57 @@
+"""Regenerate the golden fixtures under tests/golden/ from a chfem source tree.
+
+The reference's own regression data (its test/input/3D directory: two voxel images, their
+.nf settings files and the golden effective-tensor columns) is copied here so that the
+parity tests can run where the reference tree is absent.  Images are stored gzip-compressed.
+
+Usage:  python tests/golden/make_fixtures.py [/path/to/chfem]
+"""
+import gzip
+import json
+import os
+import shutil
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+CASES = {
+    # name: (image, shape z,y,x, nf file, result file, golden column, reference tolerance)
+    "thermal_ggg40": ("3D/ggg40_100.raw", (100, 100, 100), "3D/thermal/ggg40_100.nf",
+                      "3D/thermal/ggg40_100_result.bin", 0),
+    "elastic_ggg40": ("3D/ggg40_100.raw", (100, 100, 100), "3D/elastic/ggg40_100.nf",
+                      "3D/elastic/ggg40_100_result.bin", 1),
+    "fluid_fibers": ("3D/fibers_100x100x10.raw", (10, 100, 100), "3D/fluid/fibers_100x100x10.nf",
+                     "3D/fluid/fibers_100x100x10_result.bin", 2),
+}
+
+
+def main(ref_root):
+    src = os.path.join(ref_root, "test", "input")
+    manifest = {}
+    for name, (img, shape, nf, res, col) in CASES.items():
+        img_out = os.path.join(HERE, os.path.basename(img) + ".gz")
+        if not os.path.exists(img_out):
+            with open(os.path.join(src, img), "rb") as fi, gzip.open(img_out, "wb", compresslevel=9) as fo:
+                shutil.copyfileobj(fi, fo)
+        nf_out = name + ".nf"
+        shutil.copyfile(os.path.join(src, nf), os.path.join(HERE, nf_out))
+        vals = np.fromfile(os.path.join(src, res), dtype=np.float64)
+        k = 6 if name.startswith("elastic") else 3
+        C = vals[: k * k].reshape(k, k)
+        manifest[name] = {
+            "image": os.path.basename(img_out),
+            "shape_zyx": list(shape),
+            "nf": nf_out,
+            "direction": col,
+            "column": [float(v) for v in C[:, col]],
+            "reference_tolerance": 1e-4,
+            "source": f"test/input/{res}",
+        }
+    with open(os.path.join(HERE, "golden.json"), "w") as f:
+        json.dump(manifest, f, indent=1)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
