@@ -1,0 +1,961 @@
+// cudapcg_b200.cu -- the cudapcg C ABI on B200: model upload, device-resident Krylov loops
+// captured in CUDA graphs, precision modes.
+//
+// Reference counterparts: chfem/src/femhmg/cudapcg/cudapcg.cu (API object and dispatch),
+// solvers/pcg.cu, cg.cu, pminres.cu, minres.cu (iteration recurrences),
+// kernels/wrappers.cu (launches).  The recurrences, stopping tests and special cases are
+// the reference's; the execution is not: each iteration is two fused passes whose scalars
+// are finished on the device, and chunks of iterations replay as one CUDA graph.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include <chrono>
+
+#include "../../include/cudapcg_b200.h"
+#include "common.cuh"
+#include "stencil_te.cuh"
+#include "pointwise.cuh"
+#include "stencil_fluid.cuh"
+#include "minres.cuh"
+
+using namespace chfem;
+
+// ---------------------------------------------------------------------------------------
+// Errors: recorded, never fatal to the process, never reset the device.
+static std::string g_err;
+static void set_err(const char* where, const char* what) {
+  char buf[512];
+  snprintf(buf, sizeof(buf), "%s: %s", where, what);
+  g_err = buf;
+  fprintf(stderr, "chfem_b200 error: %s\n", buf);
+}
+#define CK(call)                                                   \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) {                                       \
+      set_err(#call, cudaGetErrorString(e_));                      \
+      return CUDAPCG_FALSE;                                        \
+    }                                                              \
+  } while (0)
+#define CKV(call)                                                  \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) { set_err(#call, cudaGetErrorString(e_)); return false; } \
+  } while (0)
+
+static int g_num_sms = 0;
+static int num_sms() {
+  if (!g_num_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 148;
+  }
+  return g_num_sms;
+}
+
+// ---------------------------------------------------------------------------------------
+// Dense element matrices from the reference's local-matrix formats (cudapcgSetLclMtxs).
+// Thermal: 40 stored non-zeros per material, rows 0..7 in ascending column order, the
+// zeros being the pairs of nodes that share an edge (femhmg_thermal_3D.c:42-120).
+static void sparseq1_to_dense(const double* sp, double* dense) {
+  int p = 0;
+  for (int a = 0; a < 8; a++)
+    for (int b = 0; b < 8; b++) dense[a * 8 + b] = shares_edge(a, b) ? 0.0 : sp[p++];
+}
+
+// ---------------------------------------------------------------------------------------
+struct Solver {
+  // configuration (cudapcg.cu:108-183 defaults)
+  int analysis = 0, par = 0;
+  double tol = 0.00001;
+  unsigned maxit = 100000;
+  int solver_flag = CUDAPCG_CG_SOLVER;
+  int precond = 1;
+  int resnorm = CUDAPCG_L2_NORM;
+  std::string header;
+  int precision = CHFEM_B200_FP64;
+  unsigned replace_every = 50;
+  unsigned iters_per_launch = 16;
+  // model
+  cudapcgModel_t* model = nullptr;
+  int R = 0, C = 0, L = 0;
+  long N = 0, nvars = 0, nV = 0, nB = 0;
+  int nmat = 0, nd = 1;
+  std::vector<double> Kd;   // dense element matrices (host copy)
+  bool have_K = false, have_keys = false, have_maps = false;
+  uint16_t* d_keys = nullptr;
+  uint32_t* d_dof_of_node = nullptr;
+  uint32_t* d_node_of_dof = nullptr;
+  uint8_t* d_bkeys = nullptr;
+  void* d_K = nullptr;      // T-typed dense element matrices
+  int K_prec = -1;
+  // vectors (T-typed, allocated for the precision in use)
+  int vec_prec = -1;
+  void* x = nullptr; void* r = nullptr; void* r2 = nullptr; void* d0 = nullptr; void* d1 = nullptr;
+  void* q = nullptr; void* s = nullptr; void* q2 = nullptr;
+  double* b64 = nullptr;    // right-hand side kept in FP64 (mixed-mode residual replacement)
+  double* x64 = nullptr;    // FP64 staging for host <-> device in mixed mode
+  bool arrays_alloc = false, user_arrays = false;
+  bool x0_set = false, rhs_set = false;
+  // device scalars and reductions
+  DevScalars* d_sc = nullptr;
+  DevScalars* h_sc = nullptr;  // pinned
+  double* d_part = nullptr;
+  unsigned* d_ticket = nullptr;
+  int part_cap = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+  // graph cache
+  cudaGraphExec_t gexec = nullptr;
+  int graph_key = -1;
+  // results
+  unsigned iteration = 0;
+  double residual = 1.0;
+  int found = 0;
+  double total_time = 0.0, mean_time = 0.0;
+  double solve_dev_s = 0.0, setup_dev_s = 0.0;
+  unsigned long long launches = 0;
+  unsigned long count = 0;
+};
+
+static Solver* S = nullptr;
+static cudapcgFlag_t (*g_ctor)(cudapcgModel_t**, const void*) = nullptr;
+
+static cudapcgFlag_t ctor_simple(cudapcgModel_t** ptr, const void* data) {
+  if (!data) return CUDAPCG_FALSE;
+  *ptr = (cudapcgModel_t*)data;
+  return CUDAPCG_TRUE;
+}
+
+template <typename T> static int prec_of() { return sizeof(T) == 8 ? CHFEM_B200_FP64 : CHFEM_B200_MIXED; }
+
+static void free_ptr(void* p) { if (p) cudaFree(p); }
+
+static void free_vectors() {
+  if (!S) return;
+  free_ptr(S->x); free_ptr(S->r); free_ptr(S->r2); free_ptr(S->d0); free_ptr(S->d1);
+  free_ptr(S->q); free_ptr(S->s); free_ptr(S->q2); free_ptr(S->b64); free_ptr(S->x64);
+  S->x = S->r = S->r2 = S->d0 = S->d1 = S->q = S->s = S->q2 = nullptr;
+  S->b64 = S->x64 = nullptr;
+  S->vec_prec = -1;
+  S->arrays_alloc = false;
+  if (S->gexec) { cudaGraphExecDestroy(S->gexec); S->gexec = nullptr; S->graph_key = -1; }
+}
+
+static void free_model_dev() {
+  if (!S) return;
+  free_ptr(S->d_keys); free_ptr(S->d_dof_of_node); free_ptr(S->d_node_of_dof); free_ptr(S->d_bkeys); free_ptr(S->d_K);
+  S->d_keys = nullptr; S->d_dof_of_node = S->d_node_of_dof = nullptr; S->d_bkeys = nullptr; S->d_K = nullptr;
+  S->K_prec = -1;
+  S->have_K = S->have_keys = S->have_maps = false;
+}
+
+// Vectors for precision T.  x keeps the initial guess across precision switches by
+// converting through FP64.
+template <typename T>
+static bool ensure_vectors() {
+  const int p = prec_of<T>();
+  if (S->vec_prec == p && S->x) return true;
+  const size_t n = (size_t)S->nvars;
+  // carry r and x (rhs, initial guess) across a precision change
+  std::vector<double> hx, hr;
+  if (S->vec_prec != -1 && S->x) {
+    hx.resize(n); hr.resize(n);
+    if (S->vec_prec == CHFEM_B200_FP64) {
+      cudaMemcpy(hx.data(), S->x, n * 8, cudaMemcpyDeviceToHost);
+      cudaMemcpy(hr.data(), S->r, n * 8, cudaMemcpyDeviceToHost);
+    } else {
+      std::vector<float> tx(n), tr(n);
+      cudaMemcpy(tx.data(), S->x, n * 4, cudaMemcpyDeviceToHost);
+      cudaMemcpy(tr.data(), S->r, n * 4, cudaMemcpyDeviceToHost);
+      for (size_t i = 0; i < n; i++) { hx[i] = tx[i]; hr[i] = tr[i]; }
+    }
+  }
+  double* b64 = S->b64; S->b64 = nullptr;
+  free_vectors();
+  S->b64 = b64;
+  void** vs[] = {&S->x, &S->r, &S->r2, &S->d0, &S->d1, &S->q, &S->s, &S->q2};
+  for (void** v : vs) {
+    CKV(cudaMalloc(v, std::max<size_t>(n, 1) * sizeof(T)));
+    CKV(cudaMemsetAsync(*v, 0, std::max<size_t>(n, 1) * sizeof(T), S->stream));
+  }
+  if (!S->b64) CKV(cudaMalloc(&S->b64, std::max<size_t>(n, 1) * 8));
+  CKV(cudaMalloc(&S->x64, std::max<size_t>(n, 1) * 8));
+  S->vec_prec = p;
+  if (!hx.empty()) {
+    if (p == CHFEM_B200_FP64) {
+      cudaMemcpy(S->x, hx.data(), n * 8, cudaMemcpyHostToDevice);
+      cudaMemcpy(S->r, hr.data(), n * 8, cudaMemcpyHostToDevice);
+    } else {
+      std::vector<float> tx(n), tr(n);
+      for (size_t i = 0; i < n; i++) { tx[i] = (float)hx[i]; tr[i] = (float)hr[i]; }
+      cudaMemcpy(S->x, tx.data(), n * 4, cudaMemcpyHostToDevice);
+      cudaMemcpy(S->r, tr.data(), n * 4, cudaMemcpyHostToDevice);
+    }
+  }
+  S->arrays_alloc = true;
+  return true;
+}
+
+template <typename T>
+static bool ensure_K() {
+  const int p = prec_of<T>();
+  if (S->K_prec == p && S->d_K) return true;
+  if (!S->have_K) { set_err("solve", "local matrices were not set (cudapcgSetLclMtxs)"); return false; }
+  free_ptr(S->d_K); S->d_K = nullptr;
+  std::vector<T> kt(S->Kd.size());
+  for (size_t i = 0; i < kt.size(); i++) kt[i] = (T)S->Kd[i];
+  CKV(cudaMalloc(&S->d_K, kt.size() * sizeof(T)));
+  CKV(cudaMemcpy(S->d_K, kt.data(), kt.size() * sizeof(T), cudaMemcpyHostToDevice));
+  if (S->analysis == CUDAPCG_FLUID_3D) {
+    if (sizeof(T) == 8) CKV(cudaMemcpyToSymbol(c_flK64, kt.data(), 1024 * sizeof(double)));
+    else CKV(cudaMemcpyToSymbol(c_flK32, kt.data(), 1024 * sizeof(float)));
+  }
+  S->K_prec = p;
+  return true;
+}
+
+static bool ensure_reduction(int nblocks) {
+  if (nblocks <= S->part_cap && S->d_part) return true;
+  free_ptr(S->d_part);
+  S->part_cap = std::max(nblocks, 4096);
+  CKV(cudaMalloc(&S->d_part, sizeof(double) * 8 * S->part_cap));
+  return true;
+}
+
+// ---------------------------------------------------------------------------------------
+// Launch helpers.
+static int te_lchunk() {
+  const long base = (long)((S->R + TE_TR - 1) / TE_TR) * ((S->C + TE_TC - 1) / TE_TC);
+  const long target = 4L * num_sms();
+  long lc = (S->L * base + target - 1) / target;
+  if (lc < 1) lc = 1;
+  if (lc > 16) lc = 16;
+  if (lc > S->L) lc = S->L;
+  return (int)lc;
+}
+static dim3 te_grid(int lchunk) {
+  return dim3((S->R + TE_TR - 1) / TE_TR, (S->C + TE_TC - 1) / TE_TC, (S->L + lchunk - 1) / lchunk);
+}
+static int pw_grid(long n) {
+  long g = (n + PW_NT - 1) / PW_NT;
+  const long cap = 8L * num_sms();
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+// Largest grid any pass of the current model launches (reduction partials are sized once,
+// before graph capture, which must not allocate).
+static int needed_blocks() {
+  long nb = pw_grid(S->analysis == CUDAPCG_FLUID_3D ? S->nV + S->nB : S->N);
+  if (S->analysis != CUDAPCG_FLUID_3D) {
+    const dim3 g = te_grid(te_lchunk());
+    nb = std::max<long>(nb, (long)g.x * g.y * g.z);
+  }
+  return (int)nb;
+}
+static RedCtl redctl(int nblocks) { return RedCtl{S->d_part, S->d_ticket, nblocks}; }
+static SolveCfg solvecfg() {
+  SolveCfg c;
+  c.tol = S->tol; c.maxit = (int)std::min<unsigned>(S->maxit, 0x7fffffffu); c.norm = S->resnorm; c.precond = S->precond;
+  c.nhmg = (S->analysis == CUDAPCG_FLUID_3D) ? 3 * S->nV : S->nvars;
+  return c;
+}
+
+// y = A v (+ fused direction form and dot finisher).  in1/vout only with fuse.
+template <typename T>
+static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, int finish, bool skip_if_done) {
+  if (S->analysis == CUDAPCG_FLUID_3D) {
+    FlArgs<T> a;
+    a.v = in0; a.vd = in1; a.vout = vout; a.y = y; a.x = nullptr; a.d = nullptr;
+    a.dof_of_node = S->d_dof_of_node; a.node_of_dof = S->d_node_of_dof; a.bkeys = S->d_bkeys;
+    a.R = S->R; a.C = S->C; a.L = S->L; a.nV = S->nV; a.nB = S->nB;
+    a.sc = S->d_sc; a.finish = finish; a.skip_if_done = skip_if_done;
+    a.cfg = MrCfg{S->tol, 0, S->resnorm, S->precond, 0};
+    const int g = pw_grid(S->nV + S->nB);
+    if (!ensure_reduction(g)) return false;
+    a.rc = redctl(g);
+    if (fuse) k_fl_apply<T, TE_PCG><<<g, FL_NT, 0, S->stream>>>(a);
+    else k_fl_apply<T, TE_PLAIN><<<g, FL_NT, 0, S->stream>>>(a);
+  } else {
+    const int lc = te_lchunk();
+    const dim3 grid = te_grid(lc), block(TE_TR, TE_TC);
+    const int nb = grid.x * grid.y * grid.z;
+    if (!ensure_reduction(nb)) return false;
+    if (S->nd == 1) {
+      TeArgs<1, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, (const T*)S->d_K, S->nmat, S->R, S->C, S->L, lc, S->d_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
+      const size_t sm = te_smem_bytes<1, T>(S->nmat);
+      if (fuse) k_te_apply<1, T, TE_PCG><<<grid, block, sm, S->stream>>>(a);
+      else k_te_apply<1, T, TE_PLAIN><<<grid, block, sm, S->stream>>>(a);
+    } else {
+      TeArgs<3, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, (const T*)S->d_K, S->nmat, S->R, S->C, S->L, lc, S->d_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
+      const size_t sm = te_smem_bytes<3, T>(S->nmat);
+      if (fuse) k_te_apply<3, T, TE_PCG><<<grid, block, sm, S->stream>>>(a);
+      else k_te_apply<3, T, TE_PLAIN><<<grid, block, sm, S->stream>>>(a);
+    }
+  }
+  S->launches++;
+  return cudaPeekAtLastError() == cudaSuccess;
+}
+
+// Pointwise PCG pass.
+template <typename T, int MODE>
+static bool launch_point(T* x, T* d, T* r, const T* q, T* s, const T* dold) {
+  const SolveCfg cfg = solvecfg();
+  if (S->analysis == CUDAPCG_FLUID_3D) {
+    const int g = pw_grid(S->nV + S->nB);
+    if (!ensure_reduction(g)) return false;
+    FlPw<T> a{x, d, r, q, s, dold, S->d_bkeys, S->nV, S->nB, S->d_sc, redctl(g), cfg};
+    k_fl_point<T, MODE><<<g, PW_NT, 0, S->stream>>>(a);
+  } else {
+    const int g = pw_grid(S->N);
+    if (!ensure_reduction(g)) return false;
+    if (S->nd == 1) {
+      TePw<1, T> a{x, d, r, q, s, dold, S->d_keys, (const T*)S->d_K, S->nmat, S->N, S->d_sc, redctl(g), cfg};
+      k_te_point<1, T, MODE><<<g, PW_NT, 0, S->stream>>>(a);
+    } else {
+      TePw<3, T> a{x, d, r, q, s, dold, S->d_keys, (const T*)S->d_K, S->nmat, S->N, S->d_sc, redctl(g), cfg};
+      k_te_point<3, T, MODE><<<g, PW_NT, 0, S->stream>>>(a);
+    }
+  }
+  S->launches++;
+  return cudaPeekAtLastError() == cudaSuccess;
+}
+
+template <typename T>
+static bool enqueue_minres_iteration(int parity);
+
+// ---------------------------------------------------------------------------------------
+// One PCG / CG iteration: pass 1 forms d_new = s + beta d_old on the fly, applies A and
+// finishes alpha = delta / (d_new . A d_new); pass 2 updates x, r, s and finishes delta,
+// beta and the stopping test.  Buffers: d_old/d_new alternate, so a chunk has an even
+// number of iterations.
+template <typename T>
+static bool enqueue_pcg_iteration(int parity) {
+  T* dold = (T*)(parity ? S->d1 : S->d0);
+  T* dnew = (T*)(parity ? S->d0 : S->d1);
+  if (!launch_apply<T>((const T*)S->s, dold, dnew, (T*)S->q, true, FIN_ALPHA, true)) return false;
+  return launch_point<T, PW_PCG>((T*)S->x, dnew, (T*)S->r, (const T*)S->q, (T*)S->s, nullptr);
+}
+
+// Mixed mode: true residual r = b - A x with FP64 accumulation of the subtraction.
+template <typename T>
+__global__ void k_residual_replace(const double* b, const T* Ax, T* r, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    r[i] = (T)(b[i] - (double)Ax[i]);
+}
+template <typename T>
+__global__ void k_skip_if_done_copy(const DevScalars* sc, int* flag) { if (threadIdx.x == 0 && blockIdx.x == 0) *flag = sc->done; }
+
+template <typename T>
+static bool build_graph(int key, int chunk, bool minres) {
+  if (S->gexec && S->graph_key == key) return true;
+  if (S->gexec) { cudaGraphExecDestroy(S->gexec); S->gexec = nullptr; }
+  cudaGraph_t g;
+  CKV(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
+  bool ok = true;
+  const unsigned long long l0 = S->launches;
+  for (int it = 0; it < chunk && ok; it++) {
+    if (minres) ok = enqueue_minres_iteration<T>(it & 1);
+    else ok = enqueue_pcg_iteration<T>(it & 1);
+  }
+  S->launches = l0;
+  cudaError_t e = cudaStreamEndCapture(S->stream, &g);
+  if (!ok || e != cudaSuccess) { set_err("graph capture", cudaGetErrorString(e)); return false; }
+  e = cudaGraphInstantiate(&S->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) { set_err("graph instantiate", cudaGetErrorString(e)); return false; }
+  S->graph_key = key;
+  return true;
+}
+
+static bool read_scalars() {
+  CKV(cudaMemcpyAsync(S->h_sc, S->d_sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, S->stream));
+  CKV(cudaStreamSynchronize(S->stream));
+  return true;
+}
+
+// Device loop driver shared by PCG and MINRES: launch graph chunks until the device flags
+// completion.  Between chunks the host reads 1 record of scalars.
+template <typename T>
+static bool run_chunks(bool minres) {
+  const int chunk = std::max(2u, S->iters_per_launch & ~1u);
+  const int key = (prec_of<T>() << 8) | (minres ? 0x80 : 0) | (chunk & 0x7f) | (S->resnorm << 16) | (S->precond << 20);
+  if (!build_graph<T>(key, chunk, minres)) return false;
+  const bool mixed = sizeof(T) == 4 && S->replace_every > 0;
+  unsigned next_replace = S->replace_every;
+  for (;;) {
+    if (!read_scalars()) return false;
+    if (S->h_sc->done || S->h_sc->status >= 3) break;
+    if (mixed && (unsigned)S->h_sc->iteration >= next_replace && !minres) {
+      // residual replacement: r = b - A x, s = M^-1 r, delta = r.s (keeps d and beta)
+      if (!launch_apply<T>((const T*)S->x, nullptr, nullptr, (T*)S->q2, false, FIN_NONE, true)) return false;
+      const long n = S->nvars;
+      k_residual_replace<T><<<pw_grid(n), PW_NT, 0, S->stream>>>(S->b64, (const T*)S->q2, (T*)S->r, n);
+      S->launches++;
+      if (!launch_point<T, PW_REPL>((T*)S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
+      next_replace += S->replace_every;
+    }
+    CKV(cudaGraphLaunch(S->gexec, S->stream));
+    S->launches += (unsigned long long)chunk * 2;
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------------------
+// Solve on the device; x0 (if set) is in S->x, the RHS in S->r (and S->b64).
+template <typename T>
+static bool solve_pcg_device() {
+  if (!ensure_reduction(needed_blocks())) return false;
+  CKV(cudaMemsetAsync(S->d_ticket, 0, sizeof(unsigned), S->stream));
+  CKV(cudaMemsetAsync(S->d_sc, 0, sizeof(DevScalars), S->stream));
+  const size_t n = (size_t)S->nvars;
+  if (!S->x0_set) CKV(cudaMemsetAsync(S->x, 0, n * sizeof(T), S->stream));
+  CKV(cudaMemsetAsync(S->q, 0, n * sizeof(T), S->stream));
+  CKV(cudaMemsetAsync(S->d0, 0, n * sizeof(T), S->stream));
+  CKV(cudaMemsetAsync(S->d1, 0, n * sizeof(T), S->stream));
+  CKV(cudaEventRecord(S->ev0, S->stream));
+  // zero-guess reference: s = M^-1 r, delta0 = r.s   (pcg.cu:61-81)
+  if (!launch_point<T, PW_INIT>((T*)S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
+  if (S->x0_set) {  // pcg.cu:83-99
+    if (!launch_apply<T>((const T*)S->x, nullptr, nullptr, (T*)S->q, false, FIN_NONE, true)) return false;
+    if (!launch_point<T, PW_X0>((T*)S->x, nullptr, (T*)S->r, (const T*)S->q, (T*)S->s, nullptr)) return false;
+  }
+  CKV(cudaEventRecord(S->ev1, S->stream));
+  if (!run_chunks<T>(false)) return false;
+  CKV(cudaEventRecord(S->ev2, S->stream));
+  CKV(cudaEventSynchronize(S->ev2));
+  float ms1 = 0, ms2 = 0;
+  cudaEventElapsedTime(&ms1, S->ev0, S->ev1);
+  cudaEventElapsedTime(&ms2, S->ev1, S->ev2);
+  S->setup_dev_s = ms1 * 1e-3;
+  S->solve_dev_s = ms2 * 1e-3;
+  return true;
+}
+
+#include "minres_driver.inl"
+
+// ---------------------------------------------------------------------------------------
+// Results: residual / found semantics of pcg.cu:226-233 and pminres.cu:225-227.
+static void collect_results(bool minres) {
+  const DevScalars& h = *S->h_sc;
+  S->iteration = (unsigned)h.iteration;
+  if (h.status == 1) { S->residual = 0.0; S->found = 1; return; }
+  if (h.status == 2) { S->residual = h.metric; S->found = 1; return; }
+  if (!minres && S->resnorm == CUDAPCG_L2_NORM) {
+    S->residual = sqrt(fabs(h.delta) / fabs(h.delta0));
+    S->found = !(fabs(h.delta) > S->tol * S->tol * fabs(h.delta0));
+  } else {
+    S->residual = h.metric;
+    S->found = S->residual <= S->tol;
+  }
+}
+
+template <typename T>
+static bool copy_x_to_host(double* res_x) {
+  const size_t n = (size_t)S->nvars;
+  if (sizeof(T) == 8) {
+    CKV(cudaMemcpyAsync(res_x, S->x, n * 8, cudaMemcpyDeviceToHost, S->stream));
+  } else {
+    k_convert<float, double><<<pw_grid(n), PW_NT, 0, S->stream>>>((const float*)S->x, S->x64, n);
+    S->launches++;
+    CKV(cudaMemcpyAsync(res_x, S->x64, n * 8, cudaMemcpyDeviceToHost, S->stream));
+  }
+  CKV(cudaStreamSynchronize(S->stream));
+  return true;
+}
+
+template <typename T>
+static bool solve_T(double* res_x) {
+  if (!ensure_vectors<T>() || !ensure_K<T>()) return false;
+  const bool minres = (S->solver_flag == CUDAPCG_MINRES_SOLVER || S->solver_flag == CUDAPCG_MINRES3_SOLVER);
+  bool ok = minres ? solve_minres_device<T>() : solve_pcg_device<T>();
+  if (!ok) return false;
+  collect_results(minres);
+  if (S->h_sc->status == 1 && minres) CKV(cudaMemsetAsync(S->x, 0, S->nvars * sizeof(T), S->stream));
+  return copy_x_to_host<T>(res_x);
+}
+
+// =======================================================================================
+// C ABI
+extern "C" {
+
+const char* cudapcgB200LastError(void) { return g_err.c_str(); }
+
+cudapcgFlag_t cudapcgEnd(void) {
+  if (!S) return CUDAPCG_FALSE;
+  free_vectors();
+  free_model_dev();
+  free_ptr(S->d_sc); free_ptr(S->d_part); free_ptr(S->d_ticket);
+  if (S->h_sc) cudaFreeHost(S->h_sc);
+  if (S->ev0) cudaEventDestroy(S->ev0);
+  if (S->ev1) cudaEventDestroy(S->ev1);
+  if (S->ev2) cudaEventDestroy(S->ev2);
+  if (S->stream) cudaStreamDestroy(S->stream);
+  if (S->model && S->model->freeAllowed_flag) { free(S->model->name); free(S->model); }
+  delete S;
+  S = nullptr;
+  return CUDAPCG_TRUE;  // no device reset: other contexts on a shared GPU are left alone
+}
+
+cudapcgFlag_t cudapcgInit(cudapcgFlag_t analysis_flag, cudapcgFlag_t parStrategy_flag) {
+  cudapcgEnd();
+  g_err.clear();
+  if (analysis_flag != CUDAPCG_THERMAL_3D && analysis_flag != CUDAPCG_ELASTIC_3D && analysis_flag != CUDAPCG_FLUID_3D) {
+    set_err("cudapcgInit", analysis_flag <= CUDAPCG_FLUID_3D ? "2D analyses are not provided by chfem_b200" : "invalid analysis flag");
+    return CUDAPCG_FALSE;
+  }
+  if (analysis_flag == CUDAPCG_FLUID_3D && parStrategy_flag != CUDAPCG_NBN) {
+    printf("ERROR: EBE solver is unavailable for FLUID analysis.\n");
+    set_err("cudapcgInit", "EBE is unavailable for FLUID analysis");
+    return CUDAPCG_FALSE;
+  }
+  S = new Solver();
+  S->analysis = analysis_flag;
+  S->par = parStrategy_flag;
+  S->nd = (analysis_flag == CUDAPCG_ELASTIC_3D) ? 3 : 1;
+  if (const char* e = getenv("CHFEM_B200_PRECISION")) S->precision = (!strcmp(e, "mixed") || !strcmp(e, "fp32")) ? CHFEM_B200_MIXED : CHFEM_B200_FP64;
+  if (!g_ctor) g_ctor = ctor_simple;
+  CK(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&S->ev0)); CK(cudaEventCreate(&S->ev1)); CK(cudaEventCreate(&S->ev2));
+  CK(cudaMalloc(&S->d_sc, sizeof(DevScalars)));
+  CK(cudaMallocHost(&S->h_sc, sizeof(DevScalars)));
+  CK(cudaMalloc(&S->d_ticket, sizeof(unsigned)));
+  CK(cudaMemset(S->d_ticket, 0, sizeof(unsigned)));
+  memset(S->h_sc, 0, sizeof(DevScalars));
+  return CUDAPCG_TRUE;
+}
+
+cudapcgModel_t* cudapcgNewModel(void) {
+  cudapcgModel_t* m = (cudapcgModel_t*)calloc(1, sizeof(cudapcgModel_t));
+  if (!m) return nullptr;
+  m->freeAllowed_flag = CUDAPCG_TRUE;
+  m->parStrategy_flag = CUDAPCG_NBN;
+  m->poremap_flag = CUDAPCG_POREMAP_NUM;
+  return m;
+}
+
+static cudapcgFlag_t adopt_model() {
+  cudapcgModel_t* m = S->model;
+  if (m->parametric_density_field_flag) { set_err("model", "scalar density fields are not provided by chfem_b200"); return CUDAPCG_FALSE; }
+  if (S->analysis == CUDAPCG_FLUID_3D && m->poremap_flag != CUDAPCG_POREMAP_NUM) {
+    set_err("model", "only the DOF-number pore map (-pm 1) is provided by chfem_b200");
+    return CUDAPCG_FALSE;
+  }
+  free_vectors();
+  free_model_dev();
+  S->R = (int)m->nrows; S->C = (int)m->ncols; S->L = (int)m->nlayers;
+  S->N = (long)S->R * S->C * S->L;
+  S->nvars = m->nvars; S->nV = m->nporenodes; S->nB = m->nbordernodes;
+  S->nmat = (int)m->nkeys;
+  if (S->N <= 0 || S->nvars <= 0) { set_err("model", "empty model"); return CUDAPCG_FALSE; }
+  if (S->analysis != CUDAPCG_FLUID_3D && (S->nmat < 1 || S->nmat > 4)) { set_err("model", "1 to 4 materials are supported with 16-bit keys"); return CUDAPCG_FALSE; }
+  if (S->analysis == CUDAPCG_FLUID_3D) {
+    CK(cudaMalloc(&S->d_dof_of_node, sizeof(uint32_t) * S->N));
+    CK(cudaMalloc(&S->d_node_of_dof, sizeof(uint32_t) * std::max<long>(1, S->nV + S->nB)));
+    CK(cudaMalloc(&S->d_bkeys, std::max<long>(1, S->nB)));
+  } else {
+    CK(cudaMalloc(&S->d_keys, sizeof(uint16_t) * S->N));
+  }
+  S->x0_set = false;
+  return CUDAPCG_TRUE;
+}
+
+cudapcgFlag_t cudapcgSetModel(cudapcgModel_t* model) {
+  if (!S || !model) return CUDAPCG_FALSE;
+  if (S->model && S->model != model && S->model->freeAllowed_flag) { free(S->model->name); free(S->model); }
+  S->model = model;
+  return adopt_model();
+}
+
+cudapcgFlag_t cudapcgSetModelConstructorFcn(cudapcgFlag_t (*fcn)(cudapcgModel_t**, const void*)) {
+  if (!fcn) return CUDAPCG_FALSE;
+  g_ctor = fcn;
+  return CUDAPCG_TRUE;
+}
+
+cudapcgFlag_t cudapcgBuildModel(const void* data) {
+  if (!S) return CUDAPCG_FALSE;
+  if (!S->model) S->model = cudapcgNewModel();
+  else if (S->model->freeAllowed_flag) { free(S->model->name); free(S->model); S->model = cudapcgNewModel(); }
+  if (!g_ctor(&S->model, data)) return CUDAPCG_FALSE;
+  // Device pointers of this library are kept in the Solver, not in the caller's struct.
+  return adopt_model();
+}
+
+cudapcgFlag_t cudapcgSetNumTol(cudapcgTol_t t) { if (!S) return CUDAPCG_FALSE; S->tol = t; return CUDAPCG_TRUE; }
+cudapcgFlag_t cudapcgSetMaxIterations(unsigned int n) { if (!S) return CUDAPCG_FALSE; S->maxit = n; return CUDAPCG_TRUE; }
+cudapcgFlag_t cudapcgSetXReduceMode(cudapcgFlag_t) { return S ? CUDAPCG_TRUE : CUDAPCG_FALSE; }
+cudapcgFlag_t cudapcgSetXReduceShift(unsigned int) { return S ? CUDAPCG_TRUE : CUDAPCG_FALSE; }
+cudapcgFlag_t cudapcgSetXReduceScale(double) { return S ? CUDAPCG_TRUE : CUDAPCG_FALSE; }
+cudapcgFlag_t cudapcgSetReduceStabFactor(double) { return S ? CUDAPCG_TRUE : CUDAPCG_FALSE; }
+cudapcgFlag_t cudapcgSetSolver(cudapcgFlag_t flag) {
+  if (!S) return CUDAPCG_FALSE;
+  if (flag > CUDAPCG_MINRES2_SOLVER) { printf("ERROR: Invalid \"solverFlag\" (%d).\n", flag); return CUDAPCG_FALSE; }
+  if (flag >= CUDAPCG_CG2_SOLVER) {
+    set_err("cudapcgSetSolver", "the 2-vector solvers (CG2/MINRES2) are not provided by chfem_b200");
+    return CUDAPCG_FALSE;
+  }
+  S->solver_flag = flag;  // CG3/MINRES3 run the same iterates as CG/MINRES
+  if (S->gexec) { cudaGraphExecDestroy(S->gexec); S->gexec = nullptr; S->graph_key = -1; }
+  return CUDAPCG_TRUE;
+}
+cudapcgFlag_t cudapcgSetPreconditioner(cudapcgFlag_t flag) { if (!S) return CUDAPCG_FALSE; S->precond = flag > 0; return CUDAPCG_TRUE; }
+cudapcgFlag_t cudapcgSetResNorm(cudapcgFlag_t flag) { if (!S) return CUDAPCG_FALSE; S->resnorm = flag > CUDAPCG_ERROR_NORM ? CUDAPCG_L2_NORM : flag; return CUDAPCG_TRUE; }
+unsigned int cudapcgGetNumIterations(void) { return S ? S->iteration : 0; }
+unsigned int cudapcgGetMaxNumIterations(void) { return S ? S->maxit : 0; }
+cudapcgVar_t cudapcgGetResidual(void) { return S ? S->residual : 0; }
+
+cudapcgFlag_t cudapcgAllocateArrays(void) {
+  if (!S || !S->model) return CUDAPCG_FALSE;
+  bool ok = (S->precision == CHFEM_B200_FP64) ? ensure_vectors<double>() : ensure_vectors<float>();
+  if (ok) S->user_arrays = true;
+  return ok ? CUDAPCG_TRUE : CUDAPCG_FALSE;
+}
+cudapcgFlag_t cudapcgFreeArrays(void) {
+  if (!S) return CUDAPCG_FALSE;
+  if (!S->x0_set) { free_vectors(); }
+  S->user_arrays = false;
+  return CUDAPCG_TRUE;
+}
+
+static bool upload_vec(const double* host, void* dst_T) {
+  const size_t n = (size_t)S->nvars;
+  if (S->vec_prec == CHFEM_B200_FP64) {
+    CKV(cudaMemcpyAsync(dst_T, host, n * 8, cudaMemcpyHostToDevice, S->stream));
+  } else {
+    CKV(cudaMemcpyAsync(S->x64, host, n * 8, cudaMemcpyHostToDevice, S->stream));
+    k_convert<double, float><<<pw_grid(n), PW_NT, 0, S->stream>>>(S->x64, (float*)dst_T, n);
+  }
+  return true;
+}
+
+static bool ensure_vectors_current() {
+  return (S->precision == CHFEM_B200_FP64) ? ensure_vectors<double>() : ensure_vectors<float>();
+}
+
+cudapcgFlag_t cudapcgSetRHS(cudapcgVar_t* RHS) {
+  if (!S || !S->model || !RHS) return CUDAPCG_FALSE;
+  if (!ensure_vectors_current()) return CUDAPCG_FALSE;
+  if (!upload_vec(RHS, S->r)) return CUDAPCG_FALSE;
+  CK(cudaMemcpyAsync(S->b64, RHS, S->nvars * 8, cudaMemcpyHostToDevice, S->stream));
+  CK(cudaStreamSynchronize(S->stream));
+  S->rhs_set = true;
+  return CUDAPCG_TRUE;
+}
+
+// Coarse-to-fine prolongation for recursive initial guesses (kernels/image.cu:20-123,
+// wrappers.cu:290-303): x2 injection at even nodes, then periodic midpoint fill along rows,
+// columns and layers, in that order.
+}  // extern "C"
+template <typename T>
+__global__ void k_project2(T* res, const double* v, int rows, int cols, int lays, int nd) {
+  const int rc = rows / 2, cc = cols / 2, lc = lays / 2;
+  const long nco = (long)rc * cc * (lc + (lc < 1));
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nco; i += (long)gridDim.x * blockDim.x) {
+    const long ii = i % rc, jj = (i % ((long)cc * rc)) / rc, kk = i / ((long)cc * rc);
+    const long idx = 2 * ii + 2 * jj * rows + 2 * kk * (long)rows * cols;
+    for (int j = 0; j < nd; j++) res[nd * idx + j] = (T)(2.0 * v[nd * i + j]);
+  }
+}
+extern "C" {
+}  // extern "C"
+template <typename T>
+__global__ void k_interp_pass(T* v, int rows, int cols, int lays, int nd, int pass) {
+  const long RC = (long)rows * cols, n = RC * lays;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const long ii = i % rows, jj = (i % RC) / rows, kk = i / RC;
+    long a, b;
+    if (pass == 0) {
+      if (!((ii & 1) && !(jj & 1) && !(kk & 1))) continue;
+      a = i - 1 + rows * (!(i % rows)); b = i + 1 - rows * (!((i + 1) % rows));
+    } else if (pass == 1) {
+      if (!((jj & 1) && !(kk & 1))) continue;
+      const long il = i % RC;
+      a = (il + (RC - rows)) % RC + kk * RC; b = (il + rows) % RC + kk * RC;
+    } else {
+      if (!(kk & 1)) continue;
+      a = (i + (n - RC)) % n; b = (i + RC) % n;
+    }
+    for (int j = 0; j < nd; j++) v[nd * i + j] = (T)(0.5 * (double)v[nd * a + j] + 0.5 * (double)v[nd * b + j]);
+  }
+}
+extern "C" {
+
+}  // extern "C"
+template <typename T>
+static bool interp_x0(const double* coarse_host) {
+  const int rows = S->R, cols = S->C, lays = S->L, nd = (int)(S->nvars / S->N);
+  const size_t ncoarse = (size_t)nd * (cols / 2) * (rows / 2) * (lays / 2 + (lays < 2));
+  CKV(cudaMemcpyAsync(S->x64, coarse_host, ncoarse * 8, cudaMemcpyHostToDevice, S->stream));
+  CKV(cudaMemsetAsync(S->x, 0, S->nvars * sizeof(T), S->stream));
+  const int g = pw_grid(S->N);
+  k_project2<T><<<g, PW_NT, 0, S->stream>>>((T*)S->x, S->x64, rows, cols, lays, nd);
+  for (int p = 0; p < 3; p++) k_interp_pass<T><<<g, PW_NT, 0, S->stream>>>((T*)S->x, rows, cols, lays, nd, p);
+  CKV(cudaStreamSynchronize(S->stream));
+  return true;
+}
+extern "C" {
+
+cudapcgFlag_t cudapcgSetX0(cudapcgVar_t* x0, cudapcgFlag_t mustInterpolate) {
+  if (!S || !S->model) return CUDAPCG_FALSE;
+  if (!x0) {  // cudapcg.cu:298-309
+    if (!S->x0_set) return CUDAPCG_TRUE;
+    S->x0_set = false;
+    if (S->x) CK(cudaMemset(S->x, 0, S->nvars * (S->vec_prec == CHFEM_B200_FP64 ? 8 : 4)));
+    return CUDAPCG_TRUE;
+  }
+  if (!ensure_vectors_current()) return CUDAPCG_FALSE;
+  bool ok;
+  if (mustInterpolate) ok = (S->vec_prec == CHFEM_B200_FP64) ? interp_x0<double>(x0) : interp_x0<float>(x0);
+  else { ok = upload_vec(x0, S->x); cudaStreamSynchronize(S->stream); }
+  if (!ok) return CUDAPCG_FALSE;
+  S->x0_set = true;
+  return CUDAPCG_TRUE;
+}
+
+// Node keys from a per-voxel material map (EBE input): voxel v is the element whose local
+// node 3 is node v (femhmg_3D.c:45-49), so the element in which node (r,c,l) is local node e
+// is voxel (r - drow(e) - 1, c - dcol(e), l - dlay(e)).
+}  // extern "C"
+__global__ void k_keys_from_elements(const uint16_t* em, uint16_t* keys, int R, int C, int L) {
+  const long N = (long)R * C * L;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const int r = (int)(i % R), c = (int)((i / R) % C), l = (int)(i / ((long)R * C));
+    unsigned k = 0;
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      const long v = wrap(r - drow(e) - 1, R) + (long)wrap(c - dcol(e), C) * R + (long)wrap(l - dlay(e), L) * R * C;
+      k |= ((unsigned)em[v] & 3u) << (2 * e);
+    }
+    keys[i] = (uint16_t)k;
+  }
+}
+extern "C" {
+
+cudapcgFlag_t cudapcgSetImage(cudapcgMap_t* img) {
+  if (!S || !S->model || !img) return CUDAPCG_FALSE;
+  if (S->analysis == CUDAPCG_FLUID_3D) { set_err("cudapcgSetImage", "not used for FLUID analysis"); return CUDAPCG_FALSE; }
+  if (S->par == CUDAPCG_EBE) {
+    uint16_t* tmp = nullptr;
+    CK(cudaMalloc(&tmp, sizeof(uint16_t) * S->N));
+    CK(cudaMemcpy(tmp, img, sizeof(uint16_t) * S->N, cudaMemcpyHostToDevice));
+    k_keys_from_elements<<<pw_grid(S->N), PW_NT, 0, S->stream>>>(tmp, S->d_keys, S->R, S->C, S->L);
+    CK(cudaStreamSynchronize(S->stream));
+    cudaFree(tmp);
+  } else {
+    CK(cudaMemcpy(S->d_keys, img, sizeof(uint16_t) * S->N, cudaMemcpyHostToDevice));
+  }
+  S->have_keys = true;
+  return CUDAPCG_TRUE;
+}
+cudapcgFlag_t cudapcgSetParametricDensityField(parametricScalarField_t*, double, double) {
+  set_err("cudapcgSetParametricDensityField", "scalar density fields are not provided by chfem_b200");
+  return CUDAPCG_FALSE;
+}
+cudapcgFlag_t cudapcgSetPoreMap(cudapcgFlag_t* pores) {
+  if (!S || !S->model || !pores) return CUDAPCG_FALSE;
+  if (S->analysis != CUDAPCG_FLUID_3D) return CUDAPCG_FALSE;
+  if (S->nB) CK(cudaMemcpy(S->d_bkeys, pores, S->nB, cudaMemcpyHostToDevice));
+  return CUDAPCG_TRUE;
+}
+cudapcgFlag_t cudapcgSetPeriodic2DOFMap(cudapcgIdMap_t* vars) {
+  if (!S || !S->model || !vars || S->analysis != CUDAPCG_FLUID_3D) return CUDAPCG_FALSE;
+  CK(cudaMemcpy(S->d_dof_of_node, vars, sizeof(uint32_t) * S->N, cudaMemcpyHostToDevice));
+  S->have_maps = true;
+  return CUDAPCG_TRUE;
+}
+cudapcgFlag_t cudapcgSetDOF2PeriodicMap(cudapcgIdMap_t* nodes) {
+  if (!S || !S->model || !nodes || S->analysis != CUDAPCG_FLUID_3D) return CUDAPCG_FALSE;
+  CK(cudaMemcpy(S->d_node_of_dof, nodes, sizeof(uint32_t) * (S->nV + S->nB), cudaMemcpyHostToDevice));
+  return CUDAPCG_TRUE;
+}
+
+// Stokes Jacobi tables (matrix_free.cu:663-672 pore rows, :912-925 interface rows).
+static bool set_fluid_diag() {
+  FlDiag dg;
+  const double* K = S->Kd.data();
+  double dv[3] = {0, 0, 0}, dp = 0.0;
+  for (int e = 0; e < 8; e++) {
+    for (int c = 0; c < 3; c++) dv[c] += K[(3 * e + c) * 33];
+    dp -= K[(24 + e) * 33];
+  }
+  for (int c = 0; c < 3; c++) dg.pore[c] = 1.0 / dv[c];
+  dg.pore[3] = 1.0 / dp;
+  for (int k = 0; k < 256; k++) {
+    double sum = 0.0;
+    for (int e = 0; e < 8; e++) sum -= K[(24 + e) * 33] * (double)((k >> e) & 1);
+    dg.border[k] = (sum != 0.0) ? 1.0 / sum : 0.0;
+  }
+  CKV(cudaMemcpyToSymbol(c_fldiag, &dg, sizeof(FlDiag)));
+  return true;
+}
+
+cudapcgFlag_t cudapcgSetLclMtxs(cudapcgVar_t* Lm) {
+  if (!S || !S->model || !Lm) return CUDAPCG_FALSE;
+  const int nk = S->analysis == CUDAPCG_FLUID_3D ? 1 : S->nmat;
+  if (S->analysis == CUDAPCG_THERMAL_3D) {
+    S->Kd.assign((size_t)64 * nk, 0.0);
+    for (int k = 0; k < nk; k++) sparseq1_to_dense(Lm + 40 * k, S->Kd.data() + 64 * k);
+  } else if (S->analysis == CUDAPCG_ELASTIC_3D) {
+    S->Kd.assign(Lm, Lm + (size_t)576 * nk);
+  } else {
+    S->Kd.assign(Lm, Lm + 1024);
+  }
+  S->have_K = true;
+  free_ptr(S->d_K); S->d_K = nullptr; S->K_prec = -1;
+  if (S->analysis == CUDAPCG_FLUID_3D && !set_fluid_diag()) return CUDAPCG_FALSE;
+  return CUDAPCG_TRUE;
+}
+
+cudapcgFlag_t cudapcgSolve(cudapcgVar_t* res_x) {
+  if (!S || !S->model || !res_x) return CUDAPCG_FALSE;
+  if (!S->rhs_set) { set_err("cudapcgSolve", "right-hand side was not set"); return CUDAPCG_FALSE; }
+  const auto t0 = std::chrono::steady_clock::now();
+  S->count++;
+  S->launches = 0;
+  bool ok = (S->precision == CHFEM_B200_FP64) ? solve_T<double>(res_x) : solve_T<float>(res_x);
+  const double t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  S->total_time = t;
+  S->mean_time = S->iteration ? S->solve_dev_s / S->iteration : 0.0;
+  if (!ok) { S->found = 0; return CUDAPCG_FALSE; }
+  if (S->h_sc->status == 1) printf("%sNull solution satisfied %s.\n", S->header.c_str(), S->solver_flag & 1 ? "MINRES" : (S->precond ? "PCG" : "CG"));
+  else if (S->h_sc->status == 2) printf("%sInitial guess satisfied %s.\n", S->header.c_str(), S->solver_flag & 1 ? "MINRES" : (S->precond ? "PCG" : "CG"));
+  else if (!getenv("CHFEM_B200_QUIET")) {
+    if (S->resnorm != CUDAPCG_ERROR_NORM) printf("%siteration: %d, residual: %.3e\n", S->header.c_str(), S->iteration, S->residual);
+    else printf("%siteration: %d, residual: %.3e, error: %.3e\n", S->header.c_str(), S->iteration, sqrt(fabs(S->h_sc->delta) / fabs(S->h_sc->delta0)), S->residual);
+  }
+  return (cudapcgFlag_t)S->found;
+}
+
+cudapcgFlag_t cudapcgSetHeaderString(char* header) {
+  if (!S) return CUDAPCG_FALSE;
+  S->header = header ? header : "";
+  return CUDAPCG_TRUE;
+}
+cudapcgFlag_t cudapcgPrintSolverMetrics(void) {
+  if (!S) return CUDAPCG_FALSE;
+  printf("%sMean time per iteration: %.2e s\n", S->header.c_str(), S->mean_time);
+  printf("%sElapsed time: %.2e s\n", S->header.c_str(), S->total_time);
+  return CUDAPCG_TRUE;
+}
+cudapcgFlag_t cudapcgPrintSolverMetrics2(char* dest) {
+  if (!dest || !S) return CUDAPCG_FALSE;
+  sprintf(dest, "%sMean time per iteration: %.2e s\n%sElapsed time: %.2e s\n", S->header.c_str(), S->mean_time, S->header.c_str(), S->total_time);
+  return CUDAPCG_TRUE;
+}
+cudapcgFlag_t cudapcgPrintSolverReport(void) {
+  if (!S) return CUDAPCG_FALSE;
+  if (S->found) printf("%sPCG solver found a solution in %d iterations.\n", S->header.c_str(), S->iteration);
+  else printf("%sPCG solver did not converge within provided max number of iterations (%d).\n", S->header.c_str(), S->maxit);
+  printf("%sResidual: %e\n", S->header.c_str(), S->residual);
+  return cudapcgPrintSolverMetrics();
+}
+cudapcgFlag_t cudapcgPrintSolverReport2(char* dest) {
+  if (!dest || !S) return CUDAPCG_FALSE;
+  sprintf(dest, "%sPCG solver ran through %d iterations.\n%sResidual: %e\n%sMean time per iteration: %.2e s\n%sElapsed time: %.2e s\n",
+          S->header.c_str(), S->iteration, S->header.c_str(), S->residual, S->header.c_str(), S->mean_time, S->header.c_str(), S->total_time);
+  return CUDAPCG_TRUE;
+}
+
+// ---------------- extensions ----------------
+cudapcgFlag_t cudapcgB200SetPrecision(int mode) {
+  if (!S || (mode != CHFEM_B200_FP64 && mode != CHFEM_B200_MIXED)) return CUDAPCG_FALSE;
+  S->precision = mode;
+  return CUDAPCG_TRUE;
+}
+cudapcgFlag_t cudapcgB200SetResidualReplacement(unsigned int k) { if (!S) return CUDAPCG_FALSE; S->replace_every = k; return CUDAPCG_TRUE; }
+cudapcgFlag_t cudapcgB200SetIterationsPerLaunch(unsigned int k) {
+  if (!S || k < 2 || k > 126) return CUDAPCG_FALSE;
+  S->iters_per_launch = k & ~1u;
+  if (S->gexec) { cudaGraphExecDestroy(S->gexec); S->gexec = nullptr; S->graph_key = -1; }
+  return CUDAPCG_TRUE;
+}
+
+}  // extern "C"
+template <typename T>
+static bool apply_host_T(const double* xh, double* yh, bool precond_only) {
+  if (!ensure_vectors<T>() || !ensure_K<T>()) return false;
+  const size_t n = (size_t)S->nvars;
+  // use q2 as input, q as output (solver state in x, r stays untouched)
+  if (!upload_vec(xh, S->q2)) return false;
+  if (!ensure_reduction(8 * num_sms())) return false;
+  CKV(cudaMemsetAsync(S->d_sc, 0, sizeof(DevScalars), S->stream));
+  if (precond_only) {
+    // s = M^-1 q2 via the INIT pass on a copy: r <- q2 temporarily
+    CKV(cudaMemcpyAsync(S->q, S->r, n * sizeof(T), cudaMemcpyDeviceToDevice, S->stream));  // save r in q
+    CKV(cudaMemcpyAsync(S->r, S->q2, n * sizeof(T), cudaMemcpyDeviceToDevice, S->stream));
+    if (!launch_point<T, PW_INIT>((T*)S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
+    CKV(cudaMemcpyAsync(S->r, S->q, n * sizeof(T), cudaMemcpyDeviceToDevice, S->stream));  // restore r
+    CKV(cudaMemcpyAsync(S->q, S->s, n * sizeof(T), cudaMemcpyDeviceToDevice, S->stream));
+  } else {
+    if (!launch_apply<T>((const T*)S->q2, nullptr, nullptr, (T*)S->q, false, FIN_STORE, false)) return false;
+  }
+  if (sizeof(T) == 8) {
+    CKV(cudaMemcpyAsync(yh, S->q, n * 8, cudaMemcpyDeviceToHost, S->stream));
+  } else {
+    k_convert<float, double><<<pw_grid(n), PW_NT, 0, S->stream>>>((const float*)S->q, S->x64, n);
+    CKV(cudaMemcpyAsync(yh, S->x64, n * 8, cudaMemcpyDeviceToHost, S->stream));
+  }
+  CKV(cudaStreamSynchronize(S->stream));
+  return true;
+}
+extern "C" {
+cudapcgFlag_t cudapcgB200ApplyOperator(const double* x, double* y) {
+  if (!S || !S->model || !x || !y) return CUDAPCG_FALSE;
+  bool ok = (S->precision == CHFEM_B200_FP64) ? apply_host_T<double>(x, y, false) : apply_host_T<float>(x, y, false);
+  return ok ? CUDAPCG_TRUE : CUDAPCG_FALSE;
+}
+cudapcgFlag_t cudapcgB200ApplyPreconditioner(const double* x, double* y) {
+  if (!S || !S->model || !x || !y) return CUDAPCG_FALSE;
+  bool ok = (S->precision == CHFEM_B200_FP64) ? apply_host_T<double>(x, y, true) : apply_host_T<float>(x, y, true);
+  return ok ? CUDAPCG_TRUE : CUDAPCG_FALSE;
+}
+cudapcgFlag_t cudapcgB200GetStats(cudapcgB200Stats* out) {
+  if (!S || !out) return CUDAPCG_FALSE;
+  out->iterations = S->iteration;
+  out->residual = S->residual;
+  out->solve_seconds = S->solve_dev_s;
+  out->setup_seconds = S->setup_dev_s;
+  out->kernel_launches = S->launches;
+  out->precision = S->vec_prec;
+  out->found = S->found;
+  return CUDAPCG_TRUE;
+}
+
+}  // extern "C"
+template <typename T>
+static double time_op_T(unsigned reps) {
+  if (!ensure_vectors<T>() || !ensure_K<T>()) return -1.0;
+  if (!ensure_reduction(8 * num_sms())) return -1.0;
+  cudaMemsetAsync(S->d_sc, 0, sizeof(DevScalars), S->stream);
+  for (int w = 0; w < 3; w++) launch_apply<T>((const T*)S->s, nullptr, nullptr, (T*)S->q2, false, FIN_NONE, false);
+  cudaEventRecord(S->ev0, S->stream);
+  for (unsigned i = 0; i < reps; i++) launch_apply<T>((const T*)S->s, nullptr, nullptr, (T*)S->q2, false, FIN_NONE, false);
+  cudaEventRecord(S->ev1, S->stream);
+  if (cudaEventSynchronize(S->ev1) != cudaSuccess) return -1.0;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, S->ev0, S->ev1);
+  return ms * 1e-3 / std::max(1u, reps);
+}
+extern "C" {
+double cudapcgB200TimeOperator(unsigned int reps) {
+  if (!S || !S->model) return -1.0;
+  return (S->precision == CHFEM_B200_FP64) ? time_op_T<double>(reps) : time_op_T<float>(reps);
+}
+unsigned long long cudapcgB200DeviceBytes(void) {
+  if (!S) return 0;
+  const size_t es = S->vec_prec == CHFEM_B200_FP64 ? 8 : 4;
+  unsigned long long b = 0;
+  if (S->x) b += 8ull * S->nvars * es + 16ull * S->nvars;
+  if (S->analysis == CUDAPCG_FLUID_3D) b += 4ull * S->N + 4ull * (S->nV + S->nB) + S->nB;
+  else b += 2ull * S->N;
+  return b;
+}
+
+}  // extern "C"

@@ -1,0 +1,253 @@
+// stencil_te.cuh -- matrix-free voxel operator for 3D thermal (1 DOF/node) and elastic
+// (3 DOF/node) homogenization, applied node by node like the reference
+// (chfem/src/femhmg/cudapcg/kernels/matrix_free.cu:191-323 thermal SparseQ1, :410-459
+// elastic): for node i and each of its 8 voxels e (in which i is local node e), the row
+// block of local node e of the element matrix of that voxel's material multiplies the
+// element's 8 nodal values.
+//
+// B200 design: one CTA owns a 32 (rows) x 8 (cols) column of nodes and marches through a
+// chunk of layers, keeping three layers of the input field (with a one-node periodic halo)
+// in shared memory, so every field value is read from HBM about once per apply.  The
+// element matrices of all materials sit in shared memory (a warp touching up to 4
+// materials reads up to 4 distinct addresses per load instead of serialising on the
+// constant cache).  The input field is formed while it is staged, which fuses the vector
+// update that precedes the operator in each Krylov recurrence:
+//   TE_PLAIN  v = in0                                  (plain apply)
+//   TE_PCG    v = in0 + beta*in1 = s + beta d_old       (PCG direction; written once)
+//   TE_MR     r' = in0 - alpha*in1 = r - alpha q, v = M^-1 r'   (PMINRES; r', x updated)
+#pragma once
+#include "common.cuh"
+
+namespace chfem {
+
+constexpr int TE_TR = 32;              // rows per CTA (fastest dimension, coalesced)
+constexpr int TE_TC = 8;               // cols per CTA
+constexpr int TE_NT = TE_TR * TE_TC;   // threads per CTA
+constexpr int TE_PR = TE_TR + 2;       // plane pitch (rows incl. halo)
+constexpr int TE_PC = TE_TC + 2;
+constexpr int TE_PP = TE_PR * TE_PC;   // points per plane incl. halo
+
+enum TeMode : int { TE_PLAIN = 0, TE_PCG = 1, TE_MR = 2 };
+// Finishers run by the last CTA on the grid-reduced sums.
+enum TeFinish : int { FIN_NONE = 0, FIN_ALPHA = 1, FIN_STORE = 2, FIN_MR_INIT = 3, FIN_MR_X0 = 4, FIN_MR_STEP = 5 };
+
+struct MrCfg {
+  double tol;
+  int maxit;
+  int norm;
+  int precond;
+  long nhmg;
+};
+
+template <int ND, typename T>
+struct TeArgs {
+  const T* in0;        // s (PCG) | r (MR) | field to apply
+  const T* in1;        // d_old (PCG) | q (MR)
+  T* vout;             // PCG: formed direction; MR: updated residual r'
+  T* y;                // y = A v
+  T* x;                // MR: x += alpha d
+  const T* d;          // MR
+  const uint16_t* keys;
+  const T* Kd;         // dense element matrices [nmat][8ND][8ND]
+  int nmat;
+  int R, C, L, lchunk;
+  DevScalars* sc;
+  RedCtl rc;
+  int finish;          // TeFinish
+  int skip_if_done;
+  MrCfg cfg;
+};
+
+template <int ND, typename T>
+__device__ __forceinline__ void te_node(const T* __restrict__ sK, int kstride, unsigned key,
+                                        const T* pm, const T* p0, const T* pp, int ctr, T (&out)[ND]) {
+  constexpr int ED = 8 * ND;
+#pragma unroll
+  for (int c = 0; c < ND; c++) out[c] = T(0);
+#pragma unroll
+  for (int e = 0; e < 8; e++) {
+    const T* K = sK + ((key >> (2 * e)) & 3u) * kstride + e * ND * ED;
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+      if (ND == 1 && shares_edge(e, b)) continue;  // structural zero of the Q1 conductivity matrix
+      const int dr = drow(b) - drow(e), dc = dcol(b) - dcol(e), dl = dlay(b) - dlay(e);
+      const T* P = dl < 0 ? pm : (dl == 0 ? p0 : pp);
+      const T* v = P + (ctr + dr + dc * TE_PR) * ND;
+#pragma unroll
+      for (int ci = 0; ci < ND; ci++) {
+        T s = out[ci];
+#pragma unroll
+        for (int cj = 0; cj < ND; cj++) s = fma(K[ci * ED + b * ND + cj], v[cj], s);
+        out[ci] = s;
+      }
+    }
+  }
+}
+
+// Jacobi inverse diagonal of a node from its key (matrix_free.cu:167-188, :388-408).
+template <int ND, typename T>
+__device__ __forceinline__ void te_invdiag(const T* sD, unsigned key, T (&inv)[ND]) {
+  T dg[ND];
+#pragma unroll
+  for (int c = 0; c < ND; c++) dg[c] = T(0);
+#pragma unroll
+  for (int e = 0; e < 8; e++) {
+    const T* D = sD + ((key >> (2 * e)) & 3u) * 8 * ND + e * ND;
+#pragma unroll
+    for (int c = 0; c < ND; c++) dg[c] += D[c];
+  }
+#pragma unroll
+  for (int c = 0; c < ND; c++) inv[c] = T(1) / dg[c];
+}
+
+__device__ inline void mr_finish(int fin, const double* s, DevScalars* sc, const MrCfg& cfg) {
+  // s: [0] z.Az (delta), [1] r'.z (r' M^-1 r'), [2] max|r'|, [3] max|d| (nhmg), [4] max|x| (nhmg)
+  const double tol2 = cfg.tol * cfg.tol;
+  if (fin == FIN_MR_INIT) {  // pminres.cu:58-79
+    sc->delta0 = s[0];
+    sc->res0 = (cfg.norm == 1) ? s[2] : s[1];
+    sc->iteration = 0; sc->alpha = 0.0; sc->beta = 0.0; sc->found = 0;
+    if (fabs(sc->res0) < 1e-12) { sc->done = 1; sc->found = 1; sc->metric = 0.0; sc->status = 1; }
+    else { sc->done = 0; sc->status = 0; sc->delta = s[0]; sc->delta_old = s[0]; sc->metric = 1.0; }
+  } else if (fin == FIN_MR_X0) {  // pminres.cu:81-98
+    sc->delta = s[0]; sc->delta_old = s[0]; sc->beta = 0.0;
+    if (!(fabs(s[0]) > tol2 * fabs(sc->delta0))) {
+      sc->done = 1; sc->found = 1; sc->status = 2; sc->metric = sqrt(fabs(s[0]) / fabs(sc->delta0));
+    }
+  } else if (fin == FIN_MR_STEP) {  // pminres.cu:130-160, :166-204
+    sc->iteration += 1;
+    sc->delta_old = sc->delta;
+    sc->delta = s[0];
+    bool cont;
+    if (cfg.norm == 0) { cont = fabs(s[1]) > tol2 * fabs(sc->res0); sc->metric = sqrt(fabs(s[1]) / fabs(sc->res0)); }
+    else if (cfg.norm == 1) { sc->metric = s[2] / sc->res0; cont = sc->metric > cfg.tol; }
+    else { sc->metric = fabs(sc->alpha) * s[3] / s[4]; cont = sc->metric > cfg.tol; }
+    sc->found = sc->metric <= cfg.tol;
+    sc->beta = sc->delta / sc->delta_old;
+    if (!cont || sc->iteration >= cfg.maxit) sc->done = 1;
+  }
+}
+
+template <int ND, typename T, int MODE>
+__global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a) {
+  constexpr int ED = 8 * ND;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double sred[TE_NT / 32];
+  __shared__ T sD[4 * 8 * ND];
+  if (a.skip_if_done && a.sc->done) return;
+  T* sK = reinterpret_cast<T*>(smem_raw);
+  const int kstride = ED * ED + 1;  // padded material stride spreads materials over banks
+  T* sP = sK + 4 * kstride;
+  const int tid = threadIdx.x + TE_TR * threadIdx.y;
+  // 4 material slots always (keys carry 2 bits per voxel); slots past nmat are zero.
+  for (int i = tid; i < 4 * ED * ED; i += TE_NT) sK[(i / (ED * ED)) * kstride + i % (ED * ED)] = (i < a.nmat * ED * ED) ? a.Kd[i] : T(0);
+  if (MODE == TE_MR) {
+    for (int i = tid; i < 4 * 8 * ND; i += TE_NT) {
+      const int m = i / (8 * ND), k = i % (8 * ND);
+      sD[i] = (m < a.nmat) ? a.Kd[(size_t)m * ED * ED + (size_t)k * ED + k] : T(1);
+    }
+    __syncthreads();
+  }
+  const T beta = (MODE == TE_PCG) ? T(a.sc->beta) : T(0);
+  const T alpha = (MODE == TE_MR) ? T(a.sc->alpha) : T(0);
+  const bool pre = a.cfg.precond != 0;
+  const int R = a.R, C = a.C, L = a.L;
+  const int r0 = blockIdx.x * TE_TR, c0 = blockIdx.y * TE_TC, l0 = blockIdx.z * a.lchunk;
+  const int l1 = min(l0 + a.lchunk, L);
+  const size_t RC = (size_t)R * C;
+
+  auto slot_of = [&](int l) { return ((l % 3) + 3) % 3; };
+  auto load_plane = [&](int l) {
+    const int lw = wrap(l, L);
+    T* dst = sP + slot_of(l) * TE_PP * ND;
+    for (int p = tid; p < TE_PP; p += TE_NT) {
+      const int hr = p % TE_PR, hc = p / TE_PR;
+      const int gr = wrap(r0 + hr - 1, R), gc = wrap(c0 + hc - 1, C);
+      const size_t node = (size_t)gr + (size_t)gc * R + (size_t)lw * RC;
+      T inv[ND];
+      if (MODE == TE_MR) {
+        if (pre) te_invdiag<ND, T>(sD, a.keys[node], inv);
+        else {
+#pragma unroll
+          for (int c = 0; c < ND; c++) inv[c] = T(1);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < ND; c++) {
+        T v = a.in0[node * ND + c];
+        if (MODE == TE_PCG) v = fma(beta, a.in1[node * ND + c], v);
+        if (MODE == TE_MR) v = fma(-alpha, a.in1[node * ND + c], v) * inv[c];
+        dst[p * ND + c] = v;
+      }
+    }
+  };
+
+  __syncthreads();
+  load_plane(l0 - 1);
+  load_plane(l0);
+  double acc = 0.0, acc_rz = 0.0, mr = 0.0, md = 0.0, mx = 0.0;
+  const int r = r0 + threadIdx.x, c = c0 + threadIdx.y;
+  const bool active = (r < R) && (c < C);
+  const int ctr = (threadIdx.x + 1) + (threadIdx.y + 1) * TE_PR;
+  for (int l = l0; l < l1; l++) {
+    load_plane(l + 1);
+    __syncthreads();
+    if (active) {
+      const size_t node = (size_t)r + (size_t)c * R + (size_t)l * RC;
+      const unsigned key = a.keys[node];
+      const T* pm = sP + slot_of(l - 1) * TE_PP * ND;
+      const T* p0 = sP + slot_of(l) * TE_PP * ND;
+      const T* pp = sP + slot_of(l + 1) * TE_PP * ND;
+      T out[ND];
+      te_node<ND, T>(sK, kstride, key, pm, p0, pp, ctr, out);
+#pragma unroll
+      for (int cc = 0; cc < ND; cc++) {
+        const size_t j = node * ND + cc;
+        const T v = p0[ctr * ND + cc];
+        a.y[j] = out[cc];
+        if (MODE == TE_PCG) a.vout[j] = v;
+        if (MODE == TE_MR) {
+          const T rn = fma(-alpha, a.in1[j], a.in0[j]);
+          a.vout[j] = rn;
+          const T dv = a.d[j];
+          const T xv = fma(alpha, dv, a.x[j]);
+          a.x[j] = xv;
+          acc_rz += (double)rn * (double)v;
+          mr = fmax(mr, fabs((double)rn));
+          md = fmax(md, fabs((double)dv));
+          mx = fmax(mx, fabs((double)xv));
+        }
+        acc += (double)v * (double)out[cc];
+      }
+    }
+    __syncthreads();
+  }
+  if (a.finish == FIN_NONE) return;
+  const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  if (MODE == TE_MR) {
+    const double vals[5] = {acc, acc_rz, mr, md, mx};
+    const bool ismax[5] = {false, false, true, true, true};
+    double out[5];
+    if (grid_reduce<TE_NT, 5>(vals, ismax, a.rc, bid, out, sred) && tid == 0) {
+      for (int k = 0; k < 5; k++) a.sc->red[k] = out[k];
+      mr_finish(a.finish, out, a.sc, a.cfg);
+    }
+  } else {
+    const double vals[1] = {acc};
+    const bool ismax[1] = {false};
+    double out[1];
+    if (grid_reduce<TE_NT, 1>(vals, ismax, a.rc, bid, out, sred) && tid == 0) {
+      a.sc->red[0] = out[0];
+      if (a.finish == FIN_ALPHA) a.sc->alpha = a.sc->delta / out[0];
+    }
+  }
+}
+
+template <int ND, typename T>
+inline size_t te_smem_bytes(int nmat) {
+  const int ED = 8 * ND;
+  (void)nmat;
+  return (size_t)4 * (ED * ED + 1) * sizeof(T) + (size_t)3 * TE_PP * ND * sizeof(T) + 16;
+}
+
+}  // namespace chfem

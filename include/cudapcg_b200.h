@@ -1,0 +1,157 @@
+/*
+ * cudapcg_b200.h -- C ABI of libcudapcg_b200.so, the B200 (sm_100a) solver library of
+ * chfem_b200.
+ *
+ * Part 1 is a drop-in for chfem's cudapcg library: same names, argument meaning, data
+ * formats and 1/0 return convention as chfem/src/femhmg/cudapcg/cudapcg.h:19-62, with
+ * cudapcgVar_t = double and 16-bit material keys (the reference defaults,
+ * chfem/src/femhmg/cudapcg/includes.h:46-80).  A caller built against the reference header
+ * links against this library unchanged.  Differences by design:
+ *   - errors return 0 and leave a message for cudapcgB200LastError(); the library never
+ *     calls exit() or cudaDeviceReset() (reference: error_handling.h:6-14, cudapcg.cu:201);
+ *   - 2D analyses, the scalar-density field and the 2-vector solvers (CG2/MINRES2) are
+ *     rejected with an error (outside the 3D hot path this library implements).
+ *
+ * Part 2 (cudapcgB200* / chfemB200*) has no counterpart in the reference: precision mode,
+ * operator access for tests, solve statistics.
+ */
+#ifndef CUDAPCG_B200_H
+#define CUDAPCG_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#ifndef CUDAPCG_TRUE
+#define CUDAPCG_TRUE 1
+#define CUDAPCG_FALSE 0
+#define CUDAPCG_NBN 0
+#define CUDAPCG_EBE 1
+#define CUDAPCG_POREMAP_IMG 0
+#define CUDAPCG_POREMAP_NUM 1
+#define CUDAPCG_L2_NORM 0
+#define CUDAPCG_INF_NORM 1
+#define CUDAPCG_ERROR_NORM 2
+#define CUDAPCG_THERMAL_2D 0
+#define CUDAPCG_THERMAL_3D 1
+#define CUDAPCG_ELASTIC_2D 2
+#define CUDAPCG_ELASTIC_3D 3
+#define CUDAPCG_FLUID_2D 4
+#define CUDAPCG_FLUID_3D 5
+#define CUDAPCG_CG_SOLVER 0
+#define CUDAPCG_MINRES_SOLVER 1
+#define CUDAPCG_CG3_SOLVER 2
+#define CUDAPCG_MINRES3_SOLVER 3
+#define CUDAPCG_CG2_SOLVER 4
+#define CUDAPCG_MINRES2_SOLVER 5
+typedef double cudapcgVar_t;
+typedef double cudapcgTol_t;
+typedef unsigned short int cudapcgMap_t;
+typedef uint8_t cudapcgFlag_t;
+typedef unsigned int cudapcgIdMap_t;
+typedef uint16_t parametricScalarField_t;
+
+/* Same field order as chfem/src/femhmg/cudapcg/includes.h:93-129. */
+typedef struct _pcgmodel {
+  char *name;
+  cudapcgFlag_t freeAllowed_flag;
+  cudapcgFlag_t parStrategy_flag;
+  cudapcgFlag_t poremap_flag;
+  cudapcgFlag_t parametric_density_field_flag;
+  cudapcgFlag_t SBS_flag;
+  unsigned int nrows;
+  unsigned int ncols;
+  unsigned int nlayers;
+  unsigned int nelem;
+  unsigned int nvars;
+  unsigned int nvarspernode;
+  unsigned int nkeys;
+  unsigned int localmtxdim;
+  unsigned int nporenodes;
+  unsigned int nbordernodes;
+  unsigned int nhmgvars;
+  double limits_density_field[2];
+  cudapcgMap_t *image;
+  parametricScalarField_t *parametric_density_field;
+  cudapcgFlag_t *pore_map;
+  cudapcgFlag_t *border_pore_map;
+  cudapcgIdMap_t *periodic2DOF_map;
+  cudapcgIdMap_t *DOF2periodic_map;
+} cudapcgModel_t;
+#endif
+
+/* ---------------- Part 1: drop-in cudapcg ABI (cudapcg.h:19-62) ---------------------- */
+/* cudapcg.cu:108-183 */ cudapcgFlag_t cudapcgInit(cudapcgFlag_t analysis_flag, cudapcgFlag_t parStrategy_flag);
+/* cudapcg.cu:185-203 */ cudapcgFlag_t cudapcgEnd(void);
+/* cudapcg.cu:250-254 */ cudapcgFlag_t cudapcgSetModelConstructorFcn(cudapcgFlag_t (*fcn)(cudapcgModel_t **, const void *));
+/* cudapcg.cu:256-293 */ cudapcgFlag_t cudapcgBuildModel(const void *data);
+/* cudapcg.cu:205-236 */ cudapcgModel_t *cudapcgNewModel(void);
+/* cudapcg.cu:238-247 */ cudapcgFlag_t cudapcgSetModel(cudapcgModel_t *model);
+/* cudapcg.cu:94 */      cudapcgFlag_t cudapcgSetNumTol(cudapcgTol_t t);
+/* cudapcg.cu:95 */      cudapcgFlag_t cudapcgSetMaxIterations(unsigned int n);
+/* cudapcg.cu:96 */      cudapcgFlag_t cudapcgSetXReduceMode(cudapcgFlag_t flag);
+/* cudapcg.cu:97 */      cudapcgFlag_t cudapcgSetXReduceShift(unsigned int shift);
+/* cudapcg.cu:98 */      cudapcgFlag_t cudapcgSetXReduceScale(double scl);
+/* cudapcg.cu:99 */      cudapcgFlag_t cudapcgSetReduceStabFactor(double scl);
+/* cudapcg.cu:100 */     cudapcgFlag_t cudapcgSetSolver(cudapcgFlag_t flag);
+/* cudapcg.cu:101 */     cudapcgFlag_t cudapcgSetPreconditioner(cudapcgFlag_t flag);
+/* cudapcg.cu:102 */     cudapcgFlag_t cudapcgSetResNorm(cudapcgFlag_t flag);
+/* cudapcg.cu:377-381 */ cudapcgFlag_t cudapcgAllocateArrays(void);
+/* cudapcg.cu:383-387 */ cudapcgFlag_t cudapcgFreeArrays(void);
+/* cudapcg.cu:312-317 */ cudapcgFlag_t cudapcgSetRHS(cudapcgVar_t *RHS);
+/* cudapcg.cu:295-310 */ cudapcgFlag_t cudapcgSetX0(cudapcgVar_t *x0, cudapcgFlag_t mustInterpolate);
+/* cudapcg.cu:319-325 */ cudapcgFlag_t cudapcgSetImage(cudapcgMap_t *img);
+/* cudapcg.cu:327-334 */ cudapcgFlag_t cudapcgSetParametricDensityField(parametricScalarField_t *field, double fmin, double fmax);
+/* cudapcg.cu:336-346 */ cudapcgFlag_t cudapcgSetPoreMap(cudapcgFlag_t *pores);
+/* cudapcg.cu:348-355 */ cudapcgFlag_t cudapcgSetPeriodic2DOFMap(cudapcgIdMap_t *vars);
+/* cudapcg.cu:357-363 */ cudapcgFlag_t cudapcgSetDOF2PeriodicMap(cudapcgIdMap_t *nodes);
+/* cudapcg.cu:365-375 */ cudapcgFlag_t cudapcgSetLclMtxs(cudapcgVar_t *LclMtxs);
+/* cudapcg.cu:389-409 */ cudapcgFlag_t cudapcgSolve(cudapcgVar_t *x);
+/* cudapcg.cu:411-434 */ cudapcgFlag_t cudapcgSetHeaderString(char *header);
+/* cudapcg.cu:434-448 */ cudapcgFlag_t cudapcgPrintSolverReport(void);
+/* cudapcg.cu:450-469 */ cudapcgFlag_t cudapcgPrintSolverReport2(char *dest);
+/* cudapcg.cu:471-482 */ cudapcgFlag_t cudapcgPrintSolverMetrics(void);
+/* cudapcg.cu:484-499 */ cudapcgFlag_t cudapcgPrintSolverMetrics2(char *dest);
+/* cudapcg.cu:103 */     unsigned int cudapcgGetNumIterations(void);
+/* cudapcg.cu:104 */     unsigned int cudapcgGetMaxNumIterations(void);
+/* cudapcg.cu:105 */     cudapcgVar_t cudapcgGetResidual(void);
+
+/* ---------------- Part 2: extensions (no counterpart in the reference) ---------------- */
+#define CHFEM_B200_FP64 0   /* FP64 storage and arithmetic (parity mode, default)            */
+#define CHFEM_B200_MIXED 1  /* FP32 fields/operator, FP64 dots, stopping test, replacement  */
+
+/* Last error message of this library ("" when none). */
+const char *cudapcgB200LastError(void);
+/* Precision mode for the next solves (CHFEM_B200_FP64 or CHFEM_B200_MIXED). */
+cudapcgFlag_t cudapcgB200SetPrecision(int mode);
+/* Mixed mode: replace the recursive residual by b - A x every k iterations (0 = never). */
+cudapcgFlag_t cudapcgB200SetResidualReplacement(unsigned int k);
+/* Iterations per CUDA-graph launch of the device-resident loop (even, >= 2). */
+cudapcgFlag_t cudapcgB200SetIterationsPerLaunch(unsigned int k);
+/* y = A x on the current model (host buffers of nvars doubles); for parity tests. */
+cudapcgFlag_t cudapcgB200ApplyOperator(const double *x, double *y);
+/* y = M^-1 x (Jacobi) on the current model. */
+cudapcgFlag_t cudapcgB200ApplyPreconditioner(const double *x, double *y);
+/* Statistics of the last solve. */
+typedef struct {
+  unsigned int iterations;
+  double residual;
+  double solve_seconds;        /* device time of the iteration loop (CUDA events) */
+  double setup_seconds;        /* device time of init + initial-guess handling */
+  unsigned long long kernel_launches;  /* kernels of this library launched by the last solve */
+  int precision;
+  int found;
+} cudapcgB200Stats;
+cudapcgFlag_t cudapcgB200GetStats(cudapcgB200Stats *out);
+/* Device-side operator timing: runs `reps` applies of the current model's operator on its
+   work vectors and returns the mean duration in seconds (CUDA events); for roofline reports. */
+double cudapcgB200TimeOperator(unsigned int reps);
+/* Number of bytes the library holds on the device for the current model and arrays. */
+unsigned long long cudapcgB200DeviceBytes(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUDAPCG_B200_H */
