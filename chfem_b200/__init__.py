@@ -1,0 +1,12 @@
+"""chfem_b200 -- B200-native solver hot path of chfem (image-based FEM homogenization).
+
+Public API, with chfem's names:
+  compute_property(...)            effective conductivity / stiffness / permeability
+  import_nf, import_raw, export_for_chfem   .nf / .raw I/O
+Native libraries (chfem_b200/lib): libcudapcg_b200.so (GPU solver, drop-in cudapcg C ABI),
+libchfem_b200.so (host model layer, femhmg-compatible hmg* API), chfem_exec (CLI).
+"""
+from .io import import_nf, import_raw, export_for_chfem
+from .compute_properties import compute_property
+
+__all__ = ["compute_property", "import_nf", "import_raw", "export_for_chfem"]

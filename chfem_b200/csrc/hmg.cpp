@@ -1,0 +1,482 @@
+// hmg.cpp -- femhmg-compatible host API of chfem_b200 (3D): settings and image input,
+// model set-up, the load-case loop over the cudapcg C ABI, output.
+//
+// Follows chfem/src/femhmg/femhmg.c: hmgInit :135-394, readData :1456-1586 (tag grammar and
+// the 12-entry scan limit), readMaterialMapRAW/Numpy :1644-1758 (x-fastest file order
+// transposed to the row-fastest internal order, with %refinement replication),
+// hmgSolveHomogenization :848-1198 (solver set-up, direction loop, -xi/-xo files, updateC).
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/chfem_b200.h"
+#include "../../include/cudapcg_b200.h"
+#include "hmg.h"
+
+using namespace chfem_host;
+
+namespace {
+
+Model* g_m = nullptr;
+std::string g_err;
+// solver-side flags (femhmg.c:26-29 defaults)
+int g_par = CUDAPCG_NBN, g_solver = CUDAPCG_CG_SOLVER, g_precond = 1, g_stopcrit = CUDAPCG_L2_NORM;
+int g_poremap = CUDAPCG_POREMAP_NUM;
+int g_precision = CHFEM_B200_PREC_FP64, g_multirhs = 0, g_quiet = 0;
+int g_dir_set = 0, g_dir = 6;
+bool g_export_x = false;
+std::string g_x0_file;
+bool g_use_x0 = false;
+int g_recursions = 0;
+bool g_report = false;
+std::string g_report_text;
+chfemB200SolveStats g_stats;
+
+#define SAY(...) do { if (!g_quiet) printf(__VA_ARGS__); } while (0)
+
+void fail(const std::string& e) {
+  g_err = e;
+  fprintf(stderr, "chfem_b200: %s\n", e.c_str());
+}
+
+// ---- .nf (femhmg.c:1456-1586) ---------------------------------------------------------
+bool read_nf(Model& m, const char* fn) {
+  FILE* f = fopen(fn, "r");
+  if (!f) { fail(std::string("cannot open ") + fn); return false; }
+  char tok[256];
+  unsigned count = 0;
+  const unsigned num_of_info = 12;
+  int nx = -1, ny = -1, nz = -1;
+  double tolbuf = 0;
+  bool ok = true;
+  for (int i = 0; i < 256; i++) m.props_keys[i] = -1;
+  while (count < num_of_info && fscanf(f, "%255s", tok) == 1) {
+    if (!strcmp(tok, "%type_of_analysis")) {
+      if (fscanf(f, "%d", &m.analysis) != 1) break;
+      count++;
+      if (m.analysis < 0 || m.analysis > 2) { fail("provided analysis flag does not match any possible value"); ok = false; break; }
+    } else if (!strcmp(tok, "%type_of_solver")) {
+      int v; if (fscanf(f, "%d", &v) != 1) break;
+      m.solver_flag = v; g_solver = v; count++;
+    } else if (!strcmp(tok, "%voxel_size")) {
+      if (fscanf(f, "%lf", &m.voxel) != 1) break;
+      count++;
+    } else if (!strcmp(tok, "%solver_tolerance")) {
+      if (fscanf(f, "%lf", &tolbuf) != 1) break;
+      m.tol = tolbuf; count++;
+    } else if (!strcmp(tok, "%number_of_iterations")) {
+      if (fscanf(f, "%u", &m.maxit) != 1) break;
+      count++;
+    } else if (!strcmp(tok, "%image_dimensions")) {
+      if (fscanf(f, "%d %d %d", &nx, &ny, &nz) != 3) break;
+      count++;
+    } else if (!strcmp(tok, "%refinement")) {
+      if (fscanf(f, "%u", &m.refinement) != 1) break;
+      count++;
+      if (m.refinement < 1) { fail("refinement must be >= 1"); ok = false; break; }
+    } else if (!strcmp(tok, "%number_of_materials")) {
+      if (fscanf(f, "%u", &m.nmat) != 1) break;
+      count++;
+      if (m.nmat > 256) { fail("too many materials"); ok = false; break; }
+    } else if (!strcmp(tok, "%properties_of_materials")) {
+      for (unsigned i = 0; i < m.nmat; i++) {
+        int id = -1;
+        if (m.analysis == ELASTIC) { if (fscanf(f, "%d %lf %lf", &id, &m.props[2 * i], &m.props[2 * i + 1]) != 3) break; }
+        else if (m.analysis == THERMAL) { if (fscanf(f, "%d %lf", &id, &m.props[i]) != 2) break; }
+        else { if (fscanf(f, "%d", &id) != 1) break; }
+        count++;
+        if (id < 0 || id > 255) { fail("material colour key must be 0..255"); ok = false; break; }
+        m.props_keys[id] = (int)i;
+      }
+      if (!ok) break;
+    } else if (!strcmp(tok, "%thermal_expansion")) {
+      if (m.analysis == ELASTIC) {
+        for (unsigned i = 0; i < m.nmat; i++) if (fscanf(f, "%lf", &m.alpha[i]) != 1) break;
+        m.has_thermal_expansion = true;
+      }
+    } else if (!strcmp(tok, "%data_type")) {
+      char buf[64]; if (fscanf(f, "%63s", buf) != 1) break;
+      count++;
+    } else if (!strcmp(tok, "%xreduce_scale_factor")) {
+      double v; if (fscanf(f, "%lf", &v) != 1) break;
+      count++;
+    }
+  }
+  fclose(f);
+  if (!ok) return false;
+  if (nx <= 0 || ny <= 0) { fail("%image_dimensions missing or invalid"); return false; }
+  if (nz <= 0) { fail("2D images are not provided by chfem_b200 (3D only)"); return false; }
+  if (m.analysis < 0) { fail("%type_of_analysis missing"); return false; }
+  if (m.nmat == 0) { fail("no materials"); return false; }
+  if (m.refinement > 1) m.voxel /= m.refinement;
+  m.nx = (unsigned)nx * m.refinement; m.ny = (unsigned)ny * m.refinement; m.nz = (unsigned)nz * m.refinement;
+  return true;
+}
+
+// ---- image (femhmg.c:1644-1758) -------------------------------------------------------
+bool read_image(Model& m, const uint8_t* data, const char* raw) {
+  const unsigned ref = m.refinement;
+  const unsigned rows = m.ny / ref, cols = m.nx / ref, slices = m.nz / ref;
+  const size_t nvox_file = (size_t)rows * cols * slices;
+  std::vector<uint8_t> buf;
+  const uint8_t* src = data;
+  if (!src) {
+    FILE* f = fopen(raw, "rb");
+    if (!f) { fail(std::string("cannot open image ") + raw); return false; }
+    buf.resize(nvox_file);
+    size_t got = fread(buf.data(), 1, nvox_file, f);
+    fclose(f);
+    if (got < nvox_file) { fail("reached end of image file before expected"); return false; }
+    src = buf.data();
+  }
+  m.N = (long)m.nx * m.ny * m.nz;
+  m.elem_mat.assign(m.N, 0);
+  const size_t R = m.ny, C = m.nx;
+  bool bad = false;
+  int badcol = -1;
+#pragma omp parallel for schedule(static)
+  for (long k = 0; k < (long)slices; k++)
+    for (size_t i = 0; i < rows; i++)
+      for (size_t j = 0; j < cols; j++) {
+        const uint8_t v = src[(size_t)k * rows * cols + i * cols + j];  // x fastest in the file
+        const int mat = m.props_keys[v];
+        if (mat < 0) { bad = true; badcol = v; continue; }
+        for (unsigned kk = ref * k; kk < ref * (k + 1); kk++)
+          for (unsigned ii = ref * i; ii < ref * (i + 1); ii++)
+            for (unsigned jj = ref * j; jj < ref * (j + 1); jj++) m.elem_mat[ii + jj * R + (size_t)kk * R * C] = (uint16_t)mat;
+      }
+  if (bad) { fail("image holds colour " + std::to_string(badcol) + " that the .nf does not list"); return false; }
+  return true;
+}
+
+// cudapcg model constructor (femhmg.c:54-85)
+cudapcgFlag_t model_ctor(cudapcgModel_t** ptr, const void* data) {
+  if (!data) return CUDAPCG_FALSE;
+  const Model& m = *(const Model*)data;
+  cudapcgModel_t* p = *ptr;
+  p->name = (char*)malloc(m.nf_noext.size() + 1);
+  strcpy(p->name, m.nf_noext.c_str());
+  p->parStrategy_flag = (cudapcgFlag_t)g_par;
+  p->poremap_flag = (cudapcgFlag_t)g_poremap;
+  p->parametric_density_field_flag = 0;
+  p->nrows = m.ny; p->ncols = m.nx; p->nlayers = m.nz;
+  p->nelem = (unsigned)m.N;
+  p->nvars = (unsigned)m.ndof;
+  p->nvarspernode = 3;
+  p->nkeys = m.analysis == FLUID ? 1 : m.nmat;
+  p->localmtxdim = m.analysis == THERMAL ? 40 : (m.analysis == ELASTIC ? 576 : 1024);
+  p->nporenodes = (unsigned)m.nV;
+  p->nbordernodes = (unsigned)m.nB;
+  p->nhmgvars = m.analysis == FLUID ? (unsigned)(3 * m.nV) : (unsigned)m.ndof;
+  return CUDAPCG_TRUE;
+}
+
+int pcg_flag_of(const Model& m) { return m.analysis == THERMAL ? CUDAPCG_THERMAL_3D : (m.analysis == ELASTIC ? CUDAPCG_ELASTIC_3D : CUDAPCG_FLUID_3D); }
+
+const char* DIR_STR[6] = {"X", "Y", "Z", "YZ (shear)", "XZ (shear)", "XY (shear)"};
+
+bool setup_solver(Model& m) {
+  if (!cudapcgInit((cudapcgFlag_t)pcg_flag_of(m), (cudapcgFlag_t)g_par)) { fail(std::string("cudapcgInit: ") + cudapcgB200LastError()); return false; }
+  cudapcgSetHeaderString((char*)"    | ");
+  cudapcgSetModelConstructorFcn(model_ctor);
+  if (!cudapcgBuildModel(&m)) { fail(std::string("cudapcgBuildModel: ") + cudapcgB200LastError()); return false; }
+  if (!cudapcgSetSolver((cudapcgFlag_t)g_solver)) { fail(std::string("cudapcgSetSolver: ") + cudapcgB200LastError()); return false; }
+  cudapcgSetPreconditioner((cudapcgFlag_t)g_precond);
+  cudapcgSetResNorm((cudapcgFlag_t)g_stopcrit);
+  cudapcgSetNumTol(m.tol);
+  cudapcgSetMaxIterations(m.maxit);
+  cudapcgB200SetPrecision(g_precision);
+  bool ok;
+  if (m.analysis != FLUID) {
+    ok = cudapcgSetImage(m.keys.data());
+  } else {
+    ok = cudapcgSetPeriodic2DOFMap(m.dof_of_node.data()) && cudapcgSetPoreMap(m.border_keys.data()) &&
+         cudapcgSetDOF2PeriodicMap(m.node_of_dof.data());
+  }
+  ok = ok && cudapcgSetLclMtxs(m.lcl.data()) && cudapcgAllocateArrays();
+  if (!ok) { fail(std::string("model upload: ") + cudapcgB200LastError()); return false; }
+  return true;
+}
+
+}  // namespace
+
+// =======================================================================================
+extern "C" {
+
+logical hmgInit(char* data_filename, char* elem_filename, char* sdf_filename, uint8_t* data) {
+  const auto t0 = std::chrono::steady_clock::now();
+  hmgEnd();
+  g_err.clear();
+  if (!data_filename) { fail("no .nf file"); return 0; }
+  if (sdf_filename) { fail("scalar density field input is not provided by chfem_b200"); return 0; }
+  SAY("Initializing femhmg...\n");
+  Model* m = new Model();
+  m->nf = data_filename;
+  m->nf_noext = m->nf.size() > 3 ? m->nf.substr(0, m->nf.size() - 3) : m->nf;
+  if (elem_filename) m->raw = elem_filename;
+  if (!read_nf(*m, data_filename)) { delete m; return 0; }
+  if (!data) {
+    if (!elem_filename) { fail("no image"); delete m; return 0; }
+    const size_t L = strlen(elem_filename);
+    if (L < 4 || strcmp(elem_filename + L - 4, ".raw")) { fail(std::string("file ") + elem_filename + " is not in a valid format (.raw)"); delete m; return 0; }
+  }
+  m->nd = m->analysis == ELASTIC ? 3 : 1;
+  m->C_dim = m->analysis == ELASTIC ? 36 : 9;
+  if (!read_image(*m, data, elem_filename)) { delete m; return 0; }
+  std::string err;
+  if (!build_maps(*m, err)) { fail(err); delete m; return 0; }
+  build_local_matrices(*m);
+  g_m = m;
+  g_dir_set = 0;
+  g_use_x0 = false; g_x0_file.clear(); g_export_x = false;
+  const double t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  SAY("Done.(%.2e s)\n", t);
+  return 1;
+}
+
+logical hmgEnd(void) {
+  if (!g_m) return 0;
+  delete g_m;
+  g_m = nullptr;
+  cudapcgEnd();
+  return 1;
+}
+
+void hmgSetXReduceFlag(uint8_t) {}
+void hmgSetParallelStrategyFlag(uint8_t flag) { g_par = flag ? CUDAPCG_EBE : CUDAPCG_NBN; }
+void hmgSetSolverFlag(uint8_t flag) { g_solver = flag; }
+void hmgSetPreConditionerFlag(uint8_t flag) { g_precond = flag > 0; }
+void hmgSetStoppingCriteria(uint8_t flag) { g_stopcrit = flag; }
+logical hmgSetPoreMappingStrategy(uint8_t flag) {
+  if (flag > CUDAPCG_POREMAP_NUM) return 1;  // femhmg.c:484: out-of-range flags are ignored
+  if (flag == CUDAPCG_POREMAP_IMG && g_m && g_m->analysis == FLUID) {
+    fail("the image pore map (-pm 0) is not provided by chfem_b200; use the DOF-number map (-pm 1)");
+    return 0;
+  }
+  g_poremap = flag;
+  return 1;
+}
+void hmgExportX(logical flag) { g_export_x = flag > 0; }
+void hmgImportX(char* file) {
+  if (!g_m) return;
+  g_x0_file = file ? file : "";
+  g_use_x0 = true;
+}
+void hmgFindInitialGuesses(unsigned int nlevels) {
+  g_recursions = (int)nlevels;
+  if (nlevels > 0) SAY("WARNING: recursive coarse-grid initial guesses are not provided by chfem_b200; solving from x0 = 0.\n");
+}
+void hmgSetHomogenizationFlag(hmgFlag_t flag) {
+  if (!g_m) return;
+  const int maxdir = g_m->analysis == ELASTIC ? 5 : 2;
+  if (flag > maxdir) { g_dir_set = 0; return; }
+  g_dir_set = 1;
+  g_dir = flag;
+}
+
+void hmgSolveHomogenization(void) {
+  if (!g_m) return;
+  Model& m = *g_m;
+  const auto t_all = std::chrono::steady_clock::now();
+  memset(&g_stats, 0, sizeof(g_stats));
+  int dirs[6], nd = 0;
+  if (g_dir_set) dirs[nd++] = g_dir;
+  else { nd = load_case_count(m); load_case_list(m, dirs); }
+  for (unsigned i = 0; i < m.C_dim; i++) m.C[i] = 0.0;
+  SAY("Running homogenization...\n");
+  if (!setup_solver(m)) return;
+  m.rhs.assign(m.ndof, 0.0);
+  std::vector<double> x(m.ndof, 0.0), x0;
+  g_stats.n_cases = nd;
+  g_stats.ndof = (unsigned)m.ndof;
+  for (int k = 0; k < nd; k++) {
+    const int dir = dirs[k];
+    SAY("    ------------------------------------------------------\n    Analysis on %s:\n", DIR_STR[dir]);
+    auto t = std::chrono::steady_clock::now();
+    assemble_rhs(m, dir, m.rhs.data());
+    cudapcgSetRHS(m.rhs.data());
+    g_stats.rhs_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
+    if (g_use_x0 && !g_x0_file.empty()) {  // femhmg.c:1047-1067: <prefix>_<dir>.bin
+      const std::string fn = g_x0_file + "_" + std::to_string(dir) + ".bin";
+      FILE* f = fopen(fn.c_str(), "rb");
+      if (!f) { SAY("    | Reading initial guess from %s...Failed!...\n", fn.c_str()); cudapcgSetX0(nullptr, 0); }
+      else {
+        x0.assign(m.ndof, 0.0);
+        if (fread(x0.data(), sizeof(double), m.ndof, f) < (size_t)m.ndof) SAY("WARNING: Failed to read all %ld items from %s...", m.ndof, fn.c_str());
+        fclose(f);
+        cudapcgSetX0(x0.data(), 0);
+      }
+    }
+    SAY("    Solving system of equations...\n");
+    cudapcgSolve(x.data());
+    if (!g_quiet) cudapcgPrintSolverMetrics();
+    cudapcgB200Stats st;
+    cudapcgB200GetStats(&st);
+    g_stats.direction[k] = dir;
+    g_stats.iterations[k] = st.iterations;
+    g_stats.residual[k] = st.residual;
+    g_stats.solve_seconds[k] = st.solve_seconds;
+    g_stats.kernel_launches += st.kernel_launches;
+    if (g_export_x) {  // femhmg.c:1077-1084
+      const std::string fn = m.nf_noext + "_X_" + std::to_string(dir) + ".bin";
+      FILE* f = fopen(fn.c_str(), "wb");
+      if (f) { fwrite(x.data(), sizeof(double), m.ndof, f); fclose(f); }
+    }
+    t = std::chrono::steady_clock::now();
+    update_C(m, dir, x.data());
+    g_stats.update_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
+    if (g_report) {
+      char buf[512];
+      snprintf(buf, sizeof(buf), "Analysis on %s: %u iterations, residual %.3e, solver time %.3e s\n", DIR_STR[dir], st.iterations, st.residual, st.solve_seconds);
+      g_report_text += buf;
+    }
+  }
+  cudapcgSetX0(nullptr, 0);
+  cudapcgFreeArrays();
+  cudapcgEnd();
+  g_stats.total_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_all).count();
+  SAY("    ------------------------------------------------------\nDone.(%.2e s)\n", g_stats.total_seconds);
+}
+
+void hmgPrintModelData(void) {
+  if (!g_m || g_quiet) return;
+  const Model& m = *g_m;
+  static const char* AN[3] = {"THERMAL_3D", "ELASTIC_3D", "FLUID_3D"};
+  static const char* SO[6] = {"CG", "MINRES", "CG3", "MINRES3", "CG2", "MINRES2"};
+  printf("*******************************************************\nMODEL DATA:\nAnalysis: %s\n", AN[m.analysis]);
+  printf("Number of voxels (x,y,z): [%u,%u,%u]\nNumber of voxels (total): %ld\n", m.nx, m.ny, m.nz, m.N);
+  if (m.analysis == FLUID)
+    printf("  | porosity: %05.2f%%\n  | within pores: %ld\n  | at interfaces: %ld\n", 100.0 * m.nporeelem / (double)m.N, m.nV, m.nB);
+  printf("Number of DOFs: %ld\nNumber of materials: %u\nNumerical tolerance: %.3e\nMax iterations: %u\nSolver: %s%s\n",
+         m.ndof, m.nmat, m.tol, m.maxit, g_precond ? "P" : "", SO[g_solver < 6 ? g_solver : 0]);
+  printf("Precision: %s\n*******************************************************\n", g_precision ? "mixed (FP32 fields, FP64 reductions)" : "FP64");
+}
+
+void hmgPrintConstitutiveMtx(void) {
+  if (!g_m) return;
+  const Model& m = *g_m;
+  static const char* NAME[3] = {"Thermal Conductivity", "Elasticity", "Permeability"};
+  const int n = m.analysis == ELASTIC ? 6 : 3;
+  printf("-------------------------------------------------------\nHomogenized Constitutive Matrix (%s):\n", NAME[m.analysis]);
+  for (int i = 0; i < n; i++) {
+    for (int j = 0; j < n; j++) printf("  %.8e", m.C[i * n + j]);
+    printf("\n");
+  }
+  printf("-------------------------------------------------------\n");
+}
+var* hmgGetConstitutiveMtx(void) { return g_m ? g_m->C : nullptr; }
+unsigned int hmgGetConstitutiveMtxDim(void) { return g_m ? g_m->C_dim : 0; }
+var* hmgGetThermalExpansion(void) { return nullptr; }
+unsigned int hmgGetThermalExpansionDim(void) { return 0; }
+logical hmgSaveConstitutiveMtx(const char* filename) {
+  if (!g_m) return 0;
+  FILE* f = fopen(filename, "wb");
+  if (!f) return 0;
+  fwrite(g_m->C, sizeof(double), g_m->C_dim, f);
+  fclose(f);
+  return 1;
+}
+void hmgSaveFields(logical mustExport, logical) {
+  if (mustExport) SAY("WARNING: field export (-e) is not provided by chfem_b200 yet.\n");
+}
+void hmgKeepTrackOfAnalysisReport(uint8_t flag) {
+  g_report = flag != 0;
+  if (g_report && g_m) g_report_text = "Neutral file: " + g_m->nf + "\nImage: " + g_m->raw + "\n";
+}
+uint8_t hmgPrintReport(const char* filename) {
+  if (!g_report) return 0;
+  if (!filename) { printf("%s", g_report_text.c_str()); return 1; }
+  FILE* f = fopen(filename, "w");
+  if (!f) return 0;
+  fputs(g_report_text.c_str(), f);
+  fclose(f);
+  return 1;
+}
+
+// ---------------- extensions ----------------
+void chfemB200SetPrecision(int mode) { g_precision = mode ? CHFEM_B200_PREC_MIXED : CHFEM_B200_PREC_FP64; }
+void chfemB200SetMultiRHS(int on) { g_multirhs = on; }
+void chfemB200SetQuiet(int quiet) {
+  g_quiet = quiet;
+  if (quiet) setenv("CHFEM_B200_QUIET", "1", 1); else unsetenv("CHFEM_B200_QUIET");
+}
+const char* chfemB200LastError(void) { return g_err.c_str(); }
+int chfemB200GetSolveStats(chfemB200SolveStats* out) {
+  if (!out) return 0;
+  *out = g_stats;
+  return 1;
+}
+
+int chfemB200Run(const uint8_t* voxels, const char* nf, int direction, int solver, int precondition, int precision, int multirhs,
+                 double* C_out) {
+  if (!voxels || !nf || !C_out) { fail("chfemB200Run: null argument"); return 0; }
+  g_solver = solver; g_precond = precondition > 0; g_precision = precision; g_multirhs = multirhs;
+  if (!hmgInit((char*)nf, nullptr, nullptr, (uint8_t*)voxels)) return 0;
+  g_solver = solver;  // the .nf %type_of_solver is overridden by the caller, like chfem_wrapper.c:20-24
+  if (direction < 6) hmgSetHomogenizationFlag((hmgFlag_t)direction);
+  hmgPrintModelData();
+  hmgSolveHomogenization();
+  if (!g_err.empty()) return 0;
+  const int n = g_m->analysis == ELASTIC ? 6 : 3;
+  memcpy(C_out, g_m->C, sizeof(double) * n * n);
+  return n;
+}
+
+unsigned long long chfemB200ModelArraySize(int which) {
+  if (!g_m) return 0;
+  const Model& m = *g_m;
+  switch (which) {
+    case 0: return m.keys.size() * 2;
+    case 1: return m.dof_of_node.size() * 4;
+    case 2: return m.node_of_dof.size() * 4;
+    case 3: return m.border_keys.size();
+    case 4: return m.lcl.size() * 8;
+    case 5: return m.rhs.size() * 8;
+    case 6: return m.elem_mat.size() * 2;
+    case 7: return m.CB.size() * 8;
+  }
+  return 0;
+}
+int chfemB200CopyModelArray(int which, void* dst, unsigned long long bytes) {
+  if (!g_m || !dst) return 0;
+  const Model& m = *g_m;
+  const void* src = nullptr;
+  switch (which) {
+    case 0: src = m.keys.data(); break;
+    case 1: src = m.dof_of_node.data(); break;
+    case 2: src = m.node_of_dof.data(); break;
+    case 3: src = m.border_keys.data(); break;
+    case 4: src = m.lcl.data(); break;
+    case 5: src = m.rhs.data(); break;
+    case 6: src = m.elem_mat.data(); break;
+    case 7: src = m.CB.data(); break;
+    default: return 0;
+  }
+  const unsigned long long have = chfemB200ModelArraySize(which);
+  memcpy(dst, src, bytes < have ? bytes : have);
+  return 1;
+}
+int chfemB200AssembleRHS(int direction, double* dst) {
+  if (!g_m || !dst) return 0;
+  assemble_rhs(*g_m, direction, dst);
+  return 1;
+}
+int chfemB200UpdateC(int direction, const double* x, double* C_out) {
+  if (!g_m || !x) return 0;
+  update_C(*g_m, direction, x);
+  if (C_out) memcpy(C_out, g_m->C, sizeof(double) * g_m->C_dim);
+  return 1;
+}
+int chfemB200ModelInfo(unsigned int* info) {
+  if (!g_m || !info) return 0;
+  const Model& m = *g_m;
+  info[0] = m.nx; info[1] = m.ny; info[2] = m.nz; info[3] = (unsigned)m.N; info[4] = (unsigned)m.ndof;
+  info[5] = (unsigned)m.nV; info[6] = (unsigned)m.nB; info[7] = m.nmat; info[8] = (unsigned)m.analysis;
+  return 1;
+}
+
+}  // extern "C"

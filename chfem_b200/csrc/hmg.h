@@ -1,0 +1,63 @@
+// hmg.h -- internal model of the chfem_b200 host layer (3D thermal / elastic / Stokes).
+//
+// Index conventions are chfem's (chfem/src/femhmg/femhmg.c:1644-1709,
+// physical_phenomena/femhmg_3D.c:4-75): voxel and node index i = row + col*ny + layer*ny*nx,
+// row fastest; a voxel e = (r,c,l) has its local node 3 ("left, top, near") at node e and
+// its local node k at node (r + 1 + drow(k), c + dcol(k), l + dlay(k)) (periodic).
+// Physical axes: x = +col, y = -row, z = -layer (right-handed), so the +x, +y, +z faces of
+// a voxel hold local nodes {1,2,5,6}, {2,3,6,7} and {0,1,2,3}.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace chfem_host {
+
+enum Analysis { THERMAL = 0, ELASTIC = 1, FLUID = 2 };
+
+struct Model {
+  // settings (.nf, femhmg.c:1456-1586)
+  int analysis = -1;
+  int solver_flag = 0;
+  double voxel = 1.0;
+  double tol = 1e-6;
+  unsigned maxit = 10000;
+  unsigned nx = 0, ny = 0, nz = 0;   // voxels per axis after refinement
+  unsigned refinement = 1;
+  unsigned nmat = 0;
+  double props[512] = {0};
+  int props_keys[256];               // colour -> material index (-1 when not listed)
+  double alpha[256] = {0};
+  bool has_thermal_expansion = false;
+  std::string nf, nf_noext, raw;
+  // sizes
+  long N = 0;                        // voxels = periodic nodes
+  long ndof = 0;
+  unsigned nd = 1;                   // DOF per node (thermal 1, elastic 3; Stokes layout is special)
+  unsigned C_dim = 9;
+  // maps
+  std::vector<uint16_t> elem_mat;    // material index per voxel
+  std::vector<uint16_t> keys;        // 16-bit node keys (thermal/elastic)
+  std::vector<uint8_t> fluid_keys;   // 8-bit node fluid keys (Stokes)
+  std::vector<uint32_t> dof_of_node; // Stokes: node -> DOF id
+  std::vector<uint32_t> node_of_dof; // Stokes: DOF id -> node
+  std::vector<uint8_t> border_keys;  // Stokes: fluid keys of interface nodes
+  long nV = 0, nB = 0, nporeelem = 0;
+  // local matrices in the cudapcg formats, and the stress (flux, velocity) averaging matrices
+  std::vector<double> lcl;           // thermal 40/mat, elastic 576/mat, Stokes 1024
+  std::vector<double> CB;            // thermal 8x3 (avg gradient)*k per mat, elastic 6x24 per mat, Stokes 3x24
+  std::vector<double> Kdense;        // dense element matrices (8nd x 8nd per material; Stokes 32x32)
+  // results
+  double C[36] = {0};
+  std::vector<double> rhs;
+};
+
+// physics (hmg_physics.cpp)
+bool build_maps(Model& m, std::string& err);
+void build_local_matrices(Model& m);
+void assemble_rhs(const Model& m, int direction, double* rhs);
+void update_C(Model& m, int direction, const double* x);
+int load_case_count(const Model& m);
+void load_case_list(const Model& m, int* dirs);
+
+}  // namespace chfem_host

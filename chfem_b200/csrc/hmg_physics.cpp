@@ -1,0 +1,339 @@
+// hmg_physics.cpp -- 3D physics of the chfem_b200 host layer: node keys and pore maps,
+// element matrices, right-hand sides and effective-tensor updates.
+//
+// Reference behaviour followed (chfem/src/femhmg/physical_phenomena/):
+//   node keys ................. femhmg_3D.c:19-75
+//   Stokes fluid keys, DOF ids  femhmg_fluid_3D.c:370-491 (pore nodes first, then interface
+//                               nodes, each in ascending node order)
+//   element matrices .......... femhmg_thermal_3D.c:42-120, femhmg_elastic_3D.c:51-128,
+//                               femhmg_fluid_3D.c:41-110
+//   right-hand sides .......... femhmg_thermal_3D.c:122-236, femhmg_elastic_3D.c:130-511,
+//                               femhmg_fluid_3D.c:112-182
+//   effective tensor .......... femhmg_thermal_3D.c:355-500, femhmg_elastic_3D.c:1075-1343,
+//                               femhmg_fluid_3D.c:184-285
+// The reference hard-codes the element matrices as closed-form tables and writes each load
+// case as its own loop.  Here the matrices are integrated from the trilinear shape functions
+// with 2x2x2 Gauss quadrature (exact for these integrands), and every load case is the same
+// generic statement: a unit macroscopic gradient/strain enters as a jump of one field
+// component across the periodic +face of the cell, RHS = -K_e * jump on the voxels whose
+// +face lies on that boundary, and the tensor column is the volume average of
+// (flux or stress matrix) * (x + jump).
+#include "hmg.h"
+
+#include <cmath>
+#include <cstring>
+#include <omp.h>
+
+namespace chfem_host {
+
+static inline int drow(int k) { return -((k & 3) >> 1); }
+static inline int dcol(int k) { return ((k & 3) == 1 || (k & 3) == 2) ? 1 : 0; }
+static inline int dlay(int k) { return k >> 2; }
+// Local node coordinates in the unit cube: x = +col, y = -row, z = -layer.  The reference's
+// Stokes element matrix (femhmg_fluid_3D.c:57-91) is written with z = +layer instead (its
+// u_x-u_z couplings have the opposite sign to a z = -layer derivation); `zflip` selects that.
+static inline int nxi(int k) { return dcol(k); }
+static inline int neta(int k) { return -drow(k); }
+static inline int nzeta(int k, bool zflip) { return zflip ? dlay(k) : 1 - dlay(k); }
+static inline bool shares_edge(int a, int b) {
+  return ((drow(a) != drow(b)) + (dcol(a) != dcol(b)) + (dlay(a) != dlay(b))) == 1;
+}
+static inline long wrapl(long v, long n) { v %= n; return v < 0 ? v + n : v; }
+
+// Node of local node k of voxel (r,c,l).
+static inline long elem_node(long r, long c, long l, int k, long R, long C, long L) {
+  return wrapl(r + 1 + drow(k), R) + wrapl(c + dcol(k), C) * R + wrapl(l + dlay(k), L) * R * C;
+}
+// Voxel in which node (r,c,l) is local node e.
+static inline long node_elem(long r, long c, long l, int e, long R, long C, long L) {
+  return wrapl(r - drow(e) - 1, R) + wrapl(c - dcol(e), C) * R + wrapl(l - dlay(e), L) * R * C;
+}
+
+// ---- shape functions and 2-point Gauss quadrature on [0,1]^3 --------------------------
+struct QP { double p[3]; double w; };
+static void gauss(QP* q) {
+  const double g[2] = {0.5 - 0.5 / std::sqrt(3.0), 0.5 + 0.5 / std::sqrt(3.0)};
+  int n = 0;
+  for (int k = 0; k < 2; k++)
+    for (int j = 0; j < 2; j++)
+      for (int i = 0; i < 2; i++) { q[n].p[0] = g[i]; q[n].p[1] = g[j]; q[n].p[2] = g[k]; q[n].w = 0.125; n++; }
+}
+static inline double f1(int node_at_one, double t) { return node_at_one ? t : 1.0 - t; }
+static inline double df1(int node_at_one) { return node_at_one ? 1.0 : -1.0; }
+static void shape(int a, const double* p, double& phi, double* grad, bool zflip) {
+  const int cx = nxi(a), cy = neta(a), cz = nzeta(a, zflip);
+  const double fx = f1(cx, p[0]), fy = f1(cy, p[1]), fz = f1(cz, p[2]);
+  phi = fx * fy * fz;
+  grad[0] = df1(cx) * fy * fz;
+  grad[1] = fx * df1(cy) * fz;
+  grad[2] = fx * fy * df1(cz);
+}
+
+// ---- maps -----------------------------------------------------------------------------
+bool build_maps(Model& m, std::string& err) {
+  const long R = m.ny, C = m.nx, L = m.nz, N = m.N;
+  if (m.analysis != FLUID) {
+    if (m.nmat > 4) { err = "more than 4 materials cannot be encoded in 16-bit node keys"; return false; }
+    m.keys.assign(N, 0);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < N; i++) {
+      const long r = i % R, c = (i / R) % C, l = i / (R * C);
+      unsigned k = 0;
+      for (int e = 0; e < 8; e++) k |= ((unsigned)m.elem_mat[node_elem(r, c, l, e, R, C, L)] & 3u) << (2 * e);
+      m.keys[i] = (uint16_t)k;
+    }
+    m.ndof = N * m.nd;
+    return true;
+  }
+  // Stokes: bit e of a node's fluid key = voxel e of that node is pore (material index 0)
+  m.fluid_keys.assign(N, 0);
+  long pores = 0;
+#pragma omp parallel for reduction(+ : pores) schedule(static)
+  for (long i = 0; i < N; i++) {
+    const long r = i % R, c = (i / R) % C, l = i / (R * C);
+    unsigned k = 0;
+    for (int e = 0; e < 8; e++) k |= (unsigned)(m.elem_mat[node_elem(r, c, l, e, R, C, L)] == 0) << e;
+    m.fluid_keys[i] = (uint8_t)k;
+    pores += (m.elem_mat[i] == 0);
+  }
+  m.nporeelem = pores;
+  m.dof_of_node.assign(N, 0);
+  long id = 0;
+  for (long i = 0; i < N; i++)
+    if (m.fluid_keys[i] == 255) m.dof_of_node[i] = (uint32_t)id++;
+  m.nV = id;
+  for (long i = 0; i < N; i++)
+    if (m.fluid_keys[i] != 255 && m.fluid_keys[i] != 0) m.dof_of_node[i] = (uint32_t)id++;
+  m.nB = id - m.nV;
+  if (id >= (long)0xffffffffL) { err = "too many Stokes unknowns for 32-bit DOF ids"; return false; }
+  m.node_of_dof.assign(m.nV + m.nB, 0);
+  m.border_keys.assign(m.nB, 0);
+  for (long i = 0; i < N; i++) {
+    const uint8_t k = m.fluid_keys[i];
+    if (!k) continue;
+    const uint32_t d = m.dof_of_node[i];
+    m.node_of_dof[d] = (uint32_t)i;
+    if (k != 255) m.border_keys[d - m.nV] = k;
+  }
+  m.ndof = 4 * m.nV + m.nB;
+  return true;
+}
+
+// ---- element matrices -------------------------------------------------------------------
+void build_local_matrices(Model& m) {
+  QP q[8];
+  gauss(q);
+  double phi[8][8], grad[8][8][3];  // [qp][node]
+  for (int g = 0; g < 8; g++)
+    for (int a = 0; a < 8; a++) shape(a, q[g].p, phi[g][a], grad[g][a], m.analysis == FLUID);
+  // integrals of products
+  double KL[8][8] = {{0}}, GI[8][3] = {{0}}, PI[8] = {0}, DD[8][8][3][3] = {{{{0}}}}, GP[8][3][8] = {{{0}}};
+  for (int g = 0; g < 8; g++)
+    for (int a = 0; a < 8; a++) {
+      PI[a] += q[g].w * phi[g][a];
+      for (int i = 0; i < 3; i++) GI[a][i] += q[g].w * grad[g][a][i];
+      for (int b = 0; b < 8; b++) {
+        for (int i = 0; i < 3; i++) {
+          KL[a][b] += q[g].w * grad[g][a][i] * grad[g][b][i];
+          GP[a][i][b] += q[g].w * grad[g][a][i] * phi[g][b];
+          for (int j = 0; j < 3; j++) DD[a][b][i][j] += q[g].w * grad[g][a][i] * grad[g][b][j];
+        }
+      }
+    }
+  if (m.analysis == THERMAL) {
+    m.lcl.assign(40 * m.nmat, 0.0);
+    m.Kdense.assign(64 * m.nmat, 0.0);
+    m.CB.assign(24 * m.nmat, 0.0);  // [mat][stress s][node a]
+    for (unsigned k = 0; k < m.nmat; k++) {
+      const double kp = m.props[k];
+      int p = 0;
+      for (int a = 0; a < 8; a++)
+        for (int b = 0; b < 8; b++) {
+          const double v = kp * KL[a][b];
+          m.Kdense[64 * k + 8 * a + b] = shares_edge(a, b) ? 0.0 : v;
+          if (!shares_edge(a, b)) m.lcl[40 * k + p++] = v;
+        }
+      for (int s = 0; s < 3; s++)
+        for (int a = 0; a < 8; a++) m.CB[24 * k + 8 * s + a] = kp * GI[a][s];
+    }
+  } else if (m.analysis == ELASTIC) {
+    m.lcl.assign(576 * m.nmat, 0.0);
+    m.CB.assign(144 * m.nmat, 0.0);
+    for (unsigned k = 0; k < m.nmat; k++) {
+      const double E = m.props[2 * k], nu = m.props[2 * k + 1];
+      const double lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), mu = E / (2.0 * (1.0 + nu));
+      double D[6][6] = {{0}};
+      for (int i = 0; i < 3; i++) {
+        for (int j = 0; j < 3; j++) D[i][j] = lam;
+        D[i][i] = lam + 2.0 * mu;
+        D[3 + i][3 + i] = mu;
+      }
+      // B rows (Voigt: xx, yy, zz, yz, xz, xy) at each quadrature point
+      double Kel[24][24] = {{0}}, Bav[6][24] = {{0}};
+      for (int g = 0; g < 8; g++) {
+        double B[6][24] = {{0}};
+        for (int a = 0; a < 8; a++) {
+          const double* dg = grad[g][a];
+          B[0][3 * a + 0] = dg[0];
+          B[1][3 * a + 1] = dg[1];
+          B[2][3 * a + 2] = dg[2];
+          B[3][3 * a + 1] = dg[2]; B[3][3 * a + 2] = dg[1];
+          B[4][3 * a + 0] = dg[2]; B[4][3 * a + 2] = dg[0];
+          B[5][3 * a + 0] = dg[1]; B[5][3 * a + 1] = dg[0];
+        }
+        double DB[6][24] = {{0}};
+        for (int s = 0; s < 6; s++)
+          for (int c = 0; c < 24; c++) {
+            double t = 0.0;
+            for (int u = 0; u < 6; u++) t += D[s][u] * B[u][c];
+            DB[s][c] = t;
+          }
+        for (int r = 0; r < 24; r++)
+          for (int c = 0; c < 24; c++) {
+            double t = 0.0;
+            for (int s = 0; s < 6; s++) t += B[s][r] * DB[s][c];
+            Kel[r][c] += q[g].w * t;
+          }
+        for (int s = 0; s < 6; s++)
+          for (int c = 0; c < 24; c++) Bav[s][c] += q[g].w * DB[s][c];
+      }
+      for (int r = 0; r < 24; r++)
+        for (int c = 0; c < 24; c++) m.lcl[576 * k + 24 * r + c] = Kel[r][c];
+      for (int s = 0; s < 6; s++)
+        for (int c = 0; c < 24; c++) m.CB[144 * k + 24 * s + c] = Bav[s][c];
+    }
+    m.Kdense = m.lcl;
+  } else {
+    // Stokes, unit voxel, mu = 1: [K G; G^T Stab], K = int(grad u : grad v + grad u^T : grad v),
+    // G = int(d_i phi_a psi_b), Stab = (1/6) * Q1 Laplacian (the pressure stabilisation
+    // of femhmg_fluid_3D.c:44-45).
+    m.lcl.assign(1024, 0.0);
+    for (int a = 0; a < 8; a++)
+      for (int i = 0; i < 3; i++) {
+        for (int b = 0; b < 8; b++)
+          for (int j = 0; j < 3; j++) m.lcl[(3 * a + i) * 32 + 3 * b + j] = (i == j ? KL[a][b] : 0.0) + DD[a][b][j][i];
+        for (int b = 0; b < 8; b++) {
+          m.lcl[(3 * a + i) * 32 + 24 + b] = GP[a][i][b];
+          m.lcl[(24 + b) * 32 + 3 * a + i] = GP[a][i][b];
+        }
+      }
+    for (int a = 0; a < 8; a++)
+      for (int b = 0; b < 8; b++) m.lcl[(24 + a) * 32 + 24 + b] = KL[a][b] / 6.0;
+    m.CB.assign(80, 0.0);
+    for (int i = 0; i < 3; i++)
+      for (int a = 0; a < 8; a++) m.CB[24 * i + 3 * a + i] = PI[a];
+    for (int a = 0; a < 8; a++) m.CB[72 + a] = PI[a];
+    m.Kdense = m.lcl;
+  }
+}
+
+// ---- load cases -----------------------------------------------------------------------
+int load_case_count(const Model& m) { return m.analysis == ELASTIC ? 6 : 3; }
+void load_case_list(const Model& m, int* dirs) {
+  for (int i = 0; i < load_case_count(m); i++) dirs[i] = i;
+}
+// (axis of the jump, displaced component) of a load case; X Y Z YZ XZ XY
+static void case_axis(const Model& m, int dir, int& axis, int& comp) {
+  if (m.analysis != ELASTIC) { axis = dir; comp = 0; return; }
+  static const int AX[6] = {0, 1, 2, 1, 2, 1}, CO[6] = {0, 1, 2, 2, 0, 0};
+  axis = AX[dir]; comp = CO[dir];
+}
+static const int FACE[3][4] = {{1, 2, 5, 6}, {2, 3, 6, 7}, {0, 1, 2, 3}};
+static long axis_len(const Model& m, int axis) { return axis == 0 ? m.nx : (axis == 1 ? m.ny : m.nz); }
+
+// Voxels whose +axis face is the cell's +axis boundary: last column (x), first row (y),
+// first layer (z) -- femhmg_thermal_3D.c:144, :178, :212.
+template <typename F>
+static void for_boundary_voxels(const Model& m, int axis, F f) {
+  const long R = m.ny, C = m.nx, L = m.nz;
+  if (axis == 0) { for (long l = 0; l < L; l++) for (long r = 0; r < R; r++) f(r, C - 1, l); }
+  else if (axis == 1) { for (long l = 0; l < L; l++) for (long c = 0; c < C; c++) f(0, c, l); }
+  else { for (long c = 0; c < C; c++) for (long r = 0; r < R; r++) f(r, c, 0); }
+}
+
+void assemble_rhs(const Model& m, int dir, double* rhs) {
+  std::memset(rhs, 0, sizeof(double) * m.ndof);
+  const long R = m.ny, C = m.nx, L = m.nz;
+  if (m.analysis == FLUID) {  // unit body force along dir: int(phi_a) at every pore-node velocity
+    const long N = m.N;
+    for (long e = 0; e < N; e++) {
+      if (m.elem_mat[e] != 0) continue;
+      const long r = e % R, c = (e / R) % C, l = e / (R * C);
+      for (int a = 0; a < 8; a++) {
+        const uint32_t d = m.dof_of_node[elem_node(r, c, l, a, R, C, L)];
+        if (d < (uint32_t)m.nV) rhs[3 * (size_t)d + dir] += m.CB[72 + a];
+      }
+    }
+    return;
+  }
+  int axis, comp;
+  case_axis(m, dir, axis, comp);
+  const double jump = (double)axis_len(m, axis);
+  const int nd = m.nd, ed = 8 * nd;
+  for_boundary_voxels(m, axis, [&](long r, long c, long l) {
+    const long e = r + c * R + l * R * C;
+    const double* K = m.Kdense.data() + (size_t)m.elem_mat[e] * ed * ed;
+    for (int a = 0; a < 8; a++) {
+      const long n = elem_node(r, c, l, a, R, C, L);
+      for (int ci = 0; ci < nd; ci++) {
+        double s = 0.0;
+        for (int f = 0; f < 4; f++) s += K[(a * nd + ci) * ed + FACE[axis][f] * nd + comp];
+        rhs[n * nd + ci] -= s * jump;
+      }
+    }
+  });
+}
+
+void update_C(Model& m, int dir, const double* x) {
+  const long R = m.ny, C = m.nx, L = m.nz, N = m.N;
+  if (m.analysis == FLUID) {
+    double c0 = 0, c1 = 0, c2 = 0;
+#pragma omp parallel for reduction(+ : c0, c1, c2) schedule(static)
+    for (long e = 0; e < N; e++) {
+      if (m.elem_mat[e] != 0) continue;
+      const long r = e % R, c = (e / R) % C, l = e / (R * C);
+      for (int a = 0; a < 8; a++) {
+        const uint32_t d = m.dof_of_node[elem_node(r, c, l, a, R, C, L)];
+        if (d < (uint32_t)m.nV) {
+          c0 += m.CB[3 * a] * x[3 * (size_t)d];
+          c1 += m.CB[24 + 3 * a + 1] * x[3 * (size_t)d + 1];
+          c2 += m.CB[48 + 3 * a + 2] * x[3 * (size_t)d + 2];
+        }
+      }
+    }
+    const double scl = m.voxel * m.voxel / (double)N;
+    m.C[0 + dir] = c0 * scl; m.C[3 + dir] = c1 * scl; m.C[6 + dir] = c2 * scl;
+    return;
+  }
+  int axis, comp;
+  case_axis(m, dir, axis, comp);
+  const double jump = (double)axis_len(m, axis);
+  const int nd = m.nd, ns = (m.analysis == ELASTIC) ? 6 : 3, ec = 8 * nd;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+#pragma omp parallel
+  {
+    double loc[6] = {0, 0, 0, 0, 0, 0};
+#pragma omp for schedule(static)
+    for (long e = 0; e < N; e++) {
+      const long r = e % R, c = (e / R) % C, l = e / (R * C);
+      const double* CB = m.CB.data() + (size_t)m.elem_mat[e] * ns * ec;
+      for (int a = 0; a < 8; a++) {
+        const long n = elem_node(r, c, l, a, R, C, L);
+        for (int ci = 0; ci < nd; ci++) {
+          const double v = x[n * nd + ci];
+          for (int s = 0; s < ns; s++) loc[s] += CB[s * ec + a * nd + ci] * v;
+        }
+      }
+    }
+#pragma omp critical
+    for (int s = 0; s < ns; s++) acc[s] += loc[s];
+  }
+  for_boundary_voxels(m, axis, [&](long r, long c, long l) {
+    const double* CB = m.CB.data() + (size_t)m.elem_mat[r + c * R + l * R * C] * ns * ec;
+    for (int f = 0; f < 4; f++)
+      for (int s = 0; s < ns; s++) acc[s] += CB[s * ec + FACE[axis][f] * nd + comp] * jump;
+  });
+  for (int s = 0; s < ns; s++) m.C[s * ns + dir] = acc[s] / (double)N;
+}
+
+}  // namespace chfem_host

@@ -1,0 +1,123 @@
+"""chfem input/output formats: the .nf settings file and the .raw voxel image.
+
+Same functions, arguments and file formats as chfem's Python I/O (chfem/io.py:3-109 import_nf,
+import_raw; :208-335 export_for_chfem).  A .raw image is the uint8 voxel array in C order of a
+(z, y, x) array, i.e. x fastest; the .nf file is a list of '%tag' lines each followed by its
+values.
+"""
+import numpy as np
+
+
+def import_nf(filename):
+    """Read a .nf file into a dict (keys as in chfem/io.py:3-71).
+
+    image_dimensions is returned as (nz, ny, nx) for numpy indexing of the image.
+    """
+    if not filename.endswith(".nf"):
+        raise ValueError("Filename does not end with '.nf'")
+    with open(filename) as f:
+        lines = [ln.rstrip() for ln in f]
+    data = {}
+    for key in ("type_of_analysis", "type_of_solver", "type_of_rhs", "number_of_iterations", "refinement",
+                "number_of_materials"):
+        data[key] = int(lines[lines.index(f"%{key}") + 1])
+    data["voxel_size"] = float(lines[lines.index("%voxel_size") + 1])
+    data["solver_tolerance"] = float(lines[lines.index("%solver_tolerance") + 1])
+    nx, ny, nz = (int(v) for v in lines[lines.index("%image_dimensions") + 1].split())
+    data["image_dimensions"] = (nz, ny, nx)
+    i = lines.index("%properties_of_materials")
+    data["properties_of_materials"] = []
+    for j in range(1, data["number_of_materials"] + 1):
+        parts = lines[i + j].split()
+        data["properties_of_materials"].append((int(parts[0]), *[float(p) for p in parts[1:]]))
+    data["volume_fraction"] = None
+    if "%volume_fraction" in lines:
+        data["volume_fraction"] = tuple(float(v) for v in lines[lines.index("%volume_fraction") + 1].split())
+    data["data_type"] = None
+    if "%data_type" in lines:
+        data["data_type"] = lines[lines.index("%data_type") + 1]
+    if "%thermal_expansion" in lines:
+        i = lines.index("%thermal_expansion")
+        data["thermal_expansion"] = [float(lines[i + j]) for j in range(1, data["number_of_materials"] + 1)]
+    return data
+
+
+def import_raw(filename, shape=None, dtype=np.uint8):
+    """Read a .raw file into a numpy array; shape is (z, y, x) for 3D (chfem/io.py:73-109)."""
+    if not filename.endswith(".raw"):
+        raise ValueError("Filename does not end with '.raw'")
+    with open(filename, "rb") as f:
+        raw = f.read()
+    if shape is not None:
+        expected = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        if len(raw) != expected:
+            raise ValueError(f"File size ({len(raw)}) does not match expected size ({expected})")
+    arr = np.frombuffer(raw, dtype=dtype)
+    return arr.reshape(shape) if shape is not None else arr
+
+
+def export_for_chfem(filename, array, analysis_type, mat_props=None, voxel_size=1, solver_type=0, rhs_type=0,
+                     refinement=1, export_raw=True, export_nf=True, solver_tolerance=1.e-6, solver_maxiter=10000,
+                     tmp_nf_file=None):
+    """Write the .nf (and optionally .raw) inputs of an analysis (chfem/io.py:208-335).
+
+    analysis_type: 0 conductivity ({phase: k}), 1 elasticity ({phase: (E, nu[, alpha])}),
+    2 permeability (mat_props None).  Returns the dict of written settings.
+    """
+    domain = array.astype(np.uint8)
+    ids, counts = np.unique(domain, return_counts=True)
+    materials = dict(sorted(zip(ids.tolist(), counts.tolist())))
+    if mat_props is not None:
+        props_ids, img_ids = set(mat_props.keys()), set(materials.keys())
+        if props_ids != img_ids:
+            msg = []
+            if img_ids - props_ids:
+                msg.append(f"Missing material IDs in 'mat_props' that are present in the array: {img_ids - props_ids}.")
+            if props_ids - img_ids:
+                msg.append(f"Extra material IDs in 'mat_props' that are not present in the array: {props_ids - img_ids}.")
+            raise ValueError(" ".join(msg))
+    props, alphas = [], []
+    if analysis_type == 0:
+        props = [f"{k} {v}" for k, v in mat_props.items()]
+    elif analysis_type == 1:
+        for k, v in mat_props.items():
+            props.append(f"{k} {v[0]} {v[1]}")
+            if len(v) == 3:
+                alphas.append(f"{v[2]}")
+            elif alphas:
+                alphas.append("0.0")
+    elif analysis_type == 2:
+        props = [f"{k}" for k in materials.keys()]
+    else:
+        raise ValueError("Invalid analysis type.")
+    vf = np.array(list(materials.values())) * 100.0 / np.prod(domain.shape)
+    dims = [domain.shape[1], domain.shape[0], 0] if domain.ndim == 2 else [domain.shape[2], domain.shape[1], domain.shape[0]]
+    jdata = {"type_of_analysis": analysis_type, "type_of_solver": solver_type, "type_of_rhs": rhs_type,
+             "voxel_size": voxel_size, "solver_tolerance": solver_tolerance, "number_of_iterations": solver_maxiter,
+             "image_dimensions": dims, "refinement": refinement, "number_of_materials": len(materials),
+             "properties_of_materials": props, "volume_fraction": list(np.around(vf, 2)), "data_type": "uint8"}
+    if alphas:
+        jdata["thermal_expansion"] = alphas
+    if export_nf:
+        out = []
+        for k, v in jdata.items():
+            out.append("%" + k)
+            if k in ("properties_of_materials", "thermal_expansion"):
+                out.extend(v)
+            elif isinstance(v, (list, tuple)):
+                out.append(" ".join(str(float(x)) if isinstance(x, (np.floating,)) else str(x) for x in v))
+            else:
+                out.append(str(v))
+            out.append("")
+        text = "\n".join(out).strip()
+        if tmp_nf_file is not None:
+            tmp_nf_file.write(text.encode("utf-8"))
+            tmp_nf_file.flush()
+            tmp_nf_file.seek(0)
+        else:
+            with open(filename[: len(filename) - 4] + ".nf", "w") as f:
+                f.write(text)
+    if export_raw:
+        fn = filename if filename.endswith(".raw") else filename + ".raw"
+        domain.tofile(fn)
+    return jdata

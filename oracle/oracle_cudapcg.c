@@ -84,10 +84,10 @@ static cudapcgFlag_t (*model_ctor)(cudapcgModel_t **, const void *) = NULL;
 static int g_quiet = 0;
 
 /* captured inputs (checker access) */
-static void *cap_ptr[6] = {0};
-static unsigned int cap_n[6] = {0};
-static size_t cap_elsz[6] = {sizeof(cudapcgMap_t), sizeof(cudapcgIdMap_t), sizeof(cudapcgIdMap_t),
-                             sizeof(cudapcgFlag_t), sizeof(double), sizeof(double)};
+static void *cap_ptr[7] = {0};
+static unsigned int cap_n[7] = {0};
+static size_t cap_elsz[7] = {sizeof(cudapcgMap_t), sizeof(cudapcgIdMap_t), sizeof(cudapcgIdMap_t),
+                             sizeof(cudapcgFlag_t), sizeof(double), sizeof(double), sizeof(double)};
 static double *hist = NULL;
 static unsigned int hist_n = 0, hist_cap = 0;
 #define LOG_CAP 4096
@@ -826,6 +826,7 @@ cudapcgFlag_t cudapcgSolve(cudapcgVar_t *res_x) {
   if (minres) { if (S->precond) solve_pminres(); else solve_minres(); }
   else solve_cg_family(S->precond);
   memcpy(res_x, S->x, sizeof(double) * S->model->nvars);
+  capture(6, S->x, S->model->nvars);
   S->total_time = omp_get_wtime() - t0;
   S->mean_time = S->iteration ? S->total_time / S->iteration : 0.0;
   log_solve();
@@ -888,9 +889,9 @@ int oracle_precond(const double *x, double *y) {
   return 1;
 }
 unsigned int oracle_nvars(void) { return (S && S->model) ? S->model->nvars : 0; }
-unsigned int oracle_captured_count(int which) { return (which >= 0 && which < 6) ? cap_n[which] : 0; }
+unsigned int oracle_captured_count(int which) { return (which >= 0 && which < 7) ? cap_n[which] : 0; }
 int oracle_copy_captured(int which, void *dst, unsigned int bytes) {
-  if (which < 0 || which >= 6 || !cap_ptr[which]) return 0;
+  if (which < 0 || which >= 7 || !cap_ptr[which]) return 0;
   size_t have = (size_t)cap_n[which] * cap_elsz[which];
   memcpy(dst, cap_ptr[which], bytes < have ? bytes : have);
   return 1;

@@ -131,7 +131,7 @@ int oracle_precond(const double *x, double *y);
 /* Number of unknowns of the current model (0 if none). */
 unsigned int oracle_nvars(void);
 /* Copies of what the reference host code handed over the ABI, for map/RHS parity. */
-unsigned int oracle_captured_count(int which);          /* 0 keys,1 p2dof,2 dof2p,3 porekeys,4 lclmtx,5 rhs */
+unsigned int oracle_captured_count(int which);          /* 0 keys,1 p2dof,2 dof2p,3 porekeys,4 lclmtx,5 rhs,6 x */
 int oracle_copy_captured(int which, void *dst, unsigned int bytes);
 /* Residual history of the last solve: oracle_history(NULL,0) returns its length. */
 unsigned int oracle_history(double *dst, unsigned int n);

@@ -1,0 +1,101 @@
+"""Host model layer (libchfem_b200.so) versus the reference's own host code.
+
+The reference's femhmg host code (compiled from its sources into oracle/_ref) hands its maps,
+local matrices and right-hand sides over the cudapcg ABI to the CPU oracle, which records
+them.  chfem_b200's own host layer must produce the same arrays: maps bit-exact, matrices and
+RHS to round-off, and the same effective-tensor column from the same solution vector.
+CPU only: no solve runs on a GPU here.
+"""
+import ctypes
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from tests import helpers as H
+
+pytestmark = pytest.mark.skipif(not H.oracle_available(), reason="oracle/_ref not built (needs the reference tree)")
+
+
+def host_arrays(nf, raw, direction):
+    from chfem_b200 import _native
+    lib = _native.chfem()
+    lib.chfemB200SetQuiet(1)
+    assert lib.hmgInit(nf.encode(), raw.encode(), None, None), lib.chfemB200LastError()
+    info = (ctypes.c_uint * 9)()
+    lib.chfemB200ModelInfo(info)
+    out = {}
+    dt = {0: np.uint16, 1: np.uint32, 2: np.uint32, 3: np.uint8, 4: np.float64, 6: np.uint16, 7: np.float64}
+    for w, t in dt.items():
+        nbytes = lib.chfemB200ModelArraySize(w)
+        a = np.zeros(nbytes // np.dtype(t).itemsize, dtype=t)
+        if nbytes:
+            lib.chfemB200CopyModelArray(w, a.ctypes.data_as(ctypes.c_void_p), nbytes)
+        out[w] = a
+    ndof = info[4]
+    rhs = np.zeros(ndof)
+    lib.chfemB200AssembleRHS(direction, rhs.ctypes.data_as(ctypes.c_void_p))
+    out["rhs"] = rhs
+    out["info"] = list(info)
+    return lib, out
+
+
+def updateC(lib, direction, x):
+    C = np.zeros(36)
+    lib.chfemB200UpdateC(direction, np.ascontiguousarray(x).ctypes.data_as(ctypes.c_void_p), C.ctypes.data_as(ctypes.c_void_p))
+    return C
+
+
+CASES = [
+    # name, analysis, shape (z,y,x), nmat, directions
+    ("th2", 0, (6, 9, 11), 2, [0, 1, 2]),
+    ("th4", 0, (5, 7, 4), 4, [0, 2]),
+    ("el2", 1, (5, 6, 7), 2, [0, 1, 2, 3, 4, 5]),
+    ("el3", 1, (4, 5, 3), 3, [1, 3, 5]),
+]
+
+
+@pytest.mark.parametrize("name,analysis,shape,nmat,dirs", CASES)
+def test_thermal_elastic_maps_rhs_updateC(tmp_path, name, analysis, shape, nmat, dirs):
+    img = H.small_image(shape, nmat, seed=hash(name) % 1000)
+    nf, raw = H.write_small_case(str(tmp_path), name, img, analysis, tol=1e-6, maxit=50)
+    for d in dirs:
+        ref = H.oracle_capture(nf, raw, d)
+        lib, mine = host_arrays(nf, raw, d)
+        assert np.array_equal(mine[0], ref["0"]), "node material keys differ"
+        np.testing.assert_allclose(mine[4], ref["4"], rtol=1e-12, atol=1e-12 * np.abs(ref["4"]).max())
+        np.testing.assert_allclose(mine["rhs"], ref["5"], rtol=1e-11, atol=1e-11 * np.abs(ref["5"]).max())
+        C = updateC(lib, d, ref["6"])
+        k = 6 if analysis == 1 else 3
+        col_mine = C[: k * k].reshape(k, k)[:, d]
+        col_ref = ref["C"][: k * k].reshape(k, k)[:, d]
+        assert H.rel_to_max(col_mine, col_ref) < 1e-12
+
+
+def test_fluid_maps_rhs_updateC(tmp_path):
+    from chfem_b200.synthetic import pore_grf
+    img = pore_grf((10, 12, 14), corr=2.0, porosity=0.45, seed=7)
+    assert (img == 0).any()
+    nf, raw = H.write_small_case(str(tmp_path), "fl", img, 2, tol=1e-6, maxit=50)
+    for d in [0, 1, 2]:
+        ref = H.oracle_capture(nf, raw, d)
+        lib, mine = host_arrays(nf, raw, d)
+        assert np.array_equal(mine[1], ref["1"]), "node->DOF map differs"
+        assert np.array_equal(mine[2], ref["2"]), "DOF->node map differs"
+        assert np.array_equal(mine[3], ref["3"]), "interface fluid keys differ"
+        np.testing.assert_allclose(mine[4], ref["4"], rtol=1e-12, atol=1e-14)
+        np.testing.assert_allclose(mine["rhs"], ref["5"], rtol=1e-12, atol=1e-14)
+        C = updateC(lib, d, ref["6"])
+        assert H.rel_to_max(C[:9].reshape(3, 3)[:, d], ref["C"][:9].reshape(3, 3)[:, d]) < 1e-12
+
+
+def test_refinement_and_transpose(tmp_path):
+    """%refinement replicates each voxel and the x-fastest file order is transposed."""
+    img = H.small_image((3, 4, 5), 2, seed=3)
+    nf, raw = H.write_small_case(str(tmp_path), "ref2", img, 0, tol=1e-6, maxit=50, refinement=2)
+    ref = H.oracle_capture(nf, raw, 0)
+    lib, mine = host_arrays(nf, raw, 0)
+    assert mine["info"][:3] == [10, 8, 6]
+    assert np.array_equal(mine[0], ref["0"])
+    np.testing.assert_allclose(mine["rhs"], ref["5"], rtol=1e-12, atol=1e-12)
