@@ -90,3 +90,51 @@ def solve_stats():
     st = SolveStats()
     chfem().chfemB200GetSolveStats(ctypes.byref(st))
     return st
+
+
+class CudapcgModel(ctypes.Structure):
+    """Mirror of cudapcgModel_t (include/cudapcg_b200.h; chfem/src/femhmg/cudapcg/includes.h:93-129)."""
+    _fields_ = [("name", ctypes.c_char_p), ("freeAllowed_flag", ctypes.c_uint8), ("parStrategy_flag", ctypes.c_uint8),
+                ("poremap_flag", ctypes.c_uint8), ("parametric_density_field_flag", ctypes.c_uint8), ("SBS_flag", ctypes.c_uint8),
+                ("nrows", ctypes.c_uint), ("ncols", ctypes.c_uint), ("nlayers", ctypes.c_uint), ("nelem", ctypes.c_uint),
+                ("nvars", ctypes.c_uint), ("nvarspernode", ctypes.c_uint), ("nkeys", ctypes.c_uint), ("localmtxdim", ctypes.c_uint),
+                ("nporenodes", ctypes.c_uint), ("nbordernodes", ctypes.c_uint), ("nhmgvars", ctypes.c_uint),
+                ("limits_density_field", ctypes.c_double * 2), ("image", ctypes.c_void_p), ("parametric_density_field", ctypes.c_void_p),
+                ("pore_map", ctypes.c_void_p), ("border_pore_map", ctypes.c_void_p), ("periodic2DOF_map", ctypes.c_void_p),
+                ("DOF2periodic_map", ctypes.c_void_p)]
+
+
+def setup_cudapcg_model(lib, arrays):
+    """Drive the cudapcg C ABI of `lib` with host-layer arrays: init, model, maps, local matrices.
+
+    arrays: dict with nx, ny, nz, N, ndof, nV, nB, nkeys, analysis (0/1/2), keys, dof_of_node,
+    node_of_dof, border, lcl (the formats of the cudapcg ABI)."""
+    a = arrays
+    an = {0: 1, 1: 3, 2: 5}[a["analysis"]]
+    assert lib.cudapcgInit(an, 0)
+    lib.cudapcgNewModel.restype = ctypes.POINTER(CudapcgModel)
+    m = lib.cudapcgNewModel()
+    mm = m.contents
+    mm.nrows, mm.ncols, mm.nlayers = a["ny"], a["nx"], a["nz"]
+    mm.nelem = a["N"]
+    mm.nvars = a["ndof"]
+    mm.nkeys = a["nkeys"]
+    mm.localmtxdim = a["lcl"].size // a["nkeys"]
+    mm.nporenodes, mm.nbordernodes = a["nV"], a["nB"]
+    mm.nhmgvars = 3 * a["nV"] if a["analysis"] == 2 else a["ndof"]
+    mm.poremap_flag = 1
+    assert lib.cudapcgSetModel(m)
+    import numpy as np
+    keep = []
+
+    def ptr(x):
+        x = np.ascontiguousarray(x)
+        keep.append(x)
+        return x.ctypes.data_as(ctypes.c_void_p)
+    if a["analysis"] == 2:
+        assert lib.cudapcgSetPeriodic2DOFMap(ptr(a["dof_of_node"]))
+        assert lib.cudapcgSetPoreMap(ptr(a["border"]))
+        assert lib.cudapcgSetDOF2PeriodicMap(ptr(a["node_of_dof"]))
+    else:
+        assert lib.cudapcgSetImage(ptr(a["keys"]))
+    assert lib.cudapcgSetLclMtxs(ptr(a["lcl"]))

@@ -944,6 +944,40 @@ static double time_op_T(unsigned reps) {
   return ms * 1e-3 / std::max(1u, reps);
 }
 extern "C" {
+}  // extern "C"
+template <typename T>
+static double time_kernel_T(int which, unsigned reps) {
+  if (!ensure_vectors<T>() || !ensure_K<T>()) return -1.0;
+  if (!ensure_reduction(needed_blocks())) return -1.0;
+  // each repetition resets the scalars (so no pass exits early) and brackets only the launch
+  float total = 0.f;
+  for (unsigned i = 0; i < reps + 3; i++) {
+    DevScalars h{};
+    h.delta = 1.0; h.delta0 = 1.0; h.delta_old = 1.0; h.alpha = 1e-3; h.beta = 0.5; h.res0 = 1.0; h.metric = 1.0;
+    cudaMemcpyAsync(S->d_sc, &h, sizeof(h), cudaMemcpyHostToDevice, S->stream);
+    cudaEventRecord(S->ev0, S->stream);
+    bool ok;
+    switch (which) {
+      case 0: ok = launch_apply<T>((const T*)S->s, nullptr, nullptr, (T*)S->q2, false, FIN_NONE, false); break;
+      case 1: ok = launch_apply<T>((const T*)S->s, (const T*)S->d0, (T*)S->d1, (T*)S->q, true, FIN_ALPHA, false); break;
+      case 2: ok = launch_point<T, PW_PCG>((T*)S->x, (T*)S->d1, (T*)S->r, (const T*)S->q, (T*)S->s, nullptr); break;
+      case 3: ok = launch_mr_op<T>((const T*)S->r, (T*)S->r2, FIN_MR_STEP, false); break;
+      case 4: ok = launch_mr_dir<T>((const T*)S->r); break;
+      default: ok = false;
+    }
+    cudaEventRecord(S->ev1, S->stream);
+    if (!ok || cudaEventSynchronize(S->ev1) != cudaSuccess) return -1.0;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, S->ev0, S->ev1);
+    if (i >= 3) total += ms;
+  }
+  return total * 1e-3 / std::max(1u, reps);
+}
+extern "C" {
+double cudapcgB200TimeKernel(int which, unsigned int reps) {
+  if (!S || !S->model) return -1.0;
+  return (S->precision == CHFEM_B200_FP64) ? time_kernel_T<double>(which, reps) : time_kernel_T<float>(which, reps);
+}
 double cudapcgB200TimeOperator(unsigned int reps) {
   if (!S || !S->model) return -1.0;
   return (S->precision == CHFEM_B200_FP64) ? time_op_T<double>(reps) : time_op_T<float>(reps);

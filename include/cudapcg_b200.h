@@ -148,6 +148,12 @@ cudapcgFlag_t cudapcgB200GetStats(cudapcgB200Stats *out);
 /* Device-side operator timing: runs `reps` applies of the current model's operator on its
    work vectors and returns the mean duration in seconds (CUDA events); for roofline reports. */
 double cudapcgB200TimeOperator(unsigned int reps);
+/* Mean device duration (s, CUDA events on the library's stream) of `reps` launches of one
+   kernel of the iteration on the current model and its work vectors:
+   which 0 plain operator apply, 1 PCG operator pass (direction formed on the fly + dot),
+   2 PCG pointwise update pass, 3 (P)MINRES operator pass, 4 (P)MINRES direction pass.
+   The solver scalars are reset first; results of the work vectors are meaningless after. */
+double cudapcgB200TimeKernel(int which, unsigned int reps);
 /* Number of bytes the library holds on the device for the current model and arrays. */
 unsigned long long cudapcgB200DeviceBytes(void);
 

@@ -389,6 +389,7 @@ static void free_arrays(void) {
   S->d = S->q = S->s = NULL; g_dinv = NULL;
 }
 
+static void alloc_model_arrays(void);
 cudapcgModel_t *cudapcgNewModel(void) {
   cudapcgModel_t *m = (cudapcgModel_t *)calloc(1, sizeof(cudapcgModel_t));
   if (!m) return NULL;
@@ -469,7 +470,7 @@ cudapcgFlag_t cudapcgSetModel(cudapcgModel_t *model) {
   if (S->model && S->model->freeAllowed_flag) free_model(S->model);
   S->model = model;
   free_arrays();
-  free(S->r); S->r = (double *)calloc(model->nvars, sizeof(double));
+  alloc_model_arrays();
   return CUDAPCG_TRUE;
 }
 

@@ -131,3 +131,9 @@ def write_small_case(workdir, name, img, analysis, tol=1e-8, maxit=20000, solver
                      refinement=refinement, export_raw=True, export_nf=True, solver_tolerance=tol,
                      solver_maxiter=maxit)
     return prefix + ".nf", prefix + ".raw"
+
+
+def parse_iterations(log):
+    """Iteration counts printed by a solve ("iteration: N, residual: ...")."""
+    import re
+    return [int(m) for m in re.findall(r"iteration: (\d+), residual", log)]

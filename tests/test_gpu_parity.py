@@ -1,0 +1,207 @@
+"""GPU parity of chfem_b200 against the oracle (GPU box; marked gpu).
+
+Bars (stated per test): FP64 effective tensors within 1e-6 relative to the largest entry of
+the oracle's tensor, mixed precision within 1e-4; operator applies within 1e-12 (FP64) and
+1e-5 (FP32 storage) relative to the largest entry; maps and DOF counts bit-exact (checked on
+the CPU in test_host_parity.py).  The oracle is the reference's host code plus the CPU
+restatement of its solver, run as a child process.
+"""
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import zlib
+
+import numpy as np
+import pytest
+
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-6
+MIXED_TOL = 1e-4
+
+
+def oracle_columns():
+    with open(os.path.join(H.GOLDEN, "oracle_columns.json")) as f:
+        return json.load(f)
+
+
+# ---------------------------------------------------------------------------------------
+# Golden cases through the product CLI (chfem_b200/lib/chfem_exec)
+@pytest.mark.parametrize("key,precision", [
+    ("thermal_x_pcg", "fp64"), ("elastic_y_pcg", "fp64"), ("fluid_z_pcg", "fp64"), ("fluid_z_pminres", "fp64"),
+    ("thermal_all_pcg", "fp64"), ("thermal_x_pcg", "mixed"), ("elastic_y_pcg", "mixed"), ("fluid_z_pminres", "mixed"),
+])
+def test_golden_cases(tmp_path, key, precision):
+    ref = oracle_columns()[key]
+    nf, raw, meta = H.golden_case_files(ref["case"], str(tmp_path))
+    C, log = H.run_exec(H.CHFEM_EXEC, nf, raw, *ref["flags"], "--precision", precision)
+    Cref = np.array(ref["C"])
+    tol = FP64_TOL if precision == "fp64" else MIXED_TOL
+    cols = [meta["direction"]] if "-d" in ref["flags"] else list(range(Cref.shape[1]))
+    for c in cols:
+        assert H.rel_to_max(C[:, c], Cref[:, c]) < tol, (c, C[:, c], Cref[:, c])
+    # and within the reference's own regression bar of its golden column
+    assert H.rel_to_max(C[:, meta["direction"]], meta["column"]) < meta["reference_tolerance"]
+    if precision == "fp64":  # same recurrence, same stopping test: same iteration counts (+-1 for round-off)
+        its = H.parse_iterations(log)
+        assert len(its) == len(ref["iterations"])
+        assert all(abs(a - b) <= 1 for a, b in zip(its, ref["iterations"])), (its, ref["iterations"])
+
+
+def test_python_api_golden(tmp_path):
+    """compute_property with nf_filepath, like the reference's test/test_chfem.py:6-10."""
+    from chfem_b200 import compute_property, import_raw
+    ref = oracle_columns()["thermal_x_pcg"]
+    nf, raw, meta = H.golden_case_files("thermal_ggg40", str(tmp_path))
+    arr = import_raw(raw, (100, 100, 100))
+    C = np.array(compute_property("conductivity", arr, direction="x", nf_filepath=nf))
+    assert H.rel_to_max(C[:, 0], np.array(ref["C"])[:, 0]) < FP64_TOL
+
+
+# ---------------------------------------------------------------------------------------
+# Small synthetic models: every analysis x solver x option, product CLI versus oracle CLI
+SMALL = [
+    # name, analysis, builder, cli flags
+    ("th2_pcg", 0, ("img", (14, 17, 19), 2), ["-d", "6"]),
+    ("th4_cg", 0, ("img", (9, 13, 7), 4), ["-j", "0"]),
+    ("th3_minres", 0, ("img", (10, 11, 12), 3), ["-s", "1", "-j", "0"]),
+    ("th2_inf", 0, ("img", (12, 12, 12), 2), ["-c", "1"]),
+    ("th2_err", 0, ("img", (12, 10, 9), 2), ["-c", "2"]),
+    ("th2_ebe", 0, ("img", (11, 9, 13), 2), ["-p", "1"]),
+    ("th_thin", 0, ("img", (1, 2, 33), 2), []),
+    ("el2_pcg", 1, ("img", (10, 12, 11), 2), []),
+    ("el4_pcg", 1, ("img", (7, 9, 8), 4), ["-d", "3"]),
+    ("el2_ebe", 1, ("img", (8, 8, 9), 2), ["-p", "1", "-d", "5"]),
+    ("fl_pcg", 2, ("pore", (16, 18, 20), 0.45), ["-s", "0"]),
+    ("fl_pminres", 2, ("pore", (16, 18, 20), 0.45), ["-s", "1"]),
+    ("fl_minres_nopre", 2, ("pore", (14, 14, 14), 0.5), ["-s", "1", "-j", "0", "-d", "0"]),
+]
+
+
+def build_small(tmp_path, name, analysis, spec):
+    if spec[0] == "img":
+        img = H.small_image(spec[1], spec[2], seed=zlib.crc32(name.encode()) % 10000)
+    else:
+        from chfem_b200.synthetic import pore_grf
+        img = pore_grf(spec[1], corr=2.0, porosity=spec[2], seed=zlib.crc32(name.encode()) % 10000)
+    return H.write_small_case(str(tmp_path), name, img, analysis, tol=1e-8, maxit=20000)
+
+
+@pytest.mark.parametrize("name,analysis,spec,flags", SMALL)
+def test_small_models_fp64(tmp_path, name, analysis, spec, flags):
+    nf, raw = build_small(tmp_path, name, analysis, spec)
+    Cref, _ = H.run_exec(H.ORACLE_EXEC, nf, raw, *flags)
+    C, _ = H.run_exec(H.CHFEM_EXEC, nf, raw, *flags)
+    assert H.rel_to_max(C, Cref) < FP64_TOL
+
+
+@pytest.mark.parametrize("name,analysis,spec,flags", [s for s in SMALL if s[0] in ("th2_pcg", "el2_pcg", "fl_pminres")])
+def test_small_models_mixed(tmp_path, name, analysis, spec, flags):
+    nf, raw = build_small(tmp_path, name, analysis, spec)
+    Cref, _ = H.run_exec(H.ORACLE_EXEC, nf, raw, *flags)
+    C, _ = H.run_exec(H.CHFEM_EXEC, nf, raw, *flags, "--precision", "mixed")
+    assert H.rel_to_max(C, Cref) < MIXED_TOL
+
+
+def test_homogeneous_is_exact(tmp_path):
+    """A one-phase image has the phase's own tensor: k I for conduction."""
+    img = np.zeros((8, 9, 10), np.uint8)
+    from chfem_b200.io import export_for_chfem
+    export_for_chfem(str(tmp_path / "h.raw"), img, 0, mat_props={0: 3.5}, solver_tolerance=1e-10, solver_maxiter=1000)
+    C, log = H.run_exec(H.CHFEM_EXEC, str(tmp_path / "h.nf"), str(tmp_path / "h.raw"))
+    assert np.allclose(C, 3.5 * np.eye(3), atol=1e-9)
+
+
+def test_initial_guess_roundtrip(tmp_path):
+    """-xo writes x per load case; -xi reads it back and the solve stops at once with the same tensor."""
+    nf, raw = build_small(tmp_path, "x0", 1, ("img", (8, 9, 10), 2))
+    C1, _ = H.run_exec(H.CHFEM_EXEC, nf, raw, "-d", "2", "-xo")
+    prefix = nf[:-3] + "_X"
+    assert os.path.exists(prefix + "_2.bin")
+    C2, log = H.run_exec(H.CHFEM_EXEC, nf, raw, "-d", "2", "-xi", prefix)
+    assert "Initial guess satisfied" in log
+    assert H.rel_to_max(C2[:, 2], C1[:, 2]) < 1e-12
+
+
+def test_dropin_reference_host_on_b200_library(tmp_path):
+    """The reference's unmodified host code + CLI (femhmg + main.c) linked against
+    libcudapcg_b200.so reproduces the oracle."""
+    if not os.path.exists(H.DROPIN_EXEC):
+        pytest.skip("drop-in executable not built (needs the reference tree at build time)")
+    for name, analysis, spec, flags in [SMALL[0], SMALL[7], SMALL[11]]:
+        nf, raw = build_small(tmp_path, name, analysis, spec)
+        Cref, _ = H.run_exec(H.ORACLE_EXEC, nf, raw, *flags)
+        C, _ = H.run_exec(H.DROPIN_EXEC, nf, raw, *flags)
+        assert H.rel_to_max(C, Cref) < FP64_TOL
+
+
+# ---------------------------------------------------------------------------------------
+# Operator and preconditioner applies through the C ABI, versus the standalone oracle
+from chfem_b200._native import setup_cudapcg_model as setup_model  # noqa: E402
+
+
+_ORACLE_APPLY = r'''
+import ctypes, sys, pickle, numpy as np
+sys.path.insert(0, sys.argv[3])
+from tests.test_gpu_parity import setup_model
+a = pickle.load(open(sys.argv[1], "rb"))
+lib = ctypes.CDLL(sys.argv[2], mode=ctypes.RTLD_LOCAL)
+setup_model(lib, a)
+y = np.zeros(a["ndof"]); z = np.zeros(a["ndof"])
+assert lib.oracle_apply(a["x"].ctypes.data_as(ctypes.c_void_p), y.ctypes.data_as(ctypes.c_void_p))
+assert lib.oracle_precond(a["x"].ctypes.data_as(ctypes.c_void_p), z.ctypes.data_as(ctypes.c_void_p))
+np.save(sys.argv[1] + ".y.npy", y); np.save(sys.argv[1] + ".z.npy", z)
+'''
+
+
+def host_arrays(nf, raw):
+    from chfem_b200 import _native
+    lib = _native.chfem()
+    lib.chfemB200SetQuiet(1)
+    assert lib.hmgInit(nf.encode(), raw.encode(), None, None)
+    info = (ctypes.c_uint * 9)()
+    lib.chfemB200ModelInfo(info)
+    def arr(w, t):
+        n = lib.chfemB200ModelArraySize(w)
+        x = np.zeros(n // np.dtype(t).itemsize, dtype=t)
+        if n:
+            lib.chfemB200CopyModelArray(w, x.ctypes.data_as(ctypes.c_void_p), n)
+        return x
+    a = dict(nx=info[0], ny=info[1], nz=info[2], N=info[3], ndof=info[4], nV=info[5], nB=info[6], nkeys=max(1, info[7]) if info[8] != 2 else 1,
+             analysis=info[8], keys=arr(0, np.uint16), dof_of_node=arr(1, np.uint32), node_of_dof=arr(2, np.uint32),
+             border=arr(3, np.uint8), lcl=arr(4, np.float64))
+    lib.hmgEnd()
+    return a
+
+
+@pytest.mark.parametrize("name,analysis,spec", [("th", 0, ("img", (13, 35, 17), 3)), ("el", 1, ("img", (9, 33, 10), 2)),
+                                                 ("fl", 2, ("pore", (18, 20, 22), 0.45)), ("th_small", 0, ("img", (2, 3, 1), 2))])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_operator_and_jacobi(tmp_path, name, analysis, spec, precision):
+    import pickle
+    from chfem_b200 import _native
+    nf, raw = build_small(tmp_path, name, analysis, spec)
+    a = host_arrays(nf, raw)
+    rng = np.random.default_rng(5)
+    a["x"] = rng.standard_normal(a["ndof"])
+    pk = str(tmp_path / "a.pkl")
+    pickle.dump(a, open(pk, "wb"))
+    p = subprocess.run([sys.executable, "-c", _ORACLE_APPLY, pk, os.path.join(H.ROOT, "oracle", "liboracle_cudapcg.so"), H.ROOT],
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    yref, zref = np.load(pk + ".y.npy"), np.load(pk + ".z.npy")
+    lib = _native.cudapcg()
+    setup_model(lib, a)
+    assert lib.cudapcgB200SetPrecision(precision)
+    y = np.zeros(a["ndof"]); z = np.zeros(a["ndof"])
+    assert lib.cudapcgB200ApplyOperator(a["x"].ctypes.data_as(ctypes.c_void_p), y.ctypes.data_as(ctypes.c_void_p)), lib.cudapcgB200LastError()
+    assert lib.cudapcgB200ApplyPreconditioner(a["x"].ctypes.data_as(ctypes.c_void_p), z.ctypes.data_as(ctypes.c_void_p))
+    lib.cudapcgEnd()
+    tol = 1e-12 if precision == 0 else 1e-5
+    assert H.rel_to_max(y, yref) < tol
+    assert H.rel_to_max(z, zref) < tol
