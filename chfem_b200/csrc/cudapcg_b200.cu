@@ -92,14 +92,17 @@ struct Solver {
   uint32_t* d_dof_of_node = nullptr;
   uint32_t* d_node_of_dof = nullptr;
   uint8_t* d_bkeys = nullptr;
-  void* d_K = nullptr;      // T-typed dense element matrices
-  int K_prec = -1;
-  // vectors (T-typed, allocated for the precision in use)
+  double* d_K64 = nullptr;  // dense element matrices, FP64 (FP64 solves, residual replacement)
+  float* d_K32 = nullptr;   // dense element matrices, FP32 (mixed-precision iterations)
+  // Krylov work vectors, typed for the precision in use
   int vec_prec = -1;
-  void* x = nullptr; void* r = nullptr; void* r2 = nullptr; void* d0 = nullptr; void* d1 = nullptr;
+  void* r = nullptr; void* r2 = nullptr; void* d0 = nullptr; void* d1 = nullptr;
   void* q = nullptr; void* s = nullptr; void* q2 = nullptr;
-  double* b64 = nullptr;    // right-hand side kept in FP64 (mixed-mode residual replacement)
-  double* x64 = nullptr;    // FP64 staging for host <-> device in mixed mode
+  // FP64 in every mode: the solution, the right-hand side, an operator output and staging
+  double* x = nullptr;
+  double* b64 = nullptr;
+  double* y64 = nullptr;
+  double* x64 = nullptr;
   bool arrays_alloc = false, user_arrays = false;
   bool x0_set = false, rhs_set = false;
   // device scalars and reductions
@@ -136,87 +139,78 @@ template <typename T> static int prec_of() { return sizeof(T) == 8 ? CHFEM_B200_
 
 static void free_ptr(void* p) { if (p) cudaFree(p); }
 
+static void free_work_vectors() {
+  if (!S) return;
+  free_ptr(S->r); free_ptr(S->r2); free_ptr(S->d0); free_ptr(S->d1);
+  free_ptr(S->q); free_ptr(S->s); free_ptr(S->q2);
+  S->r = S->r2 = S->d0 = S->d1 = S->q = S->s = S->q2 = nullptr;
+  S->vec_prec = -1;
+  if (S->gexec) { cudaGraphExecDestroy(S->gexec); S->gexec = nullptr; S->graph_key = -1; }
+}
 static void free_vectors() {
   if (!S) return;
-  free_ptr(S->x); free_ptr(S->r); free_ptr(S->r2); free_ptr(S->d0); free_ptr(S->d1);
-  free_ptr(S->q); free_ptr(S->s); free_ptr(S->q2); free_ptr(S->b64); free_ptr(S->x64);
-  S->x = S->r = S->r2 = S->d0 = S->d1 = S->q = S->s = S->q2 = nullptr;
-  S->b64 = S->x64 = nullptr;
-  S->vec_prec = -1;
+  free_work_vectors();
+  free_ptr(S->x); free_ptr(S->b64); free_ptr(S->y64); free_ptr(S->x64);
+  S->x = S->b64 = S->y64 = S->x64 = nullptr;
   S->arrays_alloc = false;
-  if (S->gexec) { cudaGraphExecDestroy(S->gexec); S->gexec = nullptr; S->graph_key = -1; }
 }
 
 static void free_model_dev() {
   if (!S) return;
-  free_ptr(S->d_keys); free_ptr(S->d_dof_of_node); free_ptr(S->d_node_of_dof); free_ptr(S->d_bkeys); free_ptr(S->d_K);
-  S->d_keys = nullptr; S->d_dof_of_node = S->d_node_of_dof = nullptr; S->d_bkeys = nullptr; S->d_K = nullptr;
-  S->K_prec = -1;
+  free_ptr(S->d_keys); free_ptr(S->d_dof_of_node); free_ptr(S->d_node_of_dof); free_ptr(S->d_bkeys);
+  free_ptr(S->d_K64); free_ptr(S->d_K32);
+  S->d_keys = nullptr; S->d_dof_of_node = S->d_node_of_dof = nullptr; S->d_bkeys = nullptr;
+  S->d_K64 = nullptr; S->d_K32 = nullptr;
   S->have_K = S->have_keys = S->have_maps = false;
 }
 
-// Vectors for precision T.  x keeps the initial guess across precision switches by
-// converting through FP64.
+// Work vectors for precision T (the right-hand side is carried across a precision change
+// through its FP64 copy); the FP64 vectors are allocated once per model.
 template <typename T>
 static bool ensure_vectors() {
   const int p = prec_of<T>();
-  if (S->vec_prec == p && S->x) return true;
-  const size_t n = (size_t)S->nvars;
-  // carry r and x (rhs, initial guess) across a precision change
-  std::vector<double> hx, hr;
-  if (S->vec_prec != -1 && S->x) {
-    hx.resize(n); hr.resize(n);
-    if (S->vec_prec == CHFEM_B200_FP64) {
-      cudaMemcpy(hx.data(), S->x, n * 8, cudaMemcpyDeviceToHost);
-      cudaMemcpy(hr.data(), S->r, n * 8, cudaMemcpyDeviceToHost);
-    } else {
-      std::vector<float> tx(n), tr(n);
-      cudaMemcpy(tx.data(), S->x, n * 4, cudaMemcpyDeviceToHost);
-      cudaMemcpy(tr.data(), S->r, n * 4, cudaMemcpyDeviceToHost);
-      for (size_t i = 0; i < n; i++) { hx[i] = tx[i]; hr[i] = tr[i]; }
+  const size_t n = std::max<size_t>((size_t)S->nvars, 1);
+  if (!S->x) {
+    double** v64[] = {&S->x, &S->b64, &S->y64, &S->x64};
+    for (double** v : v64) {
+      CKV(cudaMalloc(v, n * 8));
+      CKV(cudaMemsetAsync(*v, 0, n * 8, S->stream));
     }
+    S->arrays_alloc = true;
   }
-  double* b64 = S->b64; S->b64 = nullptr;
-  free_vectors();
-  S->b64 = b64;
-  void** vs[] = {&S->x, &S->r, &S->r2, &S->d0, &S->d1, &S->q, &S->s, &S->q2};
+  if (S->vec_prec == p && S->r) return true;
+  free_work_vectors();
+  void** vs[] = {&S->r, &S->r2, &S->d0, &S->d1, &S->q, &S->s, &S->q2};
   for (void** v : vs) {
-    CKV(cudaMalloc(v, std::max<size_t>(n, 1) * sizeof(T)));
-    CKV(cudaMemsetAsync(*v, 0, std::max<size_t>(n, 1) * sizeof(T), S->stream));
+    CKV(cudaMalloc(v, n * sizeof(T)));
+    CKV(cudaMemsetAsync(*v, 0, n * sizeof(T), S->stream));
   }
-  if (!S->b64) CKV(cudaMalloc(&S->b64, std::max<size_t>(n, 1) * 8));
-  CKV(cudaMalloc(&S->x64, std::max<size_t>(n, 1) * 8));
   S->vec_prec = p;
-  if (!hx.empty()) {
-    if (p == CHFEM_B200_FP64) {
-      cudaMemcpy(S->x, hx.data(), n * 8, cudaMemcpyHostToDevice);
-      cudaMemcpy(S->r, hr.data(), n * 8, cudaMemcpyHostToDevice);
-    } else {
-      std::vector<float> tx(n), tr(n);
-      for (size_t i = 0; i < n; i++) { tx[i] = (float)hx[i]; tr[i] = (float)hr[i]; }
-      cudaMemcpy(S->x, tx.data(), n * 4, cudaMemcpyHostToDevice);
-      cudaMemcpy(S->r, tr.data(), n * 4, cudaMemcpyHostToDevice);
-    }
+  if (S->rhs_set) {  // re-derive the working right-hand side from its FP64 copy
+    if (sizeof(T) == 8) CKV(cudaMemcpyAsync(S->r, S->b64, n * 8, cudaMemcpyDeviceToDevice, S->stream));
+    else k_convert<double, float><<<std::max<long>(1, std::min<long>((n + 255) / 256, 8 * 148)), 256, 0, S->stream>>>(S->b64, (float*)S->r, (long)n);
   }
-  S->arrays_alloc = true;
   return true;
 }
 
+template <typename T> static T* Kdev();
+template <> double* Kdev<double>() { return S->d_K64; }
+template <> float* Kdev<float>() { return S->d_K32; }
+
 template <typename T>
 static bool ensure_K() {
-  const int p = prec_of<T>();
-  if (S->K_prec == p && S->d_K) return true;
+  if (Kdev<T>()) return true;
   if (!S->have_K) { set_err("solve", "local matrices were not set (cudapcgSetLclMtxs)"); return false; }
-  free_ptr(S->d_K); S->d_K = nullptr;
   std::vector<T> kt(S->Kd.size());
   for (size_t i = 0; i < kt.size(); i++) kt[i] = (T)S->Kd[i];
-  CKV(cudaMalloc(&S->d_K, kt.size() * sizeof(T)));
-  CKV(cudaMemcpy(S->d_K, kt.data(), kt.size() * sizeof(T), cudaMemcpyHostToDevice));
+  T* dk = nullptr;
+  CKV(cudaMalloc(&dk, kt.size() * sizeof(T)));
+  CKV(cudaMemcpy(dk, kt.data(), kt.size() * sizeof(T), cudaMemcpyHostToDevice));
+  if (sizeof(T) == 8) S->d_K64 = (double*)dk; else S->d_K32 = (float*)dk;
   if (S->analysis == CUDAPCG_FLUID_3D) {
     if (sizeof(T) == 8) CKV(cudaMemcpyToSymbol(c_flK64, kt.data(), 1024 * sizeof(double)));
     else CKV(cudaMemcpyToSymbol(c_flK32, kt.data(), 1024 * sizeof(float)));
   }
-  S->K_prec = p;
   return true;
 }
 
@@ -288,12 +282,12 @@ static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, i
     const int nb = grid.x * grid.y * grid.z;
     if (!ensure_reduction(nb)) return false;
     if (S->nd == 1) {
-      TeArgs<1, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, (const T*)S->d_K, S->nmat, S->R, S->C, S->L, lc, S->d_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
+      TeArgs<1, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, lc, S->d_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
       const size_t sm = te_smem_bytes<1, T>(S->nmat);
       if (fuse) k_te_apply<1, T, TE_PCG><<<grid, block, sm, S->stream>>>(a);
       else k_te_apply<1, T, TE_PLAIN><<<grid, block, sm, S->stream>>>(a);
     } else {
-      TeArgs<3, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, (const T*)S->d_K, S->nmat, S->R, S->C, S->L, lc, S->d_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
+      TeArgs<3, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, lc, S->d_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
       const size_t sm = te_smem_bytes<3, T>(S->nmat);
       if (fuse) k_te_apply<3, T, TE_PCG><<<grid, block, sm, S->stream>>>(a);
       else k_te_apply<3, T, TE_PLAIN><<<grid, block, sm, S->stream>>>(a);
@@ -305,7 +299,7 @@ static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, i
 
 // Pointwise PCG pass.
 template <typename T, int MODE>
-static bool launch_point(T* x, T* d, T* r, const T* q, T* s, const T* dold) {
+static bool launch_point(double* x, T* d, T* r, const T* q, T* s, const T* dold) {
   const SolveCfg cfg = solvecfg();
   if (S->analysis == CUDAPCG_FLUID_3D) {
     const int g = pw_grid(S->nV + S->nB);
@@ -316,10 +310,10 @@ static bool launch_point(T* x, T* d, T* r, const T* q, T* s, const T* dold) {
     const int g = pw_grid(S->N);
     if (!ensure_reduction(g)) return false;
     if (S->nd == 1) {
-      TePw<1, T> a{x, d, r, q, s, dold, S->d_keys, (const T*)S->d_K, S->nmat, S->N, S->d_sc, redctl(g), cfg};
+      TePw<1, T> a{x, d, r, q, s, dold, S->d_keys, Kdev<T>(), S->nmat, S->N, S->d_sc, redctl(g), cfg};
       k_te_point<1, T, MODE><<<g, PW_NT, 0, S->stream>>>(a);
     } else {
-      TePw<3, T> a{x, d, r, q, s, dold, S->d_keys, (const T*)S->d_K, S->nmat, S->N, S->d_sc, redctl(g), cfg};
+      TePw<3, T> a{x, d, r, q, s, dold, S->d_keys, Kdev<T>(), S->nmat, S->N, S->d_sc, redctl(g), cfg};
       k_te_point<3, T, MODE><<<g, PW_NT, 0, S->stream>>>(a);
     }
   }
@@ -340,14 +334,27 @@ static bool enqueue_pcg_iteration(int parity) {
   T* dold = (T*)(parity ? S->d1 : S->d0);
   T* dnew = (T*)(parity ? S->d0 : S->d1);
   if (!launch_apply<T>((const T*)S->s, dold, dnew, (T*)S->q, true, FIN_ALPHA, true)) return false;
-  return launch_point<T, PW_PCG>((T*)S->x, dnew, (T*)S->r, (const T*)S->q, (T*)S->s, nullptr);
+  return launch_point<T, PW_PCG>(S->x, dnew, (T*)S->r, (const T*)S->q, (T*)S->s, nullptr);
 }
 
+// r = b - A x with the operator applied in FP64 to the FP64 solution (initial guesses and
+// the mixed-mode residual replacement), rounded once into the working precision.
+template <typename T>
+__global__ void k_residual_replace(const double* b, const double* Ax, T* r, long n);
+template <typename T>
+static bool residual_from_x() {
+  if (!ensure_K<double>()) return false;
+  if (!launch_apply<double>(S->x, nullptr, nullptr, S->y64, false, FIN_NONE, true)) return false;
+  const long n = S->nvars;
+  k_residual_replace<T><<<pw_grid(n), PW_NT, 0, S->stream>>>(S->b64, S->y64, (T*)S->r, n);
+  S->launches++;
+  return cudaPeekAtLastError() == cudaSuccess;
+}
 // Mixed mode: true residual r = b - A x with FP64 accumulation of the subtraction.
 template <typename T>
-__global__ void k_residual_replace(const double* b, const T* Ax, T* r, long n) {
+__global__ void k_residual_replace(const double* b, const double* Ax, T* r, long n) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    r[i] = (T)(b[i] - (double)Ax[i]);
+    r[i] = (T)(b[i] - Ax[i]);
 }
 template <typename T>
 __global__ void k_skip_if_done_copy(const DevScalars* sc, int* flag) { if (threadIdx.x == 0 && blockIdx.x == 0) *flag = sc->done; }
@@ -394,11 +401,8 @@ static bool run_chunks(bool minres) {
     if (S->h_sc->done || S->h_sc->status >= 3) break;
     if (mixed && (unsigned)S->h_sc->iteration >= next_replace && !minres) {
       // residual replacement: r = b - A x, s = M^-1 r, delta = r.s (keeps d and beta)
-      if (!launch_apply<T>((const T*)S->x, nullptr, nullptr, (T*)S->q2, false, FIN_NONE, true)) return false;
-      const long n = S->nvars;
-      k_residual_replace<T><<<pw_grid(n), PW_NT, 0, S->stream>>>(S->b64, (const T*)S->q2, (T*)S->r, n);
-      S->launches++;
-      if (!launch_point<T, PW_REPL>((T*)S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
+      if (!residual_from_x<T>()) return false;
+      if (!launch_point<T, PW_REPL>(S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
       next_replace += S->replace_every;
     }
     CKV(cudaGraphLaunch(S->gexec, S->stream));
@@ -415,16 +419,16 @@ static bool solve_pcg_device() {
   CKV(cudaMemsetAsync(S->d_ticket, 0, sizeof(unsigned), S->stream));
   CKV(cudaMemsetAsync(S->d_sc, 0, sizeof(DevScalars), S->stream));
   const size_t n = (size_t)S->nvars;
-  if (!S->x0_set) CKV(cudaMemsetAsync(S->x, 0, n * sizeof(T), S->stream));
+  if (!S->x0_set) CKV(cudaMemsetAsync(S->x, 0, n * 8, S->stream));
   CKV(cudaMemsetAsync(S->q, 0, n * sizeof(T), S->stream));
   CKV(cudaMemsetAsync(S->d0, 0, n * sizeof(T), S->stream));
   CKV(cudaMemsetAsync(S->d1, 0, n * sizeof(T), S->stream));
   CKV(cudaEventRecord(S->ev0, S->stream));
   // zero-guess reference: s = M^-1 r, delta0 = r.s   (pcg.cu:61-81)
-  if (!launch_point<T, PW_INIT>((T*)S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
-  if (S->x0_set) {  // pcg.cu:83-99
-    if (!launch_apply<T>((const T*)S->x, nullptr, nullptr, (T*)S->q, false, FIN_NONE, true)) return false;
-    if (!launch_point<T, PW_X0>((T*)S->x, nullptr, (T*)S->r, (const T*)S->q, (T*)S->s, nullptr)) return false;
+  if (!launch_point<T, PW_INIT>(S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
+  if (S->x0_set) {  // pcg.cu:83-99: r = b - A x0 (FP64 apply), then the initial-guess test
+    if (!residual_from_x<T>()) return false;
+    if (!launch_point<T, PW_X0R>(S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
   }
   CKV(cudaEventRecord(S->ev1, S->stream));
   if (!run_chunks<T>(false)) return false;
@@ -459,13 +463,7 @@ static void collect_results(bool minres) {
 template <typename T>
 static bool copy_x_to_host(double* res_x) {
   const size_t n = (size_t)S->nvars;
-  if (sizeof(T) == 8) {
-    CKV(cudaMemcpyAsync(res_x, S->x, n * 8, cudaMemcpyDeviceToHost, S->stream));
-  } else {
-    k_convert<float, double><<<pw_grid(n), PW_NT, 0, S->stream>>>((const float*)S->x, S->x64, n);
-    S->launches++;
-    CKV(cudaMemcpyAsync(res_x, S->x64, n * 8, cudaMemcpyDeviceToHost, S->stream));
-  }
+  CKV(cudaMemcpyAsync(res_x, S->x, n * 8, cudaMemcpyDeviceToHost, S->stream));
   CKV(cudaStreamSynchronize(S->stream));
   return true;
 }
@@ -477,7 +475,7 @@ static bool solve_T(double* res_x) {
   bool ok = minres ? solve_minres_device<T>() : solve_pcg_device<T>();
   if (!ok) return false;
   collect_results(minres);
-  if (S->h_sc->status == 1 && minres) CKV(cudaMemsetAsync(S->x, 0, S->nvars * sizeof(T), S->stream));
+  if (S->h_sc->status == 1 && minres) CKV(cudaMemsetAsync(S->x, 0, S->nvars * 8, S->stream));
   return copy_x_to_host<T>(res_x);
 }
 
@@ -693,10 +691,10 @@ static bool interp_x0(const double* coarse_host) {
   const int rows = S->R, cols = S->C, lays = S->L, nd = (int)(S->nvars / S->N);
   const size_t ncoarse = (size_t)nd * (cols / 2) * (rows / 2) * (lays / 2 + (lays < 2));
   CKV(cudaMemcpyAsync(S->x64, coarse_host, ncoarse * 8, cudaMemcpyHostToDevice, S->stream));
-  CKV(cudaMemsetAsync(S->x, 0, S->nvars * sizeof(T), S->stream));
+  CKV(cudaMemsetAsync(S->x, 0, S->nvars * 8, S->stream));
   const int g = pw_grid(S->N);
-  k_project2<T><<<g, PW_NT, 0, S->stream>>>((T*)S->x, S->x64, rows, cols, lays, nd);
-  for (int p = 0; p < 3; p++) k_interp_pass<T><<<g, PW_NT, 0, S->stream>>>((T*)S->x, rows, cols, lays, nd, p);
+  k_project2<double><<<g, PW_NT, 0, S->stream>>>(S->x, S->x64, rows, cols, lays, nd);
+  for (int p = 0; p < 3; p++) k_interp_pass<double><<<g, PW_NT, 0, S->stream>>>(S->x, rows, cols, lays, nd, p);
   CKV(cudaStreamSynchronize(S->stream));
   return true;
 }
@@ -707,13 +705,13 @@ cudapcgFlag_t cudapcgSetX0(cudapcgVar_t* x0, cudapcgFlag_t mustInterpolate) {
   if (!x0) {  // cudapcg.cu:298-309
     if (!S->x0_set) return CUDAPCG_TRUE;
     S->x0_set = false;
-    if (S->x) CK(cudaMemset(S->x, 0, S->nvars * (S->vec_prec == CHFEM_B200_FP64 ? 8 : 4)));
+    if (S->x) CK(cudaMemset(S->x, 0, S->nvars * 8));
     return CUDAPCG_TRUE;
   }
   if (!ensure_vectors_current()) return CUDAPCG_FALSE;
   bool ok;
   if (mustInterpolate) ok = (S->vec_prec == CHFEM_B200_FP64) ? interp_x0<double>(x0) : interp_x0<float>(x0);
-  else { ok = upload_vec(x0, S->x); cudaStreamSynchronize(S->stream); }
+  else { ok = cudaMemcpy(S->x, x0, S->nvars * 8, cudaMemcpyHostToDevice) == cudaSuccess; }
   if (!ok) return CUDAPCG_FALSE;
   S->x0_set = true;
   return CUDAPCG_TRUE;
@@ -808,7 +806,7 @@ cudapcgFlag_t cudapcgSetLclMtxs(cudapcgVar_t* Lm) {
     S->Kd.assign(Lm, Lm + 1024);
   }
   S->have_K = true;
-  free_ptr(S->d_K); S->d_K = nullptr; S->K_prec = -1;
+  free_ptr(S->d_K64); free_ptr(S->d_K32); S->d_K64 = nullptr; S->d_K32 = nullptr;
   if (S->analysis == CUDAPCG_FLUID_3D && !set_fluid_diag()) return CUDAPCG_FALSE;
   return CUDAPCG_TRUE;
 }
@@ -890,7 +888,7 @@ static bool apply_host_T(const double* xh, double* yh, bool precond_only) {
     // s = M^-1 q2 via the INIT pass on a copy: r <- q2 temporarily
     CKV(cudaMemcpyAsync(S->q, S->r, n * sizeof(T), cudaMemcpyDeviceToDevice, S->stream));  // save r in q
     CKV(cudaMemcpyAsync(S->r, S->q2, n * sizeof(T), cudaMemcpyDeviceToDevice, S->stream));
-    if (!launch_point<T, PW_INIT>((T*)S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
+    if (!launch_point<T, PW_INIT>(S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
     CKV(cudaMemcpyAsync(S->r, S->q, n * sizeof(T), cudaMemcpyDeviceToDevice, S->stream));  // restore r
     CKV(cudaMemcpyAsync(S->q, S->s, n * sizeof(T), cudaMemcpyDeviceToDevice, S->stream));
   } else {
@@ -960,7 +958,7 @@ static double time_kernel_T(int which, unsigned reps) {
     switch (which) {
       case 0: ok = launch_apply<T>((const T*)S->s, nullptr, nullptr, (T*)S->q2, false, FIN_NONE, false); break;
       case 1: ok = launch_apply<T>((const T*)S->s, (const T*)S->d0, (T*)S->d1, (T*)S->q, true, FIN_ALPHA, false); break;
-      case 2: ok = launch_point<T, PW_PCG>((T*)S->x, (T*)S->d1, (T*)S->r, (const T*)S->q, (T*)S->s, nullptr); break;
+      case 2: ok = launch_point<T, PW_PCG>(S->x, (T*)S->d1, (T*)S->r, (const T*)S->q, (T*)S->s, nullptr); break;
       case 3: ok = launch_mr_op<T>((const T*)S->r, (T*)S->r2, FIN_MR_STEP, false); break;
       case 4: ok = launch_mr_dir<T>((const T*)S->r); break;
       default: ok = false;
@@ -986,7 +984,7 @@ unsigned long long cudapcgB200DeviceBytes(void) {
   if (!S) return 0;
   const size_t es = S->vec_prec == CHFEM_B200_FP64 ? 8 : 4;
   unsigned long long b = 0;
-  if (S->x) b += 8ull * S->nvars * es + 16ull * S->nvars;
+  if (S->x) b += 7ull * S->nvars * es + 32ull * S->nvars;
   if (S->analysis == CUDAPCG_FLUID_3D) b += 4ull * S->N + 4ull * (S->nV + S->nB) + S->nB;
   else b += 2ull * S->N;
   return b;

@@ -192,7 +192,8 @@ bool setup_solver(Model& m) {
   cudapcgB200SetPrecision(g_precision);
   bool ok;
   if (m.analysis != FLUID) {
-    ok = cudapcgSetImage(m.keys.data());
+    // femhmg.c:1000-1004: node keys for NBN, the per-voxel material map for EBE
+    ok = cudapcgSetImage(g_par == CUDAPCG_EBE ? m.elem_mat.data() : m.keys.data());
   } else {
     ok = cudapcgSetPeriodic2DOFMap(m.dof_of_node.data()) && cudapcgSetPoreMap(m.border_keys.data()) &&
          cudapcgSetDOF2PeriodicMap(m.node_of_dof.data());

@@ -11,7 +11,7 @@ static bool launch_mr_op(const T* rin, T* rout, int fin, bool skip_if_done) {
   cfg.tol = sc.tol; cfg.maxit = sc.maxit; cfg.norm = sc.norm; cfg.precond = sc.precond; cfg.nhmg = sc.nhmg;
   if (S->analysis == CUDAPCG_FLUID_3D) {
     FlArgs<T> a;
-    a.v = rin; a.vd = (const T*)S->q; a.vout = rout; a.y = (T*)S->s; a.x = (T*)S->x; a.d = (const T*)S->d0;
+    a.v = rin; a.vd = (const T*)S->q; a.vout = rout; a.y = (T*)S->s; a.x = S->x; a.d = (const T*)S->d0;
     a.dof_of_node = S->d_dof_of_node; a.node_of_dof = S->d_node_of_dof; a.bkeys = S->d_bkeys;
     a.R = S->R; a.C = S->C; a.L = S->L; a.nV = S->nV; a.nB = S->nB;
     a.sc = S->d_sc; a.finish = fin; a.skip_if_done = skip_if_done; a.cfg = cfg;
@@ -25,11 +25,11 @@ static bool launch_mr_op(const T* rin, T* rout, int fin, bool skip_if_done) {
     const int nb = grid.x * grid.y * grid.z;
     if (!ensure_reduction(nb)) return false;
     if (S->nd == 1) {
-      TeArgs<1, T> a{rin, (const T*)S->q, rout, (T*)S->s, (T*)S->x, (const T*)S->d0, S->d_keys, (const T*)S->d_K, S->nmat,
+      TeArgs<1, T> a{rin, (const T*)S->q, rout, (T*)S->s, S->x, (const T*)S->d0, S->d_keys, Kdev<T>(), S->nmat,
                      S->R, S->C, S->L, lc, S->d_sc, redctl(nb), fin, skip_if_done, cfg};
       k_te_apply<1, T, TE_MR><<<grid, block, te_smem_bytes<1, T>(S->nmat), S->stream>>>(a);
     } else {
-      TeArgs<3, T> a{rin, (const T*)S->q, rout, (T*)S->s, (T*)S->x, (const T*)S->d0, S->d_keys, (const T*)S->d_K, S->nmat,
+      TeArgs<3, T> a{rin, (const T*)S->q, rout, (T*)S->s, S->x, (const T*)S->d0, S->d_keys, Kdev<T>(), S->nmat,
                      S->R, S->C, S->L, lc, S->d_sc, redctl(nb), fin, skip_if_done, cfg};
       k_te_apply<3, T, TE_MR><<<grid, block, te_smem_bytes<3, T>(S->nmat), S->stream>>>(a);
     }
@@ -49,10 +49,10 @@ static bool launch_mr_dir(const T* rcur) {
     const int g = pw_grid(S->N);
     if (!ensure_reduction(g)) return false;
     if (S->nd == 1) {
-      MrDirTe<1, T> a{(T*)S->d0, (T*)S->q, rcur, (const T*)S->s, S->d_keys, (const T*)S->d_K, S->nmat, S->N, S->d_sc, redctl(g), S->precond};
+      MrDirTe<1, T> a{(T*)S->d0, (T*)S->q, rcur, (const T*)S->s, S->d_keys, Kdev<T>(), S->nmat, S->N, S->d_sc, redctl(g), S->precond};
       k_te_mr_dir<1, T><<<g, PW_NT, 0, S->stream>>>(a);
     } else {
-      MrDirTe<3, T> a{(T*)S->d0, (T*)S->q, rcur, (const T*)S->s, S->d_keys, (const T*)S->d_K, S->nmat, S->N, S->d_sc, redctl(g), S->precond};
+      MrDirTe<3, T> a{(T*)S->d0, (T*)S->q, rcur, (const T*)S->s, S->d_keys, Kdev<T>(), S->nmat, S->N, S->d_sc, redctl(g), S->precond};
       k_te_mr_dir<3, T><<<g, PW_NT, 0, S->stream>>>(a);
     }
   }
@@ -73,17 +73,15 @@ static bool solve_minres_device() {
   CKV(cudaMemsetAsync(S->d_ticket, 0, sizeof(unsigned), S->stream));
   CKV(cudaMemsetAsync(S->d_sc, 0, sizeof(DevScalars), S->stream));
   const size_t n = (size_t)S->nvars;
-  if (!S->x0_set) CKV(cudaMemsetAsync(S->x, 0, n * sizeof(T), S->stream));
+  if (!S->x0_set) CKV(cudaMemsetAsync(S->x, 0, n * 8, S->stream));
   CKV(cudaMemsetAsync(S->q, 0, n * sizeof(T), S->stream));
   CKV(cudaMemsetAsync(S->d0, 0, n * sizeof(T), S->stream));
   CKV(cudaEventRecord(S->ev0, S->stream));
   // zero-guess reference (pminres.cu:58-79): res0 = r.M^-1 r, s = A M^-1 r, delta0 = z.s.
   // alpha is 0 here, so r' = r and x is unchanged.
   if (!launch_mr_op<T>((const T*)S->r, (T*)S->r2, FIN_MR_INIT, false)) return false;
-  if (S->x0_set) {  // pminres.cu:81-98: r -= A x0, then the same evaluation
-    if (!launch_apply<T>((const T*)S->x, nullptr, nullptr, (T*)S->q2, false, FIN_NONE, true)) return false;
-    k_sub_inplace<T><<<pw_grid(n), PW_NT, 0, S->stream>>>((T*)S->r, (const T*)S->q2, (long)n);
-    S->launches++;
+  if (S->x0_set) {  // pminres.cu:81-98: r = b - A x0 (FP64 apply), then the same evaluation
+    if (!residual_from_x<T>()) return false;
     if (!launch_mr_op<T>((const T*)S->r, (T*)S->r2, FIN_MR_X0, true)) return false;
   }
   CKV(cudaEventRecord(S->ev1, S->stream));

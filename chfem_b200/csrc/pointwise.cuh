@@ -22,6 +22,7 @@ enum PwMode : int {
   PW_PCG = 2,      // x += a d; r -= a q; s = M^-1 r; delta = r.s; stopping test
   PW_DIR = 3,      // d_new = s + beta d_old (no reduction)
   PW_REPL = 4,     // after a residual replacement: s = M^-1 r; delta = r.s; beta = delta/delta_old
+  PW_X0R = 5,      // r already holds b - A x0 (FP64 apply): s = M^-1 r; delta = r.s; initial-guess test
 };
 
 enum ResNorm : int { NORM_L2 = 0, NORM_INF = 1, NORM_ERR = 2 };
@@ -49,7 +50,7 @@ __device__ inline void pcg_finish(int mode, const double* s, DevScalars* sc, con
     } else {
       sc->done = 0; sc->delta = s[0]; sc->delta_old = s[0]; sc->metric = 1.0; sc->status = 0;
     }
-  } else if (mode == PW_X0) {
+  } else if (mode == PW_X0 || mode == PW_X0R) {
     sc->delta = s[0];
     sc->delta_old = s[0];
     sc->beta = 0.0;
@@ -85,9 +86,11 @@ __device__ inline void pcg_finish(int mode, const double* s, DevScalars* sc, con
 
 // ---------------------------------------------------------------------------------------
 // Thermal / elastic: one thread per node, ND components per node.
+// x (the solution) is FP64 in every precision mode: it accumulates the periodic fluctuation
+// plus the macroscopic ramp, whose magnitude reaches the cell size.
 template <int ND, typename T>
 struct TePw {
-  T* x; T* d; T* r; const T* q; T* s; const T* dold;
+  double* x; T* d; T* r; const T* q; T* s; const T* dold;
   const uint16_t* keys;
   const T* Kd; int nmat;
   long N;
@@ -108,7 +111,8 @@ __global__ void __launch_bounds__(PW_NT) k_te_point(TePw<ND, T> a) {
     sD[i] = (m < a.nmat) ? a.Kd[(size_t)m * ED * ED + (size_t)k * ED + k] : T(1);
   }
   __syncthreads();
-  const T alpha = (MODE == PW_PCG) ? T(a.sc->alpha) : T(0);
+  const double alpha64 = (MODE == PW_PCG) ? a.sc->alpha : 0.0;
+  const T alpha = T(alpha64);
   const T beta = (MODE == PW_DIR) ? T(a.sc->beta) : T(0);
   double sum = 0.0, mr = 0.0, md = 0.0, mx = 0.0;
   for (long i = blockIdx.x * (long)PW_NT + tid; i < a.N; i += (long)gridDim.x * PW_NT) {
@@ -142,7 +146,7 @@ __global__ void __launch_bounds__(PW_NT) k_te_point(TePw<ND, T> a) {
       if (MODE == PW_X0) { rv -= a.q[j]; a.r[j] = rv; }
       if (MODE == PW_PCG) {
         const T dv = a.d[j];
-        const T xv = fma(alpha, dv, a.x[j]);
+        const double xv = fma(alpha64, (double)dv, a.x[j]);
         a.x[j] = xv;
         rv = fma(-alpha, a.q[j], rv);
         a.r[j] = rv;

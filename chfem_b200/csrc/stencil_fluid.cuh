@@ -27,7 +27,7 @@ struct FlArgs {
   const T* vd;         // PCG: d_old | MR: q
   T* vout;             // PCG: formed direction | MR: updated residual r'
   T* y;
-  T* x;                // MR: x += alpha d
+  double* x;           // MR: x += alpha d (FP64 in every precision mode)
   const T* d;          // MR
   const uint32_t* dof_of_node;   // periodic2DOF_map
   const uint32_t* node_of_dof;   // DOF2periodic_map
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(FL_NT) k_fl_apply(FlArgs<T> a) {
         const T rn = fma(-alpha, a.vd[j], a.v[j]);
         a.vout[j] = rn;
         const T dv = a.d[j];
-        const T xv = fma(alpha, dv, a.x[j]);
+        const double xv = fma((double)alpha, (double)dv, a.x[j]);
         a.x[j] = xv;
         acc_rz += (double)rn * (double)v;
         mr = fmax(mr, fabs((double)rn));
@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(FL_NT) k_fl_apply(FlArgs<T> a) {
 
 template <typename T>
 struct FlPw {
-  T* x; T* d; T* r; const T* q; T* s; const T* dold;
+  double* x; T* d; T* r; const T* q; T* s; const T* dold;
   const uint8_t* bkeys;
   long nV, nB;
   DevScalars* sc;
@@ -184,7 +184,8 @@ __global__ void __launch_bounds__(PW_NT) k_fl_point(FlPw<T> a) {
   __shared__ double sred[PW_NT / 32];
   if (MODE != PW_INIT && a.sc->done) return;
   const long nV = a.nV, nT = a.nV + a.nB;
-  const T alpha = (MODE == PW_PCG) ? T(a.sc->alpha) : T(0);
+  const double alpha64 = (MODE == PW_PCG) ? a.sc->alpha : 0.0;
+  const T alpha = T(alpha64);
   const T beta = (MODE == PW_DIR) ? T(a.sc->beta) : T(0);
   double sum = 0.0, mr = 0.0, md = 0.0, mx = 0.0;
   for (long t = blockIdx.x * (long)PW_NT + threadIdx.x; t < nT; t += (long)gridDim.x * PW_NT) {
@@ -207,7 +208,7 @@ __global__ void __launch_bounds__(PW_NT) k_fl_point(FlPw<T> a) {
       if (MODE == PW_X0) { rv -= a.q[j]; a.r[j] = rv; }
       if (MODE == PW_PCG) {
         const T dv = a.d[j];
-        const T xv = fma(alpha, dv, a.x[j]);
+        const double xv = fma(alpha64, (double)dv, a.x[j]);
         a.x[j] = xv;
         rv = fma(-alpha, a.q[j], rv);
         a.r[j] = rv;

@@ -45,7 +45,7 @@ struct TeArgs {
   const T* in1;        // d_old (PCG) | q (MR)
   T* vout;             // PCG: formed direction; MR: updated residual r'
   T* y;                // y = A v
-  T* x;                // MR: x += alpha d
+  double* x;           // MR: x += alpha d (FP64 in every precision mode)
   const T* d;          // MR
   const uint16_t* keys;
   const T* Kd;         // dense element matrices [nmat][8ND][8ND]
@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a) {
           const T rn = fma(-alpha, a.in1[j], a.in0[j]);
           a.vout[j] = rn;
           const T dv = a.d[j];
-          const T xv = fma(alpha, dv, a.x[j]);
+          const double xv = fma((double)alpha, (double)dv, a.x[j]);
           a.x[j] = xv;
           acc_rz += (double)rn * (double)v;
           mr = fmax(mr, fabs((double)rn));
