@@ -20,6 +20,7 @@
 #include "stencil_te.cuh"
 #include "pointwise.cuh"
 #include "stencil_fluid.cuh"
+#include "stencil_el.cuh"
 #include "minres.cuh"
 
 using namespace chfem;
@@ -261,6 +262,16 @@ static SolveCfg solvecfg() {
   return c;
 }
 
+// The FP64 elastic kernel stages more than the default 48 KB of dynamic shared memory.
+template <typename T, int MODE>
+static void el_prepare() {
+  static bool done = false;
+  if (!done) {
+    cudaFuncSetAttribute(k_el_apply<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)el_smem_bytes<T>());
+    done = true;
+  }
+}
+
 // y = A v (+ fused direction form and dot finisher).  in1/vout only with fuse.
 template <typename T>
 static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, int finish, bool skip_if_done) {
@@ -288,9 +299,9 @@ static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, i
       else k_te_apply<1, T, TE_PLAIN><<<grid, block, sm, S->stream>>>(a);
     } else {
       TeArgs<3, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, lc, S->d_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
-      const size_t sm = te_smem_bytes<3, T>(S->nmat);
-      if (fuse) k_te_apply<3, T, TE_PCG><<<grid, block, sm, S->stream>>>(a);
-      else k_te_apply<3, T, TE_PLAIN><<<grid, block, sm, S->stream>>>(a);
+      const size_t sm = el_smem_bytes<T>();
+      if (fuse) { el_prepare<T, TE_PCG>(); k_el_apply<T, TE_PCG><<<grid, block, sm, S->stream>>>(a); }
+      else { el_prepare<T, TE_PLAIN>(); k_el_apply<T, TE_PLAIN><<<grid, block, sm, S->stream>>>(a); }
     }
   }
   S->launches++;

@@ -31,7 +31,8 @@ static bool launch_mr_op(const T* rin, T* rout, int fin, bool skip_if_done) {
     } else {
       TeArgs<3, T> a{rin, (const T*)S->q, rout, (T*)S->s, S->x, (const T*)S->d0, S->d_keys, Kdev<T>(), S->nmat,
                      S->R, S->C, S->L, lc, S->d_sc, redctl(nb), fin, skip_if_done, cfg};
-      k_te_apply<3, T, TE_MR><<<grid, block, te_smem_bytes<3, T>(S->nmat), S->stream>>>(a);
+      el_prepare<T, TE_MR>();
+      k_el_apply<T, TE_MR><<<grid, block, el_smem_bytes<T>(), S->stream>>>(a);
     }
   }
   S->launches++;
