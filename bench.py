@@ -40,10 +40,16 @@ WORKLOADS = {
                                 props={0: (1.0, 0.30), 255: (10.0, 0.20)}, tol=1e-6, maxit=20000, precision="fp64"),
     "thermal64_spheres_fp64": dict(analysis=0, shape=(64, 64, 64), gen="spheres", vf=0.30, seed=1000,
                                    props={0: 1.0, 255: 10.0}, tol=1e-6, maxit=20000, precision="fp64"),
+    "elastic128_grf_mixed_block": dict(analysis=1, shape=(128, 128, 128), gen="grf", corr=6.0, fraction=0.40, seed=2000,
+                                       props={0: (1.0, 0.30), 255: (10.0, 0.20)}, tol=1e-6, maxit=20000,
+                                       precision="mixed", multirhs=True),
+    "thermal64_spheres_fp64_block": dict(analysis=0, shape=(64, 64, 64), gen="spheres", vf=0.30, seed=1000,
+                                         props={0: 1.0, 255: 10.0}, tol=1e-6, maxit=20000, precision="fp64",
+                                         multirhs=True),
     "stokes128_grf_mixed": dict(analysis=2, shape=(128, 128, 128), gen="pore", corr=8.0, porosity=0.35, seed=3000,
                                 props=None, tol=1e-6, maxit=100000, precision="mixed", solver=1),
 }
-DEFAULT = "elastic128_grf_mixed"
+DEFAULT = "elastic128_grf_mixed_block"
 
 
 def make_image(w, rank):
@@ -167,8 +173,23 @@ class Resident:
         self.c.cudapcgB200SetPrecision(1 if p == "mixed" else 0)
         assert self.c.cudapcgAllocateArrays()
 
-    def step(self):
+    def step(self, multirhs=False):
         from chfem_b200._native import CudapcgStats
+        if multirhs:  # every load case in one block solve
+            nr = len(self.rhs)
+            if not hasattr(self, "xs"):
+                self.xs = [np.zeros(self.ndof) for _ in range(nr)]
+            P = ctypes.c_void_p * nr
+            prhs = P(*[r.ctypes.data for r in self.rhs])
+            px = P(*[x.ctypes.data for x in self.xs])
+            its = (ctypes.c_uint * nr)()
+            res = (ctypes.c_double * nr)()
+            self.c.cudapcgB200SolveBlock(nr, prhs, None, px, its, res)
+            err = self.c.cudapcgB200LastError()
+            assert not err, err
+            st = CudapcgStats()
+            self.c.cudapcgB200GetStats(ctypes.byref(st))
+            return st.solve_seconds + st.setup_seconds, list(its), st.kernel_launches
         dev, its, launches = 0.0, [], 0
         for r in self.rhs:
             self.c.cudapcgSetRHS(r.ctypes.data_as(ctypes.c_void_p))
@@ -198,7 +219,8 @@ def e2e_step(img, nf, w):
     C = np.zeros(36)
     t0 = time.perf_counter()
     n = lib.chfemB200Run(flat.ctypes.data_as(ctypes.c_void_p), nf.encode(), 6, w.get("solver", 0), 1,
-                         1 if w["precision"] == "mixed" else 0, 0, C.ctypes.data_as(ctypes.c_void_p))
+                         1 if w["precision"] == "mixed" else 0, int(w.get("multirhs", False)),
+                         C.ctypes.data_as(ctypes.c_void_p))
     t = time.perf_counter() - t0
     assert n, lib.chfemB200LastError()
     st = _native.solve_stats()
@@ -276,6 +298,7 @@ def config_dict(args, w, n):
     return {"workload": args.workload, "shape_zyx": list(w["shape"]), "analysis": ["thermal", "elastic", "stokes"][w["analysis"]],
             "load_cases": 6 if w["analysis"] == 1 else 3, "tol": w["tol"], "precision": w["precision"],
             "solver": "PMINRES" if w.get("solver", 0) == 1 else "PCG", "preconditioner": "Jacobi",
+            "multirhs": bool(w.get("multirhs", False)),
             "l2": "working set > L2 (vectors of the elastic 128^3 case ~25-50 MB each)", "parallelism": f"samples x{n}"}
 
 
@@ -326,20 +349,21 @@ def main():
     model = Resident(nf, raw, w)
     # plain FP64 PCG time-to-tol for comparison (once, outside the timed region)
     fp64 = None
-    if w["precision"] == "mixed":
+    block = bool(w.get("multirhs", False))
+    if w["precision"] == "mixed" or block:
         model.set_precision("fp64")
         t64, its64, _ = model.step()
         fp64 = {"time_s": t64, "iterations": its64}
-        model.set_precision("mixed")
+        model.set_precision(w["precision"])
     for _ in range(args.warmup):
-        model.step()
+        model.step(block)
     clocks = Clocks()
     barrier()
     clocks.start()
     t0 = time.perf_counter()
     dev_total, its, launches = 0.0, None, 0
     for _ in range(args.steps):
-        d, its, l = model.step()
+        d, its, l = model.step(block)
         dev_total += d
         launches += l
     wall = time.perf_counter() - t0
@@ -357,12 +381,19 @@ def main():
         units = model.ndof
     else:
         nd = 3 if w["analysis"] == 1 else 1
-        kern_which, kname = 1, f"k_te_apply<{nd},{'float' if es == 4 else 'double'},TE_PCG> (operator + direction + dot)"
-        per_unit = 4 * nd * es + 2  # s, d_old in; d_new, q out (nd comps); 16-bit key
+        tn = 'float' if es == 4 else 'double'
+        if block:
+            nr = 6 if nd == 3 else 3
+            kern_which, kname = 5, f"k_blk_apply<{nd},{tn},{nr}> (block operator + directions + dots, {nr} load cases)"
+            per_unit = nr * 4 * nd * es + 2  # per load case s, d_old in; d_new, q out; one 16-bit key
+        else:
+            kern_which, kname = 1, f"k_te_apply<{nd},{tn},TE_PCG> (operator + direction + dot)"
+            per_unit = 4 * nd * es + 2  # s, d_old in; d_new, q out (nd comps); 16-bit key
         units = model.N
     kt = model.kernel_time(kern_which, reps=30)
     achieved = per_unit * units / kt / 1e9 if kt > 0 else None
-    flops = (1152 if w["analysis"] == 1 else 80) * units / kt / 1e12 if (kt > 0 and w["analysis"] != 2) else None
+    fl_unit = (1152 if w["analysis"] == 1 else 80) * ((6 if w["analysis"] == 1 else 3) if block else 1)
+    flops = fl_unit * units / kt / 1e12 if (kt > 0 and w["analysis"] != 2) else None
     traffic = None
     tr_path = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tr_path):
@@ -380,8 +411,14 @@ def main():
     e2e_times = []
     C = None
     st = None
+    breakdown = None
     for k in range(2):
         t, C, st = e2e_step(img, nf, w)
+        if not e2e_times or t < min(e2e_times):
+            ncs = max(1, st.n_cases)
+            breakdown = {"model_build_and_upload_s": t - st.total_seconds, "rhs_assembly_s": st.rhs_seconds,
+                         "solve_device_s": float(sum(st.solve_seconds[i] for i in range(ncs))),
+                         "tensor_update_s": st.update_seconds, "solver_call_total_s": st.total_seconds}
         e2e_times.append(t)
     e2e = allmax(min(e2e_times))
     ncase = 6 if w["analysis"] == 1 else 3
@@ -402,7 +439,8 @@ def main():
                 "tensor_diag": [float(C[i, i]) for i in range(C.shape[0])] if C is not None else None,
                 "roofline": roofline, "clocks": clk, "gpu_launches": int(launches),
                 "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                        "path": "chfemB200Run (compute_property's native entry): image in host memory -> tensor"},
+                        "path": "chfemB200Run (compute_property's native entry): image in host memory -> tensor",
+                        "breakdown": breakdown},
                 "cpu_baseline": cpu, "samples_per_s": world / step_s}
         print(json.dumps(line))
     if dist:

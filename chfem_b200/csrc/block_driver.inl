@@ -1,0 +1,291 @@
+// block_driver.inl -- block multi-RHS PCG/CG (thermal, elastic); included by cudapcg_b200.cu.
+// Per right-hand side the recurrence, stopping test, initial-guess handling and (mixed
+// precision) residual replacement and final true-residual check are those of the single
+// solve; the operator and vector passes run once for all right-hand sides.
+
+struct BlockState {
+  int nr = 0, prec = -1;
+  long n = 0;
+  void *r = nullptr, *s = nullptr, *d0 = nullptr, *d1 = nullptr, *q = nullptr;  // [nr][n], work precision
+  double *x = nullptr, *b64 = nullptr;                                          // [nr][n], FP64
+  DevScalars* sc = nullptr;   // [nr]
+  DevScalars* h_sc = nullptr; // pinned [nr]
+  cudaGraphExec_t gexec = nullptr;
+  int graph_key = -1;
+};
+static BlockState* B = nullptr;
+
+static void block_invalidate() {
+  if (B && B->gexec) { cudaGraphExecDestroy(B->gexec); B->gexec = nullptr; B->graph_key = -1; }
+}
+
+static void block_free() {
+  if (!B) return;
+  void* ps[] = {B->r, B->s, B->d0, B->d1, B->q, B->x, B->b64, B->sc};
+  for (void* p : ps) free_ptr(p);
+  if (B->h_sc) cudaFreeHost(B->h_sc);
+  if (B->gexec) cudaGraphExecDestroy(B->gexec);
+  delete B;
+  B = nullptr;
+}
+
+template <typename T>
+static bool block_alloc(int nr) {
+  const int p = prec_of<T>();
+  if (B && B->nr == nr && B->prec == p && B->n == S->nvars) return true;
+  block_free();
+  B = new BlockState();
+  B->nr = nr; B->prec = p; B->n = S->nvars;
+  const size_t tot = (size_t)nr * std::max<long>(S->nvars, 1);
+  void** vs[] = {&B->r, &B->s, &B->d0, &B->d1, &B->q};
+  for (void** v : vs) { CKV(cudaMalloc(v, tot * sizeof(T))); CKV(cudaMemset(*v, 0, tot * sizeof(T))); }
+  CKV(cudaMalloc(&B->x, tot * 8));
+  CKV(cudaMalloc(&B->b64, tot * 8));
+  CKV(cudaMalloc(&B->sc, nr * sizeof(DevScalars)));
+  CKV(cudaMallocHost(&B->h_sc, nr * sizeof(DevScalars)));
+  return true;
+}
+
+template <int ND, typename T, int NR>
+static bool blk_prepare() {
+  static bool done = false;
+  if (!done) {
+    CKV(cudaFuncSetAttribute(k_blk_apply<ND, T, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)blk_smem_bytes<ND, T, NR>()));
+    done = true;
+  }
+  return true;
+}
+
+template <int ND, typename T, int NR>
+static bool launch_blk_apply(int parity) {
+  const long n = S->nvars;
+  T* dold = (T*)(parity ? B->d1 : B->d0);
+  T* dnew = (T*)(parity ? B->d0 : B->d1);
+  const int lc = te_lchunk();
+  const dim3 grid = te_grid(lc), block(TE_TR, TE_TC);
+  const int nb = grid.x * grid.y * grid.z;
+  if (!ensure_reduction(nb) || !blk_prepare<ND, T, NR>()) return false;
+  BlkArgs<ND, T> a{(const T*)B->s, dold, dnew, (T*)B->q, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, lc, n, B->sc, redctl(nb)};
+  k_blk_apply<ND, T, NR><<<grid, block, blk_smem_bytes<ND, T, NR>(), S->stream>>>(a);
+  S->launches++;
+  return cudaPeekAtLastError() == cudaSuccess;
+}
+
+template <int ND, typename T, int NR>
+static bool launch_blk_point(int parity) {
+  const long n = S->nvars;
+  T* dnew = (T*)(parity ? B->d0 : B->d1);
+  const int g = pw_grid(S->N);
+  if (!ensure_reduction(g)) return false;
+  BlkPw<ND, T> p{B->x, dnew, (T*)B->r, (const T*)B->q, (T*)B->s, S->d_keys, Kdev<T>(), S->nmat, S->N, n, B->sc, redctl(g), solvecfg()};
+  k_blk_point<ND, T, NR><<<g, PW_NT, 0, S->stream>>>(p);
+  S->launches++;
+  return cudaPeekAtLastError() == cudaSuccess;
+}
+
+template <int ND, typename T, int NR>
+static bool enqueue_blk_iteration(int parity) {
+  return launch_blk_apply<ND, T, NR>(parity) && launch_blk_point<ND, T, NR>(parity);
+}
+
+// Device time of one block operator pass (which 5) or one block vector pass (which 6), for the
+// model's natural block size (3 thermal, 6 elastic); scalars reset before each launch.
+template <typename T>
+static double time_block_kernel_T(int which, unsigned reps) {
+  const int nr = S->nd == 3 ? 6 : 3;
+  if (!ensure_vectors<T>() || !ensure_K<T>() || !block_alloc<T>(nr)) return -1.0;
+  if (!ensure_reduction(needed_blocks())) return -1.0;
+  for (int k = 0; k < nr; k++) {
+    DevScalars& h = B->h_sc[k];
+    h = DevScalars{};
+    h.delta = 1.0; h.delta0 = 1.0; h.delta_old = 1.0; h.alpha = 1e-3; h.beta = 0.5; h.res0 = 1.0; h.metric = 1.0;
+  }
+  float total = 0.f;
+  for (unsigned i = 0; i < reps + 3; i++) {
+    cudaMemcpyAsync(B->sc, B->h_sc, nr * sizeof(DevScalars), cudaMemcpyHostToDevice, S->stream);
+    cudaEventRecord(S->ev0, S->stream);
+    bool ok;
+    if (S->nd == 1) ok = which == 5 ? launch_blk_apply<1, T, 3>(0) : launch_blk_point<1, T, 3>(0);
+    else ok = which == 5 ? launch_blk_apply<3, T, 6>(0) : launch_blk_point<3, T, 6>(0);
+    cudaEventRecord(S->ev1, S->stream);
+    if (!ok || cudaEventSynchronize(S->ev1) != cudaSuccess) return -1.0;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, S->ev0, S->ev1);
+    if (i >= 3) total += ms;
+  }
+  return total * 1e-3 / std::max(1u, reps);
+}
+
+template <int ND, typename T, int NR>
+static bool blk_build_graph(int chunk) {
+  const int key = (prec_of<T>() << 12) | (ND << 8) | (NR << 4) | (S->resnorm << 2) | S->precond | (chunk << 16);
+  if (B->gexec && B->graph_key == key) return true;
+  if (B->gexec) { cudaGraphExecDestroy(B->gexec); B->gexec = nullptr; }
+  cudaGraph_t g;
+  CKV(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
+  bool ok = true;
+  const unsigned long long l0 = S->launches;
+  for (int it = 0; it < chunk && ok; it++) ok = enqueue_blk_iteration<ND, T, NR>(it & 1);
+  S->launches = l0;
+  cudaError_t e = cudaStreamEndCapture(S->stream, &g);
+  if (!ok || e != cudaSuccess) { set_err("block graph capture", cudaGetErrorString(e)); return false; }
+  e = cudaGraphInstantiate(&B->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) { set_err("block graph instantiate", cudaGetErrorString(e)); return false; }
+  B->graph_key = key;
+  return true;
+}
+
+static bool blk_read() {
+  CKV(cudaMemcpyAsync(B->h_sc, B->sc, B->nr * sizeof(DevScalars), cudaMemcpyDeviceToHost, S->stream));
+  CKV(cudaStreamSynchronize(S->stream));
+  return true;
+}
+
+// Per-RHS helpers on slices (single-RHS kernels with the k-th scalar record).
+template <typename T>
+static T* slice(void* base, int k) { return (T*)base + (size_t)k * S->nvars; }
+
+template <int ND, typename T, int NR>
+static bool solve_block_device(const bool* has_x0) {
+  const long n = S->nvars;
+  const size_t tot = (size_t)NR * n;
+  if (!ensure_reduction(needed_blocks())) return false;
+  CKV(cudaMemsetAsync(S->d_ticket, 0, sizeof(unsigned), S->stream));
+  CKV(cudaMemsetAsync(B->sc, 0, NR * sizeof(DevScalars), S->stream));
+  CKV(cudaMemsetAsync(B->q, 0, tot * sizeof(T), S->stream));
+  CKV(cudaMemsetAsync(B->d0, 0, tot * sizeof(T), S->stream));
+  CKV(cudaMemsetAsync(B->d1, 0, tot * sizeof(T), S->stream));
+  CKV(cudaEventRecord(S->ev0, S->stream));
+  for (int k = 0; k < NR; k++) {
+    S->cur_sc = B->sc + k;
+    if (!launch_point<T, PW_INIT>(slice<double>(B->x, k), nullptr, slice<T>(B->r, k), nullptr, slice<T>(B->s, k), nullptr)) { S->cur_sc = S->d_sc; return false; }
+    if (has_x0[k]) {
+      if (!residual_from_x<T>(true, slice<double>(B->x, k), slice<double>(B->b64, k), slice<T>(B->r, k)) ||
+          !launch_point<T, PW_X0R>(slice<double>(B->x, k), nullptr, slice<T>(B->r, k), nullptr, slice<T>(B->s, k), nullptr)) { S->cur_sc = S->d_sc; return false; }
+    }
+  }
+  S->cur_sc = S->d_sc;
+  CKV(cudaEventRecord(S->ev1, S->stream));
+  const int chunk = std::max(2u, S->iters_per_launch & ~1u);
+  if (!blk_build_graph<ND, T, NR>(chunk)) return false;
+  const bool mixed = sizeof(T) == 4 && S->replace_every > 0;
+  unsigned next_replace[NR];
+  double repl_delta[NR];
+  int checks[NR];
+  bool verified[NR];
+  for (int k = 0; k < NR; k++) { next_replace[k] = S->replace_every; repl_delta[k] = -1.0; checks[k] = 0; verified[k] = false; }
+  const bool trace = getenv("CHFEM_B200_TRACE") != nullptr;
+  for (;;) {
+    if (!blk_read()) return false;
+    if (trace)
+      for (int k = 0; k < NR; k++)
+        fprintf(stderr, "[block] rhs %d it %d delta %.6e delta0 %.6e alpha %.6e beta %.6e done %d found %d status %d\n", k,
+                B->h_sc[k].iteration, B->h_sc[k].delta, B->h_sc[k].delta0, B->h_sc[k].alpha, B->h_sc[k].beta, B->h_sc[k].done,
+                B->h_sc[k].found, B->h_sc[k].status);
+    bool checked[NR];
+    bool launched_check = false;
+    for (int k = 0; k < NR; k++) {
+      checked[k] = false;
+      const DevScalars& h = B->h_sc[k];
+      if (h.done) {
+        // mixed precision: confirm an apparent convergence on the true residual b - A x
+        if (mixed && h.status == 0 && h.found && !verified[k] && checks[k] < 32) {
+          checks[k]++;
+          S->cur_sc = B->sc + k;
+          bool ok = residual_from_x<T>(false, slice<double>(B->x, k), slice<double>(B->b64, k), slice<T>(B->r, k)) &&
+                    launch_point<T, PW_CHECK>(slice<double>(B->x, k), nullptr, slice<T>(B->r, k), nullptr, slice<T>(B->s, k), nullptr);
+          S->cur_sc = S->d_sc;
+          if (!ok) return false;
+          checked[k] = true;
+          launched_check = true;
+          if (trace) fprintf(stderr, "[block] rhs %d true-residual check %d\n", k, checks[k]);
+        }
+        continue;
+      }
+      if (repl_delta[k] < 0) repl_delta[k] = fabs(h.delta0);
+      if (mixed && ((unsigned)h.iteration >= next_replace[k] || fabs(h.delta) < S->replace_drop * repl_delta[k])) {
+        S->cur_sc = B->sc + k;
+        bool ok = residual_from_x<T>(true, slice<double>(B->x, k), slice<double>(B->b64, k), slice<T>(B->r, k)) &&
+                  launch_point<T, PW_REPL>(slice<double>(B->x, k), nullptr, slice<T>(B->r, k), nullptr, slice<T>(B->s, k), nullptr);
+        S->cur_sc = S->d_sc;
+        if (!ok) return false;
+        next_replace[k] = (unsigned)h.iteration + S->replace_every;
+        repl_delta[k] = fabs(h.delta);
+        if (trace) fprintf(stderr, "[block] rhs %d residual replacement at %d\n", k, h.iteration);
+      }
+    }
+    if (launched_check) {
+      if (!blk_read()) return false;
+      for (int k = 0; k < NR; k++)
+        if (checked[k]) {
+          if (B->h_sc[k].done) verified[k] = true;
+          else { next_replace[k] = (unsigned)B->h_sc[k].iteration + S->replace_every; repl_delta[k] = fabs(B->h_sc[k].delta); }
+        }
+    }
+    bool any = false;
+    for (int k = 0; k < NR; k++) any = any || !B->h_sc[k].done;
+    if (!any) break;
+    CKV(cudaGraphLaunch(B->gexec, S->stream));
+    S->launches += (unsigned long long)chunk * 2;
+  }
+  CKV(cudaEventRecord(S->ev2, S->stream));
+  CKV(cudaEventSynchronize(S->ev2));
+  float ms1 = 0, ms2 = 0;
+  cudaEventElapsedTime(&ms1, S->ev0, S->ev1);
+  cudaEventElapsedTime(&ms2, S->ev1, S->ev2);
+  S->setup_dev_s = ms1 * 1e-3;
+  S->solve_dev_s = ms2 * 1e-3;
+  return true;
+}
+
+template <typename T>
+static bool solve_block_T(int nr, const double* const* rhs, const double* const* x0, double* const* x_out,
+                          unsigned* iters, double* resid) {
+  if (!ensure_vectors<T>() || !ensure_K<T>() || !block_alloc<T>(nr)) return false;
+  const long n = S->nvars;
+  bool has_x0[BLK_MAX] = {false};
+  for (int k = 0; k < nr; k++) {
+    CKV(cudaMemcpyAsync(slice<double>(B->b64, k), rhs[k], n * 8, cudaMemcpyHostToDevice, S->stream));
+    if (sizeof(T) == 8) CKV(cudaMemcpyAsync(slice<double>(B->r, k), rhs[k], n * 8, cudaMemcpyHostToDevice, S->stream));
+    else k_convert<double, float><<<pw_grid(n), PW_NT, 0, S->stream>>>(slice<double>(B->b64, k), slice<float>(B->r, k), n);
+    if (x0 && x0[k]) { CKV(cudaMemcpyAsync(slice<double>(B->x, k), x0[k], n * 8, cudaMemcpyHostToDevice, S->stream)); has_x0[k] = true; }
+    else CKV(cudaMemsetAsync(slice<double>(B->x, k), 0, n * 8, S->stream));
+  }
+  bool ok;
+  if (S->nd == 1 && nr == 3) ok = solve_block_device<1, T, 3>(has_x0);
+  else if (S->nd == 3 && nr == 6) ok = solve_block_device<3, T, 6>(has_x0);
+  else if (S->nd == 3 && nr == 3) ok = solve_block_device<3, T, 3>(has_x0);
+  else { set_err("cudapcgB200SolveBlock", "block sizes are 3 (thermal, elastic) and 6 (elastic)"); return false; }
+  if (!ok) return false;
+  for (int k = 0; k < nr; k++) {
+    CKV(cudaMemcpyAsync(x_out[k], slice<double>(B->x, k), n * 8, cudaMemcpyDeviceToHost, S->stream));
+  }
+  CKV(cudaStreamSynchronize(S->stream));
+  unsigned maxit = 0;
+  int found_all = 1;
+  for (int k = 0; k < nr; k++) {
+    const DevScalars& h = B->h_sc[k];
+    double res;
+    int found;
+    if (h.status == 1) { res = 0.0; found = 1; }
+    else if (h.status == 2) { res = h.metric; found = 1; }
+    else if (S->resnorm == CUDAPCG_L2_NORM) { res = sqrt(fabs(h.delta) / fabs(h.delta0)); found = !(fabs(h.delta) > S->tol * S->tol * fabs(h.delta0)); }
+    else { res = h.metric; found = res <= S->tol; }
+    if (iters) iters[k] = (unsigned)h.iteration;
+    if (resid) resid[k] = res;
+    // per right-hand side, the messages cudapcgSolve prints for a single solve
+    const char* name = S->precond ? "PCG" : "CG";
+    if (h.status == 1) printf("%s[%d] Null solution satisfied %s.\n", S->header.c_str(), k, name);
+    else if (h.status == 2) printf("%s[%d] Initial guess satisfied %s.\n", S->header.c_str(), k, name);
+    else if (!getenv("CHFEM_B200_QUIET")) {
+      if (S->resnorm != CUDAPCG_ERROR_NORM) printf("%s[%d] iteration: %d, residual: %.3e\n", S->header.c_str(), k, h.iteration, res);
+      else printf("%s[%d] iteration: %d, residual: %.3e, error: %.3e\n", S->header.c_str(), k, h.iteration, sqrt(fabs(h.delta) / fabs(h.delta0)), res);
+    }
+    maxit = std::max(maxit, (unsigned)h.iteration);
+    found_all = found_all && found;
+  }
+  S->iteration = maxit;
+  S->found = found_all;
+  return true;
+}

@@ -20,7 +20,7 @@
 #include "stencil_te.cuh"
 #include "pointwise.cuh"
 #include "stencil_fluid.cuh"
-#include "stencil_el.cuh"
+#include "stencil_block.cuh"
 #include "minres.cuh"
 
 using namespace chfem;
@@ -81,6 +81,9 @@ struct Solver {
   std::string header;
   int precision = CHFEM_B200_FP64;
   unsigned replace_every = 50;
+  // mixed precision: also replace once delta = r.M^-1 r has fallen by this factor since the last
+  // replacement, before the FP32 recursive residual drifts away from b - A x
+  double replace_drop = 1e-4;
   unsigned iters_per_launch = 16;
   // model
   cudapcgModel_t* model = nullptr;
@@ -109,6 +112,7 @@ struct Solver {
   // device scalars and reductions
   DevScalars* d_sc = nullptr;
   DevScalars* h_sc = nullptr;  // pinned
+  DevScalars* cur_sc = nullptr;  // record the launch helpers target (d_sc, or one of a block's)
   double* d_part = nullptr;
   unsigned* d_ticket = nullptr;
   int part_cap = 0;
@@ -139,6 +143,13 @@ static cudapcgFlag_t ctor_simple(cudapcgModel_t** ptr, const void* data) {
 template <typename T> static int prec_of() { return sizeof(T) == 8 ? CHFEM_B200_FP64 : CHFEM_B200_MIXED; }
 
 static void free_ptr(void* p) { if (p) cudaFree(p); }
+
+static void block_invalidate();
+static void block_free();
+static void invalidate_graphs() {
+  if (S && S->gexec) { cudaGraphExecDestroy(S->gexec); S->gexec = nullptr; S->graph_key = -1; }
+  block_invalidate();
+}
 
 static void free_work_vectors() {
   if (!S) return;
@@ -219,7 +230,7 @@ static bool ensure_reduction(int nblocks) {
   if (nblocks <= S->part_cap && S->d_part) return true;
   free_ptr(S->d_part);
   S->part_cap = std::max(nblocks, 4096);
-  CKV(cudaMalloc(&S->d_part, sizeof(double) * 8 * S->part_cap));
+  CKV(cudaMalloc(&S->d_part, sizeof(double) * 32 * S->part_cap));
   return true;
 }
 
@@ -262,16 +273,6 @@ static SolveCfg solvecfg() {
   return c;
 }
 
-// The FP64 elastic kernel stages more than the default 48 KB of dynamic shared memory.
-template <typename T, int MODE>
-static void el_prepare() {
-  static bool done = false;
-  if (!done) {
-    cudaFuncSetAttribute(k_el_apply<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)el_smem_bytes<T>());
-    done = true;
-  }
-}
-
 // y = A v (+ fused direction form and dot finisher).  in1/vout only with fuse.
 template <typename T>
 static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, int finish, bool skip_if_done) {
@@ -280,7 +281,7 @@ static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, i
     a.v = in0; a.vd = in1; a.vout = vout; a.y = y; a.x = nullptr; a.d = nullptr;
     a.dof_of_node = S->d_dof_of_node; a.node_of_dof = S->d_node_of_dof; a.bkeys = S->d_bkeys;
     a.R = S->R; a.C = S->C; a.L = S->L; a.nV = S->nV; a.nB = S->nB;
-    a.sc = S->d_sc; a.finish = finish; a.skip_if_done = skip_if_done;
+    a.sc = S->cur_sc; a.finish = finish; a.skip_if_done = skip_if_done;
     a.cfg = MrCfg{S->tol, 0, S->resnorm, S->precond, 0};
     const int g = pw_grid(S->nV + S->nB);
     if (!ensure_reduction(g)) return false;
@@ -293,15 +294,15 @@ static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, i
     const int nb = grid.x * grid.y * grid.z;
     if (!ensure_reduction(nb)) return false;
     if (S->nd == 1) {
-      TeArgs<1, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, lc, S->d_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
+      TeArgs<1, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, lc, S->cur_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
       const size_t sm = te_smem_bytes<1, T>(S->nmat);
       if (fuse) k_te_apply<1, T, TE_PCG><<<grid, block, sm, S->stream>>>(a);
       else k_te_apply<1, T, TE_PLAIN><<<grid, block, sm, S->stream>>>(a);
     } else {
-      TeArgs<3, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, lc, S->d_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
-      const size_t sm = el_smem_bytes<T>();
-      if (fuse) { el_prepare<T, TE_PCG>(); k_el_apply<T, TE_PCG><<<grid, block, sm, S->stream>>>(a); }
-      else { el_prepare<T, TE_PLAIN>(); k_el_apply<T, TE_PLAIN><<<grid, block, sm, S->stream>>>(a); }
+      TeArgs<3, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, lc, S->cur_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
+      const size_t sm = te_smem_bytes<3, T>(S->nmat);
+      if (fuse) k_te_apply<3, T, TE_PCG><<<grid, block, sm, S->stream>>>(a);
+      else k_te_apply<3, T, TE_PLAIN><<<grid, block, sm, S->stream>>>(a);
     }
   }
   S->launches++;
@@ -315,16 +316,16 @@ static bool launch_point(double* x, T* d, T* r, const T* q, T* s, const T* dold)
   if (S->analysis == CUDAPCG_FLUID_3D) {
     const int g = pw_grid(S->nV + S->nB);
     if (!ensure_reduction(g)) return false;
-    FlPw<T> a{x, d, r, q, s, dold, S->d_bkeys, S->nV, S->nB, S->d_sc, redctl(g), cfg};
+    FlPw<T> a{x, d, r, q, s, dold, S->d_bkeys, S->nV, S->nB, S->cur_sc, redctl(g), cfg};
     k_fl_point<T, MODE><<<g, PW_NT, 0, S->stream>>>(a);
   } else {
     const int g = pw_grid(S->N);
     if (!ensure_reduction(g)) return false;
     if (S->nd == 1) {
-      TePw<1, T> a{x, d, r, q, s, dold, S->d_keys, Kdev<T>(), S->nmat, S->N, S->d_sc, redctl(g), cfg};
+      TePw<1, T> a{x, d, r, q, s, dold, S->d_keys, Kdev<T>(), S->nmat, S->N, S->cur_sc, redctl(g), cfg};
       k_te_point<1, T, MODE><<<g, PW_NT, 0, S->stream>>>(a);
     } else {
-      TePw<3, T> a{x, d, r, q, s, dold, S->d_keys, Kdev<T>(), S->nmat, S->N, S->d_sc, redctl(g), cfg};
+      TePw<3, T> a{x, d, r, q, s, dold, S->d_keys, Kdev<T>(), S->nmat, S->N, S->cur_sc, redctl(g), cfg};
       k_te_point<3, T, MODE><<<g, PW_NT, 0, S->stream>>>(a);
     }
   }
@@ -334,6 +335,8 @@ static bool launch_point(double* x, T* d, T* r, const T* q, T* s, const T* dold)
 
 template <typename T>
 static bool enqueue_minres_iteration(int parity);
+template <typename T>
+static bool launch_mr_op(const T* rin, T* rout, int fin, bool skip_if_done);
 
 // ---------------------------------------------------------------------------------------
 // One PCG / CG iteration: pass 1 forms d_new = s + beta d_old on the fly, applies A and
@@ -353,11 +356,12 @@ static bool enqueue_pcg_iteration(int parity) {
 template <typename T>
 __global__ void k_residual_replace(const double* b, const double* Ax, T* r, long n);
 template <typename T>
-static bool residual_from_x() {
+static bool residual_from_x(bool skip_if_done = true, double* x = nullptr, const double* b = nullptr, T* r = nullptr) {
+  if (!x) { x = S->x; b = S->b64; r = (T*)S->r; }
   if (!ensure_K<double>()) return false;
-  if (!launch_apply<double>(S->x, nullptr, nullptr, S->y64, false, FIN_NONE, true)) return false;
+  if (!launch_apply<double>(x, nullptr, nullptr, S->y64, false, FIN_NONE, skip_if_done)) return false;
   const long n = S->nvars;
-  k_residual_replace<T><<<pw_grid(n), PW_NT, 0, S->stream>>>(S->b64, S->y64, (T*)S->r, n);
+  k_residual_replace<T><<<pw_grid(n), PW_NT, 0, S->stream>>>(b, S->y64, r, n);
   S->launches++;
   return cudaPeekAtLastError() == cudaSuccess;
 }
@@ -407,14 +411,47 @@ static bool run_chunks(bool minres) {
   if (!build_graph<T>(key, chunk, minres)) return false;
   const bool mixed = sizeof(T) == 4 && S->replace_every > 0;
   unsigned next_replace = S->replace_every;
+  // progress measure for the replacement trigger: delta = r.M^-1 r (CG), squared relative
+  // residual metric ((P)MINRES); its value at the last replacement
+  auto progress = [&]() { return minres ? S->h_sc->metric * S->h_sc->metric : fabs(S->h_sc->delta); };
+  double repl_ref = -1.0;
+  int checks = 0;
+  const bool trace = getenv("CHFEM_B200_TRACE") != nullptr;
+  // the (P)MINRES error-norm stop is a step-size test, with no residual to confirm
+  const bool can_check = !minres || S->resnorm != CUDAPCG_ERROR_NORM;
   for (;;) {
     if (!read_scalars()) return false;
-    if (S->h_sc->done || S->h_sc->status >= 3) break;
-    if (mixed && (unsigned)S->h_sc->iteration >= next_replace && !minres) {
-      // residual replacement: r = b - A x, s = M^-1 r, delta = r.s (keeps d and beta)
+    if (trace)
+      fprintf(stderr, "[single] it %d delta %.6e delta0 %.6e alpha %.6e beta %.6e metric %.6e done %d found %d status %d\n", S->h_sc->iteration,
+              S->h_sc->delta, S->h_sc->delta0, S->h_sc->alpha, S->h_sc->beta, S->h_sc->metric, S->h_sc->done, S->h_sc->found, S->h_sc->status);
+    if (S->h_sc->status >= 3) break;
+    if (S->h_sc->done) {
+      // Mixed precision: an apparent convergence is confirmed on the true residual b - A x
+      // (FP64 operator, FP64 x); if it does not hold, the iteration restarts from it.
+      if (mixed && can_check && S->h_sc->status == 0 && S->h_sc->found && checks < 32) {
+        checks++;
+        if (!residual_from_x<T>(false)) return false;
+        if (minres) { if (!launch_mr_op<T>((const T*)S->r, (T*)S->r2, FIN_MR_CHECK, false)) return false; }
+        else if (!launch_point<T, PW_CHECK>(S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
+        if (!read_scalars()) return false;
+        if (trace) fprintf(stderr, "[single] true-residual check %d: done %d metric %.6e\n", checks, S->h_sc->done, S->h_sc->metric);
+        if (S->h_sc->done) break;
+        next_replace = (unsigned)S->h_sc->iteration + S->replace_every;
+        repl_ref = progress();
+      } else {
+        break;
+      }
+    }
+    if (repl_ref < 0) repl_ref = minres ? 1.0 : fabs(S->h_sc->delta0);
+    if (mixed && ((unsigned)S->h_sc->iteration >= next_replace || progress() < S->replace_drop * repl_ref)) {
+      // residual replacement: r = b - A x, then the preconditioned residual and its scalars
+      // (keeps the direction unless the recursive residual had drifted, then restarts)
       if (!residual_from_x<T>()) return false;
-      if (!launch_point<T, PW_REPL>(S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
-      next_replace += S->replace_every;
+      if (minres) { if (!launch_mr_op<T>((const T*)S->r, (T*)S->r2, FIN_MR_REPL, true)) return false; }
+      else if (!launch_point<T, PW_REPL>(S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
+      next_replace = (unsigned)S->h_sc->iteration + S->replace_every;
+      repl_ref = progress();
+      if (trace) fprintf(stderr, "[single] residual replacement at %d\n", S->h_sc->iteration);
     }
     CKV(cudaGraphLaunch(S->gexec, S->stream));
     S->launches += (unsigned long long)chunk * 2;
@@ -454,6 +491,7 @@ static bool solve_pcg_device() {
 }
 
 #include "minres_driver.inl"
+#include "block_driver.inl"
 
 // ---------------------------------------------------------------------------------------
 // Results: residual / found semantics of pcg.cu:226-233 and pminres.cu:225-227.
@@ -498,6 +536,7 @@ const char* cudapcgB200LastError(void) { return g_err.c_str(); }
 
 cudapcgFlag_t cudapcgEnd(void) {
   if (!S) return CUDAPCG_FALSE;
+  block_free();
   free_vectors();
   free_model_dev();
   free_ptr(S->d_sc); free_ptr(S->d_part); free_ptr(S->d_ticket);
@@ -533,6 +572,7 @@ cudapcgFlag_t cudapcgInit(cudapcgFlag_t analysis_flag, cudapcgFlag_t parStrategy
   CK(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
   CK(cudaEventCreate(&S->ev0)); CK(cudaEventCreate(&S->ev1)); CK(cudaEventCreate(&S->ev2));
   CK(cudaMalloc(&S->d_sc, sizeof(DevScalars)));
+  S->cur_sc = S->d_sc;
   CK(cudaMallocHost(&S->h_sc, sizeof(DevScalars)));
   CK(cudaMalloc(&S->d_ticket, sizeof(unsigned)));
   CK(cudaMemset(S->d_ticket, 0, sizeof(unsigned)));
@@ -558,6 +598,7 @@ static cudapcgFlag_t adopt_model() {
   }
   free_vectors();
   free_model_dev();
+  block_free();
   S->R = (int)m->nrows; S->C = (int)m->ncols; S->L = (int)m->nlayers;
   S->N = (long)S->R * S->C * S->L;
   S->nvars = m->nvars; S->nV = m->nporenodes; S->nB = m->nbordernodes;
@@ -818,6 +859,7 @@ cudapcgFlag_t cudapcgSetLclMtxs(cudapcgVar_t* Lm) {
   }
   S->have_K = true;
   free_ptr(S->d_K64); free_ptr(S->d_K32); S->d_K64 = nullptr; S->d_K32 = nullptr;
+  invalidate_graphs();  // captured launches hold the old matrix pointers
   if (S->analysis == CUDAPCG_FLUID_3D && !set_fluid_diag()) return CUDAPCG_FALSE;
   return CUDAPCG_TRUE;
 }
@@ -985,6 +1027,10 @@ static double time_kernel_T(int which, unsigned reps) {
 extern "C" {
 double cudapcgB200TimeKernel(int which, unsigned int reps) {
   if (!S || !S->model) return -1.0;
+  if (which == 5 || which == 6) {
+    if (S->analysis == CUDAPCG_FLUID_3D) return -1.0;
+    return (S->precision == CHFEM_B200_FP64) ? time_block_kernel_T<double>(which, reps) : time_block_kernel_T<float>(which, reps);
+  }
   return (S->precision == CHFEM_B200_FP64) ? time_kernel_T<double>(which, reps) : time_kernel_T<float>(which, reps);
 }
 double cudapcgB200TimeOperator(unsigned int reps) {
@@ -1002,3 +1048,22 @@ unsigned long long cudapcgB200DeviceBytes(void) {
 }
 
 }  // extern "C"
+
+extern "C" cudapcgFlag_t cudapcgB200SolveBlock(unsigned int nrhs, const double* const* rhs, const double* const* x0,
+                                               double* const* x_out, unsigned int* iterations, double* residuals) {
+  if (!S || !S->model || !rhs || !x_out || nrhs < 1 || nrhs > BLK_MAX) { set_err("cudapcgB200SolveBlock", "bad arguments"); return CUDAPCG_FALSE; }
+  if (S->analysis == CUDAPCG_FLUID_3D || (S->solver_flag & 1)) {
+    set_err("cudapcgB200SolveBlock", "block solves are provided for thermal and elastic CG/PCG");
+    return CUDAPCG_FALSE;
+  }
+  for (unsigned k = 0; k < nrhs; k++) if (!rhs[k] || !x_out[k]) { set_err("cudapcgB200SolveBlock", "null buffer"); return CUDAPCG_FALSE; }
+  const auto t0 = std::chrono::steady_clock::now();
+  S->count++;
+  S->launches = 0;
+  bool ok = (S->precision == CHFEM_B200_FP64) ? solve_block_T<double>((int)nrhs, rhs, x0, x_out, iterations, residuals)
+                                             : solve_block_T<float>((int)nrhs, rhs, x0, x_out, iterations, residuals);
+  S->total_time = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  S->mean_time = S->iteration ? S->solve_dev_s / S->iteration : 0.0;
+  if (!ok) { S->found = 0; return CUDAPCG_FALSE; }
+  return (cudapcgFlag_t)S->found;
+}

@@ -294,7 +294,63 @@ void hmgSolveHomogenization(void) {
   std::vector<double> x(m.ndof, 0.0), x0;
   g_stats.n_cases = nd;
   g_stats.ndof = (unsigned)m.ndof;
-  for (int k = 0; k < nd; k++) {
+  // Block multi-RHS path: all load cases of the analysis advance together (one operator pass
+  // per iteration for all of them).  Same per-case recurrence, stopping test and results.
+  const bool block = g_multirhs && m.analysis != FLUID && !(g_solver & 1) &&
+                     ((m.analysis == THERMAL && nd == 3) || (m.analysis == ELASTIC && (nd == 6 || nd == 3)));
+  if (block) {
+    std::vector<std::vector<double>> rhs(nd, std::vector<double>(m.ndof)), xs(nd, std::vector<double>(m.ndof)), x0s(nd);
+    std::vector<const double*> prhs(nd), px0(nd, nullptr);
+    std::vector<double*> px(nd);
+    auto t = std::chrono::steady_clock::now();
+    for (int k = 0; k < nd; k++) {
+      assemble_rhs(m, dirs[k], rhs[k].data());
+      prhs[k] = rhs[k].data();
+      px[k] = xs[k].data();
+      if (g_use_x0 && !g_x0_file.empty()) {
+        const std::string fn = g_x0_file + "_" + std::to_string(dirs[k]) + ".bin";
+        FILE* f = fopen(fn.c_str(), "rb");
+        if (f) {
+          x0s[k].assign(m.ndof, 0.0);
+          if (fread(x0s[k].data(), sizeof(double), m.ndof, f) < (size_t)m.ndof) SAY("WARNING: Failed to read all %ld items from %s...", m.ndof, fn.c_str());
+          fclose(f);
+          px0[k] = x0s[k].data();
+        }
+      }
+    }
+    m.rhs = rhs[nd - 1];
+    g_stats.rhs_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
+    SAY("    ------------------------------------------------------\n    Block solve of %d load cases (", nd);
+    for (int k = 0; k < nd; k++) SAY("%s%s", k ? ", " : "", DIR_STR[dirs[k]]);
+    SAY(")...\n");
+    unsigned its[6] = {0};
+    double res[6] = {0};
+    if (!cudapcgB200SolveBlock((unsigned)nd, prhs.data(), px0.data(), px.data(), its, res) && cudapcgB200LastError()[0]) {
+      fail(std::string("block solve: ") + cudapcgB200LastError());
+      cudapcgEnd();
+      return;
+    }
+    cudapcgB200Stats st;
+    cudapcgB200GetStats(&st);
+    for (int k = 0; k < nd; k++) {
+      const int dir = dirs[k];
+      g_stats.direction[k] = dir;
+      g_stats.iterations[k] = its[k];
+      g_stats.residual[k] = res[k];
+      g_stats.solve_seconds[k] = (k == 0) ? st.solve_seconds + st.setup_seconds : 0.0;
+      if (g_export_x) {
+        const std::string fn = m.nf_noext + "_X_" + std::to_string(dir) + ".bin";
+        FILE* f = fopen(fn.c_str(), "wb");
+        if (f) { fwrite(xs[k].data(), sizeof(double), m.ndof, f); fclose(f); }
+      }
+      t = std::chrono::steady_clock::now();
+      update_C(m, dir, xs[k].data());
+      g_stats.update_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
+    }
+    g_stats.kernel_launches += st.kernel_launches;
+    if (!g_quiet) cudapcgPrintSolverMetrics();
+  }
+  for (int k = 0; k < nd && !block; k++) {
     const int dir = dirs[k];
     SAY("    ------------------------------------------------------\n    Analysis on %s:\n", DIR_STR[dir]);
     auto t = std::chrono::steady_clock::now();

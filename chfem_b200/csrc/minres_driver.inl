@@ -14,7 +14,7 @@ static bool launch_mr_op(const T* rin, T* rout, int fin, bool skip_if_done) {
     a.v = rin; a.vd = (const T*)S->q; a.vout = rout; a.y = (T*)S->s; a.x = S->x; a.d = (const T*)S->d0;
     a.dof_of_node = S->d_dof_of_node; a.node_of_dof = S->d_node_of_dof; a.bkeys = S->d_bkeys;
     a.R = S->R; a.C = S->C; a.L = S->L; a.nV = S->nV; a.nB = S->nB;
-    a.sc = S->d_sc; a.finish = fin; a.skip_if_done = skip_if_done; a.cfg = cfg;
+    a.sc = S->cur_sc; a.finish = fin; a.skip_if_done = skip_if_done; a.cfg = cfg;
     const int g = pw_grid(S->nV + S->nB);
     if (!ensure_reduction(g)) return false;
     a.rc = redctl(g);
@@ -26,13 +26,12 @@ static bool launch_mr_op(const T* rin, T* rout, int fin, bool skip_if_done) {
     if (!ensure_reduction(nb)) return false;
     if (S->nd == 1) {
       TeArgs<1, T> a{rin, (const T*)S->q, rout, (T*)S->s, S->x, (const T*)S->d0, S->d_keys, Kdev<T>(), S->nmat,
-                     S->R, S->C, S->L, lc, S->d_sc, redctl(nb), fin, skip_if_done, cfg};
+                     S->R, S->C, S->L, lc, S->cur_sc, redctl(nb), fin, skip_if_done, cfg};
       k_te_apply<1, T, TE_MR><<<grid, block, te_smem_bytes<1, T>(S->nmat), S->stream>>>(a);
     } else {
       TeArgs<3, T> a{rin, (const T*)S->q, rout, (T*)S->s, S->x, (const T*)S->d0, S->d_keys, Kdev<T>(), S->nmat,
-                     S->R, S->C, S->L, lc, S->d_sc, redctl(nb), fin, skip_if_done, cfg};
-      el_prepare<T, TE_MR>();
-      k_el_apply<T, TE_MR><<<grid, block, el_smem_bytes<T>(), S->stream>>>(a);
+                     S->R, S->C, S->L, lc, S->cur_sc, redctl(nb), fin, skip_if_done, cfg};
+      k_te_apply<3, T, TE_MR><<<grid, block, te_smem_bytes<3, T>(S->nmat), S->stream>>>(a);
     }
   }
   S->launches++;
@@ -44,16 +43,16 @@ static bool launch_mr_dir(const T* rcur) {
   if (S->analysis == CUDAPCG_FLUID_3D) {
     const int g = pw_grid(S->nV + S->nB);
     if (!ensure_reduction(g)) return false;
-    MrDirFl<T> a{(T*)S->d0, (T*)S->q, rcur, (const T*)S->s, S->d_bkeys, S->nV, S->nB, S->d_sc, redctl(g), S->precond};
+    MrDirFl<T> a{(T*)S->d0, (T*)S->q, rcur, (const T*)S->s, S->d_bkeys, S->nV, S->nB, S->cur_sc, redctl(g), S->precond};
     k_fl_mr_dir<T><<<g, PW_NT, 0, S->stream>>>(a);
   } else {
     const int g = pw_grid(S->N);
     if (!ensure_reduction(g)) return false;
     if (S->nd == 1) {
-      MrDirTe<1, T> a{(T*)S->d0, (T*)S->q, rcur, (const T*)S->s, S->d_keys, Kdev<T>(), S->nmat, S->N, S->d_sc, redctl(g), S->precond};
+      MrDirTe<1, T> a{(T*)S->d0, (T*)S->q, rcur, (const T*)S->s, S->d_keys, Kdev<T>(), S->nmat, S->N, S->cur_sc, redctl(g), S->precond};
       k_te_mr_dir<1, T><<<g, PW_NT, 0, S->stream>>>(a);
     } else {
-      MrDirTe<3, T> a{(T*)S->d0, (T*)S->q, rcur, (const T*)S->s, S->d_keys, Kdev<T>(), S->nmat, S->N, S->d_sc, redctl(g), S->precond};
+      MrDirTe<3, T> a{(T*)S->d0, (T*)S->q, rcur, (const T*)S->s, S->d_keys, Kdev<T>(), S->nmat, S->N, S->cur_sc, redctl(g), S->precond};
       k_te_mr_dir<3, T><<<g, PW_NT, 0, S->stream>>>(a);
     }
   }
@@ -72,7 +71,7 @@ template <typename T>
 static bool solve_minres_device() {
   if (!ensure_reduction(needed_blocks())) return false;
   CKV(cudaMemsetAsync(S->d_ticket, 0, sizeof(unsigned), S->stream));
-  CKV(cudaMemsetAsync(S->d_sc, 0, sizeof(DevScalars), S->stream));
+  CKV(cudaMemsetAsync(S->cur_sc, 0, sizeof(DevScalars), S->stream));
   const size_t n = (size_t)S->nvars;
   if (!S->x0_set) CKV(cudaMemsetAsync(S->x, 0, n * 8, S->stream));
   CKV(cudaMemsetAsync(S->q, 0, n * sizeof(T), S->stream));

@@ -23,6 +23,7 @@ enum PwMode : int {
   PW_DIR = 3,      // d_new = s + beta d_old (no reduction)
   PW_REPL = 4,     // after a residual replacement: s = M^-1 r; delta = r.s; beta = delta/delta_old
   PW_X0R = 5,      // r already holds b - A x0 (FP64 apply): s = M^-1 r; delta = r.s; initial-guess test
+  PW_CHECK = 6,    // r holds the true residual b - A x at an apparent convergence: confirm or restart
 };
 
 enum ResNorm : int { NORM_L2 = 0, NORM_INF = 1, NORM_ERR = 2 };
@@ -79,8 +80,21 @@ __device__ inline void pcg_finish(int mode, const double* s, DevScalars* sc, con
     sc->beta = sc->delta / sc->delta_old;
     if (!cont || sc->iteration >= cfg.maxit) sc->done = 1;
   } else if (mode == PW_REPL) {
+    // The true residual replaces the recursive one.  While the two agree the direction is kept
+    // (beta from the true delta); once they have drifted apart the old direction no longer
+    // fits the new residual and the iteration restarts from it (beta = 0).
+    const double rec = sc->delta;
     sc->delta = s[0];
-    sc->beta = sc->delta / sc->delta_old;
+    if (fabs(s[0]) > 4.0 * fabs(rec) || fabs(s[0]) < 0.25 * fabs(rec)) { sc->beta = 0.0; sc->delta_old = s[0]; }
+    else sc->beta = sc->delta / sc->delta_old;
+  } else if (mode == PW_CHECK) {
+    // Mixed precision: the recursive residual may have drifted below the tolerance while the
+    // true one has not.  Confirm on the true residual, or restart the direction (beta = 0).
+    sc->delta = s[0];
+    sc->metric = sqrt(fabs(s[0]) / fabs(sc->delta0));
+    if (!(fabs(s[0]) > tol2 * fabs(sc->delta0))) { sc->done = 1; sc->found = 1; }
+    else if (sc->iteration >= cfg.maxit) { sc->done = 1; sc->found = 0; }
+    else { sc->done = 0; sc->found = 0; sc->beta = 0.0; sc->delta_old = s[0]; }
   }
 }
 
@@ -104,7 +118,7 @@ __global__ void __launch_bounds__(PW_NT) k_te_point(TePw<ND, T> a) {
   constexpr int ED = 8 * ND;
   __shared__ double sred[PW_NT / 32];
   __shared__ T sD[4 * 8 * ND];
-  if (MODE != PW_INIT && a.sc->done) return;
+  if (MODE != PW_INIT && MODE != PW_CHECK && a.sc->done) return;
   const int tid = threadIdx.x;
   for (int i = tid; i < 4 * 8 * ND; i += PW_NT) {
     const int m = i / (8 * ND), k = i % (8 * ND);

@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(FL_NT) k_fl_apply(FlArgs<T> a) {
   const long nV = a.nV, nT = a.nV + a.nB;
   const int R = a.R, C = a.C, L = a.L;
   const T beta = (MODE == TE_PCG) ? T(a.sc->beta) : T(0);
-  const T alpha = (MODE == TE_MR) ? T(a.sc->alpha) : T(0);
+  const T alpha = (MODE == TE_MR && mr_steps(a.finish)) ? T(a.sc->alpha) : T(0);
   const bool pre = a.cfg.precond != 0;
   const T ivv0 = pre ? T(c_fldiag.pore[0]) : T(1), ivv1 = pre ? T(c_fldiag.pore[1]) : T(1), ivv2 = pre ? T(c_fldiag.pore[2]) : T(1);
   const T ivp = pre ? T(c_fldiag.pore[3]) : T(1);
@@ -182,7 +182,7 @@ struct FlPw {
 template <typename T, int MODE>
 __global__ void __launch_bounds__(PW_NT) k_fl_point(FlPw<T> a) {
   __shared__ double sred[PW_NT / 32];
-  if (MODE != PW_INIT && a.sc->done) return;
+  if (MODE != PW_INIT && MODE != PW_CHECK && a.sc->done) return;
   const long nV = a.nV, nT = a.nV + a.nB;
   const double alpha64 = (MODE == PW_PCG) ? a.sc->alpha : 0.0;
   const T alpha = T(alpha64);

@@ -29,7 +29,14 @@ constexpr int TE_PP = TE_PR * TE_PC;   // points per plane incl. halo
 
 enum TeMode : int { TE_PLAIN = 0, TE_PCG = 1, TE_MR = 2 };
 // Finishers run by the last CTA on the grid-reduced sums.
-enum TeFinish : int { FIN_NONE = 0, FIN_ALPHA = 1, FIN_STORE = 2, FIN_MR_INIT = 3, FIN_MR_X0 = 4, FIN_MR_STEP = 5 };
+enum TeFinish : int {
+  FIN_NONE = 0, FIN_ALPHA = 1, FIN_STORE = 2, FIN_MR_INIT = 3, FIN_MR_X0 = 4, FIN_MR_STEP = 5,
+  FIN_MR_REPL = 6,   // mixed precision: r holds b - A x (FP64 apply); pass with alpha = 0
+  FIN_MR_CHECK = 7   // mixed precision: same, at an apparent convergence: confirm or restart
+};
+// alpha of a (P)MINRES operator pass: the replacement and check passes evaluate the current
+// residual without a step
+__device__ __forceinline__ bool mr_steps(int fin) { return fin != FIN_MR_REPL && fin != FIN_MR_CHECK; }
 
 struct MrCfg {
   double tol;
@@ -125,6 +132,24 @@ __device__ inline void mr_finish(int fin, const double* s, DevScalars* sc, const
     sc->found = sc->metric <= cfg.tol;
     sc->beta = sc->delta / sc->delta_old;
     if (!cont || sc->iteration >= cfg.maxit) sc->done = 1;
+  } else if (fin == FIN_MR_REPL || fin == FIN_MR_CHECK) {
+    // The true residual replaces the recursive one (mixed precision).
+    double m;
+    bool cont;
+    if (cfg.norm == 1) { m = s[2] / sc->res0; cont = m > cfg.tol; }
+    else { m = sqrt(fabs(s[1]) / fabs(sc->res0)); cont = fabs(s[1]) > tol2 * fabs(sc->res0); }
+    const double m_rec = sc->metric;
+    sc->delta = s[0];
+    sc->metric = m;
+    if (fin == FIN_MR_REPL) {
+      // keep the direction while the two residuals agree, else restart from the true one
+      if (m > 2.0 * m_rec || m < 0.5 * m_rec) { sc->beta = 0.0; sc->delta_old = s[0]; }
+      else sc->beta = sc->delta / sc->delta_old;
+    } else {
+      if (!cont) { sc->done = 1; sc->found = 1; }
+      else if (sc->iteration >= cfg.maxit) { sc->done = 1; sc->found = 0; }
+      else { sc->done = 0; sc->found = 0; sc->beta = 0.0; sc->delta_old = s[0]; }
+    }
   }
 }
 
@@ -149,7 +174,7 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a) {
     __syncthreads();
   }
   const T beta = (MODE == TE_PCG) ? T(a.sc->beta) : T(0);
-  const T alpha = (MODE == TE_MR) ? T(a.sc->alpha) : T(0);
+  const T alpha = (MODE == TE_MR && mr_steps(a.finish)) ? T(a.sc->alpha) : T(0);
   const bool pre = a.cfg.precond != 0;
   const int R = a.R, C = a.C, L = a.L;
   const int r0 = blockIdx.x * TE_TR, c0 = blockIdx.y * TE_TC, l0 = blockIdx.z * a.lchunk;

@@ -134,6 +134,13 @@ cudapcgFlag_t cudapcgB200SetIterationsPerLaunch(unsigned int k);
 cudapcgFlag_t cudapcgB200ApplyOperator(const double *x, double *y);
 /* y = M^-1 x (Jacobi) on the current model. */
 cudapcgFlag_t cudapcgB200ApplyPreconditioner(const double *x, double *y);
+/* Block solve of nrhs load cases of the current model at once (3 for thermal, 3 or 6 for
+   elastic; CG/PCG): rhs[k], x_out[k] are host buffers of nvars doubles, x0 may be NULL or hold
+   NULL entries.  Each right-hand side runs the recurrence and stopping test of cudapcgSolve;
+   the operator reads the model once per block apply.  iterations/residuals (nrhs entries) may
+   be NULL.  Returns 1 when every right-hand side met the tolerance. */
+cudapcgFlag_t cudapcgB200SolveBlock(unsigned int nrhs, const double *const *rhs, const double *const *x0,
+                                    double *const *x_out, unsigned int *iterations, double *residuals);
 /* Statistics of the last solve. */
 typedef struct {
   unsigned int iterations;
@@ -151,7 +158,9 @@ double cudapcgB200TimeOperator(unsigned int reps);
 /* Mean device duration (s, CUDA events on the library's stream) of `reps` launches of one
    kernel of the iteration on the current model and its work vectors:
    which 0 plain operator apply, 1 PCG operator pass (direction formed on the fly + dot),
-   2 PCG pointwise update pass, 3 (P)MINRES operator pass, 4 (P)MINRES direction pass.
+   2 PCG pointwise update pass, 3 (P)MINRES operator pass, 4 (P)MINRES direction pass,
+   5 block PCG operator pass and 6 block PCG pointwise pass (thermal: 3 right-hand sides,
+   elastic: 6; see cudapcgB200SolveBlock).
    The solver scalars are reset first; results of the work vectors are meaningless after. */
 double cudapcgB200TimeKernel(int which, unsigned int reps);
 /* Number of bytes the library holds on the device for the current model and arrays. */

@@ -103,9 +103,18 @@ def test_small_models_fp64(tmp_path, name, analysis, spec, flags):
 @pytest.mark.parametrize("name,analysis,spec,flags", [s for s in SMALL if s[0] in ("th2_pcg", "el2_pcg", "fl_pminres")])
 def test_small_models_mixed(tmp_path, name, analysis, spec, flags):
     nf, raw = build_small(tmp_path, name, analysis, spec)
-    Cref, _ = H.run_exec(H.ORACLE_EXEC, nf, raw, *flags)
-    C, _ = H.run_exec(H.CHFEM_EXEC, nf, raw, *flags, "--precision", "mixed")
+    Cref, logref = H.run_exec(H.ORACLE_EXEC, nf, raw, *flags)
+    C, log = H.run_exec(H.CHFEM_EXEC, nf, raw, *flags, "--precision", "mixed")
     assert H.rel_to_max(C, Cref) < MIXED_TOL
+    assert_mixed_converges(log, logref)
+
+
+def assert_mixed_converges(log, logref):
+    """Mixed precision reaches the tolerance (no stall up to the iteration cap) in at most
+    twice the FP64 iteration count plus one restart cycle."""
+    its, its_ref = H.parse_iterations(log), H.parse_iterations(logref)
+    assert len(its) == len(its_ref)
+    assert all(a <= 2 * b + 50 for a, b in zip(its, its_ref)), (its, its_ref)
 
 
 def test_homogeneous_is_exact(tmp_path):
@@ -205,3 +214,46 @@ def test_operator_and_jacobi(tmp_path, name, analysis, spec, precision):
     tol = 1e-12 if precision == 0 else 1e-5
     assert H.rel_to_max(y, yref) < tol
     assert H.rel_to_max(z, zref) < tol
+
+
+# ---------------------------------------------------------------------------------------
+# Block multi-RHS solves (--multirhs): every load case advances in one pass, each with its
+# own PCG scalars and stopping test.  Same bars as the one-by-one solves; FP64 iteration
+# counts within +-1 of the oracle's (the FMA order of the block operator differs).
+BLOCK = [s for s in SMALL if s[0] in ("th2_pcg", "th4_cg", "th2_inf", "th2_err", "th2_ebe", "th_thin", "el2_pcg")] + [
+    ("el3_ebe_all", 1, ("img", (8, 8, 9), 3), ["-p", "1"]),
+    ("el2_nopre", 1, ("img", (7, 6, 9), 2), ["-j", "0"]),
+]
+
+
+@pytest.mark.parametrize("name,analysis,spec,flags", BLOCK)
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_block_multirhs(tmp_path, name, analysis, spec, flags, precision):
+    nf, raw = build_small(tmp_path, name, analysis, spec)
+    Cref, logref = H.run_exec(H.ORACLE_EXEC, nf, raw, *flags)
+    C, log = H.run_exec(H.CHFEM_EXEC, nf, raw, *flags, "--multirhs", "--precision", precision)
+    assert "Block solve" in log
+    assert H.rel_to_max(C, Cref) < (FP64_TOL if precision == "fp64" else MIXED_TOL)
+    if precision == "fp64":
+        its, its_ref = H.parse_iterations(log), H.parse_iterations(logref)
+        assert len(its) == len(its_ref)
+        assert all(abs(a - b) <= 1 for a, b in zip(its, its_ref)), (its, its_ref)
+    else:
+        assert_mixed_converges(log, logref)
+
+
+@pytest.mark.parametrize("key", ["thermal_all_pcg"])
+def test_block_multirhs_golden(tmp_path, key):
+    ref = oracle_columns()[key]
+    nf, raw, meta = H.golden_case_files(ref["case"], str(tmp_path))
+    C, log = H.run_exec(H.CHFEM_EXEC, nf, raw, *ref["flags"], "--multirhs")
+    assert "Block solve" in log
+    assert H.rel_to_max(C, np.array(ref["C"])) < FP64_TOL
+
+
+def test_block_multirhs_python_api():
+    from chfem_b200 import compute_property
+    img = H.small_image((10, 11, 12), 2, seed=3)
+    C1 = np.array(compute_property("elasticity", img, mat_props={0: (10.0, 0.25), 255: (100.0, 0.3)}, solver_tolerance=1e-8))
+    C2 = np.array(compute_property("elasticity", img, mat_props={0: (10.0, 0.25), 255: (100.0, 0.3)}, solver_tolerance=1e-8, multirhs=True))
+    assert H.rel_to_max(C2, C1) < FP64_TOL
