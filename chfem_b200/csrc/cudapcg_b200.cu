@@ -1067,3 +1067,80 @@ extern "C" cudapcgFlag_t cudapcgB200SolveBlock(unsigned int nrhs, const double* 
   if (!ok) { S->found = 0; return CUDAPCG_FALSE; }
   return (cudapcgFlag_t)S->found;
 }
+
+// =======================================================================================
+// Operator apply without allocation.
+//
+// Some callers cannot allocate device memory: an embedder whose device memory is owned by
+// its own allocator or pool (a framework that hands out every buffer itself and budgets the
+// GPU), or a caller that must not pay cudaMalloc's implicit device synchronisation inside
+// its loop.  For them, this entry point applies the thermal or elastic operator to a caller
+// buffer and returns the fused dot product v.Av, taking every input and output from the
+// caller and keeping its own scratch (reduction partials, arrival ticket, result record) in
+// the file-scope array below.  It calls no cudaMalloc, cudaFree or allocating routine.
+//
+// The array is a fixed 66 KB that every GPU which loads this library holds until the process
+// exits.  Its device address is looked up once per device with cudaGetSymbolAddress, on the
+// first call made on that device with it current; that first call should therefore come
+// before any stream capture.  All calls share the one array, so calls whose executions
+// overlap on the GPU race on it; each call clears the ticket and record it needs before its
+// kernel runs (the partials are fully written before they are read).
+constexpr int NOALLOC_MAX_BLOCKS = 8192;  // reduction partials: one double per CTA
+constexpr size_t NOALLOC_HEADER = 512;    // [0,256) ticket, [256,512) result record
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_HEADER + NOALLOC_MAX_BLOCKS * sizeof(double)];
+static_assert(sizeof(DevScalars) <= 256, "result record must fit its slot");
+static void* g_noalloc_addr[64] = {nullptr};
+
+__global__ void k_noalloc_store_dot(const DevScalars* sc, double* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *out = sc->red[0];
+}
+
+extern "C" int cudapcgB200ApplyOperatorNoAlloc(int analysis_flag, unsigned int nrows, unsigned int ncols, unsigned int nlayers,
+                                               unsigned int nmat, const uint16_t* keys, const double* Kdense, const double* v,
+                                               double* y, double* vAv, void* stream) {
+  const char* who = "cudapcgB200ApplyOperatorNoAlloc";
+  if (analysis_flag != CUDAPCG_THERMAL_3D && analysis_flag != CUDAPCG_ELASTIC_3D) { set_err(who, "analysis must be THERMAL_3D (1) or ELASTIC_3D (3)"); return 0; }
+  if (!nrows || !ncols || !nlayers) { set_err(who, "empty model"); return 0; }
+  if (nmat < 1 || nmat > 4) { set_err(who, "1 to 4 materials are supported with 16-bit keys"); return 0; }
+  if (!keys || !Kdense || !v || !y || !vAv) { set_err(who, "null device pointer"); return 0; }
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) { set_err(who, cudaGetErrorString(e)); return 0; }
+  if (dev < 0 || dev >= 64) { set_err(who, "device ordinal out of range"); return 0; }
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) { set_err(who, e != cudaSuccess ? cudaGetErrorString(e) : "no symbol address"); return 0; }
+    g_noalloc_addr[dev] = p;
+  }
+  unsigned char* base = (unsigned char*)g_noalloc_addr[dev];
+  // grid: as many layer chunks as the partials allow
+  const long R = nrows, C = ncols, L = nlayers;
+  const long tiles = ((R + TE_TR - 1) / TE_TR) * ((C + TE_TC - 1) / TE_TC);
+  if (tiles > NOALLOC_MAX_BLOCKS) {
+    set_err(who, "model too large: more than 8192 column tiles of 32x8 nodes (nrows x ncols above ~2M nodes)");
+    return 0;
+  }
+  long lc = std::max<long>(1, std::min<long>(16, (L * tiles + 4L * 148 - 1) / (4L * 148)));
+  while (tiles * ((L + lc - 1) / lc) > NOALLOC_MAX_BLOCKS) lc++;
+  const dim3 grid((unsigned)((R + TE_TR - 1) / TE_TR), (unsigned)((C + TE_TC - 1) / TE_TC), (unsigned)((L + lc - 1) / lc));
+  const int nb = grid.x * grid.y * grid.z;
+  cudaStream_t st = (cudaStream_t)stream;
+  e = cudaMemsetAsync(base, 0, NOALLOC_HEADER, st);
+  if (e != cudaSuccess) { set_err(who, cudaGetErrorString(e)); return 0; }
+  DevScalars* sc = (DevScalars*)(base + 256);
+  RedCtl rc{(double*)(base + NOALLOC_HEADER), (unsigned*)base, nb};
+  const dim3 block(TE_TR, TE_TC);
+  const MrCfg cfg{0.0, 0, 0, 1, 0};
+  if (analysis_flag == CUDAPCG_THERMAL_3D) {
+    TeArgs<1, double> a{v, nullptr, nullptr, y, nullptr, nullptr, keys, Kdense, (int)nmat, (int)R, (int)C, (int)L, (int)lc, sc, rc, FIN_STORE, 0, cfg};
+    k_te_apply<1, double, TE_PLAIN><<<grid, block, te_smem_bytes<1, double>((int)nmat), st>>>(a);
+  } else {
+    TeArgs<3, double> a{v, nullptr, nullptr, y, nullptr, nullptr, keys, Kdense, (int)nmat, (int)R, (int)C, (int)L, (int)lc, sc, rc, FIN_STORE, 0, cfg};
+    k_te_apply<3, double, TE_PLAIN><<<grid, block, te_smem_bytes<3, double>((int)nmat), st>>>(a);
+  }
+  k_noalloc_store_dot<<<1, 32, 0, st>>>(sc, vAv);
+  e = cudaPeekAtLastError();
+  if (e != cudaSuccess) { set_err(who, cudaGetErrorString(e)); return 0; }
+  return 1;
+}

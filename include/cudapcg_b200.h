@@ -163,6 +163,21 @@ double cudapcgB200TimeOperator(unsigned int reps);
    elastic: 6; see cudapcgB200SolveBlock).
    The solver scalars are reset first; results of the work vectors are meaningless after. */
 double cudapcgB200TimeKernel(int which, unsigned int reps);
+/* Operator apply that allocates nothing (no counterpart in the reference).  For callers that
+   cannot allocate device memory -- an embedder whose device memory belongs to its own
+   allocator or pool, or a loop that must not pay cudaMalloc's implicit synchronisation:
+   y = A v and *vAv = v.Av for a THERMAL_3D (1) or ELASTIC_3D (3) model, all FP64, every
+   pointer a caller-owned device buffer: keys (nrows*ncols*nlayers 16-bit node keys), Kdense
+   (nmat dense element matrices of (8*dof)^2 doubles, i.e. the SparseQ1 thermal rows expanded
+   to 8x8), v and y (nvars doubles), vAv (1 double).  Scratch lives in a fixed 66 KB
+   file-scope device array held by every GPU that loads the library until exit; its address
+   is looked up on the first call on each device (make that call before any stream capture).
+   Calls that overlap on the GPU share that array and race.  Models above 8192 column tiles of
+   32x8 nodes are rejected.  stream: a cudaStream_t (NULL for the default stream).
+   Returns 1, or 0 with cudapcgB200LastError() set. */
+int cudapcgB200ApplyOperatorNoAlloc(int analysis_flag, unsigned int nrows, unsigned int ncols, unsigned int nlayers,
+                                    unsigned int nmat, const uint16_t *keys, const double *Kdense, const double *v,
+                                    double *y, double *vAv, void *stream);
 /* Number of bytes the library holds on the device for the current model and arrays. */
 unsigned long long cudapcgB200DeviceBytes(void);
 
