@@ -184,7 +184,7 @@ class Resident:
             px = P(*[x.ctypes.data for x in self.xs])
             its = (ctypes.c_uint * nr)()
             res = (ctypes.c_double * nr)()
-            self.c.cudapcgB200SolveBlock(nr, prhs, None, px, its, res)
+            self.c.cudapcgB200SolveBlock(nr, prhs, None, 0, px, its, res)
             err = self.c.cudapcgB200LastError()
             assert not err, err
             st = CudapcgStats()
@@ -288,6 +288,23 @@ def reference_arm(args, w):
                                  "sample": "reference CUDA build (its only solver path) on the same B200, full workload"},
                 "e2e": {"value": float(np.mean(walls)), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
+
+
+def profiled_traffic(workload):
+    """DRAM bytes (read + write) per launch of the dominant kernel, from the ncu summaries in
+    profiles/ (lines "dram_bytes_per_launch: <workload> <bytes>"); None when not captured."""
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    for fn in sorted(os.listdir(pdir)):
+        if not fn.endswith(".md"):
+            continue
+        with open(os.path.join(pdir, fn)) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) == 3 and parts[0] == "dram_bytes_per_launch:" and parts[1] == workload:
+                    return int(parts[2])
+    return None
 
 
 def metric_name(w):
@@ -394,12 +411,7 @@ def main():
     achieved = per_unit * units / kt / 1e9 if kt > 0 else None
     fl_unit = (1152 if w["analysis"] == 1 else 80) * ((6 if w["analysis"] == 1 else 3) if block else 1)
     flops = fl_unit * units / kt / 1e12 if (kt > 0 and w["analysis"] != 2) else None
-    traffic = None
-    tr_path = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tr_path):
-        with open(tr_path) as f:
-            tr = json.load(f)
-        traffic = tr.get(args.workload, {}).get("dram_bytes_per_launch")
+    traffic = profiled_traffic(args.workload)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                 "kernel": kname, "kernel_ms": kt * 1e3, "bytes_per_unit": per_unit, "units_per_launch": units,

@@ -239,8 +239,148 @@ static bool solve_block_device(const bool* has_x0) {
   return true;
 }
 
+// ---------------------------------------------------------------------------------------
+// Block (P)MINRES for the Stokes flow directions.  Buffers: r and r' alternate between
+// B->r and B->d1, the direction is B->d0, q = A d is B->q, s = A M^-1 r is B->s.
+template <typename T, int NR>
+static bool launch_fl_blk_dir(int parity) {
+  const T* rcur = (const T*)(parity ? B->d1 : B->r);
+  const int g = pw_grid(S->nV + S->nB);
+  if (!ensure_reduction(g)) return false;
+  FlBlkDir<T> a{(T*)B->d0, (T*)B->q, rcur, (const T*)B->s, S->d_bkeys, S->nV, S->nB, S->nvars, B->sc, redctl(g), S->precond};
+  k_fl_blk_dir<T, NR><<<g, PW_NT, 0, S->stream>>>(a);
+  S->launches++;
+  return cudaPeekAtLastError() == cudaSuccess;
+}
+template <typename T, int NR>
+static bool launch_fl_blk_apply(int parity) {
+  const T* rcur = (const T*)(parity ? B->d1 : B->r);
+  T* rnext = (T*)(parity ? B->r : B->d1);
+  const int g = pw_grid(S->nV + S->nB);
+  if (!ensure_reduction(g)) return false;
+  FlBlkArgs<T> a{rcur, (const T*)B->q, rnext, (T*)B->s, B->x, (const T*)B->d0, S->d_dof_of_node, S->d_node_of_dof, S->d_bkeys,
+                 S->R, S->C, S->L, S->nV, S->nB, S->nvars, B->sc, redctl(g), mrcfg()};
+  k_fl_blk_apply<T, NR><<<g, FL_NT, 0, S->stream>>>(a);
+  S->launches++;
+  return cudaPeekAtLastError() == cudaSuccess;
+}
+
+template <typename T, int NR>
+static bool blk_build_graph_mr(int chunk) {
+  const int key = (prec_of<T>() << 12) | (NR << 4) | (S->resnorm << 2) | S->precond | (chunk << 16) | (1 << 30);
+  if (B->gexec && B->graph_key == key) return true;
+  if (B->gexec) { cudaGraphExecDestroy(B->gexec); B->gexec = nullptr; }
+  cudaGraph_t g;
+  CKV(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
+  bool ok = true;
+  const unsigned long long l0 = S->launches;
+  for (int it = 0; it < chunk && ok; it++) ok = launch_fl_blk_dir<T, NR>(it & 1) && launch_fl_blk_apply<T, NR>(it & 1);
+  S->launches = l0;
+  cudaError_t e = cudaStreamEndCapture(S->stream, &g);
+  if (!ok || e != cudaSuccess) { set_err("block graph capture", cudaGetErrorString(e)); return false; }
+  e = cudaGraphInstantiate(&B->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) { set_err("block graph instantiate", cudaGetErrorString(e)); return false; }
+  B->graph_key = key;
+  return true;
+}
+
+template <typename T, int NR>
+static bool solve_block_minres_device(const bool* has_x0) {
+  const long n = S->nvars;
+  const size_t tot = (size_t)NR * n;
+  if (!ensure_reduction(needed_blocks())) return false;
+  CKV(cudaMemsetAsync(S->d_ticket, 0, sizeof(unsigned), S->stream));
+  CKV(cudaMemsetAsync(B->sc, 0, NR * sizeof(DevScalars), S->stream));
+  CKV(cudaMemsetAsync(B->q, 0, tot * sizeof(T), S->stream));
+  CKV(cudaMemsetAsync(B->d0, 0, tot * sizeof(T), S->stream));
+  CKV(cudaEventRecord(S->ev0, S->stream));
+  auto op_k = [&](int k, int fin, bool skip) {
+    return launch_mr_op_buf<T>(slice<T>(B->r, k), slice<T>(B->d1, k), slice<T>(B->q, k), slice<T>(B->s, k),
+                               slice<double>(B->x, k), slice<T>(B->d0, k), fin, skip);
+  };
+  for (int k = 0; k < NR; k++) {  // pminres.cu:58-98 per right-hand side
+    S->cur_sc = B->sc + k;
+    bool ok = op_k(k, FIN_MR_INIT, false);
+    if (ok && has_x0[k])
+      ok = residual_from_x<T>(true, slice<double>(B->x, k), slice<double>(B->b64, k), slice<T>(B->r, k)) && op_k(k, FIN_MR_X0, true);
+    S->cur_sc = S->d_sc;
+    if (!ok) return false;
+  }
+  CKV(cudaEventRecord(S->ev1, S->stream));
+  const int chunk = std::max(2u, S->iters_per_launch & ~1u);
+  if (!blk_build_graph_mr<T, NR>(chunk)) return false;
+  const bool mixed = sizeof(T) == 4 && S->replace_every > 0;
+  const bool can_check = S->resnorm != CUDAPCG_ERROR_NORM;
+  const bool trace = getenv("CHFEM_B200_TRACE") != nullptr;
+  unsigned next_replace[NR];
+  double repl_ref[NR];
+  int checks[NR];
+  bool verified[NR];
+  for (int k = 0; k < NR; k++) { next_replace[k] = S->replace_every; repl_ref[k] = 1.0; checks[k] = 0; verified[k] = false; }
+  for (;;) {
+    if (!blk_read()) return false;
+    if (trace)
+      for (int k = 0; k < NR; k++)
+        fprintf(stderr, "[block-mr] rhs %d it %d metric %.6e delta %.6e alpha %.6e beta %.6e done %d found %d status %d\n", k,
+                B->h_sc[k].iteration, B->h_sc[k].metric, B->h_sc[k].delta, B->h_sc[k].alpha, B->h_sc[k].beta, B->h_sc[k].done,
+                B->h_sc[k].found, B->h_sc[k].status);
+    bool checked[NR];
+    bool launched_check = false;
+    for (int k = 0; k < NR; k++) {
+      checked[k] = false;
+      const DevScalars& h = B->h_sc[k];
+      if (h.done) {
+        if (mixed && can_check && h.status == 0 && h.found && !verified[k] && checks[k] < 32) {
+          checks[k]++;
+          S->cur_sc = B->sc + k;
+          bool ok = residual_from_x<T>(false, slice<double>(B->x, k), slice<double>(B->b64, k), slice<T>(B->r, k)) &&
+                    op_k(k, FIN_MR_CHECK, false);
+          S->cur_sc = S->d_sc;
+          if (!ok) return false;
+          checked[k] = true;
+          launched_check = true;
+        }
+        continue;
+      }
+      const double prog = h.metric * h.metric;
+      if (mixed && ((unsigned)h.iteration >= next_replace[k] || prog < S->replace_drop * repl_ref[k])) {
+        S->cur_sc = B->sc + k;
+        bool ok = residual_from_x<T>(true, slice<double>(B->x, k), slice<double>(B->b64, k), slice<T>(B->r, k)) &&
+                  op_k(k, FIN_MR_REPL, true);
+        S->cur_sc = S->d_sc;
+        if (!ok) return false;
+        next_replace[k] = (unsigned)h.iteration + S->replace_every;
+        repl_ref[k] = prog;
+        if (trace) fprintf(stderr, "[block-mr] rhs %d residual replacement at %d\n", k, h.iteration);
+      }
+    }
+    if (launched_check) {
+      if (!blk_read()) return false;
+      for (int k = 0; k < NR; k++)
+        if (checked[k]) {
+          if (B->h_sc[k].done) verified[k] = true;
+          else { next_replace[k] = (unsigned)B->h_sc[k].iteration + S->replace_every; repl_ref[k] = B->h_sc[k].metric * B->h_sc[k].metric; }
+        }
+    }
+    bool any = false;
+    for (int k = 0; k < NR; k++) any = any || !B->h_sc[k].done;
+    if (!any) break;
+    CKV(cudaGraphLaunch(B->gexec, S->stream));
+    S->launches += (unsigned long long)chunk * 2;
+  }
+  CKV(cudaEventRecord(S->ev2, S->stream));
+  CKV(cudaEventSynchronize(S->ev2));
+  float ms1 = 0, ms2 = 0;
+  cudaEventElapsedTime(&ms1, S->ev0, S->ev1);
+  cudaEventElapsedTime(&ms2, S->ev1, S->ev2);
+  S->setup_dev_s = ms1 * 1e-3;
+  S->solve_dev_s = ms2 * 1e-3;
+  return true;
+}
+
 template <typename T>
-static bool solve_block_T(int nr, const double* const* rhs, const double* const* x0, double* const* x_out,
+static bool solve_block_T(int nr, const double* const* rhs, const double* const* x0, bool x0_interp, double* const* x_out,
                           unsigned* iters, double* resid) {
   if (!ensure_vectors<T>() || !ensure_K<T>() || !block_alloc<T>(nr)) return false;
   const long n = S->nvars;
@@ -249,16 +389,26 @@ static bool solve_block_T(int nr, const double* const* rhs, const double* const*
     CKV(cudaMemcpyAsync(slice<double>(B->b64, k), rhs[k], n * 8, cudaMemcpyHostToDevice, S->stream));
     if (sizeof(T) == 8) CKV(cudaMemcpyAsync(slice<double>(B->r, k), rhs[k], n * 8, cudaMemcpyHostToDevice, S->stream));
     else k_convert<double, float><<<pw_grid(n), PW_NT, 0, S->stream>>>(slice<double>(B->b64, k), slice<float>(B->r, k), n);
-    if (x0 && x0[k]) { CKV(cudaMemcpyAsync(slice<double>(B->x, k), x0[k], n * 8, cudaMemcpyHostToDevice, S->stream)); has_x0[k] = true; }
+    if (x0 && x0[k]) {
+      if (x0_interp) { if (!interp_into(x0[k], slice<double>(B->x, k))) return false; }
+      else CKV(cudaMemcpyAsync(slice<double>(B->x, k), x0[k], n * 8, cudaMemcpyHostToDevice, S->stream));
+      has_x0[k] = true;
+    }
     else CKV(cudaMemsetAsync(slice<double>(B->x, k), 0, n * 8, S->stream));
   }
   bool ok;
-  if (S->nd == 1 && nr == 3) ok = solve_block_device<1, T, 3>(has_x0);
+  if (S->analysis == CUDAPCG_FLUID_3D) {
+    if (nr != 3) { set_err("cudapcgB200SolveBlock", "Stokes blocks hold the 3 flow directions"); return false; }
+    ok = solve_block_minres_device<T, 3>(has_x0);
+  } else if (S->nd == 1 && nr == 3) ok = solve_block_device<1, T, 3>(has_x0);
   else if (S->nd == 3 && nr == 6) ok = solve_block_device<3, T, 6>(has_x0);
   else if (S->nd == 3 && nr == 3) ok = solve_block_device<3, T, 3>(has_x0);
   else { set_err("cudapcgB200SolveBlock", "block sizes are 3 (thermal, elastic) and 6 (elastic)"); return false; }
   if (!ok) return false;
+  if (!blk_read()) return false;
   for (int k = 0; k < nr; k++) {
+    // a null right-hand side under (P)MINRES returns x = 0 as cudapcgSolve does
+    if (S->analysis == CUDAPCG_FLUID_3D && B->h_sc[k].status == 1) CKV(cudaMemsetAsync(slice<double>(B->x, k), 0, n * 8, S->stream));
     CKV(cudaMemcpyAsync(x_out[k], slice<double>(B->x, k), n * 8, cudaMemcpyDeviceToHost, S->stream));
   }
   CKV(cudaStreamSynchronize(S->stream));
@@ -270,12 +420,12 @@ static bool solve_block_T(int nr, const double* const* rhs, const double* const*
     int found;
     if (h.status == 1) { res = 0.0; found = 1; }
     else if (h.status == 2) { res = h.metric; found = 1; }
-    else if (S->resnorm == CUDAPCG_L2_NORM) { res = sqrt(fabs(h.delta) / fabs(h.delta0)); found = !(fabs(h.delta) > S->tol * S->tol * fabs(h.delta0)); }
+    else if (S->resnorm == CUDAPCG_L2_NORM && S->analysis != CUDAPCG_FLUID_3D) { res = sqrt(fabs(h.delta) / fabs(h.delta0)); found = !(fabs(h.delta) > S->tol * S->tol * fabs(h.delta0)); }
     else { res = h.metric; found = res <= S->tol; }
     if (iters) iters[k] = (unsigned)h.iteration;
     if (resid) resid[k] = res;
     // per right-hand side, the messages cudapcgSolve prints for a single solve
-    const char* name = S->precond ? "PCG" : "CG";
+    const char* name = S->analysis == CUDAPCG_FLUID_3D ? "MINRES" : (S->precond ? "PCG" : "CG");
     if (h.status == 1) printf("%s[%d] Null solution satisfied %s.\n", S->header.c_str(), k, name);
     else if (h.status == 2) printf("%s[%d] Initial guess satisfied %s.\n", S->header.c_str(), k, name);
     else if (!getenv("CHFEM_B200_QUIET")) {

@@ -21,6 +21,7 @@
 #include "pointwise.cuh"
 #include "stencil_fluid.cuh"
 #include "stencil_block.cuh"
+#include "stencil_fluid_block.cuh"
 #include "minres.cuh"
 
 using namespace chfem;
@@ -491,6 +492,7 @@ static bool solve_pcg_device() {
 }
 
 #include "minres_driver.inl"
+static bool interp_into(const double* coarse_host, double* target);
 #include "block_driver.inl"
 
 // ---------------------------------------------------------------------------------------
@@ -738,18 +740,21 @@ __global__ void k_interp_pass(T* v, int rows, int cols, int lays, int nd, int pa
 extern "C" {
 
 }  // extern "C"
-template <typename T>
-static bool interp_x0(const double* coarse_host) {
+// Prolongs a coarse solution (host, nd x (cols/2)(rows/2)(lays/2) values) into the device
+// vector `target` of the current model; S->x64 stages the coarse values.
+static bool interp_into(const double* coarse_host, double* target) {
   const int rows = S->R, cols = S->C, lays = S->L, nd = (int)(S->nvars / S->N);
   const size_t ncoarse = (size_t)nd * (cols / 2) * (rows / 2) * (lays / 2 + (lays < 2));
   CKV(cudaMemcpyAsync(S->x64, coarse_host, ncoarse * 8, cudaMemcpyHostToDevice, S->stream));
-  CKV(cudaMemsetAsync(S->x, 0, S->nvars * 8, S->stream));
+  CKV(cudaMemsetAsync(target, 0, S->nvars * 8, S->stream));
   const int g = pw_grid(S->N);
-  k_project2<double><<<g, PW_NT, 0, S->stream>>>(S->x, S->x64, rows, cols, lays, nd);
-  for (int p = 0; p < 3; p++) k_interp_pass<double><<<g, PW_NT, 0, S->stream>>>(S->x, rows, cols, lays, nd, p);
+  k_project2<double><<<g, PW_NT, 0, S->stream>>>(target, S->x64, rows, cols, lays, nd);
+  for (int p = 0; p < 3; p++) k_interp_pass<double><<<g, PW_NT, 0, S->stream>>>(target, rows, cols, lays, nd, p);
   CKV(cudaStreamSynchronize(S->stream));
   return true;
 }
+template <typename T>
+static bool interp_x0(const double* coarse_host) { return interp_into(coarse_host, S->x); }
 extern "C" {
 
 cudapcgFlag_t cudapcgSetX0(cudapcgVar_t* x0, cudapcgFlag_t mustInterpolate) {
@@ -1050,18 +1055,20 @@ unsigned long long cudapcgB200DeviceBytes(void) {
 }  // extern "C"
 
 extern "C" cudapcgFlag_t cudapcgB200SolveBlock(unsigned int nrhs, const double* const* rhs, const double* const* x0,
-                                               double* const* x_out, unsigned int* iterations, double* residuals) {
+                                               int x0_interpolate, double* const* x_out, unsigned int* iterations,
+                                               double* residuals) {
   if (!S || !S->model || !rhs || !x_out || nrhs < 1 || nrhs > BLK_MAX) { set_err("cudapcgB200SolveBlock", "bad arguments"); return CUDAPCG_FALSE; }
-  if (S->analysis == CUDAPCG_FLUID_3D || (S->solver_flag & 1)) {
-    set_err("cudapcgB200SolveBlock", "block solves are provided for thermal and elastic CG/PCG");
+  const bool fluid = S->analysis == CUDAPCG_FLUID_3D;
+  if (fluid != ((S->solver_flag & 1) != 0)) {
+    set_err("cudapcgB200SolveBlock", "block solves are provided for thermal and elastic CG/PCG and Stokes MINRES/PMINRES");
     return CUDAPCG_FALSE;
   }
   for (unsigned k = 0; k < nrhs; k++) if (!rhs[k] || !x_out[k]) { set_err("cudapcgB200SolveBlock", "null buffer"); return CUDAPCG_FALSE; }
   const auto t0 = std::chrono::steady_clock::now();
   S->count++;
   S->launches = 0;
-  bool ok = (S->precision == CHFEM_B200_FP64) ? solve_block_T<double>((int)nrhs, rhs, x0, x_out, iterations, residuals)
-                                             : solve_block_T<float>((int)nrhs, rhs, x0, x_out, iterations, residuals);
+  bool ok = (S->precision == CHFEM_B200_FP64) ? solve_block_T<double>((int)nrhs, rhs, x0, x0_interpolate != 0, x_out, iterations, residuals)
+                                             : solve_block_T<float>((int)nrhs, rhs, x0, x0_interpolate != 0, x_out, iterations, residuals);
   S->total_time = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   S->mean_time = S->iteration ? S->solve_dev_s / S->iteration : 0.0;
   if (!ok) { S->found = 0; return CUDAPCG_FALSE; }

@@ -32,6 +32,10 @@ bool g_export_x = false;
 std::string g_x0_file;
 bool g_use_x0 = false;
 int g_recursions = 0;
+// recursive initial guesses: per load case, the solution on the model coarsened by 2 per axis
+// (prolonged by the library, cudapcgSetX0(x0, 1)); empty where none was found
+std::vector<double> g_x0_coarse[6];
+bool g_have_coarse = false;
 bool g_report = false;
 std::string g_report_text;
 chfemB200SolveStats g_stats;
@@ -179,14 +183,45 @@ int pcg_flag_of(const Model& m) { return m.analysis == THERMAL ? CUDAPCG_THERMAL
 
 const char* DIR_STR[6] = {"X", "Y", "Z", "YZ (shear)", "XZ (shear)", "XY (shear)"};
 
-bool setup_solver(Model& m) {
+// The model coarsened by 2 per axis for the recursive initial-guess search
+// (femhmg.c:1844-1916): floor(n/2) voxels per axis, voxel (r,c,l) takes the material of fine
+// voxel (2r,2c,2l); same voxel size, materials and local matrices.  nullptr when an axis
+// would vanish.
+Model* coarse_copy(const Model& f) {
+  if (f.nx < 2 || f.ny < 2 || f.nz < 2) return nullptr;
+  Model* c = new Model();
+  c->analysis = f.analysis; c->solver_flag = f.solver_flag; c->voxel = f.voxel; c->tol = f.tol; c->maxit = f.maxit;
+  c->refinement = f.refinement; c->nmat = f.nmat;
+  memcpy(c->props, f.props, sizeof(f.props));
+  memcpy(c->props_keys, f.props_keys, sizeof(f.props_keys));
+  memcpy(c->alpha, f.alpha, sizeof(f.alpha));
+  c->has_thermal_expansion = f.has_thermal_expansion;
+  c->nf = f.nf; c->nf_noext = f.nf_noext; c->raw = f.raw;
+  c->nd = f.nd; c->C_dim = f.C_dim;
+  c->nx = f.nx / 2; c->ny = f.ny / 2; c->nz = f.nz / 2;
+  c->N = (long)c->nx * c->ny * c->nz;
+  c->elem_mat.assign(c->N, 0);
+  const long fR = f.ny, fRC = (long)f.ny * f.nx, R = c->ny, RC = (long)c->ny * c->nx;
+  for (long l = 0; l < (long)c->nz; l++)
+    for (long col = 0; col < (long)c->nx; col++)
+      for (long r = 0; r < R; r++) c->elem_mat[r + col * R + l * RC] = f.elem_mat[2 * r + 2 * col * fR + 2 * l * fRC];
+  std::string err;
+  if (!build_maps(*c, err)) { delete c; return nullptr; }
+  c->lcl = f.lcl; c->CB = f.CB; c->Kdense = f.Kdense;
+  return c;
+}
+
+// coarse: a level of the recursive initial-guess search, which solves with CG or MINRES and the
+// L2 stopping test whatever the main settings (femhmg.c:708-714)
+bool setup_solver(Model& m, bool coarse = false) {
   if (!cudapcgInit((cudapcgFlag_t)pcg_flag_of(m), (cudapcgFlag_t)g_par)) { fail(std::string("cudapcgInit: ") + cudapcgB200LastError()); return false; }
   cudapcgSetHeaderString((char*)"    | ");
   cudapcgSetModelConstructorFcn(model_ctor);
   if (!cudapcgBuildModel(&m)) { fail(std::string("cudapcgBuildModel: ") + cudapcgB200LastError()); return false; }
-  if (!cudapcgSetSolver((cudapcgFlag_t)g_solver)) { fail(std::string("cudapcgSetSolver: ") + cudapcgB200LastError()); return false; }
+  const int solver = coarse ? ((g_solver & 1) ? CUDAPCG_MINRES_SOLVER : CUDAPCG_CG_SOLVER) : g_solver;
+  if (!cudapcgSetSolver((cudapcgFlag_t)solver)) { fail(std::string("cudapcgSetSolver: ") + cudapcgB200LastError()); return false; }
   cudapcgSetPreconditioner((cudapcgFlag_t)g_precond);
-  cudapcgSetResNorm((cudapcgFlag_t)g_stopcrit);
+  cudapcgSetResNorm((cudapcgFlag_t)(coarse ? 0 : g_stopcrit));
   cudapcgSetNumTol(m.tol);
   cudapcgSetMaxIterations(m.maxit);
   cudapcgB200SetPrecision(g_precision);
@@ -234,6 +269,8 @@ logical hmgInit(char* data_filename, char* elem_filename, char* sdf_filename, ui
   g_m = m;
   g_dir_set = 0;
   g_use_x0 = false; g_x0_file.clear(); g_export_x = false;
+  for (auto& v : g_x0_coarse) v.clear();
+  g_have_coarse = false;
   const double t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   SAY("Done.(%.2e s)\n", t);
   return 1;
@@ -269,7 +306,64 @@ void hmgImportX(char* file) {
 }
 void hmgFindInitialGuesses(unsigned int nlevels) {
   g_recursions = (int)nlevels;
-  if (nlevels > 0) SAY("WARNING: recursive coarse-grid initial guesses are not provided by chfem_b200; solving from x0 = 0.\n");
+  for (auto& v : g_x0_coarse) v.clear();
+  g_have_coarse = false;
+  if (!nlevels || !g_m) return;
+  Model& fine = *g_m;
+  if (fine.analysis == FLUID) {  // femhmg.c:565-570
+    SAY("WARNING: Initial guess estimation is not yet available for permeability analysis.\n");
+    SAY("         Null initial guess will be considered (x0 = [0]).\n");
+    return;
+  }
+  // coarse meshes: every second voxel of the finer level (femhmg.c:1844-1916)
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<Model*> levels{&fine};
+  for (unsigned i = 0; i < nlevels; i++) {
+    Model* c = coarse_copy(*levels.back());
+    if (!c) {
+      SAY("WARNING: the image cannot be coarsened %u times; using %u coarse levels.\n", nlevels, i);
+      break;
+    }
+    levels.push_back(c);
+  }
+  SAY("Building coarse meshes...[%zu/%u] (%.2e s)\n", levels.size() - 1, nlevels,
+      std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+  int dirs[6], nd = 0;
+  if (g_dir_set) dirs[nd++] = g_dir;
+  else { nd = load_case_count(fine); load_case_list(fine, dirs); }
+  // from the coarsest level up: each level starts from the prolonged solution of the one below
+  std::vector<double> prev[6];
+  bool have_prev = false;
+  for (size_t li = levels.size() - 1; li >= 1; li--) {
+    Model& m = *levels[li];
+    SAY("Computing initial guesses in coarse mesh %zu...\n", li);
+    if (!setup_solver(m, true)) { cudapcgEnd(); break; }
+    std::vector<double> rhs(m.ndof), x(m.ndof);
+    std::vector<double> cur[6];
+    for (int k = 0; k < nd; k++) {
+      SAY("    ------------------------------------------------------\n    Finding initial guess on %s:\n    Mesh dimension: [%u,%u,%u] elements\n",
+          DIR_STR[dirs[k]], m.nx, m.ny, m.nz);
+      assemble_rhs(m, dirs[k], rhs.data());
+      cudapcgSetRHS(rhs.data());
+      if (have_prev && !prev[dirs[k]].empty()) cudapcgSetX0(prev[dirs[k]].data(), 1);
+      else cudapcgSetX0(nullptr, 0);
+      const bool found = cudapcgSolve(x.data()) != 0;
+      if (!g_quiet) cudapcgPrintSolverMetrics();
+      if (found) cur[dirs[k]] = x;  // femhmg.c:787-801: only a converged solution is passed up
+    }
+    cudapcgFreeArrays();
+    cudapcgSetX0(nullptr, 0);
+    cudapcgEnd();
+    for (int d = 0; d < 6; d++) prev[d].swap(cur[d]);
+    have_prev = true;
+    if (li == 1) break;
+  }
+  for (size_t li = 1; li < levels.size(); li++) delete levels[li];
+  if (have_prev) {
+    for (int d = 0; d < 6; d++) g_x0_coarse[d].swap(prev[d]);
+    g_have_coarse = true;
+  }
+  SAY("Done.(%.2e s)\n", std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
 }
 void hmgSetHomogenizationFlag(hmgFlag_t flag) {
   if (!g_m) return;
@@ -296,8 +390,9 @@ void hmgSolveHomogenization(void) {
   g_stats.ndof = (unsigned)m.ndof;
   // Block multi-RHS path: all load cases of the analysis advance together (one operator pass
   // per iteration for all of them).  Same per-case recurrence, stopping test and results.
-  const bool block = g_multirhs && m.analysis != FLUID && !(g_solver & 1) &&
-                     ((m.analysis == THERMAL && nd == 3) || (m.analysis == ELASTIC && (nd == 6 || nd == 3)));
+  const bool block = g_multirhs && ((m.analysis != FLUID && !(g_solver & 1) &&
+                                     ((m.analysis == THERMAL && nd == 3) || (m.analysis == ELASTIC && (nd == 6 || nd == 3)))) ||
+                                    (m.analysis == FLUID && (g_solver & 1) && nd == 3));
   if (block) {
     std::vector<std::vector<double>> rhs(nd, std::vector<double>(m.ndof)), xs(nd, std::vector<double>(m.ndof)), x0s(nd);
     std::vector<const double*> prhs(nd), px0(nd, nullptr);
@@ -316,8 +411,11 @@ void hmgSolveHomogenization(void) {
           fclose(f);
           px0[k] = x0s[k].data();
         }
+      } else if (g_have_coarse && !g_x0_coarse[dirs[k]].empty()) {
+        px0[k] = g_x0_coarse[dirs[k]].data();
       }
     }
+    const int interp = (g_use_x0 && !g_x0_file.empty()) ? 0 : (g_have_coarse ? 1 : 0);
     m.rhs = rhs[nd - 1];
     g_stats.rhs_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
     SAY("    ------------------------------------------------------\n    Block solve of %d load cases (", nd);
@@ -325,7 +423,7 @@ void hmgSolveHomogenization(void) {
     SAY(")...\n");
     unsigned its[6] = {0};
     double res[6] = {0};
-    if (!cudapcgB200SolveBlock((unsigned)nd, prhs.data(), px0.data(), px.data(), its, res) && cudapcgB200LastError()[0]) {
+    if (!cudapcgB200SolveBlock((unsigned)nd, prhs.data(), px0.data(), interp, px.data(), its, res) && cudapcgB200LastError()[0]) {
       fail(std::string("block solve: ") + cudapcgB200LastError());
       cudapcgEnd();
       return;
@@ -367,6 +465,9 @@ void hmgSolveHomogenization(void) {
         fclose(f);
         cudapcgSetX0(x0.data(), 0);
       }
+    } else if (g_have_coarse) {  // femhmg.c:1048-1050: the recursive guess, prolonged
+      if (!g_x0_coarse[dir].empty()) { SAY("    | Interpolating initial guess...\n"); cudapcgSetX0(g_x0_coarse[dir].data(), 1); }
+      else cudapcgSetX0(nullptr, 0);
     }
     SAY("    Solving system of equations...\n");
     cudapcgSolve(x.data());

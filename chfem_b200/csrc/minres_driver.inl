@@ -4,14 +4,21 @@
 // operator pass updates x and r, applies A to z = M^-1 r and finishes delta, beta and the
 // stopping test.  r alternates between two buffers (read r, write r'), so chunks are even.
 
-template <typename T>
-static bool launch_mr_op(const T* rin, T* rout, int fin, bool skip_if_done) {
+static MrCfg mrcfg() {
   MrCfg cfg;
   const SolveCfg sc = solvecfg();
   cfg.tol = sc.tol; cfg.maxit = sc.maxit; cfg.norm = sc.norm; cfg.precond = sc.precond; cfg.nhmg = sc.nhmg;
+  return cfg;
+}
+
+// Operator pass of (P)MINRES on explicit buffers: r' = r - alpha q into rout, s = A M^-1 r',
+// x += alpha d, with the scalars of S->cur_sc.
+template <typename T>
+static bool launch_mr_op_buf(const T* rin, T* rout, const T* q, T* s, double* x, const T* d, int fin, bool skip_if_done) {
+  const MrCfg cfg = mrcfg();
   if (S->analysis == CUDAPCG_FLUID_3D) {
     FlArgs<T> a;
-    a.v = rin; a.vd = (const T*)S->q; a.vout = rout; a.y = (T*)S->s; a.x = S->x; a.d = (const T*)S->d0;
+    a.v = rin; a.vd = q; a.vout = rout; a.y = s; a.x = x; a.d = d;
     a.dof_of_node = S->d_dof_of_node; a.node_of_dof = S->d_node_of_dof; a.bkeys = S->d_bkeys;
     a.R = S->R; a.C = S->C; a.L = S->L; a.nV = S->nV; a.nB = S->nB;
     a.sc = S->cur_sc; a.finish = fin; a.skip_if_done = skip_if_done; a.cfg = cfg;
@@ -25,17 +32,21 @@ static bool launch_mr_op(const T* rin, T* rout, int fin, bool skip_if_done) {
     const int nb = grid.x * grid.y * grid.z;
     if (!ensure_reduction(nb)) return false;
     if (S->nd == 1) {
-      TeArgs<1, T> a{rin, (const T*)S->q, rout, (T*)S->s, S->x, (const T*)S->d0, S->d_keys, Kdev<T>(), S->nmat,
+      TeArgs<1, T> a{rin, q, rout, s, x, d, S->d_keys, Kdev<T>(), S->nmat,
                      S->R, S->C, S->L, lc, S->cur_sc, redctl(nb), fin, skip_if_done, cfg};
       k_te_apply<1, T, TE_MR><<<grid, block, te_smem_bytes<1, T>(S->nmat), S->stream>>>(a);
     } else {
-      TeArgs<3, T> a{rin, (const T*)S->q, rout, (T*)S->s, S->x, (const T*)S->d0, S->d_keys, Kdev<T>(), S->nmat,
+      TeArgs<3, T> a{rin, q, rout, s, x, d, S->d_keys, Kdev<T>(), S->nmat,
                      S->R, S->C, S->L, lc, S->cur_sc, redctl(nb), fin, skip_if_done, cfg};
       k_te_apply<3, T, TE_MR><<<grid, block, te_smem_bytes<3, T>(S->nmat), S->stream>>>(a);
     }
   }
   S->launches++;
   return cudaPeekAtLastError() == cudaSuccess;
+}
+template <typename T>
+static bool launch_mr_op(const T* rin, T* rout, int fin, bool skip_if_done) {
+  return launch_mr_op_buf<T>(rin, rout, (const T*)S->q, (T*)S->s, S->x, (const T*)S->d0, fin, skip_if_done);
 }
 
 template <typename T>

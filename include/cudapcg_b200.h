@@ -136,11 +136,14 @@ cudapcgFlag_t cudapcgB200ApplyOperator(const double *x, double *y);
 cudapcgFlag_t cudapcgB200ApplyPreconditioner(const double *x, double *y);
 /* Block solve of nrhs load cases of the current model at once (3 for thermal, 3 or 6 for
    elastic; CG/PCG): rhs[k], x_out[k] are host buffers of nvars doubles, x0 may be NULL or hold
-   NULL entries.  Each right-hand side runs the recurrence and stopping test of cudapcgSolve;
-   the operator reads the model once per block apply.  iterations/residuals (nrhs entries) may
-   be NULL.  Returns 1 when every right-hand side met the tolerance. */
+   NULL entries; with x0_interpolate set, each x0[k] is a solution on the model coarsened by 2
+   per axis and is prolonged as cudapcgSetX0(x0, 1) does.  Each right-hand side runs the
+   recurrence and stopping test of cudapcgSolve; the operator reads the model once per block
+   apply.  iterations/residuals (nrhs entries) may be NULL.  Returns 1 when every right-hand
+   side met the tolerance. */
 cudapcgFlag_t cudapcgB200SolveBlock(unsigned int nrhs, const double *const *rhs, const double *const *x0,
-                                    double *const *x_out, unsigned int *iterations, double *residuals);
+                                    int x0_interpolate, double *const *x_out, unsigned int *iterations,
+                                    double *residuals);
 /* Statistics of the last solve. */
 typedef struct {
   unsigned int iterations;

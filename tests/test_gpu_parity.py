@@ -43,14 +43,28 @@ def test_golden_cases(tmp_path, key, precision):
     Cref = np.array(ref["C"])
     tol = FP64_TOL if precision == "fp64" else MIXED_TOL
     cols = [meta["direction"]] if "-d" in ref["flags"] else list(range(Cref.shape[1]))
+    solve_tol = nf_tolerance(nf)
     for c in cols:
-        assert H.rel_to_max(C[:, c], Cref[:, c]) < tol, (c, C[:, c], Cref[:, c])
+        if precision == "mixed" and solve_tol > 1e-5:
+            # A solve stopped at relative residual tol fixes the tensor to O(tol): the loaded
+            # (largest) entry still meets the mixed bar, the near-zero entries of the column
+            # agree to 10 tol between two valid iteration paths (FP64 and mixed).
+            i = int(np.argmax(np.abs(Cref[:, c])))
+            assert abs(C[i, c] - Cref[i, c]) / abs(Cref[i, c]) < MIXED_TOL, (c, C[:, c], Cref[:, c])
+            assert H.rel_to_max(C[:, c], Cref[:, c]) < 10 * solve_tol, (c, C[:, c], Cref[:, c])
+        else:
+            assert H.rel_to_max(C[:, c], Cref[:, c]) < tol, (c, C[:, c], Cref[:, c])
     # and within the reference's own regression bar of its golden column
     assert H.rel_to_max(C[:, meta["direction"]], meta["column"]) < meta["reference_tolerance"]
     if precision == "fp64":  # same recurrence, same stopping test: same iteration counts (+-1 for round-off)
         its = H.parse_iterations(log)
         assert len(its) == len(ref["iterations"])
         assert all(abs(a - b) <= 1 for a, b in zip(its, ref["iterations"])), (its, ref["iterations"])
+
+
+def nf_tolerance(nf):
+    lines = open(nf).read().split()
+    return float(lines[lines.index("%solver_tolerance") + 1])
 
 
 def test_python_api_golden(tmp_path):
@@ -223,6 +237,9 @@ def test_operator_and_jacobi(tmp_path, name, analysis, spec, precision):
 BLOCK = [s for s in SMALL if s[0] in ("th2_pcg", "th4_cg", "th2_inf", "th2_err", "th2_ebe", "th_thin", "el2_pcg")] + [
     ("el3_ebe_all", 1, ("img", (8, 8, 9), 3), ["-p", "1"]),
     ("el2_nopre", 1, ("img", (7, 6, 9), 2), ["-j", "0"]),
+    ("fl_pminres", 2, ("pore", (16, 18, 20), 0.45), ["-s", "1"]),
+    ("fl_minres_nopre_all", 2, ("pore", (14, 14, 14), 0.5), ["-s", "1", "-j", "0"]),
+    ("fl_pminres_inf", 2, ("pore", (12, 16, 14), 0.5), ["-s", "1", "-c", "1"]),
 ]
 
 
@@ -257,3 +274,37 @@ def test_block_multirhs_python_api():
     C1 = np.array(compute_property("elasticity", img, mat_props={0: (10.0, 0.25), 255: (100.0, 0.3)}, solver_tolerance=1e-8))
     C2 = np.array(compute_property("elasticity", img, mat_props={0: (10.0, 0.25), 255: (100.0, 0.3)}, solver_tolerance=1e-8, multirhs=True))
     assert H.rel_to_max(C2, C1) < FP64_TOL
+
+
+# ---------------------------------------------------------------------------------------
+# Recursive coarse-grid initial guesses (-r N): the image coarsened by 2 per axis is solved
+# first and its prolonged solution seeds the next finer level (femhmg.c:561-846).  Tensors to
+# the FP64 bar and every level's iteration count within +-1 of the oracle's.
+RECURSIVE = [
+    ("th_r1", 0, ("img", (16, 18, 20), 2), ["-r", "1"]),
+    ("th_r2_odd", 0, ("img", (17, 21, 19), 3), ["-r", "2"]),
+    ("el_r1", 1, ("img", (12, 14, 10), 2), ["-r", "1"]),
+    ("el_r1_dir", 1, ("img", (12, 10, 14), 2), ["-r", "1", "-d", "4"]),
+    ("th_r1_cg", 0, ("img", (16, 16, 16), 2), ["-r", "1", "-j", "0"]),
+]
+
+
+@pytest.mark.parametrize("name,analysis,spec,flags", RECURSIVE)
+@pytest.mark.parametrize("extra", [[], ["--multirhs"]])
+def test_recursive_initial_guess(tmp_path, name, analysis, spec, flags, extra):
+    if extra and "-d" in flags:
+        pytest.skip("a single load case has no block")
+    nf, raw = build_small(tmp_path, name, analysis, spec)
+    Cref, logref = H.run_exec(H.ORACLE_EXEC, nf, raw, *flags)
+    C, log = H.run_exec(H.CHFEM_EXEC, nf, raw, *flags, *extra)
+    assert H.rel_to_max(C, Cref) < FP64_TOL
+    its, its_ref = H.parse_iterations(log), H.parse_iterations(logref)
+    assert len(its) == len(its_ref) and len(its) > 0
+    assert all(abs(a - b) <= 1 for a, b in zip(its, its_ref)), (its, its_ref)
+    # from a zero guess: the same tensor, and the fine level needs at least as many iterations
+    i = flags.index("-r")
+    plain = flags[:i] + flags[i + 2:]
+    C0, log0 = H.run_exec(H.CHFEM_EXEC, nf, raw, *plain, *extra)
+    assert H.rel_to_max(C0, C) < FP64_TOL
+    its0 = H.parse_iterations(log0)
+    assert sum(its[-len(its0):]) <= sum(its0) + 2 * len(its0), (its, its0)
