@@ -46,8 +46,12 @@ WORKLOADS = {
     "thermal64_spheres_fp64_block": dict(analysis=0, shape=(64, 64, 64), gen="spheres", vf=0.30, seed=1000,
                                          props={0: 1.0, 255: 10.0}, tol=1e-6, maxit=20000, precision="fp64",
                                          multirhs=True),
-    "stokes128_grf_mixed": dict(analysis=2, shape=(128, 128, 128), gen="pore", corr=8.0, porosity=0.35, seed=3000,
-                                props=None, tol=1e-6, maxit=100000, precision="mixed", solver=1),
+    # Stokes solves run in FP64 in every precision mode (the (P)MINRES recurrence nears breakdown
+    # on the indefinite system, where FP32 rounding stalls it)
+    "stokes128_grf_fp64": dict(analysis=2, shape=(128, 128, 128), gen="pore", corr=8.0, porosity=0.35, seed=3000,
+                               props=None, tol=1e-6, maxit=100000, precision="fp64", solver=1),
+    "stokes128_grf_fp64_block": dict(analysis=2, shape=(128, 128, 128), gen="pore", corr=8.0, porosity=0.35, seed=3000,
+                                     props=None, tol=1e-6, maxit=100000, precision="fp64", solver=1, multirhs=True),
 }
 DEFAULT = "elastic128_grf_mixed_block"
 
@@ -393,7 +397,7 @@ def main():
     prec = w["precision"]
     es = 4 if prec == "mixed" else 8
     if w["analysis"] == 2:
-        kern_which, kname = 3, "k_fl_apply<MR> (Stokes operator + PMINRES step)"
+        kern_which, kname = 3, "k_fl_apply<MR> (Stokes operator + PMINRES step, one right-hand side)"
         per_unit = 4 * es * 4 + 4 * 2  # per DOF row set, approximate
         units = model.ndof
     else:

@@ -61,12 +61,12 @@ static bool launch_blk_apply(int parity) {
   const long n = S->nvars;
   T* dold = (T*)(parity ? B->d1 : B->d0);
   T* dnew = (T*)(parity ? B->d0 : B->d1);
-  const int lc = te_lchunk();
-  const dim3 grid = te_grid(lc), block(TE_TR, TE_TC);
-  const int nb = grid.x * grid.y * grid.z;
-  if (!ensure_reduction(nb) || !blk_prepare<ND, T, NR>()) return false;
-  BlkArgs<ND, T> a{(const T*)B->s, dold, dnew, (T*)B->q, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, lc, n, B->sc, redctl(nb)};
-  k_blk_apply<ND, T, NR><<<grid, block, blk_smem_bytes<ND, T, NR>(), S->stream>>>(a);
+  const dim3 block(TE_TR, TE_TC);
+  if (!blk_prepare<ND, T, NR>()) return false;
+  const int nb = te_ctas(k_blk_apply<ND, T, NR>, blk_smem_bytes<ND, T, NR>());
+  if (!ensure_reduction(nb)) return false;
+  BlkArgs<ND, T> a{(const T*)B->s, dold, dnew, (T*)B->q, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, n, B->sc, redctl(nb)};
+  k_blk_apply<ND, T, NR><<<nb, block, blk_smem_bytes<ND, T, NR>(), S->stream>>>(a);
   S->launches++;
   return cudaPeekAtLastError() == cudaSuccess;
 }
@@ -78,7 +78,8 @@ static bool launch_blk_point(int parity) {
   const int g = pw_grid(S->N);
   if (!ensure_reduction(g)) return false;
   BlkPw<ND, T> p{B->x, dnew, (T*)B->r, (const T*)B->q, (T*)B->s, S->d_keys, Kdev<T>(), S->nmat, S->N, n, B->sc, redctl(g), solvecfg()};
-  k_blk_point<ND, T, NR><<<g, PW_NT, 0, S->stream>>>(p);
+  if (S->resnorm == CUDAPCG_L2_NORM) k_blk_point<ND, T, NR, false><<<g, PW_NT, 0, S->stream>>>(p);
+  else k_blk_point<ND, T, NR, true><<<g, PW_NT, 0, S->stream>>>(p);
   S->launches++;
   return cudaPeekAtLastError() == cudaSuccess;
 }
@@ -260,7 +261,8 @@ static bool launch_fl_blk_apply(int parity) {
   if (!ensure_reduction(g)) return false;
   FlBlkArgs<T> a{rcur, (const T*)B->q, rnext, (T*)B->s, B->x, (const T*)B->d0, S->d_dof_of_node, S->d_node_of_dof, S->d_bkeys,
                  S->R, S->C, S->L, S->nV, S->nB, S->nvars, B->sc, redctl(g), mrcfg()};
-  k_fl_blk_apply<T, NR><<<g, FL_NT, 0, S->stream>>>(a);
+  if (S->resnorm == CUDAPCG_L2_NORM) k_fl_blk_apply<T, NR, false><<<g, FL_NT, 0, S->stream>>>(a);
+  else k_fl_blk_apply<T, NR, true><<<g, FL_NT, 0, S->stream>>>(a);
   S->launches++;
   return cudaPeekAtLastError() == cudaSuccess;
 }
@@ -347,7 +349,8 @@ static bool solve_block_minres_device(const bool* has_x0) {
       if (mixed && ((unsigned)h.iteration >= next_replace[k] || prog < S->replace_drop * repl_ref[k])) {
         S->cur_sc = B->sc + k;
         bool ok = residual_from_x<T>(true, slice<double>(B->x, k), slice<double>(B->b64, k), slice<T>(B->r, k)) &&
-                  op_k(k, FIN_MR_REPL, true);
+                  op_k(k, FIN_MR_REPL, true) &&
+                  launch_apply<T>(slice<T>(B->d0, k), nullptr, nullptr, slice<T>(B->q, k), false, FIN_NONE, true);  // q = A d afresh
         S->cur_sc = S->d_sc;
         if (!ok) return false;
         next_replace[k] = (unsigned)h.iteration + S->replace_every;

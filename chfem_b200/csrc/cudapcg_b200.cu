@@ -237,17 +237,17 @@ static bool ensure_reduction(int nblocks) {
 
 // ---------------------------------------------------------------------------------------
 // Launch helpers.
-static int te_lchunk() {
-  const long base = (long)((S->R + TE_TR - 1) / TE_TR) * ((S->C + TE_TC - 1) / TE_TC);
-  const long target = 4L * num_sms();
-  long lc = (S->L * base + target - 1) / target;
-  if (lc < 1) lc = 1;
-  if (lc > 16) lc = 16;
-  if (lc > S->L) lc = S->L;
-  return (int)lc;
+// CTAs of a persistent stencil pass (see TeWork): as many as fit on the GPU at once for this
+// kernel and shared-memory size, but no fewer than TE_MIN_RUN layers of work each.
+static long te_work() {
+  return (long)((S->R + TE_TR - 1) / TE_TR) * ((S->C + TE_TC - 1) / TE_TC) * S->L;
 }
-static dim3 te_grid(int lchunk) {
-  return dim3((S->R + TE_TR - 1) / TE_TR, (S->C + TE_TC - 1) / TE_TC, (S->L + lchunk - 1) / lchunk);
+template <typename K>
+static int te_ctas(K kernel, size_t smem) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, TE_NT, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
+  const long resident = (long)per_sm * num_sms();
+  return (int)std::max(1L, std::min(resident, te_work() / TE_MIN_RUN));
 }
 static int pw_grid(long n) {
   long g = (n + PW_NT - 1) / PW_NT;
@@ -260,10 +260,8 @@ static int pw_grid(long n) {
 // before graph capture, which must not allocate).
 static int needed_blocks() {
   long nb = pw_grid(S->analysis == CUDAPCG_FLUID_3D ? S->nV + S->nB : S->N);
-  if (S->analysis != CUDAPCG_FLUID_3D) {
-    const dim3 g = te_grid(te_lchunk());
-    nb = std::max<long>(nb, (long)g.x * g.y * g.z);
-  }
+  // stencil passes: at most 8 resident CTAs of TE_NT = 256 threads per SM
+  if (S->analysis != CUDAPCG_FLUID_3D) nb = std::max<long>(nb, 8L * num_sms());
   return (int)nb;
 }
 static RedCtl redctl(int nblocks) { return RedCtl{S->d_part, S->d_ticket, nblocks}; }
@@ -290,20 +288,21 @@ static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, i
     if (fuse) k_fl_apply<T, TE_PCG><<<g, FL_NT, 0, S->stream>>>(a);
     else k_fl_apply<T, TE_PLAIN><<<g, FL_NT, 0, S->stream>>>(a);
   } else {
-    const int lc = te_lchunk();
-    const dim3 grid = te_grid(lc), block(TE_TR, TE_TC);
-    const int nb = grid.x * grid.y * grid.z;
-    if (!ensure_reduction(nb)) return false;
+    const dim3 block(TE_TR, TE_TC);
     if (S->nd == 1) {
-      TeArgs<1, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, lc, S->cur_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
       const size_t sm = te_smem_bytes<1, T>(S->nmat);
-      if (fuse) k_te_apply<1, T, TE_PCG><<<grid, block, sm, S->stream>>>(a);
-      else k_te_apply<1, T, TE_PLAIN><<<grid, block, sm, S->stream>>>(a);
+      const int nb = fuse ? te_ctas(k_te_apply<1, T, TE_PCG>, sm) : te_ctas(k_te_apply<1, T, TE_PLAIN>, sm);
+      if (!ensure_reduction(nb)) return false;
+      TeArgs<1, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->cur_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
+      if (fuse) k_te_apply<1, T, TE_PCG><<<nb, block, sm, S->stream>>>(a);
+      else k_te_apply<1, T, TE_PLAIN><<<nb, block, sm, S->stream>>>(a);
     } else {
-      TeArgs<3, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, lc, S->cur_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
       const size_t sm = te_smem_bytes<3, T>(S->nmat);
-      if (fuse) k_te_apply<3, T, TE_PCG><<<grid, block, sm, S->stream>>>(a);
-      else k_te_apply<3, T, TE_PLAIN><<<grid, block, sm, S->stream>>>(a);
+      const int nb = fuse ? te_ctas(k_te_apply<3, T, TE_PCG>, sm) : te_ctas(k_te_apply<3, T, TE_PLAIN>, sm);
+      if (!ensure_reduction(nb)) return false;
+      TeArgs<3, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->cur_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
+      if (fuse) k_te_apply<3, T, TE_PCG><<<nb, block, sm, S->stream>>>(a);
+      else k_te_apply<3, T, TE_PLAIN><<<nb, block, sm, S->stream>>>(a);
     }
   }
   S->launches++;
@@ -448,8 +447,12 @@ static bool run_chunks(bool minres) {
       // residual replacement: r = b - A x, then the preconditioned residual and its scalars
       // (keeps the direction unless the recursive residual had drifted, then restarts)
       if (!residual_from_x<T>()) return false;
-      if (minres) { if (!launch_mr_op<T>((const T*)S->r, (T*)S->r2, FIN_MR_REPL, true)) return false; }
-      else if (!launch_point<T, PW_REPL>(S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
+      if (minres) {
+        // (P)MINRES carries q = A d as a recursion (q = s + beta q) that drifts in FP32 like r:
+        // both are refreshed, q by an apply of the current direction
+        if (!launch_mr_op<T>((const T*)S->r, (T*)S->r2, FIN_MR_REPL, true)) return false;
+        if (!launch_apply<T>((const T*)S->d0, nullptr, nullptr, (T*)S->q, false, FIN_NONE, true)) return false;
+      } else if (!launch_point<T, PW_REPL>(S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
       next_replace = (unsigned)S->h_sc->iteration + S->replace_every;
       repl_ref = progress();
       if (trace) fprintf(stderr, "[single] residual replacement at %d\n", S->h_sc->iteration);
@@ -569,7 +572,7 @@ cudapcgFlag_t cudapcgInit(cudapcgFlag_t analysis_flag, cudapcgFlag_t parStrategy
   S->analysis = analysis_flag;
   S->par = parStrategy_flag;
   S->nd = (analysis_flag == CUDAPCG_ELASTIC_3D) ? 3 : 1;
-  if (const char* e = getenv("CHFEM_B200_PRECISION")) S->precision = (!strcmp(e, "mixed") || !strcmp(e, "fp32")) ? CHFEM_B200_MIXED : CHFEM_B200_FP64;
+  if (const char* e = getenv("CHFEM_B200_PRECISION")) cudapcgB200SetPrecision((!strcmp(e, "mixed") || !strcmp(e, "fp32")) ? CHFEM_B200_MIXED : CHFEM_B200_FP64);
   if (!g_ctor) g_ctor = ctor_simple;
   CK(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
   CK(cudaEventCreate(&S->ev0)); CK(cudaEventCreate(&S->ev1)); CK(cudaEventCreate(&S->ev2));
@@ -922,7 +925,11 @@ cudapcgFlag_t cudapcgPrintSolverReport2(char* dest) {
 // ---------------- extensions ----------------
 cudapcgFlag_t cudapcgB200SetPrecision(int mode) {
   if (!S || (mode != CHFEM_B200_FP64 && mode != CHFEM_B200_MIXED)) return CUDAPCG_FALSE;
-  S->precision = mode;
+  // Stokes stays FP64: the reference's (P)MINRES recurrence (conjugate residuals with a Jacobi
+  // diagonal that is negative on the pressure rows) comes close to breaking down on the
+  // indefinite saddle-point system -- z.Az changes sign and beta jumps by orders of magnitude
+  // even in FP64 -- and FP32 rounding at those points sends it into stagnation.
+  S->precision = (S->analysis == CUDAPCG_FLUID_3D) ? CHFEM_B200_FP64 : mode;
   return CUDAPCG_TRUE;
 }
 cudapcgFlag_t cudapcgB200SetResidualReplacement(unsigned int k) { if (!S) return CUDAPCG_FALSE; S->replace_every = k; return CUDAPCG_TRUE; }
@@ -1121,17 +1128,22 @@ extern "C" int cudapcgB200ApplyOperatorNoAlloc(int analysis_flag, unsigned int n
     g_noalloc_addr[dev] = p;
   }
   unsigned char* base = (unsigned char*)g_noalloc_addr[dev];
-  // grid: as many layer chunks as the partials allow
+  // grid: the persistent stencil schedule, at most one partial per CTA in the array
   const long R = nrows, C = ncols, L = nlayers;
   const long tiles = ((R + TE_TR - 1) / TE_TR) * ((C + TE_TC - 1) / TE_TC);
   if (tiles > NOALLOC_MAX_BLOCKS) {
     set_err(who, "model too large: more than 8192 column tiles of 32x8 nodes (nrows x ncols above ~2M nodes)");
     return 0;
   }
-  long lc = std::max<long>(1, std::min<long>(16, (L * tiles + 4L * 148 - 1) / (4L * 148)));
-  while (tiles * ((L + lc - 1) / lc) > NOALLOC_MAX_BLOCKS) lc++;
-  const dim3 grid((unsigned)((R + TE_TR - 1) / TE_TR), (unsigned)((C + TE_TC - 1) / TE_TC), (unsigned)((L + lc - 1) / lc));
-  const int nb = grid.x * grid.y * grid.z;
+  const bool thermal = analysis_flag == CUDAPCG_THERMAL_3D;
+  const size_t smem = thermal ? te_smem_bytes<1, double>((int)nmat) : te_smem_bytes<3, double>((int)nmat);
+  int per_sm = 0, sms = 0;
+  e = thermal ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_te_apply<1, double, TE_PLAIN>, TE_NT, smem)
+              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_te_apply<3, double, TE_PLAIN>, TE_NT, smem);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) { set_err(who, cudaGetErrorString(e)); return 0; }
+  const long work = tiles * L;
+  const int nb = (int)std::max(1L, std::min<long>({(long)std::max(1, per_sm) * sms, work / TE_MIN_RUN, (long)NOALLOC_MAX_BLOCKS}));
   cudaStream_t st = (cudaStream_t)stream;
   e = cudaMemsetAsync(base, 0, NOALLOC_HEADER, st);
   if (e != cudaSuccess) { set_err(who, cudaGetErrorString(e)); return 0; }
@@ -1139,12 +1151,12 @@ extern "C" int cudapcgB200ApplyOperatorNoAlloc(int analysis_flag, unsigned int n
   RedCtl rc{(double*)(base + NOALLOC_HEADER), (unsigned*)base, nb};
   const dim3 block(TE_TR, TE_TC);
   const MrCfg cfg{0.0, 0, 0, 1, 0};
-  if (analysis_flag == CUDAPCG_THERMAL_3D) {
-    TeArgs<1, double> a{v, nullptr, nullptr, y, nullptr, nullptr, keys, Kdense, (int)nmat, (int)R, (int)C, (int)L, (int)lc, sc, rc, FIN_STORE, 0, cfg};
-    k_te_apply<1, double, TE_PLAIN><<<grid, block, te_smem_bytes<1, double>((int)nmat), st>>>(a);
+  if (thermal) {
+    TeArgs<1, double> a{v, nullptr, nullptr, y, nullptr, nullptr, keys, Kdense, (int)nmat, (int)R, (int)C, (int)L, sc, rc, FIN_STORE, 0, cfg};
+    k_te_apply<1, double, TE_PLAIN><<<nb, block, smem, st>>>(a);
   } else {
-    TeArgs<3, double> a{v, nullptr, nullptr, y, nullptr, nullptr, keys, Kdense, (int)nmat, (int)R, (int)C, (int)L, (int)lc, sc, rc, FIN_STORE, 0, cfg};
-    k_te_apply<3, double, TE_PLAIN><<<grid, block, te_smem_bytes<3, double>((int)nmat), st>>>(a);
+    TeArgs<3, double> a{v, nullptr, nullptr, y, nullptr, nullptr, keys, Kdense, (int)nmat, (int)R, (int)C, (int)L, sc, rc, FIN_STORE, 0, cfg};
+    k_te_apply<3, double, TE_PLAIN><<<nb, block, smem, st>>>(a);
   }
   k_noalloc_store_dot<<<1, 32, 0, st>>>(sc, vAv);
   e = cudaPeekAtLastError();

@@ -511,7 +511,7 @@ void hmgPrintModelData(void) {
     printf("  | porosity: %05.2f%%\n  | within pores: %ld\n  | at interfaces: %ld\n", 100.0 * m.nporeelem / (double)m.N, m.nV, m.nB);
   printf("Number of DOFs: %ld\nNumber of materials: %u\nNumerical tolerance: %.3e\nMax iterations: %u\nSolver: %s%s\n",
          m.ndof, m.nmat, m.tol, m.maxit, g_precond ? "P" : "", SO[g_solver < 6 ? g_solver : 0]);
-  printf("Precision: %s\n*******************************************************\n", g_precision ? "mixed (FP32 fields, FP64 reductions)" : "FP64");
+  printf("Precision: %s\n*******************************************************\n", !g_precision ? "FP64" : (m.analysis == FLUID ? "FP64 (mixed precision is not used for Stokes)" : "mixed (FP32 fields, FP64 reductions)"));
 }
 
 void hmgPrintConstitutiveMtx(void) {

@@ -27,18 +27,21 @@ static bool launch_mr_op_buf(const T* rin, T* rout, const T* q, T* s, double* x,
     a.rc = redctl(g);
     k_fl_apply<T, TE_MR><<<g, FL_NT, 0, S->stream>>>(a);
   } else {
-    const int lc = te_lchunk();
-    const dim3 grid = te_grid(lc), block(TE_TR, TE_TC);
-    const int nb = grid.x * grid.y * grid.z;
-    if (!ensure_reduction(nb)) return false;
+    const dim3 block(TE_TR, TE_TC);
     if (S->nd == 1) {
+      const size_t sm = te_smem_bytes<1, T>(S->nmat);
+      const int nb = te_ctas(k_te_apply<1, T, TE_MR>, sm);
+      if (!ensure_reduction(nb)) return false;
       TeArgs<1, T> a{rin, q, rout, s, x, d, S->d_keys, Kdev<T>(), S->nmat,
-                     S->R, S->C, S->L, lc, S->cur_sc, redctl(nb), fin, skip_if_done, cfg};
-      k_te_apply<1, T, TE_MR><<<grid, block, te_smem_bytes<1, T>(S->nmat), S->stream>>>(a);
+                     S->R, S->C, S->L, S->cur_sc, redctl(nb), fin, skip_if_done, cfg};
+      k_te_apply<1, T, TE_MR><<<nb, block, sm, S->stream>>>(a);
     } else {
+      const size_t sm = te_smem_bytes<3, T>(S->nmat);
+      const int nb = te_ctas(k_te_apply<3, T, TE_MR>, sm);
+      if (!ensure_reduction(nb)) return false;
       TeArgs<3, T> a{rin, q, rout, s, x, d, S->d_keys, Kdev<T>(), S->nmat,
-                     S->R, S->C, S->L, lc, S->cur_sc, redctl(nb), fin, skip_if_done, cfg};
-      k_te_apply<3, T, TE_MR><<<grid, block, te_smem_bytes<3, T>(S->nmat), S->stream>>>(a);
+                     S->R, S->C, S->L, S->cur_sc, redctl(nb), fin, skip_if_done, cfg};
+      k_te_apply<3, T, TE_MR><<<nb, block, sm, S->stream>>>(a);
     }
   }
   S->launches++;

@@ -30,7 +30,7 @@ struct BlkArgs {
   const uint16_t* keys;
   const T* Kd;
   int nmat;
-  int R, C, L, lchunk;
+  int R, C, L;
   long n;           // unknowns per right-hand side
   DevScalars* sc;   // [NR]
   RedCtl rc;
@@ -132,9 +132,8 @@ __global__ void __launch_bounds__(TE_NT) k_blk_apply(BlkArgs<ND, T> a) {
   if (tid < NR) { sbeta[tid] = T(a.sc[tid].beta); sdone[tid] = a.sc[tid].done; }
   __syncthreads();
   const int R = a.R, C = a.C, L = a.L;
-  const int r0 = blockIdx.x * TE_TR, c0 = blockIdx.y * TE_TC, l0 = blockIdx.z * a.lchunk;
-  const int l1 = min(l0 + a.lchunk, L);
   const size_t RC = (size_t)R * C;
+  int r0 = 0, c0 = 0;  // column tile of the current run
   const long n = a.n;
   auto slot_of = [&](int l) { return ((l % 3) + 3) % 3; };
   auto load_plane = [&](int l) {
@@ -153,14 +152,19 @@ __global__ void __launch_bounds__(TE_NT) k_blk_apply(BlkArgs<ND, T> a) {
         }
     }
   };
-  load_plane(l0 - 1);
-  load_plane(l0);
   double acc[NR];
 #pragma unroll
   for (int k = 0; k < NR; k++) acc[k] = 0.0;
+  const int ctr = (threadIdx.x + 1) + (threadIdx.y + 1) * TE_PR;
+  const TeWork wk(R, C, L);
+  for (long w = wk.begin(), w_end = wk.end(); w < w_end;) {
+  int l0, l1;
+  wk.run(w, w_end, r0, c0, l0, l1);
   const int r = r0 + threadIdx.x, c = c0 + threadIdx.y;
   const bool active = (r < R) && (c < C);
-  const int ctr = (threadIdx.x + 1) + (threadIdx.y + 1) * TE_PR;
+  __syncthreads();
+  load_plane(l0 - 1);
+  load_plane(l0);
   for (int l = l0; l < l1; l++) {
     load_plane(l + 1);
     __syncthreads();
@@ -193,6 +197,8 @@ __global__ void __launch_bounds__(TE_NT) k_blk_apply(BlkArgs<ND, T> a) {
     }
     __syncthreads();
   }
+  w += l1 - l0;
+  }
   const bool ismax[NR] = {};
   double res[NR];
   const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
@@ -216,9 +222,12 @@ struct BlkPw {
   SolveCfg cfg;
 };
 
-template <int ND, typename T, int NR>
+// MAXN: the stopping test needs the max-norms (infinity / error norm); the L2 test needs the
+// sums r.M^-1 r only, which keeps the per-thread accumulators to NR.
+template <int ND, typename T, int NR, bool MAXN>
 __global__ void __launch_bounds__(PW_NT) k_blk_point(BlkPw<ND, T> a) {
   constexpr int ED = 8 * ND;
+  constexpr int NV = MAXN ? 4 : 1;  // reduced values per right-hand side
   __shared__ double sred[PW_NT / 32];
   __shared__ T sD[4 * 8 * ND];
   __shared__ double salpha[NR];
@@ -234,9 +243,9 @@ __global__ void __launch_bounds__(PW_NT) k_blk_point(BlkPw<ND, T> a) {
   }
   if (tid < NR) { salpha[tid] = a.sc[tid].alpha; sdone[tid] = a.sc[tid].done; }
   __syncthreads();
-  double vals[4 * NR];
+  double vals[NV * NR];
 #pragma unroll
-  for (int k = 0; k < 4 * NR; k++) vals[k] = 0.0;
+  for (int k = 0; k < NV * NR; k++) vals[k] = 0.0;
   for (long i = blockIdx.x * (long)PW_NT + tid; i < a.N; i += (long)gridDim.x * PW_NT) {
     T inv[ND];
     if (a.cfg.precond) te_invdiag<ND, T>(sD, a.keys[i], inv);
@@ -259,23 +268,27 @@ __global__ void __launch_bounds__(PW_NT) k_blk_point(BlkPw<ND, T> a) {
         a.r[j] = rv;
         const T sv = rv * inv[c];
         a.s[j] = sv;
-        vals[4 * k] += (double)rv * (double)sv;
-        vals[4 * k + 1] = fmax(vals[4 * k + 1], fabs((double)rv));
-        vals[4 * k + 2] = fmax(vals[4 * k + 2], fabs((double)dv));
-        vals[4 * k + 3] = fmax(vals[4 * k + 3], fabs(xv));
+        vals[NV * k] += (double)rv * (double)sv;
+        if constexpr (MAXN) {
+          vals[NV * k + 1] = fmax(vals[NV * k + 1], fabs((double)rv));
+          vals[NV * k + 2] = fmax(vals[NV * k + 2], fabs((double)dv));
+          vals[NV * k + 3] = fmax(vals[NV * k + 3], fabs(xv));
+        }
       }
     }
   }
-  bool ismax[4 * NR];
+  bool ismax[NV * NR];
 #pragma unroll
-  for (int k = 0; k < 4 * NR; k++) ismax[k] = (k % 4) != 0;
-  double out[4 * NR];
-  if (grid_reduce<PW_NT, 4 * NR>(vals, ismax, a.rc, blockIdx.x, out, sred) && tid == 0) {
+  for (int k = 0; k < NV * NR; k++) ismax[k] = (k % NV) != 0;
+  double out[NV * NR];
+  if (grid_reduce<PW_NT, NV * NR>(vals, ismax, a.rc, blockIdx.x, out, sred) && tid == 0) {
 #pragma unroll
     for (int k = 0; k < NR; k++) {
       if (sdone[k]) continue;
-      for (int t = 0; t < 4; t++) a.sc[k].red[t] = out[4 * k + t];
-      pcg_finish(PW_PCG, out + 4 * k, a.sc + k, a.cfg);
+      double s4[4] = {out[NV * k], 0.0, 0.0, 0.0};
+      if constexpr (MAXN) { s4[1] = out[NV * k + 1]; s4[2] = out[NV * k + 2]; s4[3] = out[NV * k + 3]; }
+      for (int t = 0; t < 4; t++) a.sc[k].red[t] = s4[t];
+      pcg_finish(PW_PCG, s4, a.sc + k, a.cfg);
     }
   }
 }

@@ -109,8 +109,11 @@ __device__ __forceinline__ void fl_blk_all_nbrs(std::integer_sequence<int, Os...
   (fl_blk_nbr<T, NR, Os>(a, fk, pore, rr, cc, ll, salpha, pre, ivv0, ivv1, ivv2, ivp, ov0, ov1, ov2, op), ...);
 }
 
-template <typename T, int NR>
-__global__ void __launch_bounds__(FL_NT) k_fl_blk_apply(FlBlkArgs<T> a) {
+// MAXN: the stopping test needs the max-norms (infinity / error norm); the L2 test needs only
+// the two sums (z'.A z', r'.z') per right-hand side.  Two CTAs per SM at least: the pass is a
+// gather whose latency wants the warps.
+template <typename T, int NR, bool MAXN>
+__global__ void __launch_bounds__(FL_NT, 2) k_fl_blk_apply(FlBlkArgs<T> a) {
   __shared__ double sred[FL_NT / 32];
   __shared__ T salpha[NR];
   __shared__ int sdone[NR];
@@ -128,9 +131,10 @@ __global__ void __launch_bounds__(FL_NT) k_fl_blk_apply(FlBlkArgs<T> a) {
   const bool pre = a.cfg.precond != 0;
   const T ivv0 = pre ? T(c_fldiag.pore[0]) : T(1), ivv1 = pre ? T(c_fldiag.pore[1]) : T(1), ivv2 = pre ? T(c_fldiag.pore[2]) : T(1);
   const T ivp = pre ? T(c_fldiag.pore[3]) : T(1);
-  double acc[NR], acc_rz[NR], mr[NR], md[NR], mx[NR];
+  constexpr int NV = MAXN ? 5 : 2;
+  double vals[NV * NR];
 #pragma unroll
-  for (int k = 0; k < NR; k++) acc[k] = acc_rz[k] = mr[k] = md[k] = mx[k] = 0.0;
+  for (int k = 0; k < NV * NR; k++) vals[k] = 0.0;
   // z' = M^-1 (r - alpha q) at vector offset off of right-hand side k
   auto zin = [&](int k, size_t off, T inv) { return fma(-salpha[k], a.q[k * n + off], a.r[k * n + off]) * inv; };
   for (long t = blockIdx.x * (long)FL_NT + threadIdx.x; t < nT; t += (long)gridDim.x * FL_NT) {
@@ -166,28 +170,27 @@ __global__ void __launch_bounds__(FL_NT) k_fl_blk_apply(FlBlkArgs<T> a) {
         const T dv = a.d[jk];
         const double xv = fma((double)salpha[k], (double)dv, a.x[jk]);
         if (!sdone[k]) a.x[jk] = xv;
-        acc_rz[k] += (double)rn * (double)z;
-        mr[k] = fmax(mr[k], fabs((double)rn));
-        if ((long)j < a.cfg.nhmg) { md[k] = fmax(md[k], fabs((double)dv)); mx[k] = fmax(mx[k], fabs(xv)); }
-        acc[k] += (double)z * (double)outv[m];
+        vals[NV * k] += (double)z * (double)outv[m];
+        vals[NV * k + 1] += (double)rn * (double)z;
+        if constexpr (MAXN) {
+          vals[NV * k + 2] = fmax(vals[NV * k + 2], fabs((double)rn));
+          if ((long)j < a.cfg.nhmg) { vals[NV * k + 3] = fmax(vals[NV * k + 3], fabs((double)dv)); vals[NV * k + 4] = fmax(vals[NV * k + 4], fabs(xv)); }
+        }
       }
     }
   }
-  double vals[5 * NR];
-  bool ismax[5 * NR];
-  double out[5 * NR];
+  bool ismax[NV * NR];
+  double out[NV * NR];
 #pragma unroll
-  for (int k = 0; k < NR; k++) {
-    vals[5 * k] = acc[k]; vals[5 * k + 1] = acc_rz[k]; vals[5 * k + 2] = mr[k]; vals[5 * k + 3] = md[k]; vals[5 * k + 4] = mx[k];
-    ismax[5 * k] = ismax[5 * k + 1] = false;
-    ismax[5 * k + 2] = ismax[5 * k + 3] = ismax[5 * k + 4] = true;
-  }
-  if (grid_reduce<FL_NT, 5 * NR>(vals, ismax, a.rc, blockIdx.x, out, sred) && threadIdx.x == 0) {
+  for (int k = 0; k < NV * NR; k++) ismax[k] = (k % NV) >= 2;
+  if (grid_reduce<FL_NT, NV * NR>(vals, ismax, a.rc, blockIdx.x, out, sred) && threadIdx.x == 0) {
 #pragma unroll
     for (int k = 0; k < NR; k++) {
       if (sdone[k]) continue;
-      for (int m = 0; m < 5; m++) a.sc[k].red[m] = out[5 * k + m];
-      mr_finish(FIN_MR_STEP, out + 5 * k, a.sc + k, a.cfg);
+      double s5[5] = {out[NV * k], out[NV * k + 1], 0.0, 0.0, 0.0};
+      if constexpr (MAXN) { s5[2] = out[NV * k + 2]; s5[3] = out[NV * k + 3]; s5[4] = out[NV * k + 4]; }
+      for (int m = 0; m < 5; m++) a.sc[k].red[m] = s5[m];
+      mr_finish(FIN_MR_STEP, s5, a.sc + k, a.cfg);
     }
   }
 }

@@ -46,6 +46,29 @@ struct MrCfg {
   long nhmg;
 };
 
+// Work schedule of a stencil pass.  The column tiles (TE_TR x TE_TC nodes) times the layers
+// form one line w = tile * L + layer; CTA b of a 1D grid of P CTAs takes the slice
+// [b W / P, (b+1) W / P) and walks it as runs of consecutive layers of one tile (restaging
+// its halo planes at each run start).  P is the number of CTAs that fit on the GPU at once,
+// so every CTA gets the same share of the work and the pass runs in a single wave.
+constexpr int TE_MIN_RUN = 4;  // layers per CTA at least (halo restaging overhead)
+struct TeWork {
+  int tiles_r, L;
+  long W;
+  __device__ TeWork(int R, int C, int L_) : tiles_r((R + TE_TR - 1) / TE_TR), L(L_),
+      W((long)((R + TE_TR - 1) / TE_TR) * ((C + TE_TC - 1) / TE_TC) * L_) {}
+  __device__ long begin() const { return (long)blockIdx.x * W / gridDim.x; }
+  __device__ long end() const { return ((long)blockIdx.x + 1) * W / gridDim.x; }
+  // the run starting at w: tile origin (r0, c0) and layers [l0, l1)
+  __device__ void run(long w, long w_end, int& r0, int& c0, int& l0, int& l1) const {
+    const long tile = w / L;
+    l0 = (int)(w % L);
+    l1 = (int)min((long)L, (long)l0 + (w_end - w));
+    r0 = (int)(tile % tiles_r) * TE_TR;
+    c0 = (int)(tile / tiles_r) * TE_TC;
+  }
+};
+
 template <int ND, typename T>
 struct TeArgs {
   const T* in0;        // s (PCG) | r (MR) | field to apply
@@ -57,7 +80,7 @@ struct TeArgs {
   const uint16_t* keys;
   const T* Kd;         // dense element matrices [nmat][8ND][8ND]
   int nmat;
-  int R, C, L, lchunk;
+  int R, C, L;
   DevScalars* sc;
   RedCtl rc;
   int finish;          // TeFinish
@@ -177,9 +200,8 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a) {
   const T alpha = (MODE == TE_MR && mr_steps(a.finish)) ? T(a.sc->alpha) : T(0);
   const bool pre = a.cfg.precond != 0;
   const int R = a.R, C = a.C, L = a.L;
-  const int r0 = blockIdx.x * TE_TR, c0 = blockIdx.y * TE_TC, l0 = blockIdx.z * a.lchunk;
-  const int l1 = min(l0 + a.lchunk, L);
   const size_t RC = (size_t)R * C;
+  int r0 = 0, c0 = 0;  // column tile of the current run
 
   auto slot_of = [&](int l) { return ((l % 3) + 3) % 3; };
   auto load_plane = [&](int l) {
@@ -207,13 +229,17 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a) {
     }
   };
 
+  double acc = 0.0, acc_rz = 0.0, mr = 0.0, md = 0.0, mx = 0.0;
+  const int ctr = (threadIdx.x + 1) + (threadIdx.y + 1) * TE_PR;
+  const TeWork wk(R, C, L);
+  for (long w = wk.begin(), w_end = wk.end(); w < w_end;) {
+  int l0, l1;
+  wk.run(w, w_end, r0, c0, l0, l1);
+  const int r = r0 + threadIdx.x, c = c0 + threadIdx.y;
+  const bool active = (r < R) && (c < C);
   __syncthreads();
   load_plane(l0 - 1);
   load_plane(l0);
-  double acc = 0.0, acc_rz = 0.0, mr = 0.0, md = 0.0, mx = 0.0;
-  const int r = r0 + threadIdx.x, c = c0 + threadIdx.y;
-  const bool active = (r < R) && (c < C);
-  const int ctr = (threadIdx.x + 1) + (threadIdx.y + 1) * TE_PR;
   for (int l = l0; l < l1; l++) {
     load_plane(l + 1);
     __syncthreads();
@@ -246,6 +272,8 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a) {
       }
     }
     __syncthreads();
+  }
+  w += l1 - l0;
   }
   if (a.finish == FIN_NONE) return;
   const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);

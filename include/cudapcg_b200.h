@@ -124,7 +124,9 @@ typedef struct _pcgmodel {
 
 /* Last error message of this library ("" when none). */
 const char *cudapcgB200LastError(void);
-/* Precision mode for the next solves (CHFEM_B200_FP64 or CHFEM_B200_MIXED). */
+/* Precision mode for the next solves (CHFEM_B200_FP64 or CHFEM_B200_MIXED).  Mixed applies to
+   THERMAL_3D and ELASTIC_3D; FLUID_3D models always solve in FP64 (its (P)MINRES recurrence
+   nears breakdown on the indefinite Stokes system, where FP32 rounding stalls it). */
 cudapcgFlag_t cudapcgB200SetPrecision(int mode);
 /* Mixed mode: replace the recursive residual by b - A x every k iterations (0 = never). */
 cudapcgFlag_t cudapcgB200SetResidualReplacement(unsigned int k);
