@@ -438,8 +438,14 @@ def main():
         e2e_times.append(t)
     e2e = allmax(min(e2e_times))
     ncase = 6 if w["analysis"] == 1 else 3
-    h2d = int(img.size + (2 * model.N if w["analysis"] != 2 else 9 * model.N) + ncase * model.ndof * 8)
-    d2h = int(ncase * model.ndof * 8)
+    maps = 2 * model.N if w["analysis"] != 2 else 9 * model.N  # node keys, or the Stokes DOF maps
+    if block:  # right-hand sides and tensor volume terms stay on the device
+        ns = 6 if w["analysis"] == 1 else 3
+        h2d = int(img.size + maps)
+        d2h = int(ncase * ns * 8)
+    else:
+        h2d = int(img.size + maps + ncase * model.ndof * 8)
+        d2h = int(ncase * model.ndof * 8)
     model.close()
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and world == 1:

@@ -10,6 +10,7 @@ struct BlockState {
   double *x = nullptr, *b64 = nullptr;                                          // [nr][n], FP64
   DevScalars* sc = nullptr;   // [nr]
   DevScalars* h_sc = nullptr; // pinned [nr]
+  double* d_mom = nullptr;    // load-case moments [BLK_MAX][8] + CB staging
   cudaGraphExec_t gexec = nullptr;
   int graph_key = -1;
 };
@@ -21,7 +22,7 @@ static void block_invalidate() {
 
 static void block_free() {
   if (!B) return;
-  void* ps[] = {B->r, B->s, B->d0, B->d1, B->q, B->x, B->b64, B->sc};
+  void* ps[] = {B->r, B->s, B->d0, B->d1, B->q, B->x, B->b64, B->sc, B->d_mom};
   for (void* p : ps) free_ptr(p);
   if (B->h_sc) cudaFreeHost(B->h_sc);
   if (B->gexec) cudaGraphExecDestroy(B->gexec);
@@ -382,16 +383,74 @@ static bool solve_block_minres_device(const bool* has_x0) {
   return true;
 }
 
+// Load cases assembled and reduced on the device (cudapcgB200SolveLoadCases).
+struct LoadCases {
+  const int* axis; const int* comp; const double* jump;
+  const double* CB; unsigned ns;
+  double* moments;  // [nr][ns] out
+};
+
+template <typename T>
+static bool rhs_on_device(const LoadCases& lc, int k) {
+  const long n = S->nvars;
+  if (S->analysis == CUDAPCG_FLUID_3D) {
+    double w = 0.0;
+    for (int a = 0; a < 8; a++) w += lc.CB[72 + a];
+    k_fl_rhs<T><<<pw_grid(n), PW_NT, 0, S->stream>>>(S->nV, n, lc.axis[k], w, slice<double>(B->b64, k), slice<T>(B->r, k));
+  } else {
+    if (!ensure_K<double>()) return false;
+    if (S->nd == 1)
+      k_rhs_load_case<1, T><<<pw_grid(S->N), PW_NT, 0, S->stream>>>(S->d_keys, S->d_K64, S->R, S->C, S->L, lc.axis[k], lc.comp[k], lc.jump[k],
+                                                                    slice<double>(B->b64, k), slice<T>(B->r, k));
+    else
+      k_rhs_load_case<3, T><<<pw_grid(S->N), PW_NT, 0, S->stream>>>(S->d_keys, S->d_K64, S->R, S->C, S->L, lc.axis[k], lc.comp[k], lc.jump[k],
+                                                                    slice<double>(B->b64, k), slice<T>(B->r, k));
+  }
+  S->launches++;
+  return cudaPeekAtLastError() == cudaSuccess;
+}
+
+// volume term of the effective tensor for every right-hand side into lc.moments (host)
+static bool moments_on_device(const LoadCases& lc, int nr) {
+  if (!B->d_mom) CKV(cudaMalloc(&B->d_mom, (size_t)BLK_MAX * 8 * sizeof(double) + 4 * 6 * 24 * sizeof(double)));
+  double* d_cb = B->d_mom + BLK_MAX * 8;
+  const int g = pw_grid(S->analysis == CUDAPCG_FLUID_3D ? S->nV : S->N);
+  if (!ensure_reduction(g)) return false;
+  if (S->analysis == CUDAPCG_FLUID_3D) {
+    double w[3] = {0, 0, 0};
+    for (int a = 0; a < 8; a++) { w[0] += lc.CB[3 * a]; w[1] += lc.CB[24 + 3 * a + 1]; w[2] += lc.CB[48 + 3 * a + 2]; }
+    for (int k = 0; k < nr; k++) k_fl_moments<<<g, PW_NT, 0, S->stream>>>(slice<double>(B->x, k), S->nV, w[0], w[1], w[2], redctl(g), B->d_mom + 8 * k);
+  } else {
+    const size_t ncb = (size_t)S->nmat * lc.ns * 8 * S->nd;
+    CKV(cudaMemsetAsync(d_cb, 0, 4 * 6 * 24 * sizeof(double), S->stream));
+    CKV(cudaMemcpyAsync(d_cb, lc.CB, ncb * sizeof(double), cudaMemcpyHostToDevice, S->stream));
+    for (int k = 0; k < nr; k++) {
+      if (S->nd == 1) k_cb_moments<1, 3><<<g, PW_NT, 0, S->stream>>>(S->d_keys, d_cb, slice<double>(B->x, k), S->N, redctl(g), B->d_mom + 8 * k);
+      else k_cb_moments<3, 6><<<g, PW_NT, 0, S->stream>>>(S->d_keys, d_cb, slice<double>(B->x, k), S->N, redctl(g), B->d_mom + 8 * k);
+    }
+  }
+  S->launches += nr;
+  double h[BLK_MAX * 8];
+  CKV(cudaMemcpyAsync(h, B->d_mom, (size_t)nr * 8 * sizeof(double), cudaMemcpyDeviceToHost, S->stream));
+  CKV(cudaStreamSynchronize(S->stream));
+  for (int k = 0; k < nr; k++)
+    for (unsigned s = 0; s < lc.ns; s++) lc.moments[k * lc.ns + s] = h[8 * k + s];
+  return true;
+}
+
 template <typename T>
 static bool solve_block_T(int nr, const double* const* rhs, const double* const* x0, bool x0_interp, double* const* x_out,
-                          unsigned* iters, double* resid) {
+                          unsigned* iters, double* resid, const LoadCases* lc = nullptr) {
   if (!ensure_vectors<T>() || !ensure_K<T>() || !block_alloc<T>(nr)) return false;
   const long n = S->nvars;
   bool has_x0[BLK_MAX] = {false};
   for (int k = 0; k < nr; k++) {
-    CKV(cudaMemcpyAsync(slice<double>(B->b64, k), rhs[k], n * 8, cudaMemcpyHostToDevice, S->stream));
-    if (sizeof(T) == 8) CKV(cudaMemcpyAsync(slice<double>(B->r, k), rhs[k], n * 8, cudaMemcpyHostToDevice, S->stream));
-    else k_convert<double, float><<<pw_grid(n), PW_NT, 0, S->stream>>>(slice<double>(B->b64, k), slice<float>(B->r, k), n);
+    if (lc) { if (!rhs_on_device<T>(*lc, k)) return false; }
+    else {
+      CKV(cudaMemcpyAsync(slice<double>(B->b64, k), rhs[k], n * 8, cudaMemcpyHostToDevice, S->stream));
+      if (sizeof(T) == 8) CKV(cudaMemcpyAsync(slice<double>(B->r, k), rhs[k], n * 8, cudaMemcpyHostToDevice, S->stream));
+      else k_convert<double, float><<<pw_grid(n), PW_NT, 0, S->stream>>>(slice<double>(B->b64, k), slice<float>(B->r, k), n);
+    }
     if (x0 && x0[k]) {
       if (x0_interp) { if (!interp_into(x0[k], slice<double>(B->x, k))) return false; }
       else CKV(cudaMemcpyAsync(slice<double>(B->x, k), x0[k], n * 8, cudaMemcpyHostToDevice, S->stream));
@@ -412,8 +471,9 @@ static bool solve_block_T(int nr, const double* const* rhs, const double* const*
   for (int k = 0; k < nr; k++) {
     // a null right-hand side under (P)MINRES returns x = 0 as cudapcgSolve does
     if (S->analysis == CUDAPCG_FLUID_3D && B->h_sc[k].status == 1) CKV(cudaMemsetAsync(slice<double>(B->x, k), 0, n * 8, S->stream));
-    CKV(cudaMemcpyAsync(x_out[k], slice<double>(B->x, k), n * 8, cudaMemcpyDeviceToHost, S->stream));
+    if (x_out && x_out[k]) CKV(cudaMemcpyAsync(x_out[k], slice<double>(B->x, k), n * 8, cudaMemcpyDeviceToHost, S->stream));
   }
+  if (lc && !moments_on_device(*lc, nr)) return false;
   CKV(cudaStreamSynchronize(S->stream));
   unsigned maxit = 0;
   int found_all = 1;

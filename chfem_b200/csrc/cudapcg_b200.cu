@@ -22,6 +22,7 @@
 #include "stencil_fluid.cuh"
 #include "stencil_block.cuh"
 #include "stencil_fluid_block.cuh"
+#include "loadcase.cuh"
 #include "minres.cuh"
 
 using namespace chfem;
@@ -1060,6 +1061,36 @@ unsigned long long cudapcgB200DeviceBytes(void) {
 }
 
 }  // extern "C"
+
+extern "C" cudapcgFlag_t cudapcgB200SolveLoadCases(unsigned int nrhs, const int* axis, const int* comp, const double* jump,
+                                                   const double* CB, unsigned int ns, const double* const* x0, int x0_interpolate,
+                                                   double* moments, double* const* x_out, unsigned int* iterations,
+                                                   double* residuals) {
+  const char* who = "cudapcgB200SolveLoadCases";
+  if (!S || !S->model || !axis || !CB || !moments || nrhs < 1 || nrhs > BLK_MAX) { set_err(who, "bad arguments"); return CUDAPCG_FALSE; }
+  const bool fluid = S->analysis == CUDAPCG_FLUID_3D;
+  if (fluid != ((S->solver_flag & 1) != 0)) {
+    set_err(who, "load-case blocks are provided for thermal and elastic CG/PCG and Stokes MINRES/PMINRES");
+    return CUDAPCG_FALSE;
+  }
+  const unsigned ns_expected = fluid ? 3u : (S->nd == 3 ? 6u : 3u);
+  if (ns != ns_expected) { set_err(who, "ns must be 3 (thermal, Stokes) or 6 (elastic)"); return CUDAPCG_FALSE; }
+  for (unsigned k = 0; k < nrhs; k++) {
+    if (axis[k] < 0 || axis[k] > 2) { set_err(who, "axis must be 0, 1 or 2"); return CUDAPCG_FALSE; }
+    if (!fluid && (!comp || !jump || comp[k] < 0 || comp[k] >= S->nd)) { set_err(who, "comp must be a DOF component of the node"); return CUDAPCG_FALSE; }
+  }
+  const auto t0 = std::chrono::steady_clock::now();
+  S->count++;
+  S->launches = 0;
+  const LoadCases lc{axis, comp, jump, CB, ns, moments};
+  bool ok = (S->precision == CHFEM_B200_FP64)
+                ? solve_block_T<double>((int)nrhs, nullptr, x0, x0_interpolate != 0, x_out, iterations, residuals, &lc)
+                : solve_block_T<float>((int)nrhs, nullptr, x0, x0_interpolate != 0, x_out, iterations, residuals, &lc);
+  S->total_time = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  S->mean_time = S->iteration ? S->solve_dev_s / S->iteration : 0.0;
+  if (!ok) { S->found = 0; return CUDAPCG_FALSE; }
+  return (cudapcgFlag_t)S->found;
+}
 
 extern "C" cudapcgFlag_t cudapcgB200SolveBlock(unsigned int nrhs, const double* const* rhs, const double* const* x0,
                                                int x0_interpolate, double* const* x_out, unsigned int* iterations,

@@ -384,8 +384,7 @@ void hmgSolveHomogenization(void) {
   for (unsigned i = 0; i < m.C_dim; i++) m.C[i] = 0.0;
   SAY("Running homogenization...\n");
   if (!setup_solver(m)) return;
-  m.rhs.assign(m.ndof, 0.0);
-  std::vector<double> x(m.ndof, 0.0), x0;
+  std::vector<double> x, x0;
   g_stats.n_cases = nd;
   g_stats.ndof = (unsigned)m.ndof;
   // Block multi-RHS path: all load cases of the analysis advance together (one operator pass
@@ -394,14 +393,17 @@ void hmgSolveHomogenization(void) {
                                      ((m.analysis == THERMAL && nd == 3) || (m.analysis == ELASTIC && (nd == 6 || nd == 3)))) ||
                                     (m.analysis == FLUID && (g_solver & 1) && nd == 3));
   if (block) {
-    std::vector<std::vector<double>> rhs(nd, std::vector<double>(m.ndof)), xs(nd, std::vector<double>(m.ndof)), x0s(nd);
-    std::vector<const double*> prhs(nd), px0(nd, nullptr);
-    std::vector<double*> px(nd);
-    auto t = std::chrono::steady_clock::now();
+    // right-hand sides and the effective-tensor volume term on the device
+    // (cudapcgB200SolveLoadCases); x comes back only to be exported
+    std::vector<std::vector<double>> xs(g_export_x ? nd : 0, std::vector<double>(m.ndof)), x0s(nd);
+    std::vector<const double*> px0(nd, nullptr);
+    std::vector<double*> px(nd, nullptr);
+    int axis[6], comp[6];
+    double jump[6], volume[36];
     for (int k = 0; k < nd; k++) {
-      assemble_rhs(m, dirs[k], rhs[k].data());
-      prhs[k] = rhs[k].data();
-      px[k] = xs[k].data();
+      case_axis(m, dirs[k], axis[k], comp[k]);
+      jump[k] = (double)axis_len(m, axis[k]);
+      if (g_export_x) px[k] = xs[k].data();
       if (g_use_x0 && !g_x0_file.empty()) {
         const std::string fn = g_x0_file + "_" + std::to_string(dirs[k]) + ".bin";
         FILE* f = fopen(fn.c_str(), "rb");
@@ -416,14 +418,14 @@ void hmgSolveHomogenization(void) {
       }
     }
     const int interp = (g_use_x0 && !g_x0_file.empty()) ? 0 : (g_have_coarse ? 1 : 0);
-    m.rhs = rhs[nd - 1];
-    g_stats.rhs_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
+    const unsigned ns = m.analysis == ELASTIC ? 6 : 3;
     SAY("    ------------------------------------------------------\n    Block solve of %d load cases (", nd);
     for (int k = 0; k < nd; k++) SAY("%s%s", k ? ", " : "", DIR_STR[dirs[k]]);
     SAY(")...\n");
     unsigned its[6] = {0};
     double res[6] = {0};
-    if (!cudapcgB200SolveBlock((unsigned)nd, prhs.data(), px0.data(), interp, px.data(), its, res) && cudapcgB200LastError()[0]) {
+    if (!cudapcgB200SolveLoadCases((unsigned)nd, axis, comp, jump, m.CB.data(), ns, px0.data(), interp, volume, px.data(), its, res) &&
+        cudapcgB200LastError()[0]) {
       fail(std::string("block solve: ") + cudapcgB200LastError());
       cudapcgEnd();
       return;
@@ -441,12 +443,16 @@ void hmgSolveHomogenization(void) {
         FILE* f = fopen(fn.c_str(), "wb");
         if (f) { fwrite(xs[k].data(), sizeof(double), m.ndof, f); fclose(f); }
       }
-      t = std::chrono::steady_clock::now();
-      update_C(m, dir, xs[k].data());
+      const auto t = std::chrono::steady_clock::now();
+      update_C_from_volume(m, dir, volume + ns * k);
       g_stats.update_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
     }
     g_stats.kernel_launches += st.kernel_launches;
     if (!g_quiet) cudapcgPrintSolverMetrics();
+  }
+  if (!block) {  // host vectors of the one-by-one path
+    m.rhs.assign(m.ndof, 0.0);
+    x.assign(m.ndof, 0.0);
   }
   for (int k = 0; k < nd && !block; k++) {
     const int dir = dirs[k];

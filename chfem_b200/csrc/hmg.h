@@ -57,6 +57,9 @@ bool build_maps(Model& m, std::string& err);
 void build_local_matrices(Model& m);
 void assemble_rhs(const Model& m, int direction, double* rhs);
 void update_C(Model& m, int direction, const double* x);
+void update_C_from_volume(Model& m, int direction, const double* volume);
+void case_axis(const Model& m, int direction, int& axis, int& comp);
+long axis_len(const Model& m, int axis);
 int load_case_count(const Model& m);
 void load_case_list(const Model& m, int* dirs);
 

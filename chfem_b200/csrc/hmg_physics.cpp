@@ -233,13 +233,13 @@ void load_case_list(const Model& m, int* dirs) {
   for (int i = 0; i < load_case_count(m); i++) dirs[i] = i;
 }
 // (axis of the jump, displaced component) of a load case; X Y Z YZ XZ XY
-static void case_axis(const Model& m, int dir, int& axis, int& comp) {
+void case_axis(const Model& m, int dir, int& axis, int& comp) {
   if (m.analysis != ELASTIC) { axis = dir; comp = 0; return; }
   static const int AX[6] = {0, 1, 2, 1, 2, 1}, CO[6] = {0, 1, 2, 2, 0, 0};
   axis = AX[dir]; comp = CO[dir];
 }
 static const int FACE[3][4] = {{1, 2, 5, 6}, {2, 3, 6, 7}, {0, 1, 2, 3}};
-static long axis_len(const Model& m, int axis) { return axis == 0 ? m.nx : (axis == 1 ? m.ny : m.nz); }
+long axis_len(const Model& m, int axis) { return axis == 0 ? m.nx : (axis == 1 ? m.ny : m.nz); }
 
 // Voxels whose +axis face is the cell's +axis boundary: last column (x), first row (y),
 // first layer (z) -- femhmg_thermal_3D.c:144, :178, :212.
@@ -334,6 +334,30 @@ void update_C(Model& m, int dir, const double* x) {
       for (int s = 0; s < ns; s++) acc[s] += CB[s * ec + FACE[axis][f] * nd + comp] * jump;
   });
   for (int s = 0; s < ns; s++) m.C[s * ns + dir] = acc[s] / (double)N;
+}
+
+// The effective-tensor column of load case dir from the volume term sum_e CB_e x_e (reduced on
+// the device, cudapcgB200SolveLoadCases) plus the boundary face term -- the same sums as
+// update_C, split where the device takes over.
+void update_C_from_volume(Model& m, int dir, const double* volume) {
+  if (m.analysis == FLUID) {
+    const double scl = m.voxel * m.voxel / (double)m.N;
+    for (int s = 0; s < 3; s++) m.C[3 * s + dir] = volume[s] * scl;
+    return;
+  }
+  int axis, comp;
+  case_axis(m, dir, axis, comp);
+  const double jump = (double)axis_len(m, axis);
+  const int nd = m.nd, ns = (m.analysis == ELASTIC) ? 6 : 3, ec = 8 * nd;
+  const long R = m.ny, C = m.nx;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int s = 0; s < ns; s++) acc[s] = volume[s];
+  for_boundary_voxels(m, axis, [&](long r, long c, long l) {
+    const double* CB = m.CB.data() + (size_t)m.elem_mat[r + c * R + l * R * C] * ns * ec;
+    for (int f = 0; f < 4; f++)
+      for (int s = 0; s < ns; s++) acc[s] += CB[s * ec + FACE[axis][f] * nd + comp] * jump;
+  });
+  for (int s = 0; s < ns; s++) m.C[s * ns + dir] = acc[s] / (double)m.N;
 }
 
 }  // namespace chfem_host

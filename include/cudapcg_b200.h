@@ -146,6 +146,22 @@ cudapcgFlag_t cudapcgB200ApplyPreconditioner(const double *x, double *y);
 cudapcgFlag_t cudapcgB200SolveBlock(unsigned int nrhs, const double *const *rhs, const double *const *x0,
                                     int x0_interpolate, double *const *x_out, unsigned int *iterations,
                                     double *residuals);
+/* Block solve of the homogenization load cases of the current model with the right-hand sides
+   assembled and the effective-tensor volume term reduced on the device, so that no full-length
+   vector crosses to or from the host.  Load case k: thermal/elastic, the macroscopic jump
+   jump[k] along axis[k] (0 x, 1 y, 2 z) in DOF component comp[k], entering through the voxels
+   on the +axis cell boundary (femhmg_thermal_3D.c:122-236, femhmg_elastic_3D.c:130-511);
+   Stokes (MINRES/PMINRES), a unit body force along axis[k] (femhmg_fluid_3D.c:112-182; comp
+   and jump unused).  CB: the effective-tensor matrices of the host layer -- nmat x ns x 8dof
+   (thermal ns = 3, elastic ns = 6) or Stokes 3 x 24 followed by the 8 body-force weights.
+   moments[k*ns + s] = sum over voxels of (CB x)_s for case k (Stokes: the mean-velocity sums),
+   to which the caller adds the boundary face term.  x0 / x0_interpolate as for
+   cudapcgB200SolveBlock; x_out may be NULL or hold NULL entries (no copy back).  Returns 1 when
+   every case met the tolerance. */
+cudapcgFlag_t cudapcgB200SolveLoadCases(unsigned int nrhs, const int *axis, const int *comp, const double *jump,
+                                        const double *CB, unsigned int ns, const double *const *x0, int x0_interpolate,
+                                        double *moments, double *const *x_out, unsigned int *iterations,
+                                        double *residuals);
 /* Statistics of the last solve. */
 typedef struct {
   unsigned int iterations;

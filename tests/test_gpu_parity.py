@@ -318,3 +318,15 @@ def test_recursive_initial_guess(tmp_path, name, analysis, spec, flags, extra):
     assert H.rel_to_max(C0, C) < FP64_TOL
     its0 = H.parse_iterations(log0)
     assert sum(its[-len(its0):]) <= sum(its0) + 2 * len(its0), (its, its0)
+
+
+def test_block_export_roundtrip(tmp_path):
+    """--multirhs with -xo brings every load case's x back to the host; -xi then starts each
+    case at its solution, which the block solve accepts at once with the same tensor."""
+    nf, raw = build_small(tmp_path, "xb", 1, ("img", (8, 9, 10), 2))
+    C1, _ = H.run_exec(H.CHFEM_EXEC, nf, raw, "--multirhs", "-xo")
+    prefix = nf[:-3] + "_X"
+    assert all(os.path.exists(f"{prefix}_{d}.bin") for d in range(6))
+    C2, log = H.run_exec(H.CHFEM_EXEC, nf, raw, "--multirhs", "-xi", prefix)
+    assert log.count("Initial guess satisfied") == 6
+    assert H.rel_to_max(C2, C1) < 1e-12
