@@ -38,6 +38,9 @@ WORKLOADS = {
                                  props={0: (1.0, 0.30), 255: (10.0, 0.20)}, tol=1e-6, maxit=20000, precision="mixed"),
     "elastic128_grf_fp64": dict(analysis=1, shape=(128, 128, 128), gen="grf", corr=6.0, fraction=0.40, seed=2000,
                                 props={0: (1.0, 0.30), 255: (10.0, 0.20)}, tol=1e-6, maxit=20000, precision="fp64"),
+    "elastic256_grf_mixed_block": dict(analysis=1, shape=(256, 256, 256), gen="grf", corr=6.0, fraction=0.40, seed=5000,
+                                       props={0: (1.0, 0.30), 255: (10.0, 0.20)}, tol=1e-6, maxit=20000,
+                                       precision="mixed", multirhs=True),
     "thermal64_spheres_fp64": dict(analysis=0, shape=(64, 64, 64), gen="spheres", vf=0.30, seed=1000,
                                    props={0: 1.0, 255: 10.0}, tol=1e-6, maxit=20000, precision="fp64"),
     "elastic128_grf_mixed_block": dict(analysis=1, shape=(128, 128, 128), gen="grf", corr=6.0, fraction=0.40, seed=2000,
@@ -52,6 +55,13 @@ WORKLOADS = {
                                props=None, tol=1e-6, maxit=100000, precision="fp64", solver=1),
     "stokes128_grf_fp64_block": dict(analysis=2, shape=(128, 128, 128), gen="pore", corr=8.0, porosity=0.35, seed=3000,
                                      props=None, tol=1e-6, maxit=100000, precision="fp64", solver=1, multirhs=True),
+    # 512 independent sphere-inclusion images, edge uniform in {32, 48, 64, 96}, volume fraction
+    # U[0.1, 0.5] (overlapping balls of radius 4-8), k1/k0 log-uniform in [2, 100], 3 load cases
+    # each, all solved in one device-resident batch
+    "thermal_batch512_mixed": dict(analysis=0, batch=512, edges=(32, 48, 64, 96), seed=4000, tol=1e-6, maxit=10000,
+                                   precision="mixed"),
+    "thermal_batch512_fp64": dict(analysis=0, batch=512, edges=(32, 48, 64, 96), seed=4000, tol=1e-6, maxit=10000,
+                                  precision="fp64"),
 }
 DEFAULT = "elastic128_grf_mixed_block"
 
@@ -256,6 +266,149 @@ def cpu_baseline(nf_dir, w, img, total_iters):
                       f"{per_it:.3e} s/iteration x {total_iters} iterations of the full FP64 job"}
 
 
+# ---------------------------------------------------------------------------------------
+# Batched thermal workload (independent samples, one batch solve per step)
+def make_batch(w, rank):
+    from chfem_b200 import synthetic
+    rng = np.random.default_rng(w["seed"] + 7919 * rank)
+    imgs, props = [], []
+    for i in range(w["batch"]):
+        e = int(rng.choice(w["edges"]))
+        vf = float(rng.uniform(0.1, 0.5))
+        ratio = float(np.exp(rng.uniform(np.log(2.0), np.log(100.0))))
+        imgs.append(synthetic.spheres((e, e, e), vf=vf, seed=w["seed"] + i + 100000 * rank, overlap=True))
+        props.append({0: 1.0, 255: ratio})
+    return imgs, props
+
+
+def batch_cpu_rate(imgs, props, w, exe, budget_s=20.0):
+    """Seconds per node-iteration of a solver CLI (oracle or reference build) on the smallest
+    samples of the batch, each homogenized in full (3 load cases), until budget_s is spent."""
+    from chfem_b200.io import export_for_chfem
+    order = sorted(range(len(imgs)), key=lambda i: imgs[i].size)
+    t_sum, ni_sum, done, walls = 0.0, 0, 0, 0.0
+    with tempfile.TemporaryDirectory() as d:
+        for i in order[:8]:
+            nf = os.path.join(d, f"s{i}.nf")
+            export_for_chfem(os.path.join(d, f"s{i}.raw"), imgs[i], 0, mat_props=props[i], voxel_size=1.0,
+                             solver_tolerance=w["tol"], solver_maxiter=w["maxit"])
+            t0 = time.perf_counter()
+            p = subprocess.run([exe, nf, os.path.join(d, f"s{i}.raw")], capture_output=True, text=True, timeout=600, cwd=d)
+            wall = time.perf_counter() - t0
+            if p.returncode != 0:
+                return None
+            its = [int(l.split("iteration:")[1].split(",")[0]) for l in p.stdout.splitlines() if "iteration:" in l and "residual" in l]
+            solve = sum(float(l.split(":")[1].split()[0]) for l in p.stdout.splitlines() if "| Elapsed time:" in l)
+            t_sum += solve if solve > 0 else wall
+            walls += wall
+            ni_sum += imgs[i].size * sum(its)
+            done += 1
+            if walls > budget_s:
+                break
+    if not ni_sum:
+        return None
+    return t_sum / ni_sum, walls / ni_sum, done
+
+
+def batch_main(args, w, world, rank, dist, allmax, barrier):
+    from chfem_b200 import compute_conductivity_batch, _native
+    imgs, props = make_batch(w, rank)
+    nodes = int(sum(a.size for a in imgs))
+
+    def step():
+        t0 = time.perf_counter()
+        C, its = compute_conductivity_batch(imgs, props, solver_tolerance=w["tol"], solver_maxiter=w["maxit"],
+                                            precision=w["precision"], return_iterations=True)
+        wall = time.perf_counter() - t0
+        st = _native.batch_stats()
+        return C, its, st, wall
+
+    first = None
+    for k in range(args.warmup):
+        r = step()
+        first = first or r
+    clocks = Clocks()
+    barrier()
+    clocks.start()
+    dev, walls, launches = [], [], 0
+    for _ in range(args.steps):
+        C, its, st, wall = step()
+        dev.append(st.setup_seconds + st.solve_seconds)
+        walls.append(wall)
+        launches += st.kernel_launches
+    barrier()
+    clk = clocks.stop()
+    step_s = allmax(float(np.mean(dev)))
+    e2e = allmax(float(np.mean(walls)))
+    st0 = first[2] if first else st
+    es = 4 if w["precision"] == "mixed" else 8
+    per_unit = 12 * es + 2
+    peak, peak_kind = load_peaks()
+    tile = {4: 0, 8: 1, 16: 2}.get(st0.tile_cols, 1)
+    kt = st0.tile_ms[tile] * 1e-3 if st0.tile_ms[tile] > 0 else None
+    achieved = per_unit * nodes / kt / 1e9 if kt else None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None, "traffic": profiled_traffic(args.workload),
+                "kernel": f"k_bt_apply<{st0.tile_cols},{'float' if es == 4 else 'double'},false> (batch operator + directions + dots, "
+                          f"{w['batch']} samples x 3 load cases; tile 32x{st0.tile_cols} chosen by the autotuner)",
+                "kernel_ms": kt * 1e3 if kt else None, "bytes_per_unit": per_unit, "units_per_launch": nodes,
+                "tile_ms_4_8_16": list(st0.tile_ms), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
+    node_its = float(sum(imgs[i].size * int(its[i].sum()) for i in range(len(imgs))))
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        exe = os.path.join(ROOT, "oracle", "_ref", "chfem_oracle_exec")
+        if os.path.exists(exe):
+            r = batch_cpu_rate(imgs, props, w, exe)
+            if r:
+                cpu = {"value": r[0] * node_its, "unit": "s", "cores": os.cpu_count() or 1, "kind": "port",
+                       "sample": f"oracle CPU FP64 PCG on the {r[2]} smallest samples, all load cases: "
+                                 f"{r[0]:.3e} s per node-iteration x {node_its:.3e} node-iterations of the batch"}
+    if rank == 0:
+        line = {"metric": metric_name(w), "value": step_s, "unit": "s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32+f64" if es == 4 else "f64", "data": "synthetic",
+                "config": config_dict(args, w, world) | {"samples": w["batch"], "nodes": nodes},
+                "iterations_max": int(its.max()), "iterations_mean": float(its.mean()),
+                "dof_iterations_per_s": node_its / step_s, "samples_per_s": world * w["batch"] / step_s,
+                "roofline": roofline, "clocks": clk, "gpu_launches": int(launches / max(1, args.steps)),
+                "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(3 * nodes),
+                        "d2h_bytes_per_step": int(w["batch"] * 9 * 8 + w["batch"] * 3 * 4),
+                        "path": "compute_conductivity_batch (images in host memory -> tensors)"},
+                "cpu_baseline": cpu}
+        print(json.dumps(line))
+
+
+def reference_batch(args, w):
+    """Reference arm of a batch workload: the reference's CUDA build run image by image (its only
+    way) on the smallest samples for a bounded time, scaled by node-iterations to the batch."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "chfem_exec_ref")
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference", "unavailable": "reference CUDA build oracle/_ref/chfem_exec_ref not built"}))
+        return
+    imgs, props = make_batch(w, 0)
+    from chfem_b200 import compute_conductivity_batch
+    C, its = compute_conductivity_batch(imgs, props, solver_tolerance=w["tol"], solver_maxiter=w["maxit"], precision="fp64",
+                                        return_iterations=True)
+    node_its = float(sum(imgs[i].size * int(its[i].sum()) for i in range(len(imgs))))
+    vals, walls = [], []
+    for _ in range(max(1, args.steps)):
+        r = batch_cpu_rate(imgs, props, w, exe, budget_s=30.0)
+        if not r:
+            print(json.dumps({"impl": "reference", "unavailable": "reference run failed"}))
+            return
+        vals.append(r[0] * node_its)
+        walls.append(r[1] * node_its)
+    v = float(np.mean(vals))
+    line = {"metric": metric_name(w), "value": v, "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference", "config": config_dict(args, w, 1) | {"samples": w["batch"]},
+            "cpu_baseline": {"value": v, "unit": "s", "cores": 0, "kind": "reference",
+                             "sample": f"reference CUDA build, one process per image, on the {r[2]} smallest samples, "
+                                       "its solver time per node-iteration scaled to the batch's node-iterations"},
+            "e2e": {"value": float(np.mean(walls)), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
 def reference_arm(args, w):
     exe = os.path.join(ROOT, "oracle", "_ref", "chfem_exec_ref")
     rank = int(os.environ.get("RANK", "0"))
@@ -312,10 +465,17 @@ def profiled_traffic(workload):
 
 
 def metric_name(w):
+    if "batch" in w:
+        return "time-to-tol 1e-6 (s): all samples x 3 load cases of the batch, device time"
     return "time-to-tol 1e-6 (s): all load cases of the workload, device time, model resident"
 
 
 def config_dict(args, w, n):
+    if "batch" in w:
+        return {"workload": args.workload, "samples": w["batch"], "edges": list(w["edges"]), "analysis": "thermal",
+                "load_cases": 3, "tol": w["tol"], "precision": w["precision"], "solver": "PCG", "preconditioner": "Jacobi",
+                "images": "overlapping balls r 4-8, vf U[0.1,0.5], k1/k0 log-U[2,100]",
+                "l2": "working set > L2 (the batch's vectors total GBs)", "parallelism": f"samples x{n}"}
     return {"workload": args.workload, "shape_zyx": list(w["shape"]), "analysis": ["thermal", "elastic", "stokes"][w["analysis"]],
             "load_cases": 6 if w["analysis"] == 1 else 3, "tol": w["tol"], "precision": w["precision"],
             "solver": "PMINRES" if w.get("solver", 0) == 1 else "PCG", "preconditioner": "Jacobi",
@@ -341,6 +501,10 @@ def main():
         devs = vis.split(",") if vis else [str(i) for i in range(64)]
         os.environ["CUDA_VISIBLE_DEVICES"] = devs[local]
     if args.impl == "reference":
+        if "batch" in w:
+            if rank == 0:
+                reference_batch(args, w)
+            return
         reference_arm(args, w)
         return
     dist = None
@@ -364,6 +528,11 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    if "batch" in w:
+        batch_main(args, w, world, rank, dist, allmax, barrier)
+        if dist:
+            dist.destroy_process_group()
+        return
     img = make_image(w, rank)
     wd = tempfile.mkdtemp()
     nf, raw = write_case(wd, w, img)

@@ -65,8 +65,31 @@ def chfem():
         lib.chfemB200UpdateC.argtypes = [c.c_int, c.c_void_p, c.c_void_p]
         lib.chfemB200Run.argtypes = [c.c_void_p, c.c_char_p, c.c_int, c.c_int, c.c_int, c.c_int, c.c_int, c.c_void_p]
         lib.chfemB200Run.restype = c.c_int
+        lib.chfemB200RunThermalBatch.argtypes = [c.c_uint, c.c_void_p, c.c_double, c.c_uint, c.c_int, c.c_void_p, c.c_void_p,
+                                                 c.c_void_p]
+        lib.chfemB200RunThermalBatch.restype = c.c_int
         lib._typed = True
     return lib
+
+
+class BatchStats(ctypes.Structure):
+    """Mirror of cudapcgB200BatchStats (include/cudapcg_b200.h)."""
+    _fields_ = [("setup_seconds", ctypes.c_double), ("solve_seconds", ctypes.c_double), ("wall_seconds", ctypes.c_double),
+                ("max_iterations", ctypes.c_uint), ("converged", ctypes.c_uint), ("kernel_launches", ctypes.c_ulonglong),
+                ("tile_cols", ctypes.c_int), ("ctas_operator", ctypes.c_int), ("ctas_pointwise", ctypes.c_int),
+                ("tile_ms", ctypes.c_double * 3)]
+
+
+def batch_stats():
+    st = BatchStats()
+    chfem().chfemB200LastBatchStats(ctypes.byref(st))
+    return st
+
+
+class ThermalSample(ctypes.Structure):
+    """Mirror of chfemB200ThermalSample (include/chfem_b200.h)."""
+    _fields_ = [("nx", ctypes.c_uint), ("ny", ctypes.c_uint), ("nz", ctypes.c_uint), ("voxels", ctypes.c_void_p),
+                ("nmat", ctypes.c_uint), ("colors", ctypes.c_uint8 * 4), ("conductivity", ctypes.c_double * 4)]
 
 
 class SolveStats(ctypes.Structure):

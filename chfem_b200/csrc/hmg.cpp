@@ -575,6 +575,62 @@ int chfemB200GetSolveStats(chfemB200SolveStats* out) {
   return 1;
 }
 
+static cudapcgB200BatchStats g_batch_stats;
+int chfemB200LastBatchStats(cudapcgB200BatchStats* out) {
+  if (!out) return 0;
+  *out = g_batch_stats;
+  return 1;
+}
+
+int chfemB200RunThermalBatch(unsigned int nsamples, const chfemB200ThermalSample* samples, double tol, unsigned int maxit,
+                             int precision, double* C_out, unsigned int* iterations, double* solve_seconds) {
+  g_err.clear();
+  if (!nsamples || !samples || !C_out) { fail("chfemB200RunThermalBatch: null argument"); return 0; }
+  for (unsigned s = 0; s < nsamples; s++) {
+    const chfemB200ThermalSample& t = samples[s];
+    if (!t.voxels || !t.nx || !t.ny || !t.nz) { fail("sample " + std::to_string(s) + ": empty image"); return 0; }
+    if (t.nmat < 1 || t.nmat > 4) { fail("sample " + std::to_string(s) + ": 1 to 4 materials"); return 0; }
+  }
+  // per sample: voxel material map, node keys and element matrices (the host model layer)
+  std::vector<Model> models(nsamples);
+  std::vector<int> ok(nsamples, 1);
+#pragma omp parallel for schedule(dynamic)
+  for (long s = 0; s < (long)nsamples; s++) {
+    const chfemB200ThermalSample& t = samples[s];
+    Model& m = models[s];
+    m.analysis = THERMAL; m.nd = 1; m.C_dim = 9; m.voxel = 1.0; m.refinement = 1; m.tol = tol; m.maxit = maxit;
+    m.nx = t.nx; m.ny = t.ny; m.nz = t.nz; m.nmat = t.nmat;
+    for (int c = 0; c < 256; c++) m.props_keys[c] = -1;
+    for (unsigned k = 0; k < t.nmat; k++) { m.props_keys[t.colors[k]] = (int)k; m.props[k] = t.conductivity[k]; }
+    std::string err;
+    if (!read_image(m, t.voxels, nullptr) || !build_maps(m, err)) { ok[s] = 0; continue; }
+    build_local_matrices(m);
+  }
+  for (unsigned s = 0; s < nsamples; s++)
+    if (!ok[s]) { if (g_err.empty()) fail("sample " + std::to_string(s) + ": image holds a colour outside its list"); return 0; }
+  std::vector<unsigned> dims(3 * nsamples), nmat(nsamples);
+  std::vector<const uint16_t*> keys(nsamples);
+  std::vector<const double*> K(nsamples), CB(nsamples);
+  for (unsigned s = 0; s < nsamples; s++) {
+    dims[3 * s] = models[s].ny; dims[3 * s + 1] = models[s].nx; dims[3 * s + 2] = models[s].nz;
+    nmat[s] = models[s].nmat; keys[s] = models[s].keys.data(); K[s] = models[s].Kdense.data(); CB[s] = models[s].CB.data();
+  }
+  std::vector<double> moments(9 * (size_t)nsamples);
+  cudapcgB200BatchStats& st = g_batch_stats;
+  const int rc = cudapcgB200SolveThermalBatch(nsamples, dims.data(), keys.data(), nmat.data(), K.data(), CB.data(), tol, maxit,
+                                              precision ? CHFEM_B200_MIXED : CHFEM_B200_FP64, 1, moments.data(), iterations,
+                                              nullptr, &st);
+  if (!rc) { fail(std::string("batch solve: ") + cudapcgB200BatchLastError()); return 0; }
+  if (solve_seconds) *solve_seconds = st.setup_seconds + st.solve_seconds;
+#pragma omp parallel for schedule(dynamic)
+  for (long s = 0; s < (long)nsamples; s++) {
+    Model& m = models[s];
+    for (int dir = 0; dir < 3; dir++) update_C_from_volume(m, dir, moments.data() + 9 * s + 3 * dir);
+    for (int t = 0; t < 9; t++) C_out[9 * s + t] = m.C[t];
+  }
+  return rc;
+}
+
 int chfemB200Run(const uint8_t* voxels, const char* nf, int direction, int solver, int precondition, int precision, int multirhs,
                  double* C_out) {
   if (!voxels || !nf || !C_out) { fail("chfemB200Run: null argument"); return 0; }

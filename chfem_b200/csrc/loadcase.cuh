@@ -104,7 +104,7 @@ __global__ void k_fl_rhs(long nV, long n, int dir, double w, double* b, T* r) {
 }
 
 // Stokes: out[j] = w_j * sum over pore nodes of the velocity component j.
-__global__ void __launch_bounds__(PW_NT) k_fl_moments(const double* x, long nV, double w0, double w1, double w2, RedCtl rc, double* out) {
+static __global__ void __launch_bounds__(PW_NT) k_fl_moments(const double* x, long nV, double w0, double w1, double w2, RedCtl rc, double* out) {
   __shared__ double sred[PW_NT / 32];
   double acc[3] = {0.0, 0.0, 0.0};
   for (long t = blockIdx.x * (long)PW_NT + threadIdx.x; t < nV; t += (long)gridDim.x * PW_NT) {

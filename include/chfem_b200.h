@@ -15,6 +15,7 @@
 #define CHFEM_B200_H
 
 #include <stdint.h>
+#include "cudapcg_b200.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -84,6 +85,27 @@ int chfemB200GetSolveStats(chfemB200SolveStats *out);
    and returns the tensor dimension (3 or 6), or 0 on error. */
 int chfemB200Run(const uint8_t *voxels, const char *nf, int direction, int solver, int precondition,
                  int precision, int multirhs, double *C_out);
+
+/* Batched thermal homogenization of many independent images (no counterpart in the reference,
+   which homogenizes one image per run): sample s is an nx*ny*nz uint8 image in C order of a
+   (z,y,x) array (the .raw layout), whose colours colors[0..nmat-1] have conductivities
+   conductivity[0..nmat-1] (nmat <= 4; unit voxel, NBN, PCG with Jacobi, L2 stopping test).  All
+   samples and their 3 load cases are solved together on the GPU (cudapcgB200SolveThermalBatch).
+   Fills C_out[9s..9s+8] (row-major 3x3 tensor of sample s) and, when not NULL,
+   iterations[3s + k].  precision: 0 FP64, 1 mixed.  Returns 1 when every load case converged,
+   2 when some stopped at maxit, 0 on error (chfemB200LastError). */
+typedef struct {
+  unsigned int nx, ny, nz;
+  const uint8_t *voxels;
+  unsigned int nmat;
+  uint8_t colors[4];
+  double conductivity[4];
+} chfemB200ThermalSample;
+int chfemB200RunThermalBatch(unsigned int nsamples, const chfemB200ThermalSample *samples, double tol,
+                             unsigned int maxit, int precision, double *C_out, unsigned int *iterations,
+                             double *solve_seconds);
+/* Statistics of the last chfemB200RunThermalBatch (the solver's cudapcgB200BatchStats). */
+int chfemB200LastBatchStats(cudapcgB200BatchStats *out);
 
 /* Parity access to the current model's maps and matrices (0 if unavailable).
    which: 0 node keys (uint16, N), 1 node->DOF map (uint32, N), 2 DOF->node map (uint32, nV+nB),

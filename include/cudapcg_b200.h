@@ -162,6 +162,36 @@ cudapcgFlag_t cudapcgB200SolveLoadCases(unsigned int nrhs, const int *axis, cons
                                         const double *CB, unsigned int ns, const double *const *x0, int x0_interpolate,
                                         double *moments, double *const *x_out, unsigned int *iterations,
                                         double *residuals);
+/* Batched thermal homogenization (no counterpart in the reference, which homogenizes one image
+   per run): nsamples independent periodic models of any sizes, each with its own 1..4
+   conductivities, solved together with all 3 load cases (X, Y, Z) of every sample; each load
+   case of each sample keeps its own PCG scalars and L2 stopping test (pcg.cu:100-224) and stops
+   on its own.  Sample s: dims[3s..3s+2] = nrows (y), ncols (x), nlayers (z); keys[s] its 16-bit
+   node keys (as cudapcgSetImage takes them, nrows*ncols*nlayers entries); Kdense[s] its nmat[s]
+   dense 8x8 conductivity matrices; CB[s] its nmat[s] 3x8 flux-averaging matrices (the host
+   layer's effective-tensor matrices).  The load-case right-hand sides are built on the device.
+   Out: moments[9s + 3k + row] = sum over voxels of (CB x_k)_row for load case k (add the face
+   term and divide by the voxel count for the tensor); iterations/residuals [3s + k] may be NULL.
+   precision CHFEM_B200_FP64 or CHFEM_B200_MIXED (FP32 fields; FP64 x, dots, replacement).
+   The operator's tile shape (32 x 4, 8 or 16 nodes) is timed once per batch signature and
+   remembered.  Returns 1 when every load case converged, 2 when some stopped at maxit, 0 on
+   error (cudapcgB200BatchLastError).  Independent of the cudapcgInit model. */
+typedef struct {
+  double setup_seconds;   /* device time of the initial pass */
+  double solve_seconds;   /* device time of the iterations and the tensor reduction */
+  double wall_seconds;    /* whole call, uploads included */
+  unsigned int max_iterations;
+  unsigned int converged; /* load cases that met the tolerance */
+  unsigned long long kernel_launches;
+  int tile_cols;          /* chosen tile: 32 x tile_cols nodes */
+  int ctas_operator, ctas_pointwise;
+  double tile_ms[3];      /* timed operator pass for tiles 32x4, 32x8, 32x16 (0 when cached) */
+} cudapcgB200BatchStats;
+int cudapcgB200SolveThermalBatch(unsigned int nsamples, const unsigned int *dims, const uint16_t *const *keys,
+                                 const unsigned int *nmat, const double *const *Kdense, const double *const *CB, double tol,
+                                 unsigned int maxit, int precision, int precondition, double *moments,
+                                 unsigned int *iterations, double *residuals, cudapcgB200BatchStats *stats);
+const char *cudapcgB200BatchLastError(void);
 /* Statistics of the last solve. */
 typedef struct {
   unsigned int iterations;

@@ -66,3 +66,19 @@ def test_cudapcg_rejects_out_of_scope():
     assert lib.cudapcgInit(0, 0) == 0            # 2D thermal
     assert b"2D" in lib.cudapcgB200LastError()
     assert lib.cudapcgInit(5, 1) == 0            # Stokes with EBE
+
+
+def test_batch_input_errors():
+    """compute_conductivity_batch rejects bad input before any GPU work."""
+    import numpy as np
+    from chfem_b200 import compute_conductivity_batch
+    img = np.zeros((4, 4, 4), np.uint8)
+    img[0, 0, 0] = 7
+    with pytest.raises(ValueError):
+        compute_conductivity_batch([img], {0: 1.0})            # colour 7 has no conductivity
+    with pytest.raises(ValueError):
+        compute_conductivity_batch([img], [{0: 1.0}, {0: 2.0}])  # one dict per image
+    with pytest.raises(ValueError):
+        compute_conductivity_batch([np.zeros((4, 4), np.uint8)], {0: 1.0})
+    with pytest.raises(ValueError):
+        compute_conductivity_batch([img], {0: 1.0, 7: 2.0}, precision="fp16")
