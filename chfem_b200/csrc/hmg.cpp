@@ -575,6 +575,15 @@ int chfemB200GetSolveStats(chfemB200SolveStats* out) {
   return 1;
 }
 
+int chfemB200UpdateCFromVolume(int direction, const double* volume, double* C_out) {
+  if (!g_m || !volume || !C_out) return 0;
+  const int nd = load_case_count(*g_m);
+  if (direction < 0 || direction >= nd) return 0;
+  update_C_from_volume(*g_m, direction, volume);
+  memcpy(C_out, g_m->C, sizeof(double) * g_m->C_dim);
+  return 1;
+}
+
 static cudapcgB200BatchStats g_batch_stats;
 int chfemB200LastBatchStats(cudapcgB200BatchStats* out) {
   if (!out) return 0;

@@ -117,6 +117,9 @@ int chfemB200CopyModelArray(int which, void *dst, unsigned long long bytes);
 int chfemB200AssembleRHS(int direction, double *dst);
 /* Effective-tensor column of load case `direction` from a solution x (ndof doubles). */
 int chfemB200UpdateC(int direction, const double *x, double *C_out);
+/* Effective-tensor column of load case `direction` from its volume term (the moments of
+   cudapcgB200SolveLoadCases) plus the host face term; copies the whole tensor to C_out. */
+int chfemB200UpdateCFromVolume(int direction, const double *volume, double *C_out);
 /* Model sizes: [nx, ny, nz, nelem, ndof, nV, nB, nmat, analysis] */
 int chfemB200ModelInfo(unsigned int *info9);
 
