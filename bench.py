@@ -41,6 +41,12 @@ WORKLOADS = {
     "elastic256_grf_mixed_block": dict(analysis=1, shape=(256, 256, 256), gen="grf", corr=6.0, fraction=0.40, seed=5000,
                                        props={0: (1.0, 0.30), 255: (10.0, 0.20)}, tol=1e-6, maxit=20000,
                                        precision="mixed", multirhs=True),
+    "elastic256_grf_mixed_block_learned": dict(analysis=1, shape=(256, 256, 256), gen="grf", corr=6.0, fraction=0.40,
+                                               seed=5000, props={0: (1.0, 0.30), 255: (10.0, 0.20)}, tol=1e-6,
+                                               maxit=20000, precision="mixed", multirhs=True, learned=True),
+    "elastic128_grf_mixed_block_learned": dict(analysis=1, shape=(128, 128, 128), gen="grf", corr=6.0, fraction=0.40,
+                                               seed=2000, props={0: (1.0, 0.30), 255: (10.0, 0.20)}, tol=1e-6,
+                                               maxit=20000, precision="mixed", multirhs=True, learned=True),
     "thermal64_spheres_fp64": dict(analysis=0, shape=(64, 64, 64), gen="spheres", vf=0.30, seed=1000,
                                    props={0: 1.0, 255: 10.0}, tol=1e-6, maxit=20000, precision="fp64"),
     "elastic128_grf_mixed_block": dict(analysis=1, shape=(128, 128, 128), gen="grf", corr=6.0, fraction=0.40, seed=2000,
@@ -63,7 +69,7 @@ WORKLOADS = {
     "thermal_batch512_fp64": dict(analysis=0, batch=512, edges=(32, 48, 64, 96), seed=4000, tol=1e-6, maxit=10000,
                                   precision="fp64"),
 }
-DEFAULT = "elastic128_grf_mixed_block"
+DEFAULT = "elastic128_grf_mixed_block_learned"
 
 
 def make_image(w, rank):
@@ -175,6 +181,8 @@ class Resident:
                  nkeys=info[7] if info[8] != 2 else 1, analysis=info[8], keys=arr(0, np.uint16),
                  dof_of_node=arr(1, np.uint32), node_of_dof=arr(2, np.uint32), border=arr(3, np.uint8),
                  lcl=arr(4, np.float64))
+        self.CB = arr(7, np.float64)
+        self.dims = (info[0], info[1], info[2])
         setup_model(self.c, a)
         self.c.cudapcgSetSolver(w.get("solver", 0))
         self.c.cudapcgSetPreconditioner(1)
@@ -215,6 +223,34 @@ class Resident:
             launches += st.kernel_launches
         return dev, its, launches
 
+    def step_learned(self, img, props):
+        """All six load cases from the trained network's guesses: device time of the network
+        (CUDA events on its stream) plus the block solve (cudapcgB200SolveLoadCases, device x0)."""
+        import torch
+        from chfem_b200 import learned
+        from chfem_b200._native import CudapcgStats
+        net = learned.default_net()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        xs = learned.device_guesses(net, img, props)
+        e1.record()
+        torch.cuda.synchronize()
+        t_net = e0.elapsed_time(e1) * 1e-3
+        P = ctypes.c_void_p * 6
+        axis = (ctypes.c_int * 6)(*learned.CASE_AXIS)
+        comp = (ctypes.c_int * 6)(*learned.CASE_COMP)
+        jump = (ctypes.c_double * 6)(*[float(self.dims[a]) for a in learned.CASE_AXIS])
+        vol = np.zeros(36)
+        its = (ctypes.c_uint * 6)()
+        res = (ctypes.c_double * 6)()
+        self.c.cudapcgB200SolveLoadCases(6, axis, comp, jump, self.CB.ctypes.data_as(ctypes.c_void_p), 6,
+                                         P(*[x.data_ptr() for x in xs]), 2, vol.ctypes.data_as(ctypes.c_void_p), None, its, res)
+        err = self.c.cudapcgB200LastError()
+        assert not err, err
+        st = CudapcgStats()
+        self.c.cudapcgB200GetStats(ctypes.byref(st))
+        return t_net + st.solve_seconds + st.setup_seconds, list(its), st.kernel_launches + 40, t_net
+
     def kernel_time(self, which, reps=20):
         self.c.cudapcgB200TimeKernel.restype = ctypes.c_double
         return self.c.cudapcgB200TimeKernel(which, reps)
@@ -227,6 +263,13 @@ class Resident:
 def e2e_step(img, nf, w):
     """One homogenization through the public API's native entry (compute_property's path)."""
     from chfem_b200 import _native
+    if w.get("learned"):
+        from chfem_b200 import compute_property
+        t0 = time.perf_counter()
+        C = np.array(compute_property("elasticity", img, mat_props=w["props"], voxel_size=1.0, solver_tolerance=w["tol"],
+                                      solver_maxiter=w["maxit"], precision=w["precision"], multirhs=True,
+                                      initial_guess="learned"))
+        return time.perf_counter() - t0, C, _native.solve_stats()
     lib = _native.chfem()
     lib.chfemB200SetQuiet(1)
     flat = np.ascontiguousarray(img.reshape(-1))
@@ -545,15 +588,27 @@ def main():
         t64, its64, _ = model.step()
         fp64 = {"time_s": t64, "iterations": its64}
         model.set_precision(w["precision"])
+    learned_run = bool(w.get("learned"))
+    net_times = []
+
+    def run_step():
+        if learned_run:
+            d, its_, l_, tn = model.step_learned(img, w["props"])
+            net_times.append(tn)
+            return d, its_, l_
+        return model.step(block)
+    zero_guess = None
+    if learned_run:  # the same block solve from the zero guess, for the iteration comparison
+        zero_guess = {"time_s": model.step(block)[0], "iterations": model.step(block)[1]}
     for _ in range(args.warmup):
-        model.step(block)
+        run_step()
     clocks = Clocks()
     barrier()
     clocks.start()
     t0 = time.perf_counter()
     dev_total, its, launches = 0.0, None, 0
     for _ in range(args.steps):
-        d, its, l = model.step(block)
+        d, its, l = run_step()
         dev_total += d
         launches += l
     wall = time.perf_counter() - t0
@@ -606,6 +661,16 @@ def main():
                          "tensor_update_s": st.update_seconds, "solver_call_total_s": st.total_seconds}
         e2e_times.append(t)
     e2e = allmax(min(e2e_times))
+    plain_e2e = None
+    if w.get("learned"):  # the plain method end to end: FP64, one load case at a time, zero guess
+        from chfem_b200 import _native as _nat
+        lib = _nat.chfem()
+        lib.chfemB200SetQuiet(1)
+        flat = np.ascontiguousarray(img.reshape(-1))
+        Cp = np.zeros(36)
+        t0 = time.perf_counter()
+        lib.chfemB200Run(flat.ctypes.data_as(ctypes.c_void_p), nf.encode(), 6, 0, 1, 0, 0, Cp.ctypes.data_as(ctypes.c_void_p))
+        plain_e2e = allmax(time.perf_counter() - t0)
     ncase = 6 if w["analysis"] == 1 else 3
     maps = 2 * model.N if w["analysis"] != 2 else 9 * model.N  # node keys, or the Stokes DOF maps
     if block:  # right-hand sides and tensor volume terms stay on the device
@@ -633,6 +698,12 @@ def main():
                         "path": "chfemB200Run (compute_property's native entry): image in host memory -> tensor",
                         "breakdown": breakdown},
                 "cpu_baseline": cpu, "samples_per_s": world / step_s}
+        if learned_run:
+            line["learned_guess"] = {"network_s": float(np.mean(net_times[-args.steps:])), "zero_guess_block": zero_guess,
+                                     "weights": "chfem_b200/weights/elastic_unet.bin"}
+            if plain_e2e is not None:
+                line["plain_fp64_e2e_s"] = plain_e2e
+                line["e2e_speedup_vs_plain_fp64"] = plain_e2e / e2e
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()

@@ -5,7 +5,9 @@ permeability, 'cg' otherwise), validation and error messages; a temporary .nf fi
 settings, the image is handed over flattened in C order, and the result is the list-of-rows
 tensor (3x3 conductivity / permeability, 6x6 stiffness).  The solve runs in chfem_b200's
 native host layer and GPU library.  Keyword-only extras (no counterpart in the reference):
-precision='fp64'|'mixed', multirhs.
+precision='fp64'|'mixed', multirhs (all load cases as one block solve), initial_guess='learned'
+(elasticity: the trained network's prediction of every load case's solution starts PCG; the
+tolerance and so the tensor are unchanged).
 """
 import ctypes
 import os
@@ -19,7 +21,7 @@ from .io import export_for_chfem
 
 def compute_property(property, array, mat_props=None, voxel_size=1e-6, solver=None, solver_tolerance=1e-6,
                      solver_maxiter=10000, precondition=True, type_of_rhs=0, refinement=1, direction='all',
-                     output_fields=None, nf_filepath=None, *, precision='fp64', multirhs=False):
+                     output_fields=None, nf_filepath=None, *, precision='fp64', multirhs=False, initial_guess=None):
     properties = {'conductivity': 0, 'elasticity': 1, 'permeability': 2}
     if property not in properties:
         raise ValueError(f"Invalid property: {property}")
@@ -64,9 +66,25 @@ def compute_property(property, array, mat_props=None, voxel_size=1e-6, solver=No
                          export_nf=True, solver_tolerance=solver_tolerance, solver_maxiter=solver_maxiter,
                          tmp_nf_file=tmp)
         nf_filename = tmp.name
+    guesses = None
+    if initial_guess not in (None, 'zero', 'learned'):
+        raise ValueError(f"Invalid initial_guess: {initial_guess}")
+    if initial_guess == 'learned':
+        # the trained network's prediction of every load case's solution (elasticity only)
+        if property != 'elasticity':
+            raise ValueError("initial_guess='learned' is provided for elasticity")
+        if mat_props is None:
+            raise ValueError("initial_guess='learned' needs mat_props")
+        if refinement != 1 or any(n % 8 for n in np.shape(array)):
+            raise ValueError("initial_guess='learned' needs refinement 1 and every axis divisible by 8")
+        from . import learned
+        guesses = learned.device_guesses(learned.default_net(), array, mat_props)
     try:
         flat = np.ascontiguousarray(np.reshape(array, array.size), dtype=np.uint8)
         lib = _native.chfem()
+        if guesses is not None:
+            P = ctypes.c_void_p * 6
+            lib.chfemB200SetInitialGuesses(6, P(*[g.data_ptr() for g in guesses]), 1)
         C = np.zeros(36, dtype=np.float64)
         n = lib.chfemB200Run(flat.ctypes.data_as(ctypes.c_void_p), nf_filename.encode(), direction_int, solver_type,
                              int(bool(precondition)), 1 if precision == 'mixed' else 0, int(bool(multirhs)),

@@ -439,7 +439,7 @@ static bool moments_on_device(const LoadCases& lc, int nr) {
 }
 
 template <typename T>
-static bool solve_block_T(int nr, const double* const* rhs, const double* const* x0, bool x0_interp, double* const* x_out,
+static bool solve_block_T(int nr, const double* const* rhs, const double* const* x0, int x0_mode, double* const* x_out,
                           unsigned* iters, double* resid, const LoadCases* lc = nullptr) {
   if (!ensure_vectors<T>() || !ensure_K<T>() || !block_alloc<T>(nr)) return false;
   const long n = S->nvars;
@@ -452,8 +452,8 @@ static bool solve_block_T(int nr, const double* const* rhs, const double* const*
       else k_convert<double, float><<<pw_grid(n), PW_NT, 0, S->stream>>>(slice<double>(B->b64, k), slice<float>(B->r, k), n);
     }
     if (x0 && x0[k]) {
-      if (x0_interp) { if (!interp_into(x0[k], slice<double>(B->x, k))) return false; }
-      else CKV(cudaMemcpyAsync(slice<double>(B->x, k), x0[k], n * 8, cudaMemcpyHostToDevice, S->stream));
+      if (x0_mode == 1) { if (!interp_into(x0[k], slice<double>(B->x, k))) return false; }
+      else CKV(cudaMemcpyAsync(slice<double>(B->x, k), x0[k], n * 8, x0_mode == 2 ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, S->stream));
       has_x0[k] = true;
     }
     else CKV(cudaMemsetAsync(slice<double>(B->x, k), 0, n * 8, S->stream));

@@ -761,6 +761,13 @@ template <typename T>
 static bool interp_x0(const double* coarse_host) { return interp_into(coarse_host, S->x); }
 extern "C" {
 
+cudapcgFlag_t cudapcgB200SetX0Device(const double* x0) {
+  if (!S || !S->model || !x0) return CUDAPCG_FALSE;
+  if (!ensure_vectors_current()) return CUDAPCG_FALSE;
+  CK(cudaMemcpy(S->x, x0, S->nvars * 8, cudaMemcpyDeviceToDevice));
+  S->x0_set = true;
+  return CUDAPCG_TRUE;
+}
 cudapcgFlag_t cudapcgSetX0(cudapcgVar_t* x0, cudapcgFlag_t mustInterpolate) {
   if (!S || !S->model) return CUDAPCG_FALSE;
   if (!x0) {  // cudapcg.cu:298-309
@@ -1084,8 +1091,8 @@ extern "C" cudapcgFlag_t cudapcgB200SolveLoadCases(unsigned int nrhs, const int*
   S->launches = 0;
   const LoadCases lc{axis, comp, jump, CB, ns, moments};
   bool ok = (S->precision == CHFEM_B200_FP64)
-                ? solve_block_T<double>((int)nrhs, nullptr, x0, x0_interpolate != 0, x_out, iterations, residuals, &lc)
-                : solve_block_T<float>((int)nrhs, nullptr, x0, x0_interpolate != 0, x_out, iterations, residuals, &lc);
+                ? solve_block_T<double>((int)nrhs, nullptr, x0, x0_interpolate, x_out, iterations, residuals, &lc)
+                : solve_block_T<float>((int)nrhs, nullptr, x0, x0_interpolate, x_out, iterations, residuals, &lc);
   S->total_time = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   S->mean_time = S->iteration ? S->solve_dev_s / S->iteration : 0.0;
   if (!ok) { S->found = 0; return CUDAPCG_FALSE; }
@@ -1105,8 +1112,8 @@ extern "C" cudapcgFlag_t cudapcgB200SolveBlock(unsigned int nrhs, const double* 
   const auto t0 = std::chrono::steady_clock::now();
   S->count++;
   S->launches = 0;
-  bool ok = (S->precision == CHFEM_B200_FP64) ? solve_block_T<double>((int)nrhs, rhs, x0, x0_interpolate != 0, x_out, iterations, residuals)
-                                             : solve_block_T<float>((int)nrhs, rhs, x0, x0_interpolate != 0, x_out, iterations, residuals);
+  bool ok = (S->precision == CHFEM_B200_FP64) ? solve_block_T<double>((int)nrhs, rhs, x0, x0_interpolate, x_out, iterations, residuals)
+                                             : solve_block_T<float>((int)nrhs, rhs, x0, x0_interpolate, x_out, iterations, residuals);
   S->total_time = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   S->mean_time = S->iteration ? S->solve_dev_s / S->iteration : 0.0;
   if (!ok) { S->found = 0; return CUDAPCG_FALSE; }

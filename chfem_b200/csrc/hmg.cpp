@@ -36,6 +36,9 @@ int g_recursions = 0;
 // (prolonged by the library, cudapcgSetX0(x0, 1)); empty where none was found
 std::vector<double> g_x0_coarse[6];
 bool g_have_coarse = false;
+// caller-provided initial guesses for the next homogenization (chfemB200SetInitialGuesses)
+const double* g_x0_user[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+int g_x0_user_device = 0;
 bool g_report = false;
 std::string g_report_text;
 chfemB200SolveStats g_stats;
@@ -413,11 +416,15 @@ void hmgSolveHomogenization(void) {
           fclose(f);
           px0[k] = x0s[k].data();
         }
+      } else if (g_x0_user[dirs[k]]) {
+        px0[k] = g_x0_user[dirs[k]];
       } else if (g_have_coarse && !g_x0_coarse[dirs[k]].empty()) {
         px0[k] = g_x0_coarse[dirs[k]].data();
       }
     }
-    const int interp = (g_use_x0 && !g_x0_file.empty()) ? 0 : (g_have_coarse ? 1 : 0);
+    bool any_user = false;
+    for (int k = 0; k < nd; k++) any_user = any_user || g_x0_user[dirs[k]];
+    const int interp = (g_use_x0 && !g_x0_file.empty()) ? 0 : (any_user ? (g_x0_user_device ? 2 : 0) : (g_have_coarse ? 1 : 0));
     const unsigned ns = m.analysis == ELASTIC ? 6 : 3;
     SAY("    ------------------------------------------------------\n    Block solve of %d load cases (", nd);
     for (int k = 0; k < nd; k++) SAY("%s%s", k ? ", " : "", DIR_STR[dirs[k]]);
@@ -471,9 +478,14 @@ void hmgSolveHomogenization(void) {
         fclose(f);
         cudapcgSetX0(x0.data(), 0);
       }
+    } else if (g_x0_user[dir]) {
+      if (g_x0_user_device) cudapcgB200SetX0Device(g_x0_user[dir]);
+      else cudapcgSetX0((double*)g_x0_user[dir], 0);
     } else if (g_have_coarse) {  // femhmg.c:1048-1050: the recursive guess, prolonged
       if (!g_x0_coarse[dir].empty()) { SAY("    | Interpolating initial guess...\n"); cudapcgSetX0(g_x0_coarse[dir].data(), 1); }
       else cudapcgSetX0(nullptr, 0);
+    } else {
+      cudapcgSetX0(nullptr, 0);  // no guess for this case: not the previous case's
     }
     SAY("    Solving system of equations...\n");
     cudapcgSolve(x.data());
@@ -502,6 +514,7 @@ void hmgSolveHomogenization(void) {
   cudapcgSetX0(nullptr, 0);
   cudapcgFreeArrays();
   cudapcgEnd();
+  for (auto& p : g_x0_user) p = nullptr;  // used once
   g_stats.total_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_all).count();
   SAY("    ------------------------------------------------------\nDone.(%.2e s)\n", g_stats.total_seconds);
 }
@@ -572,6 +585,13 @@ const char* chfemB200LastError(void) { return g_err.c_str(); }
 int chfemB200GetSolveStats(chfemB200SolveStats* out) {
   if (!out) return 0;
   *out = g_stats;
+  return 1;
+}
+
+int chfemB200SetInitialGuesses(int ncases, const double* const* x0, int on_device) {
+  if (ncases < 0 || ncases > 6 || (ncases && !x0)) return 0;
+  for (int k = 0; k < 6; k++) g_x0_user[k] = (k < ncases) ? x0[k] : nullptr;
+  g_x0_user_device = on_device ? 1 : 0;
   return 1;
 }
 

@@ -298,6 +298,25 @@ __global__ void k_features(const uint8_t* img, long img_ns, long S, const float*
   }
 }
 
+// Initial guesses from the network output: x_k[node * 3 + comp] = out[3k + comp][node] plus, on
+// the displaced component of load case k, its macroscopic ramp (col for x, (R - row) mod R for y,
+// (L - layer) mod L for z; node = row + col R + layer R C).
+struct GuessPtrs { double* x[6]; };
+__global__ void k_assemble_guess(const float* out, int L, int C, int R, GuessPtrs xs) {
+  const long S = (long)L * C * R;
+  const int AX[6] = {0, 1, 2, 1, 2, 1}, CO[6] = {0, 1, 2, 2, 0, 0};
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < S; i += (long)gridDim.x * blockDim.x) {
+    const int r = (int)(i % R), c = (int)((i / R) % C), l = (int)(i / ((long)R * C));
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      const double ramp = AX[k] == 0 ? (double)c : (AX[k] == 1 ? (double)((R - r) % R) : (double)((L - l) % L));
+#pragma unroll
+      for (int comp = 0; comp < 3; comp++)
+        xs.x[k][3 * i + comp] = (double)out[(long)(3 * k + comp) * S + i] + (comp == CO[k] ? ramp : 0.0);
+    }
+  }
+}
+
 int grid1(long n) { long g = (n + 255) / 256; return (int)(g < 1 ? 1 : (g > 65535 ? 65535 : g)); }
 bool check(const char* who) {
   const cudaError_t e = cudaPeekAtLastError();
@@ -391,6 +410,16 @@ int chfemB200NnAdam(float* p, const float* g, float* m, float* v, long n, float 
 int chfemB200NnFeatures(const uint8_t* img, long img_ns, long S, const float* table, int F, float* out, long out_ns, int N, void* stream) {
   k_features<<<grid1(S * N), 256, 0, (cudaStream_t)stream>>>(img, img_ns, S, table, F, out, out_ns, N);
   return check("chfemB200NnFeatures") ? 1 : 0;
+}
+
+// The six elastic initial-guess vectors (device, 3 L C R doubles each) from the network's output
+// [18][L][C][R] (device).
+int chfemB200NnAssembleGuess(const float* out, int L, int C, int R, double* const* x, void* stream) {
+  if (!out || !x) { g_err = "chfemB200NnAssembleGuess: null argument"; return 0; }
+  GuessPtrs p;
+  for (int k = 0; k < 6; k++) { if (!x[k]) { g_err = "chfemB200NnAssembleGuess: null vector"; return 0; } p.x[k] = x[k]; }
+  k_assemble_guess<<<grid1((long)L * C * R), 256, 0, (cudaStream_t)stream>>>(out, L, C, R, p);
+  return check("chfemB200NnAssembleGuess") ? 1 : 0;
 }
 
 }  // extern "C"

@@ -297,6 +297,32 @@ def fluctuation(xs, shape_lcr):
     return out
 
 
+_NET = {}
+
+
+def default_net():
+    """The committed trained network (loaded once)."""
+    if "net" not in _NET:
+        _NET["net"] = Net.load(DEFAULT_WEIGHTS)
+    return _NET["net"]
+
+
+def device_guesses(net, img, props):
+    """The six initial-guess vectors for one image as FP64 CUDA tensors (network forward pass
+    and the ramps assembled on the device; nothing crosses to the host)."""
+    import torch
+    lib = _lib()
+    feat = features([img], [props])
+    out = net.forward(feat)
+    L, C, R = out.shape[2:]
+    xs = [torch.empty(3 * L * C * R, dtype=torch.float64, device="cuda") for _ in range(6)]
+    P = ctypes.c_void_p * 6
+    lib.chfemB200NnAssembleGuess.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                             ctypes.c_void_p]
+    _ok(lib.chfemB200NnAssembleGuess(ptr(out), L, C, R, P(*[x.data_ptr() for x in xs]), _stream()))
+    return xs
+
+
 def initial_guesses(net, img, props, device="cuda"):
     """The six initial-guess vectors (chfem layout, float64 host arrays) for one image."""
     feat = features([img], [props], device)

@@ -117,6 +117,11 @@ int chfemB200CopyModelArray(int which, void *dst, unsigned long long bytes);
 int chfemB200AssembleRHS(int direction, double *dst);
 /* Effective-tensor column of load case `direction` from a solution x (ndof doubles). */
 int chfemB200UpdateC(int direction, const double *x, double *C_out);
+/* Initial guesses for the next hmgSolveHomogenization / chfemB200Run (used once, then cleared):
+   x0[k] for load case k (k < ncases; NULL entries start from zero), nvars doubles each, in host
+   memory or (on_device) device memory that stays valid until the solve returns.  They take
+   the place of the recursive coarse-grid guesses (-r); an -xi file still takes precedence. */
+int chfemB200SetInitialGuesses(int ncases, const double *const *x0, int on_device);
 /* Effective-tensor column of load case `direction` from its volume term (the moments of
    cudapcgB200SolveLoadCases) plus the host face term; copies the whole tensor to C_out. */
 int chfemB200UpdateCFromVolume(int direction, const double *volume, double *C_out);

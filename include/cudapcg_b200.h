@@ -138,8 +138,9 @@ cudapcgFlag_t cudapcgB200ApplyOperator(const double *x, double *y);
 cudapcgFlag_t cudapcgB200ApplyPreconditioner(const double *x, double *y);
 /* Block solve of nrhs load cases of the current model at once (3 for thermal, 3 or 6 for
    elastic; CG/PCG): rhs[k], x_out[k] are host buffers of nvars doubles, x0 may be NULL or hold
-   NULL entries; with x0_interpolate set, each x0[k] is a solution on the model coarsened by 2
-   per axis and is prolonged as cudapcgSetX0(x0, 1) does.  Each right-hand side runs the
+   NULL entries; x0_interpolate: 0 each x0[k] is a host vector of nvars doubles, 1 a host
+   solution on the model coarsened by 2 per axis, prolonged as cudapcgSetX0(x0, 1) does, 2 a
+   device vector of nvars doubles.  Each right-hand side runs the
    recurrence and stopping test of cudapcgSolve; the operator reads the model once per block
    apply.  iterations/residuals (nrhs entries) may be NULL.  Returns 1 when every right-hand
    side met the tolerance. */
@@ -192,6 +193,9 @@ int cudapcgB200SolveThermalBatch(unsigned int nsamples, const unsigned int *dims
                                  unsigned int maxit, int precision, int precondition, double *moments,
                                  unsigned int *iterations, double *residuals, cudapcgB200BatchStats *stats);
 const char *cudapcgB200BatchLastError(void);
+/* Initial guess of the next cudapcgSolve from a device vector of nvars doubles (the device
+   counterpart of cudapcgSetX0(x0, 0); cleared by cudapcgSetX0(NULL, 0)). */
+cudapcgFlag_t cudapcgB200SetX0Device(const double *x0);
 /* Statistics of the last solve. */
 typedef struct {
   unsigned int iterations;

@@ -84,3 +84,22 @@ def test_trained_guess_gains_iterations():
     C1, its1, _, _ = L.solve_elastic(img, props, tol=1e-8, precision="fp64", x0=x0, want_x=False)
     assert H.rel_to_max(C1, C0) < 1e-6
     assert sum(its1) < 0.9 * sum(its0), (its1, its0)
+
+
+@pytest.mark.parametrize("multirhs", [True, False])
+def test_compute_property_with_learned_guess(multirhs):
+    """compute_property(initial_guess='learned') returns the zero-guess tensor (both solve
+    paths take the device-resident guesses)."""
+    from chfem_b200 import compute_property
+    from chfem_b200 import learned as L
+    from chfem_b200 import synthetic
+    if not os.path.exists(L.DEFAULT_WEIGHTS):
+        pytest.skip("no trained weights committed")
+    img = synthetic.grf((40, 48, 32), corr=6.0, fraction=0.4, seed=4242)
+    props = {0: (1.0, 0.30), 255: (20.0, 0.20)}
+    kw = dict(mat_props=props, solver_tolerance=1e-8, solver_maxiter=20000, multirhs=multirhs)
+    C0 = np.array(compute_property("elasticity", img, **kw))
+    C1 = np.array(compute_property("elasticity", img, initial_guess="learned", **kw))
+    assert H.rel_to_max(C1, C0) < 1e-6
+    with pytest.raises(ValueError):
+        compute_property("elasticity", img[:, :, :30], initial_guess="learned", **kw)
