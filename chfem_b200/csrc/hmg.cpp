@@ -386,7 +386,11 @@ void hmgSolveHomogenization(void) {
   else { nd = load_case_count(m); load_case_list(m, dirs); }
   for (unsigned i = 0; i < m.C_dim; i++) m.C[i] = 0.0;
   SAY("Running homogenization...\n");
-  if (!setup_solver(m)) return;
+  {
+    const auto ts = std::chrono::steady_clock::now();
+    if (!setup_solver(m)) return;
+    g_stats.setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count();
+  }
   std::vector<double> x, x0;
   g_stats.n_cases = nd;
   g_stats.ndof = (unsigned)m.ndof;

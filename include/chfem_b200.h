@@ -76,6 +76,7 @@ typedef struct {
   double total_seconds;      /* wall time of hmgSolveHomogenization */
   unsigned long long kernel_launches;
   unsigned int ndof;
+  double setup_seconds;      /* host wall time of the solver set-up (context, uploads, allocations) */
 } chfemB200SolveStats;
 int chfemB200GetSolveStats(chfemB200SolveStats *out);
 
