@@ -46,24 +46,35 @@ struct MrCfg {
   long nhmg;
 };
 
-// Work schedule of a stencil pass.  The column tiles (TE_TR x TE_TC nodes) times the layers
-// form one line w = tile * L + layer; CTA b of a 1D grid of P CTAs takes the slice
-// [b W / P, (b+1) W / P) and walks it as runs of consecutive layers of one tile (restaging
-// its halo planes at each run start).  P is the number of CTAs that fit on the GPU at once,
-// so every CTA gets the same share of the work and the pass runs in a single wave.
+// Work schedule of a stencil pass.  The work is every (column tile of TE_TR x TE_TC nodes,
+// layer) unit; a 1D grid of P CTAs -- as many as fit on the GPU at once -- takes equal slices of
+// one line of those units, so the pass runs in a single wave of equal shares.  The line is
+// ordered chunk by chunk: layer chunks of lc = ceil(L tiles / P) layers, within a chunk tile by
+// tile, within a tile layer by layer.  A CTA's slice is then about one (tile, chunk) run, and the
+// CTAs that run at the same time cover neighbouring tiles over the same layers, so the halo
+// planes they share are read from L2 rather than DRAM.
 constexpr int TE_MIN_RUN = 4;  // layers per CTA at least (halo restaging overhead)
 struct TeWork {
-  int tiles_r, L;
-  long W;
-  __device__ TeWork(int R, int C, int L_) : tiles_r((R + TE_TR - 1) / TE_TR), L(L_),
-      W((long)((R + TE_TR - 1) / TE_TR) * ((C + TE_TC - 1) / TE_TC) * L_) {}
+  int tiles_r, L, lc, nc;
+  long tiles, W;
+  __device__ TeWork(int R, int C, int L_) : tiles_r((R + TE_TR - 1) / TE_TR), L(L_) {
+    tiles = (long)tiles_r * ((C + TE_TC - 1) / TE_TC);
+    W = tiles * L;
+    const long P = gridDim.x;
+    lc = (int)min((long)L, max(1L, (W + P - 1) / P));
+    nc = (L + lc - 1) / lc;
+  }
   __device__ long begin() const { return (long)blockIdx.x * W / gridDim.x; }
   __device__ long end() const { return ((long)blockIdx.x + 1) * W / gridDim.x; }
-  // the run starting at w: tile origin (r0, c0) and layers [l0, l1)
+  // the run starting at unit w: tile origin (r0, c0) and layers [l0, l1), not past unit w_end
   __device__ void run(long w, long w_end, int& r0, int& c0, int& l0, int& l1) const {
-    const long tile = w / L;
-    l0 = (int)(w % L);
-    l1 = (int)min((long)L, (long)l0 + (w_end - w));
+    const long per_full = (long)lc * tiles;
+    const int c = (int)min((long)nc - 1, w / per_full);
+    const int size = min(lc, L - c * lc);  // layers in this chunk
+    const long rem = w - (long)c * per_full;
+    const long tile = rem / size;
+    l0 = c * lc + (int)(rem % size);
+    l1 = (int)min((long)c * lc + size, (long)l0 + (w_end - w));
     r0 = (int)(tile % tiles_r) * TE_TR;
     c0 = (int)(tile / tiles_r) * TE_TC;
   }
