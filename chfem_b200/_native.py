@@ -65,6 +65,7 @@ def chfem():
         lib.chfemB200UpdateC.argtypes = [c.c_int, c.c_void_p, c.c_void_p]
         lib.chfemB200Run.argtypes = [c.c_void_p, c.c_char_p, c.c_int, c.c_int, c.c_int, c.c_int, c.c_int, c.c_void_p]
         lib.chfemB200Run.restype = c.c_int
+        lib.chfemB200SetExportFields.argtypes = [c.c_int]
         lib.chfemB200RunThermalBatch.argtypes = [c.c_uint, c.c_void_p, c.c_double, c.c_uint, c.c_int, c.c_void_p, c.c_void_p,
                                                  c.c_void_p]
         lib.chfemB200RunThermalBatch.restype = c.c_int

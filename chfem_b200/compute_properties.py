@@ -7,7 +7,10 @@ tensor (3x3 conductivity / permeability, 6x6 stiffness).  The solve runs in chfe
 native host layer and GPU library.  Keyword-only extras (no counterpart in the reference):
 precision='fp64'|'mixed', multirhs (all load cases as one block solve), initial_guess='learned'
 (elasticity: the trained network's prediction of every load case's solution starts PCG; the
-tolerance and so the tensor are unchanged).
+tolerance and so the tensor are unchanged).  output_fields=prefix writes, per load case, the
+solution and its field as <prefix>_temperature|displacement|velocity_<case>.bin and
+<prefix>_flux|stress|pressure_<case>.bin (read them with import_*_field_from_chfem), like
+chfem_exec -e.
 """
 import ctypes
 import os
@@ -34,13 +37,14 @@ def compute_property(property, array, mat_props=None, voxel_size=1e-6, solver=No
     if thermal_expansion:
         raise ValueError("Thermal expansion analysis is not provided by chfem_b200.")
     output_fields_flag = 1 if output_fields is not None else 0
-    if output_fields_flag:
-        raise ValueError("Field export is not provided by chfem_b200 yet.")
     if solver is None:
         solver = 'minres' if property == 'permeability' else 'cg'
     solvers = {'cg': 0, 'minres': 1, 'cg3': 2, 'minres3': 3, 'cg2': 4, 'minres2': 5}
     if solver not in solvers:
         raise ValueError(f"Invalid solver type: {solver}")
+    if solver in ('cg2', 'minres2') and (output_fields_flag or property != 'permeability'):
+        raise ValueError(f"Invalid solver type: {solver}. Two-vectors solvers do not produce fields to be exported, "
+                         "nor are implemented for conductivy or elasticity analyses.")
     if solver in ('cg2', 'minres2'):
         raise ValueError(f"Invalid solver type: {solver}. The two-vector solvers are not provided by chfem_b200.")
     solver_type = solvers[solver]
@@ -60,7 +64,14 @@ def compute_property(property, array, mat_props=None, voxel_size=1e-6, solver=No
             raise ValueError("Domain must be uint8 dtype.")
         if 0 not in np.unique(array):  # the reference checks this for every property (compute_properties.py:105-107)
             raise ValueError("No fluid phase found in the domain.")
-        tmp = tempfile.NamedTemporaryFile(delete=False, suffix=".nf")
+        if output_fields is None:
+            tmp = tempfile.NamedTemporaryFile(delete=False, suffix=".nf")
+        else:
+            # the fields are written beside the .nf file: <output_fields>_temperature_<case>.bin, ...
+            path, _ = os.path.split(output_fields)
+            if path != '' and not os.path.exists(path):
+                raise ValueError(f"Output fields directory {path} does not exist.")
+            tmp = open(output_fields + ".nf", 'wb')
         export_for_chfem(None, array, analysis_type=analysis_type, mat_props=mat_props, voxel_size=voxel_size,
                          solver_type=solver_type, rhs_type=type_of_rhs, refinement=refinement, export_raw=False,
                          export_nf=True, solver_tolerance=solver_tolerance, solver_maxiter=solver_maxiter,
@@ -82,6 +93,7 @@ def compute_property(property, array, mat_props=None, voxel_size=1e-6, solver=No
     try:
         flat = np.ascontiguousarray(np.reshape(array, array.size), dtype=np.uint8)
         lib = _native.chfem()
+        lib.chfemB200SetExportFields(output_fields_flag)
         if guesses is not None:
             P = ctypes.c_void_p * 6
             lib.chfemB200SetInitialGuesses(6, P(*[g.data_ptr() for g in guesses]), 1)

@@ -23,6 +23,7 @@
 #include "stencil_block.cuh"
 #include "stencil_fluid_block.cuh"
 #include "loadcase.cuh"
+#include "fields.cuh"
 #include "minres.cuh"
 
 using namespace chfem;
@@ -1068,6 +1069,32 @@ unsigned long long cudapcgB200DeviceBytes(void) {
 }
 
 }  // extern "C"
+
+extern "C" cudapcgFlag_t cudapcgB200ComputeFields(int block_index, int axis, int comp, double jump, const double* props,
+                                                  double* field_out) {
+  const char* who = "cudapcgB200ComputeFields";
+  if (!S || !S->model || !props || !field_out) { set_err(who, "bad arguments"); return CUDAPCG_FALSE; }
+  if (S->analysis == CUDAPCG_FLUID_3D) { set_err(who, "Stokes fields are the solution itself (velocity, pressure)"); return CUDAPCG_FALSE; }
+  if (axis < 0 || axis > 2 || comp < 0 || comp >= S->nd) { set_err(who, "bad load case"); return CUDAPCG_FALSE; }
+  const double* x = nullptr;
+  if (block_index < 0) x = S->x;
+  else if (B && block_index < B->nr) x = (const double*)B->x + (size_t)block_index * S->nvars;
+  if (!x) { set_err(who, "no solution on the device"); return CUDAPCG_FALSE; }
+  FieldProps fp{};
+  const int np = S->nd == 1 ? S->nmat : 2 * S->nmat;
+  for (int i = 0; i < np && i < 8; i++) fp.p[i] = props[i];
+  const int nf = S->nd == 1 ? 3 : 6;
+  double* d_out = nullptr;
+  CK(cudaMalloc(&d_out, sizeof(double) * nf * S->N));
+  if (S->nd == 1) k_nodal_fields<1><<<pw_grid(S->N), PW_NT, 0, S->stream>>>(S->d_keys, x, S->R, S->C, S->L, axis, comp, jump, fp, d_out);
+  else k_nodal_fields<3><<<pw_grid(S->N), PW_NT, 0, S->stream>>>(S->d_keys, x, S->R, S->C, S->L, axis, comp, jump, fp, d_out);
+  cudaError_t e = cudaPeekAtLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(field_out, d_out, sizeof(double) * nf * S->N, cudaMemcpyDeviceToHost, S->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
+  cudaFree(d_out);
+  if (e != cudaSuccess) { set_err(who, cudaGetErrorString(e)); return CUDAPCG_FALSE; }
+  return CUDAPCG_TRUE;
+}
 
 extern "C" cudapcgFlag_t cudapcgB200SolveLoadCases(unsigned int nrhs, const int* axis, const int* comp, const double* jump,
                                                    const double* CB, unsigned int ns, const double* const* x0, int x0_interpolate,

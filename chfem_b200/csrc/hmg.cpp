@@ -29,6 +29,8 @@ int g_poremap = CUDAPCG_POREMAP_NUM;
 int g_precision = CHFEM_B200_PREC_FP64, g_multirhs = 0, g_quiet = 0;
 int g_dir_set = 0, g_dir = 6;
 bool g_export_x = false;
+bool g_export_fields = false;
+
 std::string g_x0_file;
 bool g_use_x0 = false;
 int g_recursions = 0;
@@ -48,6 +50,43 @@ chfemB200SolveStats g_stats;
 void fail(const std::string& e) {
   g_err = e;
   fprintf(stderr, "chfem_b200: %s\n", e.c_str());
+}
+
+// -e (femhmg.c:1112-1118): the solution and its field per load case, as the reference writes
+// them -- thermal <nf>_temperature_<dir>.bin and _flux_ (3 per node); elastic _displacement_ and
+// _stress_ (6 per node); Stokes _velocity_ (3 per node, pore nodes) and _pressure_ (fluid nodes).
+// block_index: the block solve's right-hand side holding this case (-1: the last single solve).
+void write_bin(const std::string& fn, const double* v, size_t n) {
+  FILE* f = fopen(fn.c_str(), "wb");
+  if (!f) { SAY("WARNING: cannot write %s\n", fn.c_str()); return; }
+  fwrite(v, sizeof(double), n, f);
+  fclose(f);
+}
+void export_fields(const Model& m, int dir, const double* x, int block_index) {
+  const std::string pre = m.nf_noext + "_";
+  const std::string suf = "_" + std::to_string(dir) + ".bin";
+  if (m.analysis == FLUID) {  // femhmg_fluid_3D.c:312-360
+    std::vector<double> u(3 * (size_t)m.N, 0.0), p(m.N, 0.0);
+    for (long n = 0; n < m.N; n++) {
+      const uint32_t id = m.dof_of_node[n];
+      const uint8_t fk = m.fluid_keys[n];
+      if (fk == 255) { u[3 * n] = x[3 * (size_t)id]; u[3 * n + 1] = x[3 * (size_t)id + 1]; u[3 * n + 2] = x[3 * (size_t)id + 2]; }
+      if (fk) p[n] = x[3 * (size_t)m.nV + id];
+    }
+    write_bin(pre + "velocity" + suf, u.data(), u.size());
+    write_bin(pre + "pressure" + suf, p.data(), p.size());
+    return;
+  }
+  write_bin(pre + (m.analysis == THERMAL ? "temperature" : "displacement") + suf, x, m.ndof);
+  int axis, comp;
+  case_axis(m, dir, axis, comp);
+  const int nf = m.analysis == THERMAL ? 3 : 6;
+  std::vector<double> field((size_t)nf * m.N);
+  if (!cudapcgB200ComputeFields(block_index, axis, comp, (double)axis_len(m, axis), m.props, field.data())) {
+    SAY("WARNING: field computation failed: %s\n", cudapcgB200LastError());
+    return;
+  }
+  write_bin(pre + (m.analysis == THERMAL ? "flux" : "stress") + suf, field.data(), field.size());
 }
 
 // ---- .nf (femhmg.c:1456-1586) ---------------------------------------------------------
@@ -271,7 +310,7 @@ logical hmgInit(char* data_filename, char* elem_filename, char* sdf_filename, ui
   build_local_matrices(*m);
   g_m = m;
   g_dir_set = 0;
-  g_use_x0 = false; g_x0_file.clear(); g_export_x = false;
+  g_use_x0 = false; g_x0_file.clear(); g_export_x = false; g_export_fields = false;
   for (auto& v : g_x0_coarse) v.clear();
   g_have_coarse = false;
   const double t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -402,7 +441,8 @@ void hmgSolveHomogenization(void) {
   if (block) {
     // right-hand sides and the effective-tensor volume term on the device
     // (cudapcgB200SolveLoadCases); x comes back only to be exported
-    std::vector<std::vector<double>> xs(g_export_x ? nd : 0, std::vector<double>(m.ndof)), x0s(nd);
+    const bool want_x = g_export_x || g_export_fields;
+    std::vector<std::vector<double>> xs(want_x ? nd : 0, std::vector<double>(m.ndof)), x0s(nd);
     std::vector<const double*> px0(nd, nullptr);
     std::vector<double*> px(nd, nullptr);
     int axis[6], comp[6];
@@ -410,7 +450,7 @@ void hmgSolveHomogenization(void) {
     for (int k = 0; k < nd; k++) {
       case_axis(m, dirs[k], axis[k], comp[k]);
       jump[k] = (double)axis_len(m, axis[k]);
-      if (g_export_x) px[k] = xs[k].data();
+      if (want_x) px[k] = xs[k].data();
       if (g_use_x0 && !g_x0_file.empty()) {
         const std::string fn = g_x0_file + "_" + std::to_string(dirs[k]) + ".bin";
         FILE* f = fopen(fn.c_str(), "rb");
@@ -454,6 +494,7 @@ void hmgSolveHomogenization(void) {
         FILE* f = fopen(fn.c_str(), "wb");
         if (f) { fwrite(xs[k].data(), sizeof(double), m.ndof, f); fclose(f); }
       }
+      if (g_export_fields) export_fields(m, dir, xs[k].data(), k);
       const auto t = std::chrono::steady_clock::now();
       update_C_from_volume(m, dir, volume + ns * k);
       g_stats.update_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
@@ -501,6 +542,7 @@ void hmgSolveHomogenization(void) {
     g_stats.residual[k] = st.residual;
     g_stats.solve_seconds[k] = st.solve_seconds;
     g_stats.kernel_launches += st.kernel_launches;
+    if (g_export_fields) export_fields(m, dir, x.data(), -1);
     if (g_export_x) {  // femhmg.c:1077-1084
       const std::string fn = m.nf_noext + "_X_" + std::to_string(dir) + ".bin";
       FILE* f = fopen(fn.c_str(), "wb");
@@ -561,9 +603,9 @@ logical hmgSaveConstitutiveMtx(const char* filename) {
   fclose(f);
   return 1;
 }
-void hmgSaveFields(logical mustExport, logical) {
-  if (mustExport) SAY("WARNING: field export (-e) is not provided by chfem_b200 yet.\n");
-}
+void hmgSaveFields(logical mustExport, logical) { g_export_fields = mustExport != 0; }
+static int g_run_export_fields = 0;  // for the next chfemB200Run
+void chfemB200SetExportFields(int on) { g_export_fields = on != 0; g_run_export_fields = on != 0; }
 void hmgKeepTrackOfAnalysisReport(uint8_t flag) {
   g_report = flag != 0;
   if (g_report && g_m) g_report_text = "Neutral file: " + g_m->nf + "\nImage: " + g_m->raw + "\n";
@@ -668,7 +710,10 @@ int chfemB200Run(const uint8_t* voxels, const char* nf, int direction, int solve
                  double* C_out) {
   if (!voxels || !nf || !C_out) { fail("chfemB200Run: null argument"); return 0; }
   g_solver = solver; g_precond = precondition > 0; g_precision = precision; g_multirhs = multirhs;
+  const int export_fields = g_run_export_fields;
+  g_run_export_fields = 0;
   if (!hmgInit((char*)nf, nullptr, nullptr, (uint8_t*)voxels)) return 0;
+  g_export_fields = export_fields != 0;
   g_solver = solver;  // the .nf %type_of_solver is overridden by the caller, like chfem_wrapper.c:20-24
   if (direction < 6) hmgSetHomogenizationFlag((hmgFlag_t)direction);
   hmgPrintModelData();

@@ -121,3 +121,43 @@ def export_for_chfem(filename, array, analysis_type, mat_props=None, voxel_size=
         fn = filename if filename.endswith(".raw") else filename + ".raw"
         domain.tofile(fn)
     return jdata
+
+
+# ---- exported fields (-e / compute_property(output_fields=...)) ------------------------------
+# A field file holds float64 node values with the row index fastest, then column, then layer
+# (node = row + col*ny + layer*ny*nx) and the per-node components innermost: a C-order
+# [z][x][y](, k) array.  The readers below hand it back as [z][y][x] (image order) or, with
+# rotate_domain, as [x][y][z]; the component axis comes first.  Same functions, arguments and
+# results as chfem/io.py:111-206 (3D; 2D fields are stored [x][y](, k)).
+
+def _read_field(filename, domain_shape, ncomp, rotate_domain, dtype):
+    data = np.fromfile(filename, dtype=dtype)
+    if len(domain_shape) == 2:
+        ny, nx = domain_shape
+        a = data.reshape((nx, ny) + ((ncomp,) if ncomp else ()))
+        if ncomp:
+            return a.transpose(2, 0, 1) if rotate_domain else a.transpose(2, 1, 0)
+        return a if rotate_domain else a.T
+    nz, ny, nx = domain_shape
+    a = data.reshape((nz, nx, ny) + ((ncomp,) if ncomp else ()))
+    if ncomp:
+        return a.transpose(3, 1, 2, 0) if rotate_domain else a.transpose(3, 0, 2, 1)
+    return a.transpose(1, 2, 0) if rotate_domain else a.transpose(0, 2, 1)
+
+
+def import_scalar_field_from_chfem(filename, domain_shape, rotate_domain=False, dtype=np.float64):
+    """Scalar node field (temperature, pressure) of an image of shape domain_shape ((nz, ny, nx)
+    or (ny, nx)); returned as [z][y][x] ([y][x]), or [x][y][z] ([x][y]) with rotate_domain."""
+    return _read_field(filename, domain_shape, 0, rotate_domain, dtype)
+
+
+def import_vector_field_from_chfem(filename, domain_shape, rotate_domain=False, dtype=np.float64):
+    """Vector node field (flux, displacement, velocity): [k][z][y][x] with k = 3 (2 in 2D), or
+    [k][x][y][z] with rotate_domain."""
+    return _read_field(filename, domain_shape, 2 if len(domain_shape) == 2 else 3, rotate_domain, dtype)
+
+
+def import_stress_field_from_chfem(filename, domain_shape, rotate_domain=False, dtype=np.float64):
+    """Stress node field: [k][z][y][x] with k = 6 Voigt components xx yy zz yz xz xy (3 in 2D),
+    or [k][x][y][z] with rotate_domain."""
+    return _read_field(filename, domain_shape, 3 if len(domain_shape) == 2 else 6, rotate_domain, dtype)

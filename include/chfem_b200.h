@@ -118,6 +118,9 @@ int chfemB200CopyModelArray(int which, void *dst, unsigned long long bytes);
 int chfemB200AssembleRHS(int direction, double *dst);
 /* Effective-tensor column of load case `direction` from a solution x (ndof doubles). */
 int chfemB200UpdateC(int direction, const double *x, double *C_out);
+/* Export the solution and its field for every load case of the next solve (as hmgSaveFields
+   does; for the one-call chfemB200Run, which re-initializes the model). */
+void chfemB200SetExportFields(int on);
 /* Initial guesses for the next hmgSolveHomogenization / chfemB200Run (used once, then cleared):
    x0[k] for load case k (k < ncases; NULL entries start from zero), nvars doubles each, in host
    memory or (on_device) device memory that stays valid until the solve returns.  They take

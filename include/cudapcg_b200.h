@@ -193,6 +193,15 @@ int cudapcgB200SolveThermalBatch(unsigned int nsamples, const unsigned int *dims
                                  unsigned int maxit, int precision, int precondition, double *moments,
                                  unsigned int *iterations, double *residuals, cudapcgB200BatchStats *stats);
 const char *cudapcgB200BatchLastError(void);
+/* Exported field of a solution still on the device (chfem's -e output,
+   femhmg_thermal_3D.c:674-1111, femhmg_elastic_3D.c:1800-2650): the nodal heat flux (3 per node)
+   or stress (6 per node, Voigt xx yy zz yz xz xy), each node's value the mean over its 8 voxels
+   of the voxel's field at that node's corner; boundary voxels see the load case's jump (the
+   displaced component comp on their +axis face nodes).  block_index -1: the solution of the last
+   cudapcgSolve; k >= 0: right-hand side k of the last block solve.  props: conductivity per
+   material (thermal) or (E, nu) per material (elastic).  field_out: host, nf * nodes doubles. */
+cudapcgFlag_t cudapcgB200ComputeFields(int block_index, int axis, int comp, double jump, const double *props,
+                                       double *field_out);
 /* Initial guess of the next cudapcgSolve from a device vector of nvars doubles (the device
    counterpart of cudapcgSetX0(x0, 0); cleared by cudapcgSetX0(NULL, 0)). */
 cudapcgFlag_t cudapcgB200SetX0Device(const double *x0);
