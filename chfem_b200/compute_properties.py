@@ -45,8 +45,6 @@ def compute_property(property, array, mat_props=None, voxel_size=1e-6, solver=No
     if solver in ('cg2', 'minres2') and (output_fields_flag or property != 'permeability'):
         raise ValueError(f"Invalid solver type: {solver}. Two-vectors solvers do not produce fields to be exported, "
                          "nor are implemented for conductivy or elasticity analyses.")
-    if solver in ('cg2', 'minres2'):
-        raise ValueError(f"Invalid solver type: {solver}. The two-vector solvers are not provided by chfem_b200.")
     solver_type = solvers[solver]
     if precision not in ('fp64', 'mixed'):
         raise ValueError(f"Invalid precision: {precision}")

@@ -172,12 +172,13 @@ __global__ void __launch_bounds__(TE_TR * TC) k_bt_apply(BtData<TV> a, const TV*
   long nbase = 0, vbase = 0, Ns = 0;
   bool any_on = false;
   auto flush = [&](int i) {
-    if constexpr (RES) return;
+    if constexpr (!RES) {
 #pragma unroll
-    for (int k = 0; k < BT_NR; k++) {
-      const double t = block_sum<NT>(acc[k], sred);
-      if (tid == 0) a.part[((long)bid + i) * BT_NR + k] = t;
-      acc[k] = 0.0;
+      for (int k = 0; k < BT_NR; k++) {
+        const double t = block_sum<NT>(acc[k], sred);
+        if (tid == 0) a.part[((long)bid + i) * BT_NR + k] = t;
+        acc[k] = 0.0;
+      }
     }
   };
   int i = (w0 < w1) ? bt_find(a.wpre, sch.n_act, w0) : 0;

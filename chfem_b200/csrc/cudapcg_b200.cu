@@ -20,6 +20,7 @@
 #include "stencil_te.cuh"
 #include "pointwise.cuh"
 #include "stencil_fluid.cuh"
+#include "stencil_fluid2.cuh"
 #include "stencil_block.cuh"
 #include "stencil_fluid_block.cuh"
 #include "loadcase.cuh"
@@ -132,6 +133,13 @@ struct Solver {
   double solve_dev_s = 0.0, setup_dev_s = 0.0;
   unsigned long long launches = 0;
   unsigned long count = 0;
+  // 2-vector solvers (cudapcg.cu:154-156 defaults): reduction of the solution, the loaded
+  // velocity component, the scale of the reduced sums; their device accumulators
+  unsigned xr_mode = CUDAPCG_XREDUCE_FULL, xr_shift = 0;
+  double xr_scale = 1.0;
+  double* d_xa = nullptr;
+  double* d_hist = nullptr;
+  size_t xa_cap = 0, hist_cap = 0;
 };
 
 static Solver* S = nullptr;
@@ -167,6 +175,9 @@ static void free_vectors() {
   free_work_vectors();
   free_ptr(S->x); free_ptr(S->b64); free_ptr(S->y64); free_ptr(S->x64);
   S->x = S->b64 = S->y64 = S->x64 = nullptr;
+  free_ptr(S->d_xa); free_ptr(S->d_hist);
+  S->d_xa = S->d_hist = nullptr;
+  S->xa_cap = S->hist_cap = 0;
   S->arrays_alloc = false;
 }
 
@@ -524,6 +535,8 @@ static bool copy_x_to_host(double* res_x) {
   return true;
 }
 
+#include "two_vector_driver.inl"
+
 template <typename T>
 static bool solve_T(double* res_x) {
   if (!ensure_vectors<T>() || !ensure_K<T>()) return false;
@@ -647,16 +660,25 @@ cudapcgFlag_t cudapcgBuildModel(const void* data) {
 
 cudapcgFlag_t cudapcgSetNumTol(cudapcgTol_t t) { if (!S) return CUDAPCG_FALSE; S->tol = t; return CUDAPCG_TRUE; }
 cudapcgFlag_t cudapcgSetMaxIterations(unsigned int n) { if (!S) return CUDAPCG_FALSE; S->maxit = n; return CUDAPCG_TRUE; }
-cudapcgFlag_t cudapcgSetXReduceMode(cudapcgFlag_t) { return S ? CUDAPCG_TRUE : CUDAPCG_FALSE; }
-cudapcgFlag_t cudapcgSetXReduceShift(unsigned int) { return S ? CUDAPCG_TRUE : CUDAPCG_FALSE; }
-cudapcgFlag_t cudapcgSetXReduceScale(double) { return S ? CUDAPCG_TRUE : CUDAPCG_FALSE; }
+cudapcgFlag_t cudapcgSetXReduceMode(cudapcgFlag_t flag) {
+  if (!S) return CUDAPCG_FALSE;
+  S->xr_mode = flag <= CUDAPCG_XREDUCE_FULL ? flag : CUDAPCG_XREDUCE_FULL;
+  return CUDAPCG_TRUE;
+}
+cudapcgFlag_t cudapcgSetXReduceShift(unsigned int shift) { if (!S) return CUDAPCG_FALSE; S->xr_shift = shift; return CUDAPCG_TRUE; }
+cudapcgFlag_t cudapcgSetXReduceScale(double scl) { if (!S) return CUDAPCG_FALSE; S->xr_scale = scl; return CUDAPCG_TRUE; }
+// The reference rescales the terms of its NONE-mode sums by max|d| x this factor before adding
+// them (xreduce.cu:8-13) to protect FP32 accumulation; the sums here are FP64 in a fixed order,
+// so the factor is accepted and has no effect on the result.
 cudapcgFlag_t cudapcgSetReduceStabFactor(double) { return S ? CUDAPCG_TRUE : CUDAPCG_FALSE; }
 cudapcgFlag_t cudapcgSetSolver(cudapcgFlag_t flag) {
   if (!S) return CUDAPCG_FALSE;
   if (flag > CUDAPCG_MINRES2_SOLVER) { printf("ERROR: Invalid \"solverFlag\" (%d).\n", flag); return CUDAPCG_FALSE; }
-  if (flag >= CUDAPCG_CG2_SOLVER) {
-    set_err("cudapcgSetSolver", "the 2-vector solvers (CG2/MINRES2) are not provided by chfem_b200");
-    return CUDAPCG_FALSE;
+  // the 2-vector solvers keep another set of device vectors: a switch drops the old set
+  if ((flag >= CUDAPCG_CG2_SOLVER) != (S->solver_flag >= CUDAPCG_CG2_SOLVER) && S->r) {
+    free_vectors();
+    S->rhs_set = false;
+    S->x0_set = false;
   }
   S->solver_flag = flag;  // CG3/MINRES3 run the same iterates as CG/MINRES
   if (S->gexec) { cudaGraphExecDestroy(S->gexec); S->gexec = nullptr; S->graph_key = -1; }
@@ -670,7 +692,7 @@ cudapcgVar_t cudapcgGetResidual(void) { return S ? S->residual : 0; }
 
 cudapcgFlag_t cudapcgAllocateArrays(void) {
   if (!S || !S->model) return CUDAPCG_FALSE;
-  bool ok = (S->precision == CHFEM_B200_FP64) ? ensure_vectors<double>() : ensure_vectors<float>();
+  bool ok = lean_solver() ? ensure_lean_vectors() : (S->precision == CHFEM_B200_FP64) ? ensure_vectors<double>() : ensure_vectors<float>();
   if (ok) S->user_arrays = true;
   return ok ? CUDAPCG_TRUE : CUDAPCG_FALSE;
 }
@@ -693,12 +715,18 @@ static bool upload_vec(const double* host, void* dst_T) {
 }
 
 static bool ensure_vectors_current() {
+  if (lean_solver()) return ensure_lean_vectors();
   return (S->precision == CHFEM_B200_FP64) ? ensure_vectors<double>() : ensure_vectors<float>();
 }
 
 cudapcgFlag_t cudapcgSetRHS(cudapcgVar_t* RHS) {
   if (!S || !S->model || !RHS) return CUDAPCG_FALSE;
   if (!ensure_vectors_current()) return CUDAPCG_FALSE;
+  if (lean_solver()) {  // the 2-vector solvers consume r in place; no other copy is kept
+    CK(cudaMemcpy(S->r, RHS, S->nvars * 8, cudaMemcpyHostToDevice));
+    S->rhs_set = true;
+    return CUDAPCG_TRUE;
+  }
   if (!upload_vec(RHS, S->r)) return CUDAPCG_FALSE;
   CK(cudaMemcpyAsync(S->b64, RHS, S->nvars * 8, cudaMemcpyHostToDevice, S->stream));
   CK(cudaStreamSynchronize(S->stream));
@@ -765,7 +793,7 @@ extern "C" {
 cudapcgFlag_t cudapcgB200SetX0Device(const double* x0) {
   if (!S || !S->model || !x0) return CUDAPCG_FALSE;
   if (!ensure_vectors_current()) return CUDAPCG_FALSE;
-  CK(cudaMemcpy(S->x, x0, S->nvars * 8, cudaMemcpyDeviceToDevice));
+  CK(cudaMemcpy(lean_solver() ? (double*)S->d0 : S->x, x0, S->nvars * 8, cudaMemcpyDeviceToDevice));
   S->x0_set = true;
   return CUDAPCG_TRUE;
 }
@@ -778,6 +806,12 @@ cudapcgFlag_t cudapcgSetX0(cudapcgVar_t* x0, cudapcgFlag_t mustInterpolate) {
     return CUDAPCG_TRUE;
   }
   if (!ensure_vectors_current()) return CUDAPCG_FALSE;
+  if (lean_solver()) {  // the 2-vector solvers hold x0 in d (cudapcg.cu:302)
+    if (mustInterpolate) { set_err("cudapcgSetX0", "coarse-grid guesses are not provided for Stokes"); return CUDAPCG_FALSE; }
+    CK(cudaMemcpy(S->d0, x0, S->nvars * 8, cudaMemcpyHostToDevice));
+    S->x0_set = true;
+    return CUDAPCG_TRUE;
+  }
   bool ok;
   if (mustInterpolate) ok = (S->vec_prec == CHFEM_B200_FP64) ? interp_x0<double>(x0) : interp_x0<float>(x0);
   else { ok = cudaMemcpy(S->x, x0, S->nvars * 8, cudaMemcpyHostToDevice) == cudaSuccess; }
@@ -887,7 +921,7 @@ cudapcgFlag_t cudapcgSolve(cudapcgVar_t* res_x) {
   const auto t0 = std::chrono::steady_clock::now();
   S->count++;
   S->launches = 0;
-  bool ok = (S->precision == CHFEM_B200_FP64) ? solve_T<double>(res_x) : solve_T<float>(res_x);
+  bool ok = lean_solver() ? solve_two_vector(res_x) : (S->precision == CHFEM_B200_FP64) ? solve_T<double>(res_x) : solve_T<float>(res_x);
   const double t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   S->total_time = t;
   S->mean_time = S->iteration ? S->solve_dev_s / S->iteration : 0.0;
@@ -1063,6 +1097,8 @@ unsigned long long cudapcgB200DeviceBytes(void) {
   const size_t es = S->vec_prec == CHFEM_B200_FP64 ? 8 : 4;
   unsigned long long b = 0;
   if (S->x) b += 7ull * S->nvars * es + 32ull * S->nvars;
+  // the 2-vector solvers: r and d, the reduction accumulator and the per-step sums
+  if (S->vec_prec == VEC_LEAN) b += 16ull * S->nvars + 8ull * (S->xa_cap + S->hist_cap);
   if (S->analysis == CUDAPCG_FLUID_3D) b += 4ull * S->N + 4ull * (S->nV + S->nB) + S->nB;
   else b += 2ull * S->N;
   return b;
@@ -1102,6 +1138,7 @@ extern "C" cudapcgFlag_t cudapcgB200SolveLoadCases(unsigned int nrhs, const int*
                                                    double* residuals) {
   const char* who = "cudapcgB200SolveLoadCases";
   if (!S || !S->model || !axis || !CB || !moments || nrhs < 1 || nrhs > BLK_MAX) { set_err(who, "bad arguments"); return CUDAPCG_FALSE; }
+  if (lean_solver()) { set_err(who, "block solves run CG/MINRES(3); the 2-vector solvers reduce one load case at a time"); return CUDAPCG_FALSE; }
   const bool fluid = S->analysis == CUDAPCG_FLUID_3D;
   if (fluid != ((S->solver_flag & 1) != 0)) {
     set_err(who, "load-case blocks are provided for thermal and elastic CG/PCG and Stokes MINRES/PMINRES");
@@ -1130,6 +1167,7 @@ extern "C" cudapcgFlag_t cudapcgB200SolveBlock(unsigned int nrhs, const double* 
                                                int x0_interpolate, double* const* x_out, unsigned int* iterations,
                                                double* residuals) {
   if (!S || !S->model || !rhs || !x_out || nrhs < 1 || nrhs > BLK_MAX) { set_err("cudapcgB200SolveBlock", "bad arguments"); return CUDAPCG_FALSE; }
+  if (lean_solver()) { set_err("cudapcgB200SolveBlock", "block solves run CG/MINRES(3), not the 2-vector solvers"); return CUDAPCG_FALSE; }
   const bool fluid = S->analysis == CUDAPCG_FLUID_3D;
   if (fluid != ((S->solver_flag & 1) != 0)) {
     set_err("cudapcgB200SolveBlock", "block solves are provided for thermal and elastic CG/PCG and Stokes MINRES/PMINRES");

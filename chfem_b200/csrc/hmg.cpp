@@ -28,6 +28,7 @@ int g_par = CUDAPCG_NBN, g_solver = CUDAPCG_CG_SOLVER, g_precond = 1, g_stopcrit
 int g_poremap = CUDAPCG_POREMAP_NUM;
 int g_precision = CHFEM_B200_PREC_FP64, g_multirhs = 0, g_quiet = 0;
 int g_dir_set = 0, g_dir = 6;
+int g_xreduce = CUDAPCG_XREDUCE_FULL;  // femhmg.c:23
 bool g_export_x = false;
 bool g_export_fields = false;
 
@@ -149,6 +150,7 @@ bool read_nf(Model& m, const char* fn) {
       count++;
     } else if (!strcmp(tok, "%xreduce_scale_factor")) {
       double v; if (fscanf(f, "%lf", &v) != 1) break;
+      m.xreduce_stab = v;
       count++;
     }
   }
@@ -159,6 +161,8 @@ bool read_nf(Model& m, const char* fn) {
   if (m.analysis < 0) { fail("%type_of_analysis missing"); return false; }
   if (m.nmat == 0) { fail("no materials"); return false; }
   if (m.refinement > 1) m.voxel /= m.refinement;
+  // femhmg.c:1583-1584: the x-reduce stabilisation factor defaults to tol^2, or 1e-12 below 5e-7
+  if (m.xreduce_stab < 0) m.xreduce_stab = m.tol >= 0.0000005 ? m.tol * m.tol : 0.000000000001;
   m.nx = (unsigned)nx * m.refinement; m.ny = (unsigned)ny * m.refinement; m.nz = (unsigned)nz * m.refinement;
   return true;
 }
@@ -259,6 +263,10 @@ bool setup_solver(Model& m, bool coarse = false) {
   if (!cudapcgInit((cudapcgFlag_t)pcg_flag_of(m), (cudapcgFlag_t)g_par)) { fail(std::string("cudapcgInit: ") + cudapcgB200LastError()); return false; }
   cudapcgSetHeaderString((char*)"    | ");
   cudapcgSetModelConstructorFcn(model_ctor);
+  // femhmg.c:919-926: reduction of the 2-vector solvers, its scale h^2 / nelem and factor
+  cudapcgSetXReduceMode((cudapcgFlag_t)g_xreduce);
+  cudapcgSetXReduceScale((m.voxel * m.voxel) / (double)m.N);
+  cudapcgSetReduceStabFactor(m.xreduce_stab);
   if (!cudapcgBuildModel(&m)) { fail(std::string("cudapcgBuildModel: ") + cudapcgB200LastError()); return false; }
   const int solver = coarse ? ((g_solver & 1) ? CUDAPCG_MINRES_SOLVER : CUDAPCG_CG_SOLVER) : g_solver;
   if (!cudapcgSetSolver((cudapcgFlag_t)solver)) { fail(std::string("cudapcgSetSolver: ") + cudapcgB200LastError()); return false; }
@@ -326,9 +334,9 @@ logical hmgEnd(void) {
   return 1;
 }
 
-void hmgSetXReduceFlag(uint8_t) {}
 void hmgSetParallelStrategyFlag(uint8_t flag) { g_par = flag ? CUDAPCG_EBE : CUDAPCG_NBN; }
 void hmgSetSolverFlag(uint8_t flag) { g_solver = flag; }
+void hmgSetXReduceFlag(uint8_t flag) { g_xreduce = flag <= CUDAPCG_XREDUCE_FULL ? flag : CUDAPCG_XREDUCE_FULL; }
 void hmgSetPreConditionerFlag(uint8_t flag) { g_precond = flag > 0; }
 void hmgSetStoppingCriteria(uint8_t flag) { g_stopcrit = flag; }
 logical hmgSetPoreMappingStrategy(uint8_t flag) {
@@ -424,6 +432,15 @@ void hmgSolveHomogenization(void) {
   if (g_dir_set) dirs[nd++] = g_dir;
   else { nd = load_case_count(m); load_case_list(m, dirs); }
   for (unsigned i = 0; i < m.C_dim; i++) m.C[i] = 0.0;
+  if (m.analysis != FLUID && g_solver > CUDAPCG_MINRES3_SOLVER) {  // femhmg.c:852-856
+    SAY("WARNING: CG2 and MINRES2 are only available for FLUID.\n");
+    SAY("         Defaulting to %s.\n", g_solver == CUDAPCG_CG2_SOLVER ? "CG3" : "MINRES3");
+    g_solver = g_solver == CUDAPCG_CG2_SOLVER ? CUDAPCG_CG3_SOLVER : CUDAPCG_MINRES3_SOLVER;
+  }
+  // the 2-vector solvers never form the solution: its exports have nothing to write
+  const bool two_vector = g_solver >= CUDAPCG_CG2_SOLVER;
+  if (two_vector && (g_export_fields || g_export_x))
+    SAY("WARNING: the 2-vector solvers (CG2/MINRES2) reduce the solution on the fly; fields and x are not exported.\n");
   SAY("Running homogenization...\n");
   {
     const auto ts = std::chrono::steady_clock::now();
@@ -435,7 +452,7 @@ void hmgSolveHomogenization(void) {
   g_stats.ndof = (unsigned)m.ndof;
   // Block multi-RHS path: all load cases of the analysis advance together (one operator pass
   // per iteration for all of them).  Same per-case recurrence, stopping test and results.
-  const bool block = g_multirhs && ((m.analysis != FLUID && !(g_solver & 1) &&
+  const bool block = g_multirhs && !two_vector && ((m.analysis != FLUID && !(g_solver & 1) &&
                                      ((m.analysis == THERMAL && nd == 3) || (m.analysis == ELASTIC && (nd == 6 || nd == 3)))) ||
                                     (m.analysis == FLUID && (g_solver & 1) && nd == 3));
   if (block) {
@@ -533,6 +550,7 @@ void hmgSolveHomogenization(void) {
       cudapcgSetX0(nullptr, 0);  // no guess for this case: not the previous case's
     }
     SAY("    Solving system of equations...\n");
+    if (two_vector) cudapcgSetXReduceShift(dir <= 2 ? dir : 0);  // femhmg.c:1068
     cudapcgSolve(x.data());
     if (!g_quiet) cudapcgPrintSolverMetrics();
     cudapcgB200Stats st;
@@ -542,6 +560,19 @@ void hmgSolveHomogenization(void) {
     g_stats.residual[k] = st.residual;
     g_stats.solve_seconds[k] = st.solve_seconds;
     g_stats.kernel_launches += st.kernel_launches;
+    if (two_vector) {  // femhmg.c:1087-1094: the reduced sums are the column of C
+      SAY("    Effective fields:\n");
+      for (int jj = 0; jj < 3; jj++) {
+        SAY("        %.8e\n", x[jj]);
+        m.C[jj * 3 + dir] = x[jj];
+      }
+      if (g_report) {
+        char buf[512];
+        snprintf(buf, sizeof(buf), "Analysis on %s: %u iterations, residual %.3e, solver time %.3e s\n", DIR_STR[dir], st.iterations, st.residual, st.solve_seconds);
+        g_report_text += buf;
+      }
+      continue;
+    }
     if (g_export_fields) export_fields(m, dir, x.data(), -1);
     if (g_export_x) {  // femhmg.c:1077-1084
       const std::string fn = m.nf_noext + "_X_" + std::to_string(dir) + ".bin";
@@ -576,6 +607,7 @@ void hmgPrintModelData(void) {
     printf("  | porosity: %05.2f%%\n  | within pores: %ld\n  | at interfaces: %ld\n", 100.0 * m.nporeelem / (double)m.N, m.nV, m.nB);
   printf("Number of DOFs: %ld\nNumber of materials: %u\nNumerical tolerance: %.3e\nMax iterations: %u\nSolver: %s%s\n",
          m.ndof, m.nmat, m.tol, m.maxit, g_precond ? "P" : "", SO[g_solver < 6 ? g_solver : 0]);
+  if (g_solver >= CUDAPCG_CG2_SOLVER) printf("xreduce stab factor: %.2e\n", m.xreduce_stab);
   printf("Precision: %s\n*******************************************************\n", !g_precision ? "FP64" : (m.analysis == FLUID ? "FP64 (mixed precision is not used for Stokes)" : "mixed (FP32 fields, FP64 reductions)"));
 }
 

@@ -29,6 +29,7 @@ struct Model {
   int props_keys[256];               // colour -> material index (-1 when not listed)
   double alpha[256] = {0};
   bool has_thermal_expansion = false;
+  double xreduce_stab = -1.0;        // %xreduce_scale_factor (negative: not given)
   std::string nf, nf_noext, raw;
   // sizes
   long N = 0;                        // voxels = periodic nodes

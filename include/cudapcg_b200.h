@@ -9,8 +9,13 @@
  * links against this library unchanged.  Differences by design:
  *   - errors return 0 and leave a message for cudapcgB200LastError(); the library never
  *     calls exit() or cudaDeviceReset() (reference: error_handling.h:6-14, cudapcg.cu:201);
- *   - 2D analyses, the scalar-density field and the 2-vector solvers (CG2/MINRES2) are
- *     rejected with an error (outside the 3D hot path this library implements).
+ *   - 2D analyses and the scalar-density field are rejected with an error (outside the 3D
+ *     hot path this library implements);
+ *   - the 2-vector solvers (CG2/MINRES2, solvers/cg2.cu, pcg2.cu, minres2.cu, pminres2.cu)
+ *     run for Stokes: cudapcgSolve then writes the 3 reduced velocity sums of the solution
+ *     (x[0..2], scaled by cudapcgSetXReduceScale) and <model name>_xreduce_metrics_<n>.bin;
+ *     for thermal / elastic models they return an error (the reference's host never runs them
+ *     there, femhmg.c:852-856).
  *
  * Part 2 (cudapcgB200* / chfemB200*) has no counterpart in the reference: precision mode,
  * operator access for tests, solve statistics.
@@ -46,6 +51,10 @@ extern "C" {
 #define CUDAPCG_MINRES3_SOLVER 3
 #define CUDAPCG_CG2_SOLVER 4
 #define CUDAPCG_MINRES2_SOLVER 5
+/* includes.h:42-44: how the 2-vector solvers reduce the solution */
+#define CUDAPCG_XREDUCE_NONE 0
+#define CUDAPCG_XREDUCE_ONLYDIR 1
+#define CUDAPCG_XREDUCE_FULL 2
 typedef double cudapcgVar_t;
 typedef double cudapcgTol_t;
 typedef unsigned short int cudapcgMap_t;
@@ -108,7 +117,7 @@ typedef struct _pcgmodel {
 /* cudapcg.cu:348-355 */ cudapcgFlag_t cudapcgSetPeriodic2DOFMap(cudapcgIdMap_t *vars);
 /* cudapcg.cu:357-363 */ cudapcgFlag_t cudapcgSetDOF2PeriodicMap(cudapcgIdMap_t *nodes);
 /* cudapcg.cu:365-375 */ cudapcgFlag_t cudapcgSetLclMtxs(cudapcgVar_t *LclMtxs);
-/* cudapcg.cu:389-409 */ cudapcgFlag_t cudapcgSolve(cudapcgVar_t *x);
+/* cudapcg.cu:389-409 */ cudapcgFlag_t cudapcgSolve(cudapcgVar_t *x);  /* CG2/MINRES2: x[0..2] = reduced sums */
 /* cudapcg.cu:411-434 */ cudapcgFlag_t cudapcgSetHeaderString(char *header);
 /* cudapcg.cu:434-448 */ cudapcgFlag_t cudapcgPrintSolverReport(void);
 /* cudapcg.cu:450-469 */ cudapcgFlag_t cudapcgPrintSolverReport2(char *dest);

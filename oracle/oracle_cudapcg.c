@@ -10,8 +10,9 @@
  *
  * Each function cites the reference file:line it follows (paths inside cortezpedro/chfem).
  * Scope: 3D thermal (1 DOF/node), 3D elastic (3 DOF/node), 3D Stokes with the DOF-number
- * pore map (CUDAPCG_POREMAP_NUM).  2D analyses, the scalar-density-field input and the
- * 2-vector solvers (CG2/MINRES2) are outside the hot path and rejected with an error.
+ * pore map (CUDAPCG_POREMAP_NUM), including the 2-vector solvers with on-the-fly reduction of
+ * the solution (CG2/PCG2/MINRES2/PMINRES2, Stokes).  2D analyses and the scalar-density-field
+ * input are outside the hot path and rejected with an error.
  *
  * Operator restatement.  The reference applies A node-by-node: for node i and each of the
  * 8 voxels (elements) around it, i is local node e of element e, and the row block of the
@@ -73,6 +74,10 @@ typedef struct {
   double total_time, mean_time;
   int found;
   double *x, *r, *d, *q, *s;
+  /* 2-vector solvers: reduction mode, shift (loaded velocity component), scale, solve count */
+  unsigned int xr_mode, xr_shift;
+  double xr_scale;
+  unsigned long count;
   double *Kd;        /* dense element matrices, nkeys x (ed x ed) */
   unsigned int ed;   /* element matrix dimension: 8, 24 or 32 */
   unsigned int nkeys;
@@ -423,6 +428,7 @@ cudapcgFlag_t cudapcgInit(cudapcgFlag_t analysis_flag, cudapcgFlag_t par) {
   S->analysis = analysis_flag; S->par = par;
   S->tol = CUDAPCG_TOLERANCE; S->maxit = CUDAPCG_MAX_ITERATIONS;
   S->solver_flag = CUDAPCG_CG_SOLVER; S->precond = 1; S->resnorm = CUDAPCG_L2_NORM;
+  S->xr_mode = CUDAPCG_XREDUCE_FULL; S->xr_shift = 0; S->xr_scale = 1.0;  /* cudapcg.cu:154-156 */
   S->residual = 1.0;
   S->header = strdup("");
   if (!model_ctor) model_ctor = ctor_simple;
@@ -476,14 +482,16 @@ cudapcgFlag_t cudapcgSetModel(cudapcgModel_t *model) {
 
 cudapcgFlag_t cudapcgSetNumTol(cudapcgTol_t t) { if (!S) return 0; S->tol = t; return 1; }
 cudapcgFlag_t cudapcgSetMaxIterations(unsigned int n) { if (!S) return 0; S->maxit = n; return 1; }
-cudapcgFlag_t cudapcgSetXReduceMode(cudapcgFlag_t f) { (void)f; return S ? 1 : 0; }
-cudapcgFlag_t cudapcgSetXReduceShift(unsigned int s) { (void)s; return S ? 1 : 0; }
-cudapcgFlag_t cudapcgSetXReduceScale(double s) { (void)s; return S ? 1 : 0; }
+/* cudapcg.cu:96-99.  The stabilisation factor only rescales the terms of a sum in the      */
+/* reference (xreduce.cu:8-13); the oracle sums in FP64 directly.                          */
+cudapcgFlag_t cudapcgSetXReduceMode(cudapcgFlag_t f) { if (!S) return 0; S->xr_mode = f <= CUDAPCG_XREDUCE_FULL ? f : CUDAPCG_XREDUCE_FULL; return 1; }
+cudapcgFlag_t cudapcgSetXReduceShift(unsigned int s) { if (!S) return 0; S->xr_shift = s; return 1; }
+cudapcgFlag_t cudapcgSetXReduceScale(double s) { if (!S) return 0; S->xr_scale = s; return 1; }
 cudapcgFlag_t cudapcgSetReduceStabFactor(double s) { (void)s; return S ? 1 : 0; }
 /* cudapcg.cu:597-671: 3-vector variants run the same iterates; 2-vector variants are out of scope. */
 cudapcgFlag_t cudapcgSetSolver(cudapcgFlag_t flag) {
   if (!S) return 0;
-  if (flag > CUDAPCG_MINRES3_SOLVER) { printf("ERROR: solver %d (2-vector, x-reduce) is not provided by the oracle.\n", flag); return 0; }
+  if (flag > CUDAPCG_MINRES2_SOLVER) { printf("ERROR: Invalid \"solverFlag\" (%d).\n", flag); return 0; }
   S->solver_flag = flag;
   return 1;
 }
@@ -815,6 +823,227 @@ static void solve_minres(void) {
   free(tmp);
 }
 
+/* ------------------------------------------------------------------------------------ */
+/* 2-vector solvers (solvers/cg2.cu, pcg2.cu, minres2.cu, pminres2.cu): only r and d are   */
+/* kept; the solution is never stored, only reduced on the fly into the per-component sums */
+/* of its velocity part (xreduce.cu:4-27), which are the effective-permeability column.    */
+/*   NONE    res[c][it] = a * sum_j d[3j+c]   (the sums are accumulated at the end)        */
+/*   ONLYDIR x[j] += a d[3j+shift];  res[shift][it] = sum_j x[j]                           */
+/*   FULL    x[i] += a d[i] (velocity DOFs);  res[c][it] = sum_j x[3j+c]                    */
+typedef struct {
+  double *res[3];
+  double *xa;          /* reduction accumulator (ONLYDIR: nV values, FULL: 3 nV, NONE: none) */
+  unsigned int nv;     /* velocity nodes */
+} xred_t;
+
+static double sum_stride(const double *v, unsigned int nv, unsigned int stride, unsigned int c) {
+  double s = 0.0;
+#pragma omp parallel for reduction(+ : s) schedule(static)
+  for (long j = 0; j < (long)nv; j++) s += v[(size_t)j * stride + c];
+  return s;
+}
+static void xred_update(xred_t *X, unsigned int it, double a, const double *d) {
+  const unsigned int nv = X->nv;
+  switch (S->xr_mode) {
+    case CUDAPCG_XREDUCE_NONE:
+      for (unsigned int c = 0; c < 3; c++) X->res[c][it] = a * sum_stride(d, nv, 3, c);
+      break;
+    case CUDAPCG_XREDUCE_ONLYDIR:
+#pragma omp parallel for schedule(static)
+      for (long j = 0; j < (long)nv; j++) X->xa[j] += a * d[3 * (size_t)j + S->xr_shift];
+      X->res[S->xr_shift][it] = sum_stride(X->xa, nv, 1, 0);
+      break;
+    default:
+      axpy_iny(X->xa, d, a, 3 * nv);
+      for (unsigned int c = 0; c < 3; c++) X->res[c][it] = sum_stride(X->xa, nv, 3, c);
+  }
+}
+/* the x0 stored in d enters the accumulator and the first sums (cg2.cu:131-146) */
+static void xred_x0(xred_t *X, const double *d) {
+  const unsigned int nv = X->nv;
+  if (S->xr_mode == CUDAPCG_XREDUCE_ONLYDIR) {
+#pragma omp parallel for schedule(static)
+    for (long j = 0; j < (long)nv; j++) X->xa[j] += d[3 * (size_t)j + S->xr_shift];
+  } else if (S->xr_mode == CUDAPCG_XREDUCE_FULL) {
+    memcpy(X->xa, d, sizeof(double) * 3 * nv);
+  }
+  for (unsigned int c = 0; c < 3; c++) X->res[c][0] = sum_stride(d, nv, 3, c);
+}
+/* the largest |x| the solver holds, for the error norm of CG2/PCG2 (cg2.cu:181); without */
+/* an accumulator (NONE) the denominator is 1, as in (P)MINRES2                            */
+static double xred_absmax(const xred_t *X) {
+  if (S->xr_mode == CUDAPCG_XREDUCE_NONE) return 1.0;
+  return absmax(X->xa, S->xr_mode == CUDAPCG_XREDUCE_ONLYDIR ? X->nv : 3 * X->nv);
+}
+/* save_xreduce (xreduce.cu:29-48) and the result (pcg2.cu:262-280) */
+static void xred_finish(xred_t *X, unsigned int it, double *res_x) {
+  const double scl = S->xr_scale;
+  for (unsigned int c = 0; c < 3; c++)
+    for (unsigned int j = 0; j <= it; j++) X->res[c][j] *= scl;
+  char fn[2048];
+  snprintf(fn, sizeof fn, "%s_xreduce_metrics_%lu.bin", S->model->name ? S->model->name : "", S->count);
+  FILE *f = fopen(fn, "wb");
+  if (f) {
+    if (S->xr_mode != CUDAPCG_XREDUCE_ONLYDIR) for (unsigned int c = 0; c < 3; c++) fwrite(X->res[c], sizeof(double), it + 1, f);
+    else fwrite(X->res[S->xr_shift], sizeof(double), it + 1, f);
+    fclose(f);
+  }
+  for (unsigned int c = 0; c < 3; c++) {
+    double *p = X->res[c];
+    switch (S->xr_mode) {
+      case CUDAPCG_XREDUCE_NONE:
+        for (unsigned int j = it; j > 0; j--) p[j - 1] += p[j];
+        res_x[c] = p[0];
+        break;
+      case CUDAPCG_XREDUCE_ONLYDIR: res_x[c] = S->xr_shift == c ? p[it] : 0.0; break;
+      default: res_x[c] = p[it];
+    }
+  }
+}
+
+/* solve_pcg2 (pcg2.cu:24-290) / solve_cg2 (cg2.cu:62-320) */
+static void solve_cg2_family(int pre, xred_t *X, double *res_x) {
+  cudapcgModel_t *m = S->model;
+  const unsigned int n = m->nvars, nstop = m->nhmgvars;
+  double *r = S->r, *d = S->d, *q = S->q;
+  double a = 0.0, delta, delta0, delta_old, stop_metric = 1.0, res0;
+  int cont = 1;
+  S->iteration = 0;
+  hist_n = 0;
+  if (pre) { apply_precond(r, NULL, 1.0, 0.0, q); delta0 = dot(r, q, n); }
+  else delta0 = dot(r, r, n);
+  res0 = (S->resnorm == CUDAPCG_INF_NORM) ? absmax(r, n) : delta0;
+  if (fabs(res0) < 1e-12) {
+    S->residual = 0.0; S->found = 1;
+    if (!g_quiet) printf("%sNull solution satisfied %s.\n", S->header, pre ? "PCG" : "CG");
+    return;
+  }
+  if (S->x0_set) {
+    Aprod_scl(d, -1.0, 1.0, r, q);
+    if (pre) { apply_precond(r, NULL, 1.0, 0.0, q); delta = dot(r, q, n); }
+    else delta = dot(r, r, n);
+    xred_x0(X, d);
+    if (!above_tol(delta, delta0, S->tol)) {
+      S->residual = eval_res(delta, delta0); S->found = 1;
+      if (!g_quiet) printf("%sInitial guess satisfied %s.\n", S->header, pre ? "PCG" : "CG");
+      return;
+    }
+  } else delta = delta0;
+  delta_old = delta;
+  for (;;) {
+    S->iteration++;
+    if (S->iteration == 1) { if (pre) apply_precond(r, NULL, 1.0, 0.0, d); else arrcpy(r, n, d); }
+    else if (pre) apply_precond(r, d, 1.0, delta / delta_old, d);
+    else axpy_to(r, d, delta / delta_old, n, d);
+    Aprod(d, q);
+    a = delta / dot(d, q, n);
+    xred_update(X, S->iteration, a, d);
+    axpy_iny(r, q, -a, n);
+    delta_old = delta;
+    if (pre) { apply_precond(r, NULL, 1.0, 0.0, q); delta = dot(r, q, n); }
+    else delta = dot(r, r, n);
+    switch (S->resnorm) {
+      case CUDAPCG_L2_NORM: stop_metric = eval_res(delta, delta0); cont = above_tol(delta, delta0, S->tol); break;
+      case CUDAPCG_INF_NORM: stop_metric = absmax(r, n) / res0; cont = stop_metric > S->tol; break;
+      default:
+        stop_metric = fabs(a) * absmax(d, nstop) / xred_absmax(X);
+        cont = !((stop_metric <= S->tol) || !above_tol(delta, delta0, S->tol));
+    }
+    hist_push(stop_metric);
+    if (!(cont && S->iteration < S->maxit)) break;
+  }
+  report_line(stop_metric, delta, delta0);
+  finish(stop_metric, delta, delta0, 1);
+  xred_finish(X, S->iteration, res_x);
+}
+
+/* solve_pminres2 (pminres2.cu:20-278) / solve_minres2 (minres2.cu:62-320): preconditioned   */
+/* conjugate residual with r and d only (A d is applied twice per iteration, A M^-1 r once). */
+static void solve_minres2_family(int pre, xred_t *X, double *res_x) {
+  cudapcgModel_t *m = S->model;
+  const unsigned int n = m->nvars, nstop = m->nhmgvars;
+  double *r = S->r, *d = S->d, *q = S->q, *t = S->s;
+  double a = 0.0, b, delta, delta0, delta_old, stop_metric = 1.0, res0;
+  int cont = 1;
+  S->iteration = 0;
+  hist_n = 0;
+  if (S->resnorm == CUDAPCG_INF_NORM) res0 = absmax(r, n);
+  else res0 = pre ? dot_precond(r, 1.0) : dot(r, r, n);
+  if (pre) apply_precond(r, NULL, 1.0, 0.0, r);
+  Aprod(r, q);
+  delta0 = dot(r, q, n);
+  if (pre) apply_invprecond(r, 1.0, r);
+  if (fabs(res0) < 1e-12) {
+    S->residual = 0.0; S->found = 1;
+    if (!g_quiet) printf("%sNull solution satisfied MINRES.\n", S->header);
+    return;
+  }
+  if (S->x0_set) {
+    Aprod_scl(d, -1.0, 1.0, r, q);
+    if (pre) apply_precond(r, NULL, 1.0, 0.0, r);
+    Aprod(r, q);
+    delta = dot(r, q, n);
+    if (pre) apply_invprecond(r, 1.0, r);
+    xred_x0(X, d);
+    if (!above_tol(delta, delta0, S->tol)) {
+      S->residual = eval_res(delta, delta0); S->found = 1;
+      if (!g_quiet) printf("%sInitial guess satisfied MINRES.\n", S->header);
+      return;
+    }
+  } else delta = delta0;
+  delta_old = delta;
+  for (;;) {
+    S->iteration++;
+    b = S->iteration == 1 ? 0.0 : delta / delta_old;
+    if (pre) apply_precond(r, S->iteration == 1 ? NULL : d, 1.0, b, d);
+    else if (S->iteration == 1) arrcpy(r, n, d);
+    else axpy_to(r, d, b, n, d);
+    Aprod(d, q);
+    if (pre) { apply_precond(q, NULL, 1.0, 0.0, t); a = delta / dot(q, t, n); }
+    else a = delta / dot(q, q, n);
+    xred_update(X, S->iteration, a, d);
+    axpy_iny(r, q, -a, n);
+    if (pre) apply_precond(r, NULL, 1.0, 0.0, r);
+    Aprod(r, q);
+    delta_old = delta;
+    delta = dot(r, q, n);
+    if (pre) apply_invprecond(r, 1.0, r);
+    switch (S->resnorm) {
+      case CUDAPCG_L2_NORM:
+        stop_metric = pre ? dot_precond(r, 1.0) : dot(r, r, n);
+        cont = above_tol(stop_metric, res0, S->tol);
+        stop_metric = eval_res(stop_metric, res0);
+        break;
+      case CUDAPCG_INF_NORM: stop_metric = absmax(r, n) / res0; cont = stop_metric > S->tol; break;
+      default: stop_metric = fabs(a) * absmax(d, nstop); cont = stop_metric > S->tol;
+    }
+    hist_push(stop_metric);
+    if (!(cont && S->iteration < S->maxit)) break;
+  }
+  report_line(stop_metric, delta, delta0);
+  S->residual = stop_metric;
+  S->found = S->residual <= S->tol;
+  xred_finish(X, S->iteration, res_x);
+}
+
+static void solve_two_vector(double *res_x) {
+  cudapcgModel_t *m = S->model;
+  xred_t X;
+  X.nv = m->nporenodes;
+  double *buf = (double *)calloc((size_t)3 * (S->maxit + 1), sizeof(double));
+  for (int c = 0; c < 3; c++) X.res[c] = buf + (size_t)c * (S->maxit + 1);
+  X.xa = (S->xr_mode == CUDAPCG_XREDUCE_NONE) ? NULL
+       : (double *)calloc(S->xr_mode == CUDAPCG_XREDUCE_ONLYDIR ? X.nv : 3 * (size_t)X.nv, sizeof(double));
+  /* the x0 lives in d (cudapcg.cu:302) */
+  if (S->x0_set) memcpy(S->d, S->x, sizeof(double) * m->nvars);
+  res_x[0] = res_x[1] = res_x[2] = 0.0;
+  const int minres = S->solver_flag == CUDAPCG_MINRES2_SOLVER;
+  if (minres) solve_minres2_family(S->precond, &X, res_x);
+  else solve_cg2_family(S->precond, &X, res_x);
+  free(X.xa);
+  free(buf);
+}
+
 /* cudapcgSolve (cudapcg.cu:389-409). */
 cudapcgFlag_t cudapcgSolve(cudapcgVar_t *res_x) {
   if (!S || !S->model || !res_x) return 0;
@@ -823,11 +1052,22 @@ cudapcgFlag_t cudapcgSolve(cudapcgVar_t *res_x) {
   cudapcgAllocateArrays();
   inv_diag(g_dinv);
   S->found = 0;
-  int minres = (S->solver_flag == CUDAPCG_MINRES_SOLVER || S->solver_flag == CUDAPCG_MINRES3_SOLVER);
-  if (minres) { if (S->precond) solve_pminres(); else solve_minres(); }
-  else solve_cg_family(S->precond);
-  memcpy(res_x, S->x, sizeof(double) * S->model->nvars);
-  capture(6, S->x, S->model->nvars);
+  S->count++;
+  if (S->solver_flag >= CUDAPCG_CG2_SOLVER) {
+    if (S->analysis != CUDAPCG_FLUID_3D) {
+      printf("ERROR: the 2-vector solvers reduce Stokes velocities; use CG3/MINRES3.\n");
+      if (must_free) free_arrays();
+      return 0;
+    }
+    solve_two_vector(res_x);
+    capture(6, res_x, 3);
+  } else {
+    int minres = (S->solver_flag == CUDAPCG_MINRES_SOLVER || S->solver_flag == CUDAPCG_MINRES3_SOLVER);
+    if (minres) { if (S->precond) solve_pminres(); else solve_minres(); }
+    else solve_cg_family(S->precond);
+    memcpy(res_x, S->x, sizeof(double) * S->model->nvars);
+    capture(6, S->x, S->model->nvars);
+  }
   S->total_time = omp_get_wtime() - t0;
   S->mean_time = S->iteration ? S->total_time / S->iteration : 0.0;
   log_solve();
