@@ -43,6 +43,8 @@ def cudapcg():
         lib.cudapcgB200DeviceBytes.restype = c.c_ulonglong
         lib.cudapcgGetResidual.restype = c.c_double
         lib.cudapcgSetNumTol.argtypes = [c.c_double]
+        lib.cudapcgB200SetImageColors.restype = c.c_ubyte
+        lib.cudapcgB200SetImageColors.argtypes = [c.c_void_p, c.c_uint, c.c_uint, c.c_uint, c.c_uint, c.c_void_p]
         lib._typed = True
     return lib
 

@@ -139,6 +139,8 @@ struct Solver {
   double xr_scale = 1.0;
   double* d_xa = nullptr;
   double* d_hist = nullptr;
+  // one-by-one path on the device: element averaging matrices and the reduced volume term
+  double* d_vt = nullptr;
   size_t xa_cap = 0, hist_cap = 0;
 };
 
@@ -545,7 +547,7 @@ static bool solve_T(double* res_x) {
   if (!ok) return false;
   collect_results(minres);
   if (S->h_sc->status == 1 && minres) CKV(cudaMemsetAsync(S->x, 0, S->nvars * 8, S->stream));
-  return copy_x_to_host<T>(res_x);
+  return res_x ? copy_x_to_host<T>(res_x) : true;  // NULL: the solution stays on the device
 }
 
 // =======================================================================================
@@ -559,7 +561,7 @@ cudapcgFlag_t cudapcgEnd(void) {
   block_free();
   free_vectors();
   free_model_dev();
-  free_ptr(S->d_sc); free_ptr(S->d_part); free_ptr(S->d_ticket);
+  free_ptr(S->d_sc); free_ptr(S->d_part); free_ptr(S->d_ticket); free_ptr(S->d_vt);
   if (S->h_sc) cudaFreeHost(S->h_sc);
   if (S->ev0) cudaEventDestroy(S->ev0);
   if (S->ev1) cudaEventDestroy(S->ev1);
@@ -837,6 +839,27 @@ __global__ void k_keys_from_elements(const uint16_t* em, uint16_t* keys, int R, 
     keys[i] = (uint16_t)k;
   }
 }
+// Node keys straight from the image's colours: the file holds one byte per voxel with x
+// fastest (femhmg.c:1644-1700), each voxel split into ref^3 refined voxels; a colour maps to
+// its material index through the .nf material list.  A colour the list lacks raises *bad.
+struct ColorMap { int16_t mat[256]; };
+__global__ void k_keys_from_colors(const uint8_t* colors, ColorMap cm, uint16_t* keys, int R, int C, int L, int ref, int* bad) {
+  const long N = (long)R * C * L;
+  const int frows = R / ref, fcols = C / ref;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const int r = (int)(i % R), c = (int)((i / R) % C), l = (int)(i / ((long)R * C));
+    unsigned k = 0;
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      const int vr = wrap(r - drow(e) - 1, R), vc = wrap(c - dcol(e), C), vl = wrap(l - dlay(e), L);
+      const long f = (long)(vl / ref) * frows * fcols + (long)(vr / ref) * fcols + vc / ref;
+      const int m = cm.mat[colors[f]];
+      if (m < 0) { *bad = 1; continue; }
+      k |= ((unsigned)m & 3u) << (2 * e);
+    }
+    keys[i] = (uint16_t)k;
+  }
+}
 extern "C" {
 
 cudapcgFlag_t cudapcgSetImage(cudapcgMap_t* img) {
@@ -853,6 +876,42 @@ cudapcgFlag_t cudapcgSetImage(cudapcgMap_t* img) {
     CK(cudaMemcpy(S->d_keys, img, sizeof(uint16_t) * S->N, cudaMemcpyHostToDevice));
   }
   S->have_keys = true;
+  return CUDAPCG_TRUE;
+}
+cudapcgFlag_t cudapcgB200SetImageColors(const uint8_t* colors, unsigned int rows, unsigned int cols, unsigned int slices,
+                                         unsigned int refinement, const int* material_of_color) {
+  const char* who = "cudapcgB200SetImageColors";
+  if (!S || !S->model || !colors || !material_of_color || refinement < 1) { set_err(who, "bad arguments"); return CUDAPCG_FALSE; }
+  if (S->analysis == CUDAPCG_FLUID_3D) { set_err(who, "not used for FLUID analysis"); return CUDAPCG_FALSE; }
+  if ((long)rows * refinement != S->R || (long)cols * refinement != S->C || (long)slices * refinement != S->L) {
+    set_err(who, "image dimensions times refinement differ from the model's");
+    return CUDAPCG_FALSE;
+  }
+  ColorMap cm;
+  for (int c = 0; c < 256; c++) {
+    const int m = material_of_color[c];
+    cm.mat[c] = (int16_t)((m >= 0 && m < 4) ? m : -1);
+  }
+  const size_t nfile = (size_t)rows * cols * slices;
+  uint8_t* d_col = nullptr;
+  int* d_bad = nullptr;
+  CK(cudaMalloc(&d_col, nfile));
+  cudaError_t e = cudaMalloc(&d_bad, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_bad, 0, sizeof(int), S->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_col, colors, nfile, cudaMemcpyHostToDevice, S->stream);
+  if (e == cudaSuccess) {
+    k_keys_from_colors<<<pw_grid(S->N), PW_NT, 0, S->stream>>>(d_col, cm, S->d_keys, S->R, S->C, S->L, (int)refinement, d_bad);
+    e = cudaPeekAtLastError();
+  }
+  int bad = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, S->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
+  cudaFree(d_col);
+  if (d_bad) cudaFree(d_bad);
+  if (e != cudaSuccess) { set_err(who, cudaGetErrorString(e)); return CUDAPCG_FALSE; }
+  if (bad) { set_err(who, "the image holds a colour without a material (or a material index above 3)"); return CUDAPCG_FALSE; }
+  S->have_keys = true;
+  invalidate_graphs();
   return CUDAPCG_TRUE;
 }
 cudapcgFlag_t cudapcgSetParametricDensityField(parametricScalarField_t*, double, double) {
@@ -916,7 +975,7 @@ cudapcgFlag_t cudapcgSetLclMtxs(cudapcgVar_t* Lm) {
 }
 
 cudapcgFlag_t cudapcgSolve(cudapcgVar_t* res_x) {
-  if (!S || !S->model || !res_x) return CUDAPCG_FALSE;
+  if (!S || !S->model || (!res_x && lean_solver())) return CUDAPCG_FALSE;
   if (!S->rhs_set) { set_err("cudapcgSolve", "right-hand side was not set"); return CUDAPCG_FALSE; }
   const auto t0 = std::chrono::steady_clock::now();
   S->count++;
@@ -1129,6 +1188,69 @@ extern "C" cudapcgFlag_t cudapcgB200ComputeFields(int block_index, int axis, int
   if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
   cudaFree(d_out);
   if (e != cudaSuccess) { set_err(who, cudaGetErrorString(e)); return CUDAPCG_FALSE; }
+  return CUDAPCG_TRUE;
+}
+
+// ---------------------------------------------------------------------------------------
+// The one-by-one path on the device: a load case's right-hand side from the node keys (or, for
+// Stokes, the pore map), and the volume term of its tensor column from the solution left on the
+// device, so neither the right-hand side nor x crosses PCIe.
+template <typename T>
+static bool load_case_rhs_T(int axis, int comp, double jump, const double* CB) {
+  const long n = S->nvars;
+  double* b = lean_solver() ? (double*)S->r : S->b64;  // the 2-vector solvers keep no copy of b
+  if (S->analysis == CUDAPCG_FLUID_3D) {
+    double w = 0.0;
+    for (int a = 0; a < 8; a++) w += CB[72 + a];
+    k_fl_rhs<T><<<pw_grid(n), PW_NT, 0, S->stream>>>(S->nV, n, axis, w, b, (T*)S->r);
+  } else {
+    if (!ensure_K<double>()) return false;
+    if (S->nd == 1)
+      k_rhs_load_case<1, T><<<pw_grid(S->N), PW_NT, 0, S->stream>>>(S->d_keys, S->d_K64, S->R, S->C, S->L, axis, comp, jump, b, (T*)S->r);
+    else
+      k_rhs_load_case<3, T><<<pw_grid(S->N), PW_NT, 0, S->stream>>>(S->d_keys, S->d_K64, S->R, S->C, S->L, axis, comp, jump, b, (T*)S->r);
+  }
+  CKV(cudaPeekAtLastError());
+  CKV(cudaStreamSynchronize(S->stream));
+  return true;
+}
+
+extern "C" cudapcgFlag_t cudapcgB200SetLoadCaseRHS(int axis, int comp, double jump, const double* CB) {
+  const char* who = "cudapcgB200SetLoadCaseRHS";
+  if (!S || !S->model || axis < 0 || axis > 2) { set_err(who, "bad arguments"); return CUDAPCG_FALSE; }
+  const bool fluid = S->analysis == CUDAPCG_FLUID_3D;
+  if (fluid ? !CB : (comp < 0 || comp >= S->nd)) { set_err(who, "bad load case"); return CUDAPCG_FALSE; }
+  if (!fluid && !S->have_keys) { set_err(who, "the model's keys were not set"); return CUDAPCG_FALSE; }
+  if (!ensure_vectors_current()) return CUDAPCG_FALSE;
+  const bool ok = (S->vec_prec == CHFEM_B200_MIXED) ? load_case_rhs_T<float>(axis, comp, jump, CB) : load_case_rhs_T<double>(axis, comp, jump, CB);
+  if (!ok) return CUDAPCG_FALSE;
+  S->rhs_set = true;
+  return CUDAPCG_TRUE;
+}
+
+extern "C" cudapcgFlag_t cudapcgB200VolumeTerm(const double* CB, unsigned int ns, double* moments) {
+  const char* who = "cudapcgB200VolumeTerm";
+  if (!S || !S->model || !CB || !moments || !S->x) { set_err(who, "bad arguments or no solution on the device"); return CUDAPCG_FALSE; }
+  const bool fluid = S->analysis == CUDAPCG_FLUID_3D;
+  if (ns != (fluid ? 3u : (S->nd == 3 ? 6u : 3u))) { set_err(who, "ns must be 3 (thermal, Stokes) or 6 (elastic)"); return CUDAPCG_FALSE; }
+  if (!S->d_vt) CK(cudaMalloc(&S->d_vt, (8 + 4 * 6 * 24) * sizeof(double)));
+  double* d_cb = S->d_vt + 8;
+  const int g = pw_grid(fluid ? S->nV : S->N);
+  if (!ensure_reduction(g)) return CUDAPCG_FALSE;
+  if (fluid) {
+    double w[3] = {0, 0, 0};
+    for (int a = 0; a < 8; a++) { w[0] += CB[3 * a]; w[1] += CB[24 + 3 * a + 1]; w[2] += CB[48 + 3 * a + 2]; }
+    k_fl_moments<<<g, PW_NT, 0, S->stream>>>(S->x, S->nV, w[0], w[1], w[2], redctl(g), S->d_vt);
+  } else {
+    const size_t ncb = (size_t)S->nmat * ns * 8 * S->nd;
+    CK(cudaMemsetAsync(d_cb, 0, 4 * 6 * 24 * sizeof(double), S->stream));
+    CK(cudaMemcpyAsync(d_cb, CB, ncb * sizeof(double), cudaMemcpyHostToDevice, S->stream));
+    if (S->nd == 1) k_cb_moments<1, 3><<<g, PW_NT, 0, S->stream>>>(S->d_keys, d_cb, S->x, S->N, redctl(g), S->d_vt);
+    else k_cb_moments<3, 6><<<g, PW_NT, 0, S->stream>>>(S->d_keys, d_cb, S->x, S->N, redctl(g), S->d_vt);
+  }
+  CK(cudaPeekAtLastError());
+  CK(cudaMemcpyAsync(moments, S->d_vt, ns * sizeof(double), cudaMemcpyDeviceToHost, S->stream));
+  CK(cudaStreamSynchronize(S->stream));
   return CUDAPCG_TRUE;
 }
 

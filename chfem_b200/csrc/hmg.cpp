@@ -168,38 +168,55 @@ bool read_nf(Model& m, const char* fn) {
 }
 
 // ---- image (femhmg.c:1644-1758) -------------------------------------------------------
-bool read_image(Model& m, const uint8_t* data, const char* raw) {
+// The image's colour bytes (file order, x fastest), checked against the .nf material list.
+bool read_colors(Model& m, const uint8_t* data, const char* raw) {
   const unsigned ref = m.refinement;
-  const unsigned rows = m.ny / ref, cols = m.nx / ref, slices = m.nz / ref;
-  const size_t nvox_file = (size_t)rows * cols * slices;
-  std::vector<uint8_t> buf;
-  const uint8_t* src = data;
-  if (!src) {
+  m.frows = m.ny / ref; m.fcols = m.nx / ref; m.fslices = m.nz / ref;
+  const size_t nvox_file = (size_t)m.frows * m.fcols * m.fslices;
+  m.colors.resize(nvox_file);
+  if (data) {
+    memcpy(m.colors.data(), data, nvox_file);
+  } else {
     FILE* f = fopen(raw, "rb");
     if (!f) { fail(std::string("cannot open image ") + raw); return false; }
-    buf.resize(nvox_file);
-    size_t got = fread(buf.data(), 1, nvox_file, f);
+    size_t got = fread(m.colors.data(), 1, nvox_file, f);
     fclose(f);
     if (got < nvox_file) { fail("reached end of image file before expected"); return false; }
-    src = buf.data();
   }
   m.N = (long)m.nx * m.ny * m.nz;
+  bool seen[256] = {false};
+  const uint8_t* c = m.colors.data();
+  for (size_t i = 0; i < nvox_file; i++) seen[c[i]] = true;
+  for (int v = 0; v < 256; v++)
+    if (seen[v] && m.props_keys[v] < 0) { fail("image holds colour " + std::to_string(v) + " that the .nf does not list"); return false; }
+  return true;
+}
+
+// Voxel material map in the model's order (row fastest, refined) from the colours.
+void build_elem_mat(Model& m) {
+  const unsigned ref = m.refinement, rows = m.frows, cols = m.fcols, slices = m.fslices;
   m.elem_mat.assign(m.N, 0);
   const size_t R = m.ny, C = m.nx;
-  bool bad = false;
-  int badcol = -1;
+  const uint8_t* src = m.colors.data();
 #pragma omp parallel for schedule(static)
   for (long k = 0; k < (long)slices; k++)
     for (size_t i = 0; i < rows; i++)
       for (size_t j = 0; j < cols; j++) {
-        const uint8_t v = src[(size_t)k * rows * cols + i * cols + j];  // x fastest in the file
-        const int mat = m.props_keys[v];
-        if (mat < 0) { bad = true; badcol = v; continue; }
+        const int mat = m.props_keys[src[(size_t)k * rows * cols + i * cols + j]];  // x fastest in the file
         for (unsigned kk = ref * k; kk < ref * (k + 1); kk++)
           for (unsigned ii = ref * i; ii < ref * (i + 1); ii++)
             for (unsigned jj = ref * j; jj < ref * (j + 1); jj++) m.elem_mat[ii + jj * R + (size_t)kk * R * C] = (uint16_t)mat;
       }
-  if (bad) { fail("image holds colour " + std::to_string(badcol) + " that the .nf does not list"); return false; }
+}
+
+// The host maps of a thermal / elastic model, for the paths that read them (one-by-one
+// right-hand sides and tensor updates, coarse levels, EBE input, the model-array hooks).
+bool ensure_host_maps(Model& m) {
+  if (m.host_maps) return true;
+  build_elem_mat(m);
+  std::string err;
+  if (!build_maps(m, err)) { fail(err); return false; }
+  m.host_maps = true;
   return true;
 }
 
@@ -253,6 +270,7 @@ Model* coarse_copy(const Model& f) {
       for (long r = 0; r < R; r++) c->elem_mat[r + col * R + l * RC] = f.elem_mat[2 * r + 2 * col * fR + 2 * l * fRC];
   std::string err;
   if (!build_maps(*c, err)) { delete c; return nullptr; }
+  c->host_maps = true;
   c->lcl = f.lcl; c->CB = f.CB; c->Kdense = f.Kdense;
   return c;
 }
@@ -277,8 +295,15 @@ bool setup_solver(Model& m, bool coarse = false) {
   cudapcgB200SetPrecision(g_precision);
   bool ok;
   if (m.analysis != FLUID) {
-    // femhmg.c:1000-1004: node keys for NBN, the per-voxel material map for EBE
-    ok = cudapcgSetImage(g_par == CUDAPCG_EBE ? m.elem_mat.data() : m.keys.data());
+    // femhmg.c:1000-1004: node keys for NBN, the per-voxel material map for EBE; without host
+    // maps the device builds the keys from the colours
+    if (g_par == CUDAPCG_NBN && !m.host_maps) {
+      int lut[256];
+      for (int c = 0; c < 256; c++) lut[c] = m.props_keys[c];
+      ok = cudapcgB200SetImageColors(m.colors.data(), m.frows, m.fcols, m.fslices, m.refinement, lut);
+    } else {
+      ok = ensure_host_maps(m) && cudapcgSetImage(g_par == CUDAPCG_EBE ? m.elem_mat.data() : m.keys.data());
+    }
   } else {
     ok = cudapcgSetPeriodic2DOFMap(m.dof_of_node.data()) && cudapcgSetPoreMap(m.border_keys.data()) &&
          cudapcgSetDOF2PeriodicMap(m.node_of_dof.data());
@@ -312,9 +337,17 @@ logical hmgInit(char* data_filename, char* elem_filename, char* sdf_filename, ui
   }
   m->nd = m->analysis == ELASTIC ? 3 : 1;
   m->C_dim = m->analysis == ELASTIC ? 36 : 9;
-  if (!read_image(*m, data, elem_filename)) { delete m; return 0; }
-  std::string err;
-  if (!build_maps(*m, err)) { fail(err); delete m; return 0; }
+  if (!read_colors(*m, data, elem_filename)) { delete m; return 0; }
+  if (m->analysis == FLUID) {
+    build_elem_mat(*m);
+    std::string err;
+    if (!build_maps(*m, err)) { fail(err); delete m; return 0; }
+    m->host_maps = true;
+  } else {
+    // the node keys are built on the device from the colours (cudapcgB200SetImageColors)
+    if (m->nmat > 4) { fail("more than 4 materials cannot be encoded in 16-bit node keys"); delete m; return 0; }
+    m->ndof = m->N * m->nd;
+  }
   build_local_matrices(*m);
   g_m = m;
   g_dir_set = 0;
@@ -365,6 +398,7 @@ void hmgFindInitialGuesses(unsigned int nlevels) {
     SAY("         Null initial guess will be considered (x0 = [0]).\n");
     return;
   }
+  if (!ensure_host_maps(fine)) return;
   // coarse meshes: every second voxel of the finer level (femhmg.c:1844-1916)
   const auto t0 = std::chrono::steady_clock::now();
   std::vector<Model*> levels{&fine};
@@ -519,16 +553,30 @@ void hmgSolveHomogenization(void) {
     g_stats.kernel_launches += st.kernel_launches;
     if (!g_quiet) cudapcgPrintSolverMetrics();
   }
-  if (!block) {  // host vectors of the one-by-one path
-    m.rhs.assign(m.ndof, 0.0);
-    x.assign(m.ndof, 0.0);
+  // One-by-one path: right-hand side, solution and tensor volume term stay on the device unless
+  // x must come back to the host (-xo, -e: the solution files are written from it).
+  const bool on_device = !g_export_x && !g_export_fields;
+  if (!block) {  // host vectors (and, for the host path, maps) of the one-by-one path
+    if (!on_device && !ensure_host_maps(m)) { cudapcgEnd(); return; }
+    m.rhs.assign(on_device ? 0 : m.ndof, 0.0);
+    x.assign(on_device ? 3 : m.ndof, 0.0);  // 3: the 2-vector solvers' reduced sums
   }
   for (int k = 0; k < nd && !block; k++) {
     const int dir = dirs[k];
     SAY("    ------------------------------------------------------\n    Analysis on %s:\n", DIR_STR[dir]);
     auto t = std::chrono::steady_clock::now();
-    assemble_rhs(m, dir, m.rhs.data());
-    cudapcgSetRHS(m.rhs.data());
+    int axis = dir, comp = 0;
+    if (m.analysis != FLUID) case_axis(m, dir, axis, comp);
+    if (on_device) {
+      if (!cudapcgB200SetLoadCaseRHS(axis, comp, (double)axis_len(m, axis), m.CB.data())) {
+        fail(std::string("right-hand side: ") + cudapcgB200LastError());
+        cudapcgEnd();
+        return;
+      }
+    } else {
+      assemble_rhs(m, dir, m.rhs.data());
+      cudapcgSetRHS(m.rhs.data());
+    }
     g_stats.rhs_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
     if (g_use_x0 && !g_x0_file.empty()) {  // femhmg.c:1047-1067: <prefix>_<dir>.bin
       const std::string fn = g_x0_file + "_" + std::to_string(dir) + ".bin";
@@ -551,7 +599,7 @@ void hmgSolveHomogenization(void) {
     }
     SAY("    Solving system of equations...\n");
     if (two_vector) cudapcgSetXReduceShift(dir <= 2 ? dir : 0);  // femhmg.c:1068
-    cudapcgSolve(x.data());
+    cudapcgSolve(on_device && !two_vector ? nullptr : x.data());
     if (!g_quiet) cudapcgPrintSolverMetrics();
     cudapcgB200Stats st;
     cudapcgB200GetStats(&st);
@@ -580,7 +628,18 @@ void hmgSolveHomogenization(void) {
       if (f) { fwrite(x.data(), sizeof(double), m.ndof, f); fclose(f); }
     }
     t = std::chrono::steady_clock::now();
-    update_C(m, dir, x.data());
+    if (on_device) {  // the volume term reduced on the device, the face term here
+      double volume[6];
+      const unsigned ns = m.analysis == ELASTIC ? 6 : 3;
+      if (!cudapcgB200VolumeTerm(m.CB.data(), ns, volume)) {
+        fail(std::string("tensor update: ") + cudapcgB200LastError());
+        cudapcgEnd();
+        return;
+      }
+      update_C_from_volume(m, dir, volume);
+    } else {
+      update_C(m, dir, x.data());
+    }
     g_stats.update_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
     if (g_report) {
       char buf[512];
@@ -710,7 +769,10 @@ int chfemB200RunThermalBatch(unsigned int nsamples, const chfemB200ThermalSample
     for (int c = 0; c < 256; c++) m.props_keys[c] = -1;
     for (unsigned k = 0; k < t.nmat; k++) { m.props_keys[t.colors[k]] = (int)k; m.props[k] = t.conductivity[k]; }
     std::string err;
-    if (!read_image(m, t.voxels, nullptr) || !build_maps(m, err)) { ok[s] = 0; continue; }
+    if (!read_colors(m, t.voxels, nullptr)) { ok[s] = 0; continue; }
+    build_elem_mat(m);
+    if (!build_maps(m, err)) { ok[s] = 0; continue; }
+    m.host_maps = true;
     build_local_matrices(m);
   }
   for (unsigned s = 0; s < nsamples; s++)
@@ -757,7 +819,7 @@ int chfemB200Run(const uint8_t* voxels, const char* nf, int direction, int solve
 }
 
 unsigned long long chfemB200ModelArraySize(int which) {
-  if (!g_m) return 0;
+  if (!g_m || !ensure_host_maps(*g_m)) return 0;
   const Model& m = *g_m;
   switch (which) {
     case 0: return m.keys.size() * 2;
@@ -791,12 +853,12 @@ int chfemB200CopyModelArray(int which, void* dst, unsigned long long bytes) {
   return 1;
 }
 int chfemB200AssembleRHS(int direction, double* dst) {
-  if (!g_m || !dst) return 0;
+  if (!g_m || !dst || !ensure_host_maps(*g_m)) return 0;
   assemble_rhs(*g_m, direction, dst);
   return 1;
 }
 int chfemB200UpdateC(int direction, const double* x, double* C_out) {
-  if (!g_m || !x) return 0;
+  if (!g_m || !x || !ensure_host_maps(*g_m)) return 0;
   update_C(*g_m, direction, x);
   if (C_out) memcpy(C_out, g_m->C, sizeof(double) * g_m->C_dim);
   return 1;

@@ -36,7 +36,12 @@ struct Model {
   long ndof = 0;
   unsigned nd = 1;                   // DOF per node (thermal 1, elastic 3; Stokes layout is special)
   unsigned C_dim = 9;
-  // maps
+  // the image as read: one colour byte per voxel of the file, x fastest (refinement not applied)
+  std::vector<uint8_t> colors;
+  unsigned frows = 0, fcols = 0, fslices = 0;
+  // maps (thermal / elastic: built on the host only when a host path needs them, else the
+  // device builds the node keys from the colours)
+  bool host_maps = false;
   std::vector<uint16_t> elem_mat;    // material index per voxel
   std::vector<uint16_t> keys;        // 16-bit node keys (thermal/elastic)
   std::vector<uint8_t> fluid_keys;   // 8-bit node fluid keys (Stokes)
@@ -58,6 +63,8 @@ bool build_maps(Model& m, std::string& err);
 void build_local_matrices(Model& m);
 void assemble_rhs(const Model& m, int direction, double* rhs);
 void update_C(Model& m, int direction, const double* x);
+// material index of model voxel (r, c, l) (refined grid), from elem_mat or from the colours
+int voxel_material(const Model& m, long r, long c, long l);
 void update_C_from_volume(Model& m, int direction, const double* volume);
 void case_axis(const Model& m, int direction, int& axis, int& comp);
 long axis_len(const Model& m, int axis);

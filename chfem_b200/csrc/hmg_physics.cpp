@@ -336,6 +336,12 @@ void update_C(Model& m, int dir, const double* x) {
   for (int s = 0; s < ns; s++) m.C[s * ns + dir] = acc[s] / (double)N;
 }
 
+int voxel_material(const Model& m, long r, long c, long l) {
+  if (!m.elem_mat.empty()) return m.elem_mat[r + c * (long)m.ny + l * (long)m.ny * m.nx];
+  const long ref = m.refinement;
+  return m.props_keys[m.colors[(size_t)(l / ref) * m.frows * m.fcols + (size_t)(r / ref) * m.fcols + (size_t)(c / ref)]];
+}
+
 // The effective-tensor column of load case dir from the volume term sum_e CB_e x_e (reduced on
 // the device, cudapcgB200SolveLoadCases) plus the boundary face term -- the same sums as
 // update_C, split where the device takes over.
@@ -349,11 +355,10 @@ void update_C_from_volume(Model& m, int dir, const double* volume) {
   case_axis(m, dir, axis, comp);
   const double jump = (double)axis_len(m, axis);
   const int nd = m.nd, ns = (m.analysis == ELASTIC) ? 6 : 3, ec = 8 * nd;
-  const long R = m.ny, C = m.nx;
   double acc[6] = {0, 0, 0, 0, 0, 0};
   for (int s = 0; s < ns; s++) acc[s] = volume[s];
   for_boundary_voxels(m, axis, [&](long r, long c, long l) {
-    const double* CB = m.CB.data() + (size_t)m.elem_mat[r + c * R + l * R * C] * ns * ec;
+    const double* CB = m.CB.data() + (size_t)voxel_material(m, r, c, l) * ns * ec;
     for (int f = 0; f < 4; f++)
       for (int s = 0; s < ns; s++) acc[s] += CB[s * ec + FACE[axis][f] * nd + comp] * jump;
   });

@@ -117,7 +117,9 @@ typedef struct _pcgmodel {
 /* cudapcg.cu:348-355 */ cudapcgFlag_t cudapcgSetPeriodic2DOFMap(cudapcgIdMap_t *vars);
 /* cudapcg.cu:357-363 */ cudapcgFlag_t cudapcgSetDOF2PeriodicMap(cudapcgIdMap_t *nodes);
 /* cudapcg.cu:365-375 */ cudapcgFlag_t cudapcgSetLclMtxs(cudapcgVar_t *LclMtxs);
-/* cudapcg.cu:389-409 */ cudapcgFlag_t cudapcgSolve(cudapcgVar_t *x);  /* CG2/MINRES2: x[0..2] = reduced sums */
+/* cudapcg.cu:389-409 */ cudapcgFlag_t cudapcgSolve(cudapcgVar_t *x);  /* CG2/MINRES2: x[0..2] = reduced sums;
+                                                                        x = NULL (CG/MINRES): the solution stays
+                                                                        on the device only */
 /* cudapcg.cu:411-434 */ cudapcgFlag_t cudapcgSetHeaderString(char *header);
 /* cudapcg.cu:434-448 */ cudapcgFlag_t cudapcgPrintSolverReport(void);
 /* cudapcg.cu:450-469 */ cudapcgFlag_t cudapcgPrintSolverReport2(char *dest);
@@ -211,6 +213,24 @@ const char *cudapcgB200BatchLastError(void);
    material (thermal) or (E, nu) per material (elastic).  field_out: host, nf * nodes doubles. */
 cudapcgFlag_t cudapcgB200ComputeFields(int block_index, int axis, int comp, double jump, const double *props,
                                        double *field_out);
+/* The one-by-one load-case loop on the device (femhmg.c:1030-1110 without the host's RHS
+   assembly, x copy and updateC loop): cudapcgB200SetLoadCaseRHS builds the right-hand side of
+   load case (axis, comp, jump) from the node keys and element matrices (thermal / elastic) or
+   the pore map (Stokes: CB = the model's 3x24 + 8 velocity-averaging entries, axis = flow
+   direction), as the host's assembly (femhmg_thermal_3D.c / femhmg_elastic_3D.c / _fluid_3D.c
+   assembleRHS); after cudapcgSolve, cudapcgB200VolumeTerm returns the volume term sum_e CB_e x_e
+   of the tensor column (ns = 3 thermal / Stokes, 6 elastic; CB per material in the layout of
+   cudapcgB200SolveLoadCases).  The face term is the caller's (a few boundary voxels). */
+cudapcgFlag_t cudapcgB200SetLoadCaseRHS(int axis, int comp, double jump, const double *CB);
+cudapcgFlag_t cudapcgB200VolumeTerm(const double *CB, unsigned int ns, double *moments);
+/* Node material keys built on the device from the voxel image's colours (thermal / elastic,
+   NBN): colors = rows x cols x slices bytes with x fastest (the .raw order, femhmg.c:1644-1700),
+   each voxel split into refinement^3 model voxels; material_of_color[256] = the material index
+   of each colour (-1: not listed, which is an error).  Replaces building the keys on the host
+   and cudapcgSetImage(keys) (femhmg.c:1000-1004, femhmg_3D.c:19-75): one byte per voxel
+   crosses PCIe instead of two. */
+cudapcgFlag_t cudapcgB200SetImageColors(const uint8_t *colors, unsigned int rows, unsigned int cols, unsigned int slices,
+                                        unsigned int refinement, const int *material_of_color);
 /* Initial guess of the next cudapcgSolve from a device vector of nvars doubles (the device
    counterpart of cudapcgSetX0(x0, 0); cleared by cudapcgSetX0(NULL, 0)). */
 cudapcgFlag_t cudapcgB200SetX0Device(const double *x0);

@@ -330,3 +330,38 @@ def test_block_export_roundtrip(tmp_path):
     C2, log = H.run_exec(H.CHFEM_EXEC, nf, raw, "--multirhs", "-xi", prefix)
     assert log.count("Initial guess satisfied") == 6
     assert H.rel_to_max(C2, C1) < 1e-12
+
+
+# ---------------------------------------------------------------------------------------
+# Node keys built on the device from the image's colours (the one-call and block paths) are
+# the host's keys bit for bit: the operator applied with either is identical.
+@pytest.mark.parametrize("name,analysis,shape,nmat,refinement", [("th4", 0, (5, 7, 6), 4, 1), ("el3_ref2", 1, (3, 4, 5), 3, 2)])
+def test_device_keys_from_colors(tmp_path, name, analysis, shape, nmat, refinement):
+    from chfem_b200 import _native
+    from chfem_b200.io import import_nf
+    img = H.small_image(shape, nmat, seed=zlib.crc32(name.encode()) % 10000)
+    nf, raw = H.write_small_case(str(tmp_path), name, img, analysis, refinement=refinement)
+    a = host_arrays(nf, raw)
+    lut = (ctypes.c_int * 256)(*([-1] * 256))  # colour -> material index
+    for i, p in enumerate(import_nf(nf)["properties_of_materials"]):
+        lut[p[0]] = i
+    x = np.random.default_rng(2).standard_normal(a["ndof"])
+    lib = _native.cudapcg()
+    colors = np.ascontiguousarray(img.reshape(-1))
+    nz, ny, nx = img.shape
+    ys = []
+    for device_keys in (False, True):
+        setup_model(lib, a)
+        if device_keys:
+            assert lib.cudapcgB200SetImageColors(colors.ctypes.data_as(ctypes.c_void_p), ny, nx, nz, refinement, lut), \
+                lib.cudapcgB200LastError()
+        y = np.zeros(a["ndof"])
+        assert lib.cudapcgB200ApplyOperator(x.ctypes.data_as(ctypes.c_void_p), y.ctypes.data_as(ctypes.c_void_p))
+        lib.cudapcgEnd()
+        ys.append(y)
+    np.testing.assert_array_equal(ys[0], ys[1])
+    # a colour outside the list is an error, not a key
+    setup_model(lib, a)
+    lut[int(colors[0])] = -1
+    assert not lib.cudapcgB200SetImageColors(colors.ctypes.data_as(ctypes.c_void_p), ny, nx, nz, refinement, lut)
+    lib.cudapcgEnd()
