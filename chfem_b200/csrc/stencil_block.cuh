@@ -12,6 +12,7 @@
 // follows the single-solve recurrence; only the summation order of the operator differs
 // (neighbour by neighbour instead of element by element).
 #pragma once
+#include <type_traits>
 #include <utility>
 #include "common.cuh"
 #include "stencil_te.cuh"
@@ -101,8 +102,21 @@ __device__ __forceinline__ void blk_pair_step(const T* pl0, const T* pl1, const 
 #pragma unroll
     for (int cj = 0; cj < ND; cj++) {
       const T kv = K[ci * ED + cj];
+      if constexpr (std::is_same<T, float>::value && NR >= 2) {
+        // two right-hand sides per instruction (packed FP32 FMA of sm_100): the same rounding
+        // as two scalar FMAs, half the issue slots of the FMA stream; an odd last one alone
+        const float2 kk = make_float2(kv, kv);
 #pragma unroll
-      for (int k = 0; k < NR; k++) out[k][ci] = fma(kv, v[k][cj], out[k][ci]);
+        for (int k = 0; k + 1 < NR; k += 2) {
+          const float2 o = __ffma2_rn(kk, make_float2(v[k][cj], v[k + 1][cj]), make_float2(out[k][ci], out[k + 1][ci]));
+          out[k][ci] = o.x;
+          out[k + 1][ci] = o.y;
+        }
+        if constexpr (NR % 2) out[NR - 1][ci] = fma(kv, v[NR - 1][cj], out[NR - 1][ci]);
+      } else {
+#pragma unroll
+        for (int k = 0; k < NR; k++) out[k][ci] = fma(kv, v[k][cj], out[k][ci]);
+      }
     }
 }
 template <int ND, typename T, int NR, int... Ps>
