@@ -33,9 +33,16 @@ def compute_property(property, array, mat_props=None, voxel_size=1e-6, solver=No
     if direction not in directions:
         raise ValueError(f"Invalid direction: {direction}")
     direction_int = directions[direction]
-    thermal_expansion = mat_props is not None and analysis_type == 1 and any(len(p) == 3 for p in mat_props.values())
+    # elasticity with (young, poisson, alpha): the effective thermal expansion is returned as one
+    # more row (compute_properties.py:66-79 of chfem, chfem_wrapper.c:43-80)
+    thermal_expansion = (mat_props is not None and analysis_type == 1 and
+                         any(hasattr(p, '__len__') and len(p) == 3 for p in mat_props.values()))
     if thermal_expansion:
-        raise ValueError("Thermal expansion analysis is not provided by chfem_b200.")
+        if direction != 'all':
+            raise ValueError(f"Invalid direction for thermal expansion analysis: {direction}. Must be \"all\".")
+        for mat, props in mat_props.items():
+            if len(props) < 3:
+                raise ValueError(f"Invalid properties {props} for material {mat}. Expected thermal expansion coefficient.")
     output_fields_flag = 1 if output_fields is not None else 0
     if solver is None:
         solver = 'minres' if property == 'permeability' else 'cg'
@@ -101,8 +108,14 @@ def compute_property(property, array, mat_props=None, voxel_size=1e-6, solver=No
                              C.ctypes.data_as(ctypes.c_void_p))
         if n == 0:
             raise RuntimeError("chfem_b200 failed: " + lib.chfemB200LastError().decode())
+        out = C[: n * n].reshape(n, n).tolist()
+        if thermal_expansion:
+            lib.hmgGetThermalExpansion.restype = ctypes.POINTER(ctypes.c_double)
+            na = lib.hmgGetThermalExpansionDim()
+            if na:
+                out.append(lib.hmgGetThermalExpansion()[:na])
     finally:
         if tmp is not None:
             tmp.close()
             os.remove(tmp.name)
-    return C[: n * n].reshape(n, n).tolist()
+    return out

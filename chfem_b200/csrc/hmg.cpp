@@ -647,6 +647,20 @@ void hmgSolveHomogenization(void) {
       g_report_text += buf;
     }
   }
+  if (m.analysis == ELASTIC && m.has_thermal_expansion) {
+    // femhmg.c:1121-1168: one more solve, under a unit temperature rise, after the load cases;
+    // the effective expansion follows from its stress and the tensor just computed
+    SAY("    ------------------------------------------------------\n    Thermal expansion analysis:\n");
+    if (!ensure_host_maps(m)) { cudapcgEnd(); return; }
+    std::vector<double> rhs(m.ndof);
+    assemble_rhs_thermal_expansion(m, rhs.data());
+    double volume[6];
+    const bool ok = cudapcgSetRHS(rhs.data()) && cudapcgSetX0(nullptr, 0) && (cudapcgSolve(nullptr), true) &&
+                    cudapcgB200VolumeTerm(m.CB.data(), 6, volume);
+    if (!ok) { fail(std::string("thermal expansion: ") + cudapcgB200LastError()); cudapcgEnd(); return; }
+    if (!g_quiet) cudapcgPrintSolverMetrics();
+    update_thermal_expansion(m, volume);
+  }
   cudapcgSetX0(nullptr, 0);
   cudapcgFreeArrays();
   cudapcgEnd();
@@ -681,16 +695,23 @@ void hmgPrintConstitutiveMtx(void) {
     printf("\n");
   }
   printf("-------------------------------------------------------\n");
+  if (m.analysis == ELASTIC && m.has_thermal_expansion) {  // femhmg_elastic_3D.c:1625-1631
+    const double* a = m.thermal_expansion;
+    printf("Effective thermal expansion:\n");
+    printf("  %.8e  %.8e  %.8e\n  %.8e  %.8e  %.8e\n  %.8e  %.8e  %.8e\n", a[0], a[5], a[4], a[5], a[1], a[3], a[4], a[3], a[2]);
+    printf("-------------------------------------------------------\n");
+  }
 }
 var* hmgGetConstitutiveMtx(void) { return g_m ? g_m->C : nullptr; }
 unsigned int hmgGetConstitutiveMtxDim(void) { return g_m ? g_m->C_dim : 0; }
-var* hmgGetThermalExpansion(void) { return nullptr; }
-unsigned int hmgGetThermalExpansionDim(void) { return 0; }
+var* hmgGetThermalExpansion(void) { return (g_m && g_m->analysis == ELASTIC && g_m->has_thermal_expansion) ? g_m->thermal_expansion : nullptr; }
+unsigned int hmgGetThermalExpansionDim(void) { return hmgGetThermalExpansion() ? 6 : 0; }
 logical hmgSaveConstitutiveMtx(const char* filename) {
   if (!g_m) return 0;
   FILE* f = fopen(filename, "wb");
   if (!f) return 0;
   fwrite(g_m->C, sizeof(double), g_m->C_dim, f);
+  if (hmgGetThermalExpansionDim()) fwrite(g_m->thermal_expansion, sizeof(double), 6, f);  // femhmg.c:1362-1363
   fclose(f);
   return 1;
 }

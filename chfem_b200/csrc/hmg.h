@@ -29,6 +29,7 @@ struct Model {
   int props_keys[256];               // colour -> material index (-1 when not listed)
   double alpha[256] = {0};
   bool has_thermal_expansion = false;
+  double thermal_expansion[6] = {0, 0, 0, 0, 0, 0};  // effective, Voigt xx yy zz yz xz xy
   double xreduce_stab = -1.0;        // %xreduce_scale_factor (negative: not given)
   std::string nf, nf_noext, raw;
   // sizes
@@ -63,6 +64,10 @@ bool build_maps(Model& m, std::string& err);
 void build_local_matrices(Model& m);
 void assemble_rhs(const Model& m, int direction, double* rhs);
 void update_C(Model& m, int direction, const double* x);
+// thermal expansion load case (elastic): right-hand side of a unit temperature rise, and the
+// effective expansion from the tensor C and the volume term of its solution
+void assemble_rhs_thermal_expansion(const Model& m, double* rhs);
+void update_thermal_expansion(Model& m, const double* volume);
 // material index of model voxel (r, c, l) (refined grid), from elem_mat or from the colours
 int voxel_material(const Model& m, long r, long c, long l);
 void update_C_from_volume(Model& m, int direction, const double* volume);

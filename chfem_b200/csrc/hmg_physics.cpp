@@ -336,6 +336,73 @@ void update_C(Model& m, int dir, const double* x) {
   for (int s = 0; s < ns; s++) m.C[s * ns + dir] = acc[s] / (double)N;
 }
 
+// ---- thermal expansion (femhmg_elastic_3D.c:464-505 RHS, :863-1074 effective expansion) ----
+// A unit temperature rise gives material m the eigenstrain alpha_m (1,1,1,0,0,0) and the stress
+// sigma_m = D_m alpha_m (1,1,1,0,0,0) = alpha_m E_m / (1 - 2 nu_m) on the normal components.
+// The reference evaluates the element load B^T sigma at the voxel centre, where every shape
+// gradient is 1/4 (+-1, +-1, +-1), with the sign + where the node sits at coordinate 1.
+static double thermal_stress(const Model& m, int mat) {
+  const double E = m.props[2 * mat], nu = m.props[2 * mat + 1];
+  return m.alpha[mat] * E / (1.0 - 2.0 * nu);
+}
+
+void assemble_rhs_thermal_expansion(const Model& m, double* rhs) {
+  std::memset(rhs, 0, sizeof(double) * m.ndof);
+  const long R = m.ny, C = m.nx, L = m.nz, N = m.N;
+  double f[4][24];
+  for (unsigned mat = 0; mat < m.nmat && mat < 4; mat++) {
+    const double sn = thermal_stress(m, (int)mat);
+    for (int a = 0; a < 8; a++) {
+      const int x = dcol(a), y = -drow(a), z = 1 - dlay(a);
+      f[mat][3 * a + 0] = 0.25 * sn * (x ? 1.0 : -1.0);
+      f[mat][3 * a + 1] = 0.25 * sn * (y ? 1.0 : -1.0);
+      f[mat][3 * a + 2] = 0.25 * sn * (z ? 1.0 : -1.0);
+    }
+  }
+  for (long e = 0; e < N; e++) {
+    const long r = e % R, c = (e / R) % C, l = e / (R * C);
+    const double* fe = f[m.elem_mat[e]];
+    for (int a = 0; a < 8; a++) {
+      const long n = elem_node(r, c, l, a, R, C, L);
+      for (int ci = 0; ci < 3; ci++) rhs[3 * n + ci] += fe[3 * a + ci];
+    }
+  }
+}
+
+// volume: sum_e CB_e x_e of the thermal-expansion solution (6 values).  The mean strain of the
+// periodic fluctuation, which the reference also adds (C times it), is zero: every node enters
+// the sum once per local index and the centre gradients of the 8 shape functions sum to zero.
+void update_thermal_expansion(Model& m, const double* volume) {
+  double count[4] = {0, 0, 0, 0};
+  const long ref3 = (long)m.refinement * m.refinement * m.refinement;
+  for (uint8_t c : m.colors) count[m.props_keys[c]] += (double)ref3;
+  double stress[6], beta[6];
+  for (int k = 0; k < 6; k++) stress[k] = volume[k];
+  for (unsigned mat = 0; mat < m.nmat && mat < 4; mat++)
+    for (int k = 0; k < 3; k++) stress[k] -= count[mat] * thermal_stress(m, (int)mat);
+  for (int k = 0; k < 6; k++) beta[k] = -stress[k] / (double)m.N;
+  // effective expansion: C alpha = beta (6x6 elimination with partial pivoting)
+  double M[6][7];
+  for (int i = 0; i < 6; i++) {
+    for (int j = 0; j < 6; j++) M[i][j] = m.C[6 * i + j];
+    M[i][6] = beta[i];
+  }
+  for (int i = 0; i < 6; i++) {
+    int p = i;
+    for (int j = i + 1; j < 6; j++) if (std::fabs(M[j][i]) > std::fabs(M[p][i])) p = j;
+    if (p != i) for (int k = 0; k < 7; k++) std::swap(M[i][k], M[p][k]);
+    for (int j = i + 1; j < 6; j++) {
+      const double s = M[j][i] / M[i][i];
+      for (int k = i; k < 7; k++) M[j][k] -= s * M[i][k];
+    }
+  }
+  for (int i = 5; i >= 0; i--) {
+    double v = M[i][6];
+    for (int j = i + 1; j < 6; j++) v -= M[i][j] * m.thermal_expansion[j];
+    m.thermal_expansion[i] = v / M[i][i];
+  }
+}
+
 int voxel_material(const Model& m, long r, long c, long l) {
   if (!m.elem_mat.empty()) return m.elem_mat[r + c * (long)m.ny + l * (long)m.ny * m.nx];
   const long ref = m.refinement;
