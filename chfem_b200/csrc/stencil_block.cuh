@@ -42,9 +42,18 @@ struct BlkArgs {
 template <int ND, int NR>
 __host__ __device__ constexpr int blk_ps() { return (NR * ND) % 2 ? NR * ND : NR * ND + 1; }
 
+// Element matrices in shared memory.  FP32 elastic: "quad" layout, the 3 columns of one
+// (row, local node b) block padded to 4 so one 16-byte load brings all three; a material's
+// 24 x 8 quads are followed by 4 padding words, which puts the 4 materials' copies of a quad
+// in different banks.  Otherwise row-major ED x ED per material plus one padding word.
+template <int ND, typename T>
+__host__ __device__ constexpr bool blk_quad() { return ND == 3 && std::is_same<T, float>::value; }
+template <int ND, typename T>
+__host__ __device__ constexpr int blk_kstride() { return blk_quad<ND, T>() ? 24 * 8 * 4 + 4 : 64 * ND * ND + 1; }
+
 template <int ND, typename T, int NR>
 inline size_t blk_smem_bytes() {
-  return (size_t)4 * (64 * ND * ND + 1) * sizeof(T) + (size_t)3 * TE_PP * blk_ps<ND, NR>() * sizeof(T) + 16;
+  return (size_t)4 * blk_kstride<ND, T>() * sizeof(T) + (size_t)3 * TE_PP * blk_ps<ND, NR>() * sizeof(T) + 16;
 }
 
 // The (voxel e, local node b) pairs of the node-centred operator, ordered by the neighbour
@@ -98,10 +107,14 @@ __device__ __forceinline__ void blk_pair_step(const T* pl0, const T* pl1, const 
   }
   const T* K = kb[e] + e * ND * ED + b * ND;
 #pragma unroll
-  for (int ci = 0; ci < ND; ci++)
+  for (int ci = 0; ci < ND; ci++) {
+    [[maybe_unused]] float4 kq;
+    if constexpr (blk_quad<ND, T>()) kq = *reinterpret_cast<const float4*>(kb[e] + ((e * ND + ci) * 8 + b) * 4);
 #pragma unroll
     for (int cj = 0; cj < ND; cj++) {
-      const T kv = K[ci * ED + cj];
+      T kv;
+      if constexpr (blk_quad<ND, T>()) kv = cj == 0 ? kq.x : (cj == 1 ? kq.y : kq.z);
+      else kv = K[ci * ED + cj];
       if constexpr (std::is_same<T, float>::value && NR >= 2) {
         // two right-hand sides per instruction (packed FP32 FMA of sm_100): the same rounding
         // as two scalar FMAs, half the issue slots of the FMA stream; an odd last one alone
@@ -118,6 +131,7 @@ __device__ __forceinline__ void blk_pair_step(const T* pl0, const T* pl1, const 
         for (int k = 0; k < NR; k++) out[k][ci] = fma(kv, v[k][cj], out[k][ci]);
       }
     }
+  }
 }
 template <int ND, typename T, int NR, int... Ps>
 __device__ __forceinline__ void blk_all_pairs(std::integer_sequence<int, Ps...>, const T* pl0, const T* pl1, const T* pl2, int ctr,
@@ -139,10 +153,18 @@ __global__ void __launch_bounds__(TE_NT) k_blk_apply(BlkArgs<ND, T> a) {
   for (int k = 0; k < NR; k++) all_done = all_done && a.sc[k].done;
   if (all_done) return;
   T* sK = reinterpret_cast<T*>(smem_raw);
-  const int kstride = ED * ED + 1;
+  constexpr int kstride = blk_kstride<ND, T>();
   T* sP = sK + 4 * kstride;
   const int tid = threadIdx.x + TE_TR * threadIdx.y;
-  for (int i = tid; i < 4 * ED * ED; i += TE_NT) sK[(i / (ED * ED)) * kstride + i % (ED * ED)] = (i < a.nmat * ED * ED) ? a.Kd[i] : T(0);
+  if constexpr (blk_quad<ND, T>()) {
+    for (int q = tid; q < 4 * kstride; q += TE_NT) {
+      const int mat = q / kstride, w = q % kstride, row = w / 32, b = (w / 4) % 8, cj = w % 4;
+      const bool used = w < 24 * 8 * 4 && cj < 3 && mat < a.nmat;
+      sK[q] = used ? a.Kd[(size_t)mat * ED * ED + row * ED + b * 3 + cj] : T(0);
+    }
+  } else {
+    for (int i = tid; i < 4 * ED * ED; i += TE_NT) sK[(i / (ED * ED)) * kstride + i % (ED * ED)] = (i < a.nmat * ED * ED) ? a.Kd[i] : T(0);
+  }
   if (tid < NR) { sbeta[tid] = T(a.sc[tid].beta); sdone[tid] = a.sc[tid].done; }
   __syncthreads();
   const int R = a.R, C = a.C, L = a.L;
