@@ -10,7 +10,8 @@ precision='fp64'|'mixed', multirhs (all load cases as one block solve), initial_
 tolerance and so the tensor are unchanged).  output_fields=prefix writes, per load case, the
 solution and its field as <prefix>_temperature|displacement|velocity_<case>.bin and
 <prefix>_flux|stress|pressure_<case>.bin (read them with import_*_field_from_chfem), like
-chfem_exec -e.
+chfem_exec -e.  Elasticity with {phase: (young, poisson, alpha)} also returns the effective thermal
+expansion (Voigt xx yy zz yz xz xy) as a seventh row, like the reference.
 """
 import ctypes
 import os
