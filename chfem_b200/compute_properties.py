@@ -68,7 +68,7 @@ def compute_property(property, array, mat_props=None, voxel_size=1e-6, solver=No
                              "[(phase_id, young, poisson),] for elasticity.")
         if array.dtype != np.uint8:
             raise ValueError("Domain must be uint8 dtype.")
-        if 0 not in np.unique(array):  # the reference checks this for every property (compute_properties.py:105-107)
+        if not (array == 0).any():  # the reference checks this for every property (compute_properties.py:105-107)
             raise ValueError("No fluid phase found in the domain.")
         if output_fields is None:
             tmp = tempfile.NamedTemporaryFile(delete=False, suffix=".nf")

@@ -65,8 +65,9 @@ def export_for_chfem(filename, array, analysis_type, mat_props=None, voxel_size=
     2 permeability (mat_props None).  Returns the dict of written settings.
     """
     domain = array.astype(np.uint8)
-    ids, counts = np.unique(domain, return_counts=True)
-    materials = dict(sorted(zip(ids.tolist(), counts.tolist())))
+    hist = np.bincount(domain.reshape(-1), minlength=256)  # voxels per colour (a sort-free count)
+    ids = np.nonzero(hist)[0]
+    materials = dict(zip(ids.tolist(), hist[ids].tolist()))
     if mat_props is not None:
         props_ids, img_ids = set(mat_props.keys()), set(materials.keys())
         if props_ids != img_ids:
