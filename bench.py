@@ -182,6 +182,8 @@ class Resident:
                  dof_of_node=arr(1, np.uint32), node_of_dof=arr(2, np.uint32), border=arr(3, np.uint8),
                  lcl=arr(4, np.float64))
         self.CB = arr(7, np.float64)
+        self.lcl_size = int(a["lcl"].size)
+        self.nmat = int(a["nkeys"])
         self.dims = (info[0], info[1], info[2])
         setup_model(self.c, a)
         self.c.cudapcgSetSolver(w.get("solver", 0))
@@ -461,6 +463,13 @@ def reference_arm(args, w):
         print(json.dumps({"impl": "reference", "unavailable": "reference CUDA build oracle/_ref/chfem_exec_ref not built"}))
         return
     img = make_image(w, 0)
+    ncase = 6 if w["analysis"] == 1 else 3
+    ndof = img.size * (3 if w["analysis"] == 1 else 1) if w["analysis"] != 2 else None
+    if ndof:  # stock FP64 path: 2-byte keys, element matrices; per load case RHS up and x down
+        h2d = int(2 * img.size + 8 * 2 * 576 + ncase * 8 * ndof)
+        d2h = int(ncase * 8 * ndof)
+    else:
+        h2d, d2h = None, None
     with tempfile.TemporaryDirectory() as wd:
         nf, raw = write_case(wd, w, img)
         times, walls, its = [], [], []
@@ -482,11 +491,15 @@ def reference_arm(args, w):
         line = {"metric": metric_name(w), "value": v, "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic", "impl": "reference",
-                "config": config_dict(args, w, 1) | {"reference_build": "stock FP64, 16-bit keys, 128 threads/block, sm_100a"},
+                "config": config_dict(args, w, 1) | {"precision": "fp64", "multirhs": False, "initial_guess": "zero",
+                                                     "reference_build": "stock FP64, 16-bit keys, 128 threads/block, sm_100a"},
                 "iterations": its,
-                "cpu_baseline": {"value": v, "unit": "s", "cores": 0, "kind": "reference",
-                                 "sample": "reference CUDA build (its only solver path) on the same B200, full workload"},
-                "e2e": {"value": float(np.mean(walls)), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                "cpu_baseline": {"value": v, "unit": "s", "cores": os.cpu_count() or 1, "kind": "reference",
+                                 "sample": "the reference's CUDA build on the same B200 (its only solver path: it has no CPU "
+                                           "solver), full workload; host threads = its OpenMP host code"},
+                "e2e": {"value": float(np.mean(walls)), "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "path": "chfem_exec process wall time (files in, tensor out); copies: node keys, element matrices, "
+                                "and per load case its right-hand side up and its solution down"}}
         print(json.dumps(line))
 
 
@@ -522,7 +535,7 @@ def config_dict(args, w, n):
     return {"workload": args.workload, "shape_zyx": list(w["shape"]), "analysis": ["thermal", "elastic", "stokes"][w["analysis"]],
             "load_cases": 6 if w["analysis"] == 1 else 3, "tol": w["tol"], "precision": w["precision"],
             "solver": "PMINRES" if w.get("solver", 0) == 1 else "PCG", "preconditioner": "Jacobi",
-            "multirhs": bool(w.get("multirhs", False)),
+            "multirhs": bool(w.get("multirhs", False)), "initial_guess": "learned" if w.get("learned") else "zero",
             "l2": "working set > L2 (vectors of the elastic 128^3 case ~25-50 MB each)", "parallelism": f"samples x{n}"}
 
 
@@ -534,6 +547,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-check", action="store_true", help="skip the untimed reference run (tensor error, same-precision ratio)")
+    ap.add_argument("--no-north-star", action="store_true", help="skip the 256^3 north-star sub-record of the default workload")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -616,10 +631,102 @@ def main():
     clk = clocks.stop()
     step_s = allmax(dev_total / args.steps)
     wall_step = allmax(wall / args.steps)
-    # dominant kernel, timed live on the library's stream
+    dev_bytes = int(model.c.cudapcgB200DeviceBytes())
+    roofline = dominant_kernel_roofline(model, w, block, args.workload)
+    total_its = sum(its)
+    dof_its = model.ndof * total_its / (dev_total / args.steps)
+    # e2e through the public API (host image in, tensor out): one untimed call, then the mean of
+    # as many calls as timed steps, like the device-time value
+    e2e_step(img, nf, w)
+    e2e_times, breakdowns = [], []
+    C = None
+    for k in range(args.steps):
+        t, C, st = e2e_step(img, nf, w)
+        ncs = max(1, st.n_cases)
+        breakdowns.append([t - st.total_seconds, st.rhs_seconds, float(sum(st.solve_seconds[i] for i in range(ncs))),
+                           st.update_seconds, st.setup_seconds, st.total_seconds])
+        e2e_times.append(t)
+    bm = np.mean(np.array(breakdowns), axis=0)
+    breakdown = {"model_build_and_upload_s": bm[0], "rhs_assembly_s": bm[1], "solve_device_s": bm[2],
+                 "tensor_update_s": bm[3], "solver_setup_s": bm[4], "solver_call_total_s": bm[5]}
+    e2e = allmax(float(np.mean(e2e_times)))
+    # the plain method end to end (FP64, one load case at a time, zero guess): its tensor is the
+    # FP64 reference of the mixed / block / learned one
+    plain_e2e, Cp = None, None
+    if w["precision"] == "mixed" or block or learned_run:
+        from chfem_b200 import _native as _nat
+        lib = _nat.chfem()
+        lib.chfemB200SetQuiet(1)
+        flat = np.ascontiguousarray(img.reshape(-1))
+        Cp = np.zeros(36)
+        t0 = time.perf_counter()
+        n = lib.chfemB200Run(flat.ctypes.data_as(ctypes.c_void_p), nf.encode(), 6, w.get("solver", 0), 1, 0, 0,
+                             Cp.ctypes.data_as(ctypes.c_void_p))
+        plain_e2e = allmax(time.perf_counter() - t0)
+        Cp = Cp[: n * n].reshape(n, n)
+    ncase = 6 if w["analysis"] == 1 else 3
+    ns = 6 if w["analysis"] == 1 else 3
+    # copies of one call: the 1-byte image (node keys are built on the device from it; Stokes
+    # pore maps on the host), the element matrices and tensor matrices, and out the volume-term
+    # moments of every load case
+    maps = 9 * model.N if w["analysis"] == 2 else 0
+    h2d = int(img.size + maps + 8 * (model.lcl_size + model.CB.size))
+    d2h = int(ncase * ns * 8)
+    model.close()
+    cpu, ref = None, None
+    if rank == 0 and world == 1:
+        if not args.no_cpu_baseline:
+            its64 = sum(fp64["iterations"]) if fp64 else total_its
+            cpu = cpu_baseline(wd, w, img, its64)
+        if not args.no_reference_check:
+            ref = reference_once(wd, w, img)
+    if rank == 0:
+        line = {"metric": metric_name(w), "value": step_s, "unit": "s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32+f64" if w["precision"] == "mixed" else "f64", "data": "synthetic",
+                "config": config_dict(args, w, world),
+                "iterations": its, "dof_iterations_per_s": dof_its, "wall_s_per_step": wall_step,
+                "plain_fp64_pcg": fp64, "speedup_vs_plain_fp64": (fp64["time_s"] / step_s) if fp64 else None,
+                "tensor_diag": [float(C[i, i]) for i in range(C.shape[0])] if C is not None else None,
+                "roofline": roofline, "clocks": clk, "gpu_launches": int(launches / max(1, args.steps)),
+                "device_bytes_per_dof": dev_bytes / model.ndof,
+                "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "path": ("compute_property(..., initial_guess='learned')" if learned_run else
+                                 "chfemB200Run (compute_property's native entry)") + ": image in host memory -> tensor; "
+                                f"mean of {args.steps} calls after one untimed call",
+                        "breakdown": breakdown},
+                "cpu_baseline": cpu, "samples_per_s": world / step_s}
+        if Cp is not None and C is not None:
+            line["tensor_rel_err_vs_plain_fp64"] = rel_to_max(C, Cp)
+        if plain_e2e is not None:
+            line["plain_fp64_e2e_s"] = plain_e2e
+            line["e2e_speedup_vs_plain_fp64"] = plain_e2e / e2e
+        if ref is not None:
+            line["reference_check"] = ref
+            if C is not None and ref.get("C") is not None:
+                line["tensor_rel_err_vs_reference"] = rel_to_max(C, np.array(ref["C"]))
+            if fp64 and ref.get("solve_s"):
+                line["same_precision_ratio"] = ref["solve_s"] / fp64["time_s"]
+        if learned_run:
+            line["learned_guess"] = {"network_s": float(np.mean(net_times[-args.steps:])), "zero_guess_block": zero_guess,
+                                     "weights": "chfem_b200/weights/elastic_unet.bin"}
+        if rank == 0 and world == 1 and not args.no_north_star and args.workload == DEFAULT:
+            line["north_star_256"] = north_star_256()
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def rel_to_max(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def dominant_kernel_roofline(model, w, block, workload):
+    """The dominant kernel timed live on the library's stream (CUDA events around each launch),
+    its algorithmic bytes per node against the measured HBM peak."""
     peak, peak_kind = load_peaks()
-    prec = w["precision"]
-    es = 4 if prec == "mixed" else 8
+    es = 4 if w["precision"] == "mixed" else 8
     if w["analysis"] == 2:
         kern_which, kname = 3, "k_fl_apply<MR> (Stokes operator + PMINRES step, one right-hand side)"
         per_unit = 4 * es * 4 + 4 * 2  # per DOF row set, approximate
@@ -629,7 +736,11 @@ def main():
         tn = 'float' if es == 4 else 'double'
         if block:
             nr = 6 if nd == 3 else 3
-            kern_which, kname = 5, f"k_blk_apply<{nd},{tn},{nr}> (block operator + directions + dots, {nr} load cases)"
+            asm = model.nmat <= 2 and os.environ.get("CHFEM_B200_BLOCK_OP") != "element"
+            kern_which = 5
+            kname = (f"k_asm_apply<{nd},{tn},{nr}> (block operator, stencil assembled per material configuration, "
+                     f"+ directions + dots, {nr} load cases)" if asm else
+                     f"k_blk_apply<{nd},{tn},{nr}> (block operator + directions + dots, {nr} load cases)")
             per_unit = nr * 4 * nd * es + 2  # per load case s, d_old in; d_new, q out; one 16-bit key
         else:
             kern_which, kname = 1, f"k_te_apply<{nd},{tn},TE_PCG> (operator + direction + dot)"
@@ -637,78 +748,70 @@ def main():
         units = model.N
     kt = model.kernel_time(kern_which, reps=30)
     achieved = per_unit * units / kt / 1e9 if kt > 0 else None
+    # FP work of the operator as the reference formulates it (64 element blocks per node)
     fl_unit = (1152 if w["analysis"] == 1 else 80) * ((6 if w["analysis"] == 1 else 3) if block else 1)
     flops = fl_unit * units / kt / 1e12 if (kt > 0 and w["analysis"] != 2) else None
-    traffic = profiled_traffic(args.workload)
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                "kernel": kname, "kernel_ms": kt * 1e3, "bytes_per_unit": per_unit, "units_per_launch": units,
-                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
-                "fp_tflops_achieved": flops}
-    total_its = sum(its)
-    dof_its = model.ndof * total_its / (dev_total / args.steps)
-    # e2e through the public API (host image in, tensor out)
-    e2e_times = []
-    C = None
-    st = None
-    breakdown = None
-    for k in range(3):
-        t, C, st = e2e_step(img, nf, w)
-        if not e2e_times or t < min(e2e_times):
-            ncs = max(1, st.n_cases)
-            breakdown = {"model_build_and_upload_s": t - st.total_seconds, "rhs_assembly_s": st.rhs_seconds,
-                         "solve_device_s": float(sum(st.solve_seconds[i] for i in range(ncs))),
-                         "tensor_update_s": st.update_seconds, "solver_setup_s": st.setup_seconds,
-                         "solver_call_total_s": st.total_seconds}
-        e2e_times.append(t)
-    e2e = allmax(min(e2e_times))
-    plain_e2e = None
-    if w.get("learned"):  # the plain method end to end: FP64, one load case at a time, zero guess
-        from chfem_b200 import _native as _nat
-        lib = _nat.chfem()
-        lib.chfemB200SetQuiet(1)
-        flat = np.ascontiguousarray(img.reshape(-1))
-        Cp = np.zeros(36)
-        t0 = time.perf_counter()
-        lib.chfemB200Run(flat.ctypes.data_as(ctypes.c_void_p), nf.encode(), 6, 0, 1, 0, 0, Cp.ctypes.data_as(ctypes.c_void_p))
-        plain_e2e = allmax(time.perf_counter() - t0)
-    ncase = 6 if w["analysis"] == 1 else 3
-    maps = 2 * model.N if w["analysis"] != 2 else 9 * model.N  # node keys, or the Stokes DOF maps
-    if block:  # right-hand sides and tensor volume terms stay on the device
-        ns = 6 if w["analysis"] == 1 else 3
-        h2d = int(img.size + maps)
-        d2h = int(ncase * ns * 8)
-    else:
-        h2d = int(img.size + maps + ncase * model.ndof * 8)
-        d2h = int(ncase * model.ndof * 8)
-    model.close()
-    cpu = None
-    if rank == 0 and not args.no_cpu_baseline and world == 1:
-        its64 = sum(fp64["iterations"]) if fp64 else total_its
-        cpu = cpu_baseline(wd, w, img, its64)
-    if rank == 0:
-        line = {"metric": metric_name(w), "value": step_s, "unit": "s", "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": False, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32+f64" if prec == "mixed" else "f64", "data": "synthetic",
-                "config": config_dict(args, w, world),
-                "iterations": its, "dof_iterations_per_s": dof_its, "wall_s_per_step": wall_step,
-                "plain_fp64_pcg": fp64, "speedup_vs_plain_fp64": (fp64["time_s"] / step_s) if fp64 else None,
-                "tensor_diag": [float(C[i, i]) for i in range(C.shape[0])] if C is not None else None,
-                "roofline": roofline, "clocks": clk, "gpu_launches": int(launches),
-                "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                        "path": "chfemB200Run (compute_property's native entry): image in host memory -> tensor",
-                        "breakdown": breakdown},
-                "cpu_baseline": cpu, "samples_per_s": world / step_s}
-        if learned_run:
-            line["learned_guess"] = {"network_s": float(np.mean(net_times[-args.steps:])), "zero_guess_block": zero_guess,
-                                     "weights": "chfem_b200/weights/elastic_unet.bin"}
-            if plain_e2e is not None:
-                line["plain_fp64_e2e_s"] = plain_e2e
-                line["e2e_speedup_vs_plain_fp64"] = plain_e2e / e2e
-        print(json.dumps(line))
-    if dist:
-        dist.destroy_process_group()
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None, "traffic": profiled_traffic(workload),
+            "kernel": kname, "kernel_ms": kt * 1e3, "bytes_per_unit": per_unit, "units_per_launch": units,
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+            "fp_tflops_reference_formulation": flops}
 
+
+def reference_once(wd, w, img):
+    """One run of the reference's CUDA build (stock FP64, one load case at a time) on the same
+    workload, outside the timed region: its tensor (for the tensor error of this line) and its
+    summed solver times (for the same-precision ratio against this library's plain FP64 PCG)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "chfem_exec_ref")
+    if not os.path.exists(exe):
+        return None
+    nf, raw = write_case(wd, w, img)
+    out = os.path.join(wd, "ref_C.bin")
+    p = subprocess.run([exe, nf, raw, "-d", "6", "-b", out], capture_output=True, text=True, timeout=3000, cwd=wd)
+    if p.returncode != 0 or not os.path.exists(out):
+        return {"error": p.stdout[-200:]}
+    C = np.fromfile(out)
+    k = int(round(np.sqrt(C.size)))
+    solve = sum(float(l.split(":")[1].split()[0]) for l in p.stdout.splitlines() if "| Elapsed time:" in l)
+    its = [int(l.split("iteration:")[1].split(",")[0]) for l in p.stdout.splitlines() if "iteration:" in l and "residual" in l]
+    return {"C": C[: k * k].reshape(k, k).tolist(), "solve_s": solve, "iterations": its,
+            "build": "reference CUDA build, stock FP64 PCG one load case at a time, zero guess"}
+
+
+def north_star_256():
+    """The 256^3 elastic job of the north star, once: mixed + block + learned guess against the
+    plain FP64 PCG (one load case at a time), end to end through the public API, with the device
+    time, iterations and tensor error of each, and the block operator's roofline at that size."""
+    from chfem_b200 import _native, compute_property
+    w = WORKLOADS["elastic256_grf_mixed_block_learned"]
+    img = make_image(w, 0)
+    wd = tempfile.mkdtemp()
+    nf, raw = write_case(wd, w, img)
+    kw = dict(mat_props=w["props"], voxel_size=1.0, solver_tolerance=w["tol"], solver_maxiter=w["maxit"])
+    compute_property("elasticity", img, precision="mixed", multirhs=True, initial_guess="learned", **kw)  # warm
+    t0 = time.perf_counter()
+    C = np.array(compute_property("elasticity", img, precision="mixed", multirhs=True, initial_guess="learned", **kw))
+    t_fast = time.perf_counter() - t0
+    st = _native.solve_stats()
+    fast = {"e2e_s": t_fast, "device_solve_s": float(sum(st.solve_seconds[i] for i in range(max(1, st.n_cases)))),
+            "iterations": [int(st.iterations[i]) for i in range(max(1, st.n_cases))]}
+    lib = _native.chfem()
+    lib.chfemB200SetQuiet(1)
+    flat = np.ascontiguousarray(img.reshape(-1))
+    Cp = np.zeros(36)
+    t0 = time.perf_counter()
+    lib.chfemB200Run(flat.ctypes.data_as(ctypes.c_void_p), nf.encode(), 6, 0, 1, 0, 0, Cp.ctypes.data_as(ctypes.c_void_p))
+    t_plain = time.perf_counter() - t0
+    st = _native.solve_stats()
+    plain = {"e2e_s": t_plain, "device_solve_s": float(sum(st.solve_seconds[i] for i in range(max(1, st.n_cases)))),
+             "iterations": [int(st.iterations[i]) for i in range(max(1, st.n_cases))]}
+    Cp = Cp.reshape(6, 6)
+    m = Resident(nf, raw, w)
+    rl = dominant_kernel_roofline(m, w, True, "elastic256_grf_mixed_block_learned")
+    m.close()
+    return {"workload": "elastic256_grf_mixed_block_learned", "shape_zyx": list(w["shape"]), "dof": 3 * img.size, "load_cases": 6,
+            "mixed_block_learned": fast, "plain_fp64_pcg": plain, "e2e_speedup": t_plain / t_fast,
+            "tensor_rel_err_vs_plain_fp64": rel_to_max(C, Cp), "roofline": rl}
 
 if __name__ == "__main__":
     main()

@@ -26,7 +26,7 @@ def _load(name):
     if not os.path.exists(path):
         raise NativeLibraryMissing(
             f"{path} is missing: build the chfem_b200 native libraries first "
-            "(python -m chfem_b200.build)")
+            "(python -c 'import __graft_entry__; __graft_entry__.build()' at the repository root)")
     lib = ctypes.CDLL(path, mode=ctypes.RTLD_LOCAL)
     _libs[name] = lib
     return lib

@@ -57,11 +57,40 @@ static bool blk_prepare() {
   return true;
 }
 
+// tile of the FP32 elastic assembled operator: CHFEM_B200_ASM_TILE = "8x1", "6x2", "8x2" or "4x2"
+// (columns x layers per thread)
+static int asm_tile_choice() {
+  static int choice = -1;
+  if (choice < 0) {
+    const char* e = getenv("CHFEM_B200_ASM_TILE");
+    choice = ASM_TILE_6x2;
+    if (e && !strcmp(e, "8x1")) choice = ASM_TILE_8x1;
+    if (e && !strcmp(e, "8x2")) choice = ASM_TILE_8x2;
+    if (e && !strcmp(e, "4x2")) choice = ASM_TILE_4x2;
+  }
+  return choice;
+}
+
+// The assembled-stencil block operator pass (stencil_asm.cuh, launched from asm_apply.cu).
+template <int ND, typename T, int NR>
+static bool launch_asm_block(T* dold, T* dnew) {
+  const int tile = asm_tile_choice();
+  const int nb = asm_block_ctas<ND, T, NR>(S->R, S->C, S->L, num_sms(), tile);
+  if (nb < 1) { set_err("assembled block operator", "launch configuration"); return false; }
+  if (!ensure_reduction(nb)) return false;
+  BlkArgs<ND, T> a{(const T*)B->s, dold, dnew, (T*)B->q, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->nvars, B->sc, redctl(nb)};
+  const cudaError_t e = asm_block_launch<ND, T, NR>(a, tabdev<T>(), nb, tile, S->stream);
+  S->launches++;
+  if (e != cudaSuccess) { set_err("assembled block operator", cudaGetErrorString(e)); return false; }
+  return true;
+}
+
 template <int ND, typename T, int NR>
 static bool launch_blk_apply(int parity) {
   const long n = S->nvars;
   T* dold = (T*)(parity ? B->d1 : B->d0);
   T* dnew = (T*)(parity ? B->d0 : B->d1);
+  if (asm_applies()) return launch_asm_block<ND, T, NR>(dold, dnew);
   const dim3 block(TE_TR, TE_TC);
   if (!blk_prepare<ND, T, NR>()) return false;
   const int nb = te_ctas(k_blk_apply<ND, T, NR>, blk_smem_bytes<ND, T, NR>());
@@ -96,6 +125,7 @@ template <typename T>
 static double time_block_kernel_T(int which, unsigned reps) {
   const int nr = S->nd == 3 ? 6 : 3;
   if (!ensure_vectors<T>() || !ensure_K<T>() || !block_alloc<T>(nr)) return -1.0;
+  if (asm_applies() && !ensure_tab<T>()) return -1.0;
   if (!ensure_reduction(needed_blocks())) return -1.0;
   for (int k = 0; k < nr; k++) {
     DevScalars& h = B->h_sc[k];
@@ -442,6 +472,7 @@ template <typename T>
 static bool solve_block_T(int nr, const double* const* rhs, const double* const* x0, int x0_mode, double* const* x_out,
                           unsigned* iters, double* resid, const LoadCases* lc = nullptr) {
   if (!ensure_vectors<T>() || !ensure_K<T>() || !block_alloc<T>(nr)) return false;
+  if (asm_applies() && !ensure_tab<T>()) return false;
   const long n = S->nvars;
   bool has_x0[BLK_MAX] = {false};
   for (int k = 0; k < nr; k++) {
@@ -500,5 +531,42 @@ static bool solve_block_T(int nr, const double* const* rhs, const double* const*
   }
   S->iteration = maxit;
   S->found = found_all;
+  return true;
+}
+
+// y_k = A v_k for nr host vectors through the block operator pass of the block solver (the
+// assembled-stencil pass for two-material models): direction formed with beta = 0, so
+// d_new = v and q = A v.
+template <typename T>
+static bool apply_block_T(int nr, const double* const* v, double* const* y) {
+  if (!ensure_vectors<T>() || !ensure_K<T>() || !block_alloc<T>(nr)) return false;
+  if (asm_applies() && !ensure_tab<T>()) return false;
+  if (!ensure_reduction(needed_blocks())) return false;
+  const long n = S->nvars;
+  for (int k = 0; k < nr; k++) {
+    CKV(cudaMemcpyAsync(slice<double>(B->b64, k), v[k], n * 8, cudaMemcpyHostToDevice, S->stream));
+    if (sizeof(T) == 8) CKV(cudaMemcpyAsync(slice<double>(B->s, k), slice<double>(B->b64, k), n * 8, cudaMemcpyDeviceToDevice, S->stream));
+    else k_convert<double, float><<<pw_grid(n), PW_NT, 0, S->stream>>>(slice<double>(B->b64, k), slice<float>(B->s, k), n);
+  }
+  CKV(cudaMemsetAsync(B->d0, 0, (size_t)nr * n * sizeof(T), S->stream));
+  for (int k = 0; k < nr; k++) {
+    DevScalars& h = B->h_sc[k];
+    h = DevScalars{};
+    h.delta = 1.0; h.delta0 = 1.0; h.delta_old = 1.0;
+  }
+  CKV(cudaMemcpyAsync(B->sc, B->h_sc, nr * sizeof(DevScalars), cudaMemcpyHostToDevice, S->stream));
+  CKV(cudaMemsetAsync(S->d_ticket, 0, sizeof(unsigned), S->stream));
+  bool ok;
+  if (S->nd == 1 && nr == 3) ok = launch_blk_apply<1, T, 3>(0);
+  else if (S->nd == 3 && nr == 6) ok = launch_blk_apply<3, T, 6>(0);
+  else if (S->nd == 3 && nr == 3) ok = launch_blk_apply<3, T, 3>(0);
+  else { set_err("cudapcgB200ApplyBlockOperator", "block sizes are 3 (thermal, elastic) and 6 (elastic)"); return false; }
+  if (!ok) { set_err("cudapcgB200ApplyBlockOperator", cudaGetErrorString(cudaGetLastError())); return false; }
+  for (int k = 0; k < nr; k++) {
+    if (sizeof(T) == 4) k_convert<float, double><<<pw_grid(n), PW_NT, 0, S->stream>>>(slice<float>(B->q, k), slice<double>(B->b64, k), n);
+    else CKV(cudaMemcpyAsync(slice<double>(B->b64, k), slice<double>(B->q, k), n * 8, cudaMemcpyDeviceToDevice, S->stream));
+    CKV(cudaMemcpyAsync(y[k], slice<double>(B->b64, k), n * 8, cudaMemcpyDeviceToHost, S->stream));
+  }
+  CKV(cudaStreamSynchronize(S->stream));
   return true;
 }

@@ -22,6 +22,8 @@
 #include "stencil_fluid.cuh"
 #include "stencil_fluid2.cuh"
 #include "stencil_block.cuh"
+#include "stencil_asm.cuh"
+#include "asm_apply.h"
 #include "stencil_fluid_block.cuh"
 #include "loadcase.cuh"
 #include "fields.cuh"
@@ -102,6 +104,9 @@ struct Solver {
   uint8_t* d_bkeys = nullptr;
   double* d_K64 = nullptr;  // dense element matrices, FP64 (FP64 solves, residual replacement)
   float* d_K32 = nullptr;   // dense element matrices, FP32 (mixed-precision iterations)
+  // assembled neighbour blocks of a two-material model (stencil_asm.cuh), per precision
+  double* d_tab64 = nullptr;
+  float* d_tab32 = nullptr;
   // Krylov work vectors, typed for the precision in use
   int vec_prec = -1;
   void* r = nullptr; void* r2 = nullptr; void* d0 = nullptr; void* d1 = nullptr;
@@ -186,9 +191,9 @@ static void free_vectors() {
 static void free_model_dev() {
   if (!S) return;
   free_ptr(S->d_keys); free_ptr(S->d_dof_of_node); free_ptr(S->d_node_of_dof); free_ptr(S->d_bkeys);
-  free_ptr(S->d_K64); free_ptr(S->d_K32);
+  free_ptr(S->d_K64); free_ptr(S->d_K32); free_ptr(S->d_tab64); free_ptr(S->d_tab32);
   S->d_keys = nullptr; S->d_dof_of_node = S->d_node_of_dof = nullptr; S->d_bkeys = nullptr;
-  S->d_K64 = nullptr; S->d_K32 = nullptr;
+  S->d_K64 = nullptr; S->d_K32 = nullptr; S->d_tab64 = nullptr; S->d_tab32 = nullptr;
   S->have_K = S->have_keys = S->have_maps = false;
 }
 
@@ -221,6 +226,31 @@ static bool ensure_vectors() {
   return true;
 }
 
+// Assembled neighbour blocks (stencil_asm.cuh) of a thermal/elastic model of at most two
+// materials; CHFEM_B200_BLOCK_OP=element keeps the element-by-element block operator.
+static bool asm_applies() {
+  if (S->analysis == CUDAPCG_FLUID_3D || S->nmat > 2) return false;
+  const char* e = getenv("CHFEM_B200_BLOCK_OP");
+  return !(e && !strcmp(e, "element"));
+}
+template <typename T> static T*& tabdev();
+template <> double*& tabdev<double>() { return S->d_tab64; }
+template <> float*& tabdev<float>() { return S->d_tab32; }
+template <typename T>
+static bool ensure_tab() {
+  if (tabdev<T>()) return true;
+  if (!S->have_K) { set_err("solve", "local matrices were not set (cudapcgSetLclMtxs)"); return false; }
+  const int bs = S->nd == 1 ? 1 : (sizeof(T) == 4 ? 12 : 9);  // AsmLayout<ND, T, NR>::BS
+  std::vector<double> t64((size_t)ASM_NBLK * bs);
+  asm_build_table(S->nd, S->nmat, S->Kd.data(), bs, t64.data());
+  std::vector<T> t(t64.begin(), t64.end());
+  T* d = nullptr;
+  CKV(cudaMalloc(&d, t.size() * sizeof(T)));
+  CKV(cudaMemcpy(d, t.data(), t.size() * sizeof(T), cudaMemcpyHostToDevice));
+  tabdev<T>() = d;
+  return true;
+}
+
 template <typename T> static T* Kdev();
 template <> double* Kdev<double>() { return S->d_K64; }
 template <> float* Kdev<float>() { return S->d_K32; }
@@ -235,6 +265,7 @@ static bool ensure_K() {
   CKV(cudaMalloc(&dk, kt.size() * sizeof(T)));
   CKV(cudaMemcpy(dk, kt.data(), kt.size() * sizeof(T), cudaMemcpyHostToDevice));
   if (sizeof(T) == 8) S->d_K64 = (double*)dk; else S->d_K32 = (float*)dk;
+  if (asm_applies() && !ensure_tab<T>()) return false;
   if (S->analysis == CUDAPCG_FLUID_3D) {
     if (sizeof(T) == 8) CKV(cudaMemcpyToSymbol(c_flK64, kt.data(), 1024 * sizeof(double)));
     else CKV(cudaMemcpyToSymbol(c_flK32, kt.data(), 1024 * sizeof(float)));
@@ -302,6 +333,23 @@ static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, i
     a.rc = redctl(g);
     if (fuse) k_fl_apply<T, TE_PCG><<<g, FL_NT, 0, S->stream>>>(a);
     else k_fl_apply<T, TE_PLAIN><<<g, FL_NT, 0, S->stream>>>(a);
+  } else if (asm_applies()) {
+    int nb;
+    cudaError_t e;
+    if (S->nd == 1) {
+      nb = fuse ? asm_te_ctas<1, T, TE_PCG>(S->R, S->C, S->L, num_sms()) : asm_te_ctas<1, T, TE_PLAIN>(S->R, S->C, S->L, num_sms());
+      if (nb < 1 || !ensure_reduction(nb)) return false;
+      TeArgs<1, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->cur_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
+      e = fuse ? asm_te_launch<1, T, TE_PCG>(a, tabdev<T>(), nb, S->stream) : asm_te_launch<1, T, TE_PLAIN>(a, tabdev<T>(), nb, S->stream);
+    } else {
+      nb = fuse ? asm_te_ctas<3, T, TE_PCG>(S->R, S->C, S->L, num_sms()) : asm_te_ctas<3, T, TE_PLAIN>(S->R, S->C, S->L, num_sms());
+      if (nb < 1 || !ensure_reduction(nb)) return false;
+      TeArgs<3, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->cur_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
+      e = fuse ? asm_te_launch<3, T, TE_PCG>(a, tabdev<T>(), nb, S->stream) : asm_te_launch<3, T, TE_PLAIN>(a, tabdev<T>(), nb, S->stream);
+    }
+    S->launches++;
+    if (e != cudaSuccess) { set_err("operator pass", cudaGetErrorString(e)); return false; }
+    return true;
   } else {
     const dim3 block(TE_TR, TE_TC);
     if (S->nd == 1) {
@@ -969,6 +1017,7 @@ cudapcgFlag_t cudapcgSetLclMtxs(cudapcgVar_t* Lm) {
   }
   S->have_K = true;
   free_ptr(S->d_K64); free_ptr(S->d_K32); S->d_K64 = nullptr; S->d_K32 = nullptr;
+  free_ptr(S->d_tab64); free_ptr(S->d_tab32); S->d_tab64 = nullptr; S->d_tab32 = nullptr;
   invalidate_graphs();  // captured launches hold the old matrix pointers
   if (S->analysis == CUDAPCG_FLUID_3D && !set_fluid_diag()) return CUDAPCG_FALSE;
   return CUDAPCG_TRUE;
@@ -1285,6 +1334,14 @@ extern "C" cudapcgFlag_t cudapcgB200SolveLoadCases(unsigned int nrhs, const int*
   return (cudapcgFlag_t)S->found;
 }
 
+extern "C" cudapcgFlag_t cudapcgB200ApplyBlockOperator(unsigned int nrhs, const double* const* v, double* const* y) {
+  if (!S || !S->model || !v || !y || nrhs < 1 || nrhs > BLK_MAX) { set_err("cudapcgB200ApplyBlockOperator", "bad arguments"); return CUDAPCG_FALSE; }
+  if (S->analysis == CUDAPCG_FLUID_3D) { set_err("cudapcgB200ApplyBlockOperator", "thermal and elastic models only"); return CUDAPCG_FALSE; }
+  for (unsigned k = 0; k < nrhs; k++) if (!v[k] || !y[k]) { set_err("cudapcgB200ApplyBlockOperator", "null buffer"); return CUDAPCG_FALSE; }
+  const bool ok = (S->precision == CHFEM_B200_FP64) ? apply_block_T<double>((int)nrhs, v, y) : apply_block_T<float>((int)nrhs, v, y);
+  return ok ? CUDAPCG_TRUE : CUDAPCG_FALSE;
+}
+
 extern "C" cudapcgFlag_t cudapcgB200SolveBlock(unsigned int nrhs, const double* const* rhs, const double* const* x0,
                                                int x0_interpolate, double* const* x_out, unsigned int* iterations,
                                                double* residuals) {
@@ -1342,25 +1399,47 @@ extern "C" int cudapcgB200ApplyOperatorNoAlloc(int analysis_flag, unsigned int n
   if (!nrows || !ncols || !nlayers) { set_err(who, "empty model"); return 0; }
   if (nmat < 1 || nmat > 4) { set_err(who, "1 to 4 materials are supported with 16-bit keys"); return 0; }
   if (!keys || !Kdense || !v || !y || !vAv) { set_err(who, "null device pointer"); return 0; }
+  // the kernels index rows, columns and layers with int, and each of the three is stepped
+  // past by one halo node
+  if (nrows > 0x7ffffff0u || ncols > 0x7ffffff0u || nlayers > 0x7ffffff0u) { set_err(who, "model dimension above 2^31 - 16"); return 0; }
+  const bool thermal = analysis_flag == CUDAPCG_THERMAL_3D;
+  const size_t nvals = (size_t)nrows * ncols * nlayers * (thermal ? 1 : 3);
+  // y is written while other CTAs still read v (halo planes), keys and Kdense: no overlap
+  auto overlaps = [](const void* a, size_t na, const void* b, size_t nb_) {
+    const char *pa = (const char*)a, *pb = (const char*)b;
+    return pa < pb + nb_ && pb < pa + na;
+  };
+  const size_t ybytes = nvals * sizeof(double), kbytes = (size_t)nmat * (thermal ? 64 : 576) * sizeof(double);
+  if (overlaps(y, ybytes, v, ybytes) || overlaps(y, ybytes, keys, nvals / (thermal ? 1 : 3) * sizeof(uint16_t)) ||
+      overlaps(y, ybytes, Kdense, kbytes) || overlaps(vAv, sizeof(double), y, ybytes) || overlaps(vAv, sizeof(double), v, ybytes)) {
+    set_err(who, "y (and vAv) must not overlap v, keys or Kdense");
+    return 0;
+  }
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) { set_err(who, cudaGetErrorString(e)); return 0; }
   if (dev < 0 || dev >= 64) { set_err(who, "device ordinal out of range"); return 0; }
-  if (!g_noalloc_addr[dev]) {
+  cudaStream_t st = (cudaStream_t)stream;
+  // The array's device address: looked up again on every call made outside stream capture (a
+  // device reset or a new primary context moves it); a captured call uses the address of the
+  // last uncaptured call on this device.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(st, &cap);
+  if (e != cudaSuccess) { set_err(who, cudaGetErrorString(e)); return 0; }
+  if (cap == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) { set_err(who, e != cudaSuccess ? cudaGetErrorString(e) : "no symbol address"); return 0; }
     g_noalloc_addr[dev] = p;
-  }
-  unsigned char* base = (unsigned char*)g_noalloc_addr[dev];
-  // grid: the persistent stencil schedule, at most one partial per CTA in the array
-  const long R = nrows, C = ncols, L = nlayers;
-  const long tiles = ((R + TE_TR - 1) / TE_TR) * ((C + TE_TC - 1) / TE_TC);
-  if (tiles > NOALLOC_MAX_BLOCKS) {
-    set_err(who, "model too large: more than 8192 column tiles of 32x8 nodes (nrows x ncols above ~2M nodes)");
+  } else if (!g_noalloc_addr[dev]) {
+    set_err(who, "first call on this device made under stream capture: make one call outside capture first");
     return 0;
   }
-  const bool thermal = analysis_flag == CUDAPCG_THERMAL_3D;
+  unsigned char* base = (unsigned char*)g_noalloc_addr[dev];
+  // grid: the persistent stencil schedule (any number of column tiles), at most
+  // NOALLOC_MAX_BLOCKS CTAs, one reduction partial each in the array
+  const long R = nrows, C = ncols, L = nlayers;
+  const long tiles = ((R + TE_TR - 1) / TE_TR) * ((C + TE_TC - 1) / TE_TC);
   const size_t smem = thermal ? te_smem_bytes<1, double>((int)nmat) : te_smem_bytes<3, double>((int)nmat);
   int per_sm = 0, sms = 0;
   e = thermal ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_te_apply<1, double, TE_PLAIN>, TE_NT, smem)
@@ -1369,7 +1448,7 @@ extern "C" int cudapcgB200ApplyOperatorNoAlloc(int analysis_flag, unsigned int n
   if (e != cudaSuccess) { set_err(who, cudaGetErrorString(e)); return 0; }
   const long work = tiles * L;
   const int nb = (int)std::max(1L, std::min<long>({(long)std::max(1, per_sm) * sms, work / TE_MIN_RUN, (long)NOALLOC_MAX_BLOCKS}));
-  cudaStream_t st = (cudaStream_t)stream;
+  (void)cudaGetLastError();  // an earlier call's pending launch error is not this call's
   e = cudaMemsetAsync(base, 0, NOALLOC_HEADER, st);
   if (e != cudaSuccess) { set_err(who, cudaGetErrorString(e)); return 0; }
   DevScalars* sc = (DevScalars*)(base + 256);
@@ -1383,8 +1462,10 @@ extern "C" int cudapcgB200ApplyOperatorNoAlloc(int analysis_flag, unsigned int n
     TeArgs<3, double> a{v, nullptr, nullptr, y, nullptr, nullptr, keys, Kdense, (int)nmat, (int)R, (int)C, (int)L, sc, rc, FIN_STORE, 0, cfg};
     k_te_apply<3, double, TE_PLAIN><<<nb, block, smem, st>>>(a);
   }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) { set_err(who, cudaGetErrorString(e)); return 0; }
   k_noalloc_store_dot<<<1, 32, 0, st>>>(sc, vAv);
-  e = cudaPeekAtLastError();
+  e = cudaGetLastError();
   if (e != cudaSuccess) { set_err(who, cudaGetErrorString(e)); return 0; }
   return 1;
 }

@@ -26,6 +26,23 @@ static bool launch_mr_op_buf(const T* rin, T* rout, const T* q, T* s, double* x,
     if (!ensure_reduction(g)) return false;
     a.rc = redctl(g);
     k_fl_apply<T, TE_MR><<<g, FL_NT, 0, S->stream>>>(a);
+  } else if (asm_applies()) {
+    int nb;
+    cudaError_t e;
+    if (S->nd == 1) {
+      nb = asm_te_ctas<1, T, TE_MR>(S->R, S->C, S->L, num_sms());
+      if (nb < 1 || !ensure_reduction(nb)) return false;
+      TeArgs<1, T> a{rin, q, rout, s, x, d, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->cur_sc, redctl(nb), fin, skip_if_done, cfg};
+      e = asm_te_launch<1, T, TE_MR>(a, tabdev<T>(), nb, S->stream);
+    } else {
+      nb = asm_te_ctas<3, T, TE_MR>(S->R, S->C, S->L, num_sms());
+      if (nb < 1 || !ensure_reduction(nb)) return false;
+      TeArgs<3, T> a{rin, q, rout, s, x, d, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->cur_sc, redctl(nb), fin, skip_if_done, cfg};
+      e = asm_te_launch<3, T, TE_MR>(a, tabdev<T>(), nb, S->stream);
+    }
+    S->launches++;
+    if (e != cudaSuccess) { set_err("operator pass", cudaGetErrorString(e)); return false; }
+    return true;
   } else {
     const dim3 block(TE_TR, TE_TC);
     if (S->nd == 1) {

@@ -1,0 +1,321 @@
+// stencil_asm.cuh -- block operator pass for images of at most two materials, with each node's
+// 27-neighbour stencil assembled from the table of per-material-configuration blocks
+// (asm_table.cuh).
+//
+// Each thread computes ZB nodes stacked along the layers, so the values of the neighbour planes
+// the ZB nodes share are read from shared memory once for all of them.
+#pragma once
+#include <algorithm>
+#include <type_traits>
+#include <utility>
+#include "common.cuh"
+#include "asm_table.cuh"
+#include "stencil_te.cuh"
+#include "stencil_block.cuh"
+
+namespace chfem {
+
+// raw staging record of a point (ASYNC): s then d_old for every right-hand side in global order,
+// an odd word count so that consecutive lanes' records fall on distinct banks
+template <int ND, int NR>
+__host__ __device__ constexpr int asm_raw_stride() { return 2 * NR * ND + 1; }
+
+template <int ND, typename T, int NR, int TC, int ZB, bool ASYNC = false>
+inline size_t asm_smem_bytes() {
+  using Lo = AsmLayout<ND, T, NR>;
+  const size_t pp = (size_t)(TE_TR + 2) * (TC + 2);
+  return ((size_t)ASM_NBLK * Lo::BS + (size_t)(ZB + 2) * pp * Lo::PS + (ASYNC ? (size_t)ZB * pp * asm_raw_stride<ND, NR>() : 0)) * sizeof(T);
+}
+
+// 4-byte (or 8-byte) asynchronous global -> shared copy (sm_80+ cp.async; completion by
+// cp.async.wait_all of the issuing thread)
+template <typename T>
+__device__ __forceinline__ void asm_cp_async(T* dst, const T* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(T) == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+// L2 prefetch of [p, p + bytes) rounded out to 16-byte boundaries (sm_90+ bulk prefetch)
+__device__ __forceinline__ void asm_prefetch_l2(const void* p, size_t bytes) {
+  const size_t a0 = (size_t)p & ~(size_t)15, a1 = ((size_t)p + bytes + 15) & ~(size_t)15;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a0), "r"((unsigned)(a1 - a0)) : "memory");
+}
+__device__ __forceinline__ void asm_cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void asm_cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// does any of the ZB nodes use the neighbour position (Q plane, DR row, DC column)?
+template <int ND, int ZB>
+__host__ __device__ constexpr bool asm_pos_used(int Q, int DR, int DC) {
+  for (int z = 0; z < ZB; z++) {
+    const int dl = Q - z;
+    if (dl >= -1 && dl <= 1 && asm_used<ND>((DR + 1) + 3 * (DC + 1) + 9 * (dl + 1))) return true;
+  }
+  return false;
+}
+
+template <int ND, typename T, int NR, int ZB, int Q, int DR, int DC, int Z>
+__device__ __forceinline__ void asm_to_node(const T* __restrict__ sT, const unsigned (&m)[ZB],
+                                            const typename AsmLayout<ND, T, NR>::V (&val)[ND][AsmLayout<ND, T, NR>::NW],
+                                            typename AsmLayout<ND, T, NR>::V (&out)[ZB][ND][AsmLayout<ND, T, NR>::NW]) {
+  constexpr int DL = Q - Z;
+  if constexpr (DL >= -1 && DL <= 1) asm_block<ND, T, (DR + 1) + 3 * (DC + 1) + 9 * (DL + 1)>(sT, m[Z], val, out[Z]);
+}
+template <int ND, typename T, int NR, int ZB, int Q, int DR, int DC, int... Zs>
+__device__ __forceinline__ void asm_to_nodes(std::integer_sequence<int, Zs...>, const T* __restrict__ sT, const unsigned (&m)[ZB],
+                                             const typename AsmLayout<ND, T, NR>::V (&val)[ND][AsmLayout<ND, T, NR>::NW],
+                                             typename AsmLayout<ND, T, NR>::V (&out)[ZB][ND][AsmLayout<ND, T, NR>::NW]) {
+  (asm_to_node<ND, T, NR, ZB, Q, DR, DC, Zs>(sT, m, val, out), ...);
+}
+
+// Position P of the (ZB + 2) x 3 x 3 neighbour positions: plane Q = P / 9 - 1 relative to the
+// first node's layer, row DR = P % 3 - 1, column DC = (P / 3) % 3 - 1.  Loads the position's
+// values for every right-hand side once and adds them into each node that reaches it.
+template <int ND, typename T, int NR, int ZB, int P>
+__device__ __forceinline__ void asm_position(const T* const (&pl)[ZB + 2], int ctr, const T* __restrict__ sT, const unsigned (&m)[ZB],
+                                             typename AsmLayout<ND, T, NR>::V (&out)[ZB][ND][AsmLayout<ND, T, NR>::NW]) {
+  constexpr int Q = P / 9 - 1, DR = P % 3 - 1, DC = (P / 3) % 3 - 1;
+  if constexpr (asm_pos_used<ND, ZB>(Q, DR, DC)) {
+    using Lo = AsmLayout<ND, T, NR>;
+    using V = typename Lo::V;
+    const V* pv = reinterpret_cast<const V*>(pl[Q + 1] + (ctr + DR + DC * TE_PR) * Lo::PS);
+    V val[ND][Lo::NW];
+#pragma unroll
+    for (int cj = 0; cj < ND; cj++)
+#pragma unroll
+      for (int w = 0; w < Lo::NW; w++) val[cj][w] = pv[cj * Lo::NW + w];
+    asm_to_nodes<ND, T, NR, ZB, Q, DR, DC>(std::make_integer_sequence<int, ZB>{}, sT, m, val, out);
+  }
+}
+template <int ND, typename T, int NR, int ZB, int... Ps>
+__device__ __forceinline__ void asm_positions(std::integer_sequence<int, Ps...>, const T* const (&pl)[ZB + 2], int ctr,
+                                              const T* __restrict__ sT, const unsigned (&m)[ZB],
+                                              typename AsmLayout<ND, T, NR>::V (&out)[ZB][ND][AsmLayout<ND, T, NR>::NW]) {
+  (asm_position<ND, T, NR, ZB, Ps>(pl, ctr, sT, m, out), ...);
+}
+
+// The block PCG operator pass (same contract as k_blk_apply): d_new_k = s_k + beta_k d_old_k,
+// q_k = A d_new_k, and per right-hand side the sum d_new_k . q_k reduced over the grid, whose
+// last CTA sets alpha_k = delta_k / (d_new_k . q_k).  A CTA owns a 32 x TC column of nodes and
+// marches through its run of layers ZB at a time, with ZB + 2 halo'd planes of d_new staged in
+// shared memory (d_new is formed while staging).  Requires node keys of materials 0 and 1 only.
+//
+// ASYNC: the input planes of the next step are copied (s and d_old as they are) by cp.async
+// into a raw buffer while the current step computes, and d_new is formed from it afterwards
+// shared memory to shared memory, so the global-memory latency of the staging overlaps the
+// arithmetic within the CTA.
+//
+// PF: at the start of a step the CTA asks L2 to prefetch (bulk prefetch, one request per
+// contiguous column segment of every input vector) the planes it will stage after the step, so
+// the staging loads that follow the arithmetic find them in L2.
+template <int ND, typename T, int NR, int TC, int ZB, bool ASYNC = false, bool PF = false>
+__global__ void __launch_bounds__(TE_TR * TC) k_asm_apply(BlkArgs<ND, T> a, const T* __restrict__ tab) {
+  using Lo = AsmLayout<ND, T, NR>;
+  using V = typename Lo::V;
+  constexpr int NW = Lo::NW;
+  constexpr int NT = TE_TR * TC;
+  constexpr int PS = Lo::PS;
+  constexpr int PP = TE_PR * (TC + 2);
+  constexpr int NPL = ZB + 2;
+  constexpr int PPT = (PP + NT - 1) / NT;  // staged points per thread and plane
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double sred[NT / 32];
+  __shared__ T sbeta[NR];
+  __shared__ int sdone[NR];
+  bool all_done = true;
+#pragma unroll
+  for (int k = 0; k < NR; k++) all_done = all_done && a.sc[k].done;
+  if (all_done) return;
+  T* sT = reinterpret_cast<T*>(smem_raw);
+  T* sP = sT + ASM_NBLK * Lo::BS;  // ASM_NBLK * BS words keep 16-byte alignment (416 = 16 * 26)
+  const int tid = threadIdx.x + TE_TR * threadIdx.y;
+  for (int i = tid; i < ASM_NBLK * Lo::BS; i += NT) sT[i] = tab[i];
+  if (tid < NR) { sbeta[tid] = T(a.sc[tid].beta); sdone[tid] = a.sc[tid].done; }
+  __syncthreads();
+  const int R = a.R, C = a.C, L = a.L;
+  const size_t RC = (size_t)R * C;
+  const long n = a.n;
+  T beta[NR];
+#pragma unroll
+  for (int k = 0; k < NR; k++) beta[k] = sbeta[k];
+  int r0 = 0, c0 = 0;
+  size_t poff[PPT];  // in-layer node index of this thread's staged points (for the current tile)
+  constexpr int RS = asm_raw_stride<ND, NR>();
+  T* sRaw = sP + NPL * PP * PS;  // ASYNC: ZB raw planes
+  auto slot_of = [&](int l) { return ((l % NPL) + NPL) % NPL; };
+  // PF: L2 prefetch of plane l of the current tile: per input vector and tile column, the rows
+  // of the tile and its halo that are contiguous in memory (a wrapped halo row is left out)
+  auto prefetch_plane = [&](int l) {
+    const size_t lo = (size_t)wrap(l, L) * RC;
+    const int ra = max(r0 - 1, 0), rb = min(r0 + TE_TR, R - 1);
+    for (int i = tid; i < 2 * NR * (TC + 2); i += NT) {
+      const int k = i % NR, arr = (i / NR) % 2, hc = i / (2 * NR);
+      const size_t node = (size_t)ra + (size_t)wrap(c0 + hc - 1, C) * R + lo;
+      const T* base = (arr ? a.dold : a.s) + (size_t)k * n + node * ND;
+      asm_prefetch_l2(base, (size_t)(rb - ra + 1) * ND * sizeof(T));
+    }
+  };
+  // ASYNC: copy plane l into raw slot i
+  auto issue_plane = [&](int l, int i) {
+    const size_t lo = (size_t)wrap(l, L) * RC;
+    T* dst = sRaw + (size_t)i * PP * RS;
+#pragma unroll
+    for (int pi = 0; pi < PPT; pi++) {
+      const int p = tid + pi * NT;
+      if (PP % NT == 0 || p < PP) {
+        const size_t node = poff[pi] + lo;
+#pragma unroll
+        for (int k = 0; k < NR; k++)
+#pragma unroll
+          for (int c = 0; c < ND; c++) {
+            const size_t j = (size_t)k * n + node * ND + c;
+            asm_cp_async(dst + p * RS + k * ND + c, a.s + j);
+            asm_cp_async(dst + p * RS + NR * ND + k * ND + c, a.dold + j);
+          }
+      }
+    }
+  };
+  // ASYNC: d_new of plane l from raw slot i into its ring slot
+  auto form_plane = [&](int l, int i) {
+    const T* src = sRaw + (size_t)i * PP * RS;
+    T* dst = sP + slot_of(l) * PP * PS;
+    for (int p = tid; p < PP; p += NT) {
+#pragma unroll
+      for (int c = 0; c < ND; c++)
+#pragma unroll
+        for (int k = 0; k < NR; k++) dst[p * PS + c * NR + k] = fma(beta[k], src[p * RS + NR * ND + k * ND + c], src[p * RS + k * ND + c]);
+    }
+  };
+  auto load_plane = [&](int l) {
+    const size_t lo = (size_t)wrap(l, L) * RC;
+    T* dst = sP + slot_of(l) * PP * PS;
+#pragma unroll
+    for (int i = 0; i < PPT; i++) {
+      const int p = tid + i * NT;
+      if (PP % NT == 0 || p < PP) {
+        const size_t node = poff[i] + lo;
+#pragma unroll
+        for (int k = 0; k < NR; k++)
+#pragma unroll
+          for (int c = 0; c < ND; c++) {
+            const size_t j = (size_t)k * n + node * ND + c;
+            dst[p * PS + c * NR + k] = fma(beta[k], a.dold[j], a.s[j]);
+          }
+      }
+    }
+  };
+  double acc[NR];
+#pragma unroll
+  for (int k = 0; k < NR; k++) acc[k] = 0.0;
+  const int ctr = (threadIdx.x + 1) + (threadIdx.y + 1) * TE_PR;
+  const TeWork wk(R, C, L, TC);
+  for (long w = wk.begin(), w_end = wk.end(); w < w_end;) {
+    int l0, l1;
+    wk.run(w, w_end, r0, c0, l0, l1);
+    const int r = r0 + threadIdx.x, c = c0 + threadIdx.y;
+    const bool active = (r < R) && (c < C);
+#pragma unroll
+    for (int i = 0; i < PPT; i++) {
+      const int p = min(tid + i * NT, PP - 1);
+      const int gr = wrap(r0 + p % TE_PR - 1, R), gc = wrap(c0 + p / TE_PR - 1, C);
+      poff[i] = (size_t)gr + (size_t)gc * R;
+    }
+    // node keys are fetched one step ahead, so their global-memory latency overlaps the
+    // staging and the previous step's arithmetic; past the run any valid node of the column
+    // stands in (its result is not stored)
+    const size_t col = active ? (size_t)r + (size_t)c * R : 0;
+    unsigned kc[ZB];
+#pragma unroll
+    for (int z = 0; z < ZB; z++) kc[z] = a.keys[col + (size_t)(l0 + z < l1 ? l0 + z : l0) * RC];
+    __syncthreads();  // the previous run's planes are no longer read
+#pragma unroll
+    for (int q = -1; q <= ZB; q++) load_plane(l0 + q);
+    if constexpr (ASYNC) {
+      if (l0 + ZB < l1) {
+#pragma unroll
+        for (int q = 1; q <= ZB; q++) issue_plane(l0 + ZB + q, q - 1);
+        asm_cp_commit();
+      }
+    }
+    __syncthreads();
+    for (int l = l0; l < l1; l += ZB) {
+      if constexpr (PF) {
+        if (l + ZB < l1) {
+#pragma unroll
+          for (int q = 1; q <= ZB; q++) prefetch_plane(l + ZB + q);
+        }
+      }
+      unsigned kn[ZB];
+#pragma unroll
+      for (int z = 0; z < ZB; z++) kn[z] = a.keys[col + (size_t)(l + ZB + z < l1 ? l + ZB + z : l) * RC];
+      if (active) {
+        const T* pl[NPL];
+#pragma unroll
+        for (int q = 0; q < NPL; q++) pl[q] = sP + slot_of(l - 1 + q) * PP * PS;
+        unsigned m[ZB];
+#pragma unroll
+        for (int z = 0; z < ZB; z++) m[z] = asm_config(kc[z]);
+        V out[ZB][ND][NW];
+#pragma unroll
+        for (int z = 0; z < ZB; z++)
+#pragma unroll
+          for (int ci = 0; ci < ND; ci++)
+#pragma unroll
+            for (int ww = 0; ww < NW; ww++) {
+              if constexpr (Lo::PAIRS) out[z][ci][ww] = make_float2(0.f, 0.f);
+              else out[z][ci][ww] = T(0);
+            }
+        asm_positions<ND, T, NR, ZB>(std::make_integer_sequence<int, 9 * (ZB + 2)>{}, pl, ctr, sT, m, out);
+#pragma unroll
+        for (int z = 0; z < ZB; z++) {
+          if (l + z >= l1) break;
+          const size_t node = (size_t)r + (size_t)c * R + (size_t)(l + z) * RC;
+          const T* pc = pl[z + 1] + ctr * PS;
+#pragma unroll
+          for (int ci = 0; ci < ND; ci++)
+#pragma unroll
+            for (int k = 0; k < NR; k++) {
+              T qv;
+              if constexpr (Lo::PAIRS) qv = (k & 1) ? out[z][ci][k >> 1].y : out[z][ci][k >> 1].x;
+              else qv = out[z][ci][k];
+              const size_t j = (size_t)k * n + node * ND + ci;
+              const T vv = pc[ci * NR + k];
+              a.q[j] = qv;
+              a.dnew[j] = vv;
+              acc[k] += (double)vv * (double)qv;
+            }
+        }
+      }
+#pragma unroll
+      for (int z = 0; z < ZB; z++) kc[z] = kn[z];
+      if (l + ZB < l1) {
+        if constexpr (ASYNC) {
+          asm_cp_wait_all();
+          __syncthreads();  // the raw planes have landed; planes l - 1 .. l + ZB - 2 are no longer read
+#pragma unroll
+          for (int q = 1; q <= ZB; q++) form_plane(l + ZB + q, q - 1);
+          __syncthreads();  // the raw slots are free again
+          if (l + 2 * ZB < l1) {
+#pragma unroll
+            for (int q = 1; q <= ZB; q++) issue_plane(l + 2 * ZB + q, q - 1);
+            asm_cp_commit();
+          }
+        } else {
+          __syncthreads();  // planes l - 1 .. l + ZB - 2 are no longer read
+#pragma unroll
+          for (int q = 1; q <= ZB; q++) load_plane(l + ZB + q);
+          __syncthreads();
+        }
+      }
+    }
+    w += l1 - l0;
+  }
+  const bool ismax[NR] = {};
+  double res[NR];
+  if (grid_reduce<NT, NR>(acc, ismax, a.rc, blockIdx.x, res, sred) && tid == 0) {
+#pragma unroll
+    for (int k = 0; k < NR; k++)
+      if (!sdone[k]) { a.sc[k].red[0] = res[k]; a.sc[k].alpha = a.sc[k].delta / res[k]; }
+  }
+}
+
+}  // namespace chfem

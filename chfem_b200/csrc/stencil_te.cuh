@@ -16,7 +16,9 @@
 //   TE_PCG    v = in0 + beta*in1 = s + beta d_old       (PCG direction; written once)
 //   TE_MR     r' = in0 - alpha*in1 = r - alpha q, v = M^-1 r'   (PMINRES; r', x updated)
 #pragma once
+#include <utility>
 #include "common.cuh"
+#include "asm_table.cuh"
 
 namespace chfem {
 
@@ -55,10 +57,10 @@ struct MrCfg {
 // planes they share are read from L2 rather than DRAM.
 constexpr int TE_MIN_RUN = 4;  // layers per CTA at least (halo restaging overhead)
 struct TeWork {
-  int tiles_r, L, lc, nc;
+  int tiles_r, L, lc, nc, tc;
   long tiles, W;
-  __device__ TeWork(int R, int C, int L_) : tiles_r((R + TE_TR - 1) / TE_TR), L(L_) {
-    tiles = (long)tiles_r * ((C + TE_TC - 1) / TE_TC);
+  __device__ TeWork(int R, int C, int L_, int tc_ = TE_TC) : tiles_r((R + TE_TR - 1) / TE_TR), L(L_), tc(tc_) {
+    tiles = (long)tiles_r * ((C + tc - 1) / tc);
     W = tiles * L;
     const long P = gridDim.x;
     lc = (int)min((long)L, max(1L, (W + P - 1) / P));
@@ -76,7 +78,7 @@ struct TeWork {
     l0 = c * lc + (int)(rem % size);
     l1 = (int)min((long)c * lc + size, (long)l0 + (w_end - w));
     r0 = (int)(tile % tiles_r) * TE_TR;
-    c0 = (int)(tile / tiles_r) * TE_TC;
+    c0 = (int)(tile / tiles_r) * tc;
   }
 };
 
@@ -187,8 +189,36 @@ __device__ inline void mr_finish(int fin, const double* s, DevScalars* sc, const
   }
 }
 
-template <int ND, typename T, int MODE>
-__global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a) {
+// The node's row as 27 assembled neighbour blocks (asm_table.cuh; models of at most two
+// materials): out = sum over neighbours o of A(n, n+o) v(n+o).
+template <int ND, typename T, int O>
+__device__ __forceinline__ void asm_te_offset(const T* __restrict__ sT, unsigned m, const T* pm, const T* p0, const T* pp, int ctr,
+                                              T (&out)[ND][1]) {
+  if constexpr (asm_used<ND>(O)) {
+    constexpr int dr = O % 3 - 1, dc = (O / 3) % 3 - 1, dl = O / 9 - 1;
+    const T* v = (dl < 0 ? pm : (dl == 0 ? p0 : pp)) + (ctr + dr + dc * TE_PR) * ND;
+    T val[ND][1];
+#pragma unroll
+    for (int c = 0; c < ND; c++) val[c][0] = v[c];
+    asm_block<ND, T, O>(sT, m, val, out);
+  }
+}
+template <int ND, typename T, int... Os>
+__device__ __forceinline__ void asm_te_node(std::integer_sequence<int, Os...>, const T* __restrict__ sT, unsigned key, const T* pm,
+                                            const T* p0, const T* pp, int ctr, T (&out)[ND]) {
+  T o[ND][1];
+#pragma unroll
+  for (int c = 0; c < ND; c++) o[c][0] = T(0);
+  const unsigned m = asm_config(key);
+  (asm_te_offset<ND, T, Os>(sT, m, pm, p0, pp, ctr, o), ...);
+#pragma unroll
+  for (int c = 0; c < ND; c++) out[c] = o[c][0];
+}
+
+// ASM: the operator from the assembled neighbour blocks (a.Kd still supplies the Jacobi
+// diagonal); the shared-memory head then holds the table instead of the element matrices.
+template <int ND, typename T, int MODE, bool ASM = false>
+__global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a, const T* __restrict__ tab = nullptr) {
   constexpr int ED = 8 * ND;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double sred[TE_NT / 32];
@@ -196,10 +226,15 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a) {
   if (a.skip_if_done && a.sc->done) return;
   T* sK = reinterpret_cast<T*>(smem_raw);
   const int kstride = ED * ED + 1;  // padded material stride spreads materials over banks
-  T* sP = sK + 4 * kstride;
+  constexpr int TAB = ASM_NBLK * AsmLayout<ND, T, 1>::BS;
+  T* sP = sK + (ASM ? TAB : 4 * kstride);
   const int tid = threadIdx.x + TE_TR * threadIdx.y;
-  // 4 material slots always (keys carry 2 bits per voxel); slots past nmat are zero.
-  for (int i = tid; i < 4 * ED * ED; i += TE_NT) sK[(i / (ED * ED)) * kstride + i % (ED * ED)] = (i < a.nmat * ED * ED) ? a.Kd[i] : T(0);
+  if constexpr (ASM) {
+    for (int i = tid; i < TAB; i += TE_NT) sK[i] = tab[i];
+  } else {
+    // 4 material slots always (keys carry 2 bits per voxel); slots past nmat are zero.
+    for (int i = tid; i < 4 * ED * ED; i += TE_NT) sK[(i / (ED * ED)) * kstride + i % (ED * ED)] = (i < a.nmat * ED * ED) ? a.Kd[i] : T(0);
+  }
   if (MODE == TE_MR) {
     for (int i = tid; i < 4 * 8 * ND; i += TE_NT) {
       const int m = i / (8 * ND), k = i % (8 * ND);
@@ -248,20 +283,25 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a) {
   wk.run(w, w_end, r0, c0, l0, l1);
   const int r = r0 + threadIdx.x, c = c0 + threadIdx.y;
   const bool active = (r < R) && (c < C);
+  // the node key is fetched one layer ahead (its latency overlaps the previous layer's work)
+  const size_t col = active ? (size_t)r + (size_t)c * R : 0;
+  unsigned key_next = a.keys[col + (size_t)l0 * RC];
   __syncthreads();
   load_plane(l0 - 1);
   load_plane(l0);
   for (int l = l0; l < l1; l++) {
+    const unsigned key = key_next;
+    key_next = a.keys[col + (size_t)(l + 1 < l1 ? l + 1 : l) * RC];
     load_plane(l + 1);
     __syncthreads();
     if (active) {
       const size_t node = (size_t)r + (size_t)c * R + (size_t)l * RC;
-      const unsigned key = a.keys[node];
       const T* pm = sP + slot_of(l - 1) * TE_PP * ND;
       const T* p0 = sP + slot_of(l) * TE_PP * ND;
       const T* pp = sP + slot_of(l + 1) * TE_PP * ND;
       T out[ND];
-      te_node<ND, T>(sK, kstride, key, pm, p0, pp, ctr, out);
+      if constexpr (ASM) asm_te_node<ND, T>(std::make_integer_sequence<int, 27>{}, sK, key, pm, p0, pp, ctr, out);
+      else te_node<ND, T>(sK, kstride, key, pm, p0, pp, ctr, out);
 #pragma unroll
       for (int cc = 0; cc < ND; cc++) {
         const size_t j = node * ND + cc;
@@ -305,6 +345,11 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a) {
       if (a.finish == FIN_ALPHA) a.sc->alpha = a.sc->delta / out[0];
     }
   }
+}
+
+template <int ND, typename T>
+inline size_t te_asm_smem_bytes() {
+  return (size_t)ASM_NBLK * AsmLayout<ND, T, 1>::BS * sizeof(T) + (size_t)3 * TE_PP * ND * sizeof(T) + 16;
 }
 
 template <int ND, typename T>

@@ -6,7 +6,7 @@
  * formats and 1/0 return convention as chfem/src/femhmg/cudapcg/cudapcg.h:19-62, with
  * cudapcgVar_t = double and 16-bit material keys (the reference defaults,
  * chfem/src/femhmg/cudapcg/includes.h:46-80).  A caller built against the reference header
- * links against this library unchanged (see INTEGRATION.md).  Differences by design:
+ * links against this library unchanged.  Differences by design:
  *   - errors return 0 and leave a message for cudapcgB200LastError(); the library never
  *     calls exit() or cudaDeviceReset() (reference: error_handling.h:6-14, cudapcg.cu:201);
  *   - 2D analyses and the scalar-density field are rejected with an error (outside the 3D
@@ -158,6 +158,9 @@ cudapcgFlag_t cudapcgB200ApplyPreconditioner(const double *x, double *y);
 cudapcgFlag_t cudapcgB200SolveBlock(unsigned int nrhs, const double *const *rhs, const double *const *x0,
                                     int x0_interpolate, double *const *x_out, unsigned int *iterations,
                                     double *residuals);
+/* y[k] = A v[k] for nrhs host vectors of nvars doubles (3 thermal, 3 or 6 elastic) through the
+   block operator pass that cudapcgB200SolveBlock runs; for parity tests. */
+cudapcgFlag_t cudapcgB200ApplyBlockOperator(unsigned int nrhs, const double *const *v, double *const *y);
 /* Block solve of the homogenization load cases of the current model with the right-hand sides
    assembled and the effective-tensor volume term reduced on the device, so that no full-length
    vector crosses to or from the host.  Load case k: thermal/elastic, the macroscopic jump
@@ -262,11 +265,14 @@ double cudapcgB200TimeKernel(int which, unsigned int reps);
    y = A v and *vAv = v.Av for a THERMAL_3D (1) or ELASTIC_3D (3) model, all FP64, every
    pointer a caller-owned device buffer: keys (nrows*ncols*nlayers 16-bit node keys), Kdense
    (nmat dense element matrices of (8*dof)^2 doubles, i.e. the SparseQ1 thermal rows expanded
-   to 8x8), v and y (nvars doubles), vAv (1 double).  Scratch lives in a fixed 66 KB
-   file-scope device array held by every GPU that loads the library until exit; its address
-   is looked up on the first call on each device (make that call before any stream capture).
-   Calls that overlap on the GPU share that array and race.  Models above 8192 column tiles of
-   32x8 nodes are rejected.  stream: a cudaStream_t (NULL for the default stream).
+   to 8x8), v and y (nvars doubles), vAv (1 double); y and vAv must not overlap v, keys or
+   Kdense (rejected).  Scratch lives in a fixed 66 KB file-scope device array held by every
+   GPU that loads the library until exit; its address is looked up on every call made outside
+   stream capture, and a call under capture uses the one of the last uncaptured call on that
+   device (so the first call on a device, and the first after a device reset, must be made
+   outside capture).  Calls that overlap on the GPU share that array and race.  Any model size
+   is accepted (the operator runs on at most 8192 CTAs, one reduction slot each); each
+   dimension must stay below 2^31 - 16.  stream: a cudaStream_t (NULL for the default stream).
    Returns 1, or 0 with cudapcgB200LastError() set. */
 int cudapcgB200ApplyOperatorNoAlloc(int analysis_flag, unsigned int nrows, unsigned int ncols, unsigned int nlayers,
                                     unsigned int nmat, const uint16_t *keys, const double *Kdense, const double *v,

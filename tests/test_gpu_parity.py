@@ -238,6 +238,57 @@ def test_operator_and_jacobi(tmp_path, name, analysis, spec, precision):
     assert H.rel_to_max(z, zref) < tol
 
 
+_ORACLE_APPLY_MANY = r'''
+import ctypes, sys, pickle, numpy as np
+sys.path.insert(0, sys.argv[3])
+from tests.test_gpu_parity import setup_model
+a = pickle.load(open(sys.argv[1], "rb"))
+lib = ctypes.CDLL(sys.argv[2], mode=ctypes.RTLD_LOCAL)
+setup_model(lib, a)
+ys = []
+for x in a["xs"]:
+    y = np.zeros(a["ndof"])
+    assert lib.oracle_apply(np.ascontiguousarray(x).ctypes.data_as(ctypes.c_void_p), y.ctypes.data_as(ctypes.c_void_p))
+    ys.append(y)
+np.save(sys.argv[1] + ".ys.npy", np.array(ys))
+'''
+
+
+# The block operator pass of the block solver (for one- and two-material models the stencil
+# assembled per material configuration, otherwise element by element), applied to 3 or 6
+# random fields at once; each output against the oracle's single apply.  Bars as above.
+@pytest.mark.parametrize("name,analysis,spec,nr", [
+    ("th2", 0, ("img", (13, 35, 17), 2), 3), ("th1", 0, ("img", (9, 8, 11), 1), 3), ("th3", 0, ("img", (10, 33, 9), 3), 3),
+    ("el2", 1, ("img", (9, 33, 10), 2), 6), ("el2_3", 1, ("img", (11, 7, 13), 2), 3), ("el4", 1, ("img", (7, 9, 8), 4), 6),
+    ("el2_odd", 1, ("img", (33, 10, 7), 2), 6), ("th2_tiny", 0, ("img", (2, 3, 1), 2), 3)])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_block_operator(tmp_path, name, analysis, spec, nr, precision):
+    import pickle
+    from chfem_b200 import _native
+    nf, raw = build_small(tmp_path, name, analysis, spec)
+    a = host_arrays(nf, raw)
+    rng = np.random.default_rng(7)
+    a["xs"] = [rng.standard_normal(a["ndof"]) for _ in range(nr)]
+    pk = str(tmp_path / "a.pkl")
+    pickle.dump(a, open(pk, "wb"))
+    p = subprocess.run([sys.executable, "-c", _ORACLE_APPLY_MANY, pk, os.path.join(H.ROOT, "oracle", "liboracle_cudapcg.so"), H.ROOT],
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    yref = np.load(pk + ".ys.npy")
+    lib = _native.cudapcg()
+    setup_model(lib, a)
+    assert lib.cudapcgB200SetPrecision(precision)
+    ys = [np.zeros(a["ndof"]) for _ in range(nr)]
+    P = ctypes.c_void_p * nr
+    ok = lib.cudapcgB200ApplyBlockOperator(nr, P(*[x.ctypes.data for x in a["xs"]]), P(*[y.ctypes.data for y in ys]))
+    err = lib.cudapcgB200LastError()
+    lib.cudapcgEnd()
+    assert ok, err
+    tol = 1e-12 if precision == 0 else 1e-5
+    for k in range(nr):
+        assert H.rel_to_max(ys[k], yref[k]) < tol, (k, H.rel_to_max(ys[k], yref[k]))
+
+
 # ---------------------------------------------------------------------------------------
 # Block multi-RHS solves (--multirhs): every load case advances in one pass, each with its
 # own PCG scalars and stopping test.  Same bars as the one-by-one solves; FP64 iteration

@@ -41,7 +41,9 @@ def _dense(lcl, analysis, nmat):
     return out
 
 
-@pytest.mark.parametrize("analysis,shape,nmat", [(1, (9, 33, 10), 2), (0, (13, 35, 17), 3)])
+# the last case has more column tiles (35 x 263 of 32 x 8 nodes) than the array has reduction
+# slots (8192): the persistent schedule gives each CTA several tiles
+@pytest.mark.parametrize("analysis,shape,nmat", [(1, (9, 33, 10), 2), (0, (13, 35, 17), 3), (0, (1, 1100, 2100), 2)])
 def test_no_alloc_matches_regular_entry_point(tmp_path, analysis, shape, nmat):
     import torch
     from chfem_b200 import _native
@@ -85,14 +87,20 @@ def test_no_alloc_matches_regular_entry_point(tmp_path, analysis, shape, nmat):
         assert abs(vav.item() - float(x @ yref)) <= OP_TOL * abs(float(x @ yref)) * 10
 
 
-def test_no_alloc_rejects_oversized_and_bad_input():
+def test_no_alloc_rejects_bad_input():
+    """Argument errors are reported before any device work (the pointers here are never read)."""
     from chfem_b200 import _native
     lib = _native.cudapcg()
     fn = lib.cudapcgB200ApplyOperatorNoAlloc
     fn.argtypes = [ctypes.c_int] + [ctypes.c_uint] * 4 + [ctypes.c_void_p] * 6
     fn.restype = ctypes.c_int
-    dummy = ctypes.c_void_p(16)
-    assert fn(3, 32 * 8193, 8, 1, 2, dummy, dummy, dummy, dummy, dummy, None) == 0
-    assert b"too large" in lib.cudapcgB200LastError()
-    assert fn(5, 8, 8, 8, 1, dummy, dummy, dummy, dummy, dummy, None) == 0
-    assert fn(3, 8, 8, 8, 7, dummy, dummy, dummy, dummy, dummy, None) == 0
+    keys, kd, v, y, vav = (ctypes.c_void_p(1 << 40), ctypes.c_void_p(2 << 40), ctypes.c_void_p(3 << 40),
+                           ctypes.c_void_p(4 << 40), ctypes.c_void_p(5 << 40))
+    assert fn(3, 0x7fffffff, 8, 1, 2, keys, kd, v, y, vav, None) == 0
+    assert b"dimension" in lib.cudapcgB200LastError()
+    assert fn(3, 8, 8, 8, 2, keys, kd, v, v, vav, None) == 0  # in place: y == v
+    assert b"overlap" in lib.cudapcgB200LastError()
+    assert fn(3, 8, 8, 8, 2, keys, kd, v, ctypes.c_void_p((3 << 40) + 8), vav, None) == 0  # y inside v
+    assert b"overlap" in lib.cudapcgB200LastError()
+    assert fn(5, 8, 8, 8, 1, keys, kd, v, y, vav, None) == 0
+    assert fn(3, 8, 8, 8, 7, keys, kd, v, y, vav, None) == 0
