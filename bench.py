@@ -415,7 +415,7 @@ def batch_main(args, w, world, rank, dist, allmax, barrier):
                 "config": config_dict(args, w, world) | {"samples": w["batch"], "nodes": nodes},
                 "iterations_max": int(its.max()), "iterations_mean": float(its.mean()),
                 "dof_iterations_per_s": node_its / step_s, "samples_per_s": world * w["batch"] / step_s,
-                "roofline": roofline, "clocks": clk, "gpu_launches": int(launches / max(1, args.steps)),
+                "roofline": roofline, "clocks": clk, "gpu_launches": int(launches),
                 "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(3 * nodes),
                         "d2h_bytes_per_step": int(w["batch"] * 9 * 8 + w["batch"] * 3 * 4),
                         "path": "compute_conductivity_batch (images in host memory -> tensors)"},
@@ -688,7 +688,7 @@ def main():
                 "iterations": its, "dof_iterations_per_s": dof_its, "wall_s_per_step": wall_step,
                 "plain_fp64_pcg": fp64, "speedup_vs_plain_fp64": (fp64["time_s"] / step_s) if fp64 else None,
                 "tensor_diag": [float(C[i, i]) for i in range(C.shape[0])] if C is not None else None,
-                "roofline": roofline, "clocks": clk, "gpu_launches": int(launches / max(1, args.steps)),
+                "roofline": roofline, "clocks": clk, "gpu_launches": int(launches),
                 "device_bytes_per_dof": dev_bytes / model.ndof,
                 "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "path": ("compute_property(..., initial_guess='learned')" if learned_run else

@@ -63,8 +63,8 @@ static int asm_tile_choice() {
   static int choice = -1;
   if (choice < 0) {
     const char* e = getenv("CHFEM_B200_ASM_TILE");
-    choice = ASM_TILE_6x2;
-    if (e && !strcmp(e, "8x1")) choice = ASM_TILE_8x1;
+    choice = ASM_TILE_8x1;
+    if (e && !strcmp(e, "6x2")) choice = ASM_TILE_6x2;
     if (e && !strcmp(e, "8x2")) choice = ASM_TILE_8x2;
     if (e && !strcmp(e, "4x2")) choice = ASM_TILE_4x2;
   }
@@ -105,10 +105,15 @@ template <int ND, typename T, int NR>
 static bool launch_blk_point(int parity) {
   const long n = S->nvars;
   T* dnew = (T*)(parity ? B->d0 : B->d1);
-  const int g = pw_grid(S->N);
+  // whole 16-byte chunks per thread when every right-hand side's vectors start aligned
+  const bool chunks = n % 4 == 0;
+  const int g = pw_grid(chunks ? n / 4 : S->N);
   if (!ensure_reduction(g)) return false;
   BlkPw<ND, T> p{B->x, dnew, (T*)B->r, (const T*)B->q, (T*)B->s, S->d_keys, Kdev<T>(), S->nmat, S->N, n, B->sc, redctl(g), solvecfg()};
-  if (S->resnorm == CUDAPCG_L2_NORM) k_blk_point<ND, T, NR, false><<<g, PW_NT, 0, S->stream>>>(p);
+  if (chunks) {
+    if (S->resnorm == CUDAPCG_L2_NORM) k_blk_point4<ND, T, NR, false><<<g, PW_NT, 0, S->stream>>>(p);
+    else k_blk_point4<ND, T, NR, true><<<g, PW_NT, 0, S->stream>>>(p);
+  } else if (S->resnorm == CUDAPCG_L2_NORM) k_blk_point<ND, T, NR, false><<<g, PW_NT, 0, S->stream>>>(p);
   else k_blk_point<ND, T, NR, true><<<g, PW_NT, 0, S->stream>>>(p);
   S->launches++;
   return cudaPeekAtLastError() == cudaSuccess;

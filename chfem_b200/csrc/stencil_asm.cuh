@@ -20,11 +20,12 @@ namespace chfem {
 template <int ND, int NR>
 __host__ __device__ constexpr int asm_raw_stride() { return 2 * NR * ND + 1; }
 
-template <int ND, typename T, int NR, int TC, int ZB, bool ASYNC = false>
+template <int ND, typename T, int NR, int TC, int ZB, bool ASYNC = false, bool TG = false>
 inline size_t asm_smem_bytes() {
   using Lo = AsmLayout<ND, T, NR>;
   const size_t pp = (size_t)(TE_TR + 2) * (TC + 2);
-  return ((size_t)ASM_NBLK * Lo::BS + (size_t)(ZB + 2) * pp * Lo::PS + (ASYNC ? (size_t)ZB * pp * asm_raw_stride<ND, NR>() : 0)) * sizeof(T);
+  return ((TG ? 0 : (size_t)ASM_NBLK * Lo::BS) + (size_t)(ZB + 2) * pp * Lo::PS + (ASYNC ? (size_t)ZB * pp * asm_raw_stride<ND, NR>() : 0)) *
+         sizeof(T);
 }
 
 // 4-byte (or 8-byte) asynchronous global -> shared copy (sm_80+ cp.async; completion by
@@ -107,8 +108,12 @@ __device__ __forceinline__ void asm_positions(std::integer_sequence<int, Ps...>,
 // PF: at the start of a step the CTA asks L2 to prefetch (bulk prefetch, one request per
 // contiguous column segment of every input vector) the planes it will stage after the step, so
 // the staging loads that follow the arithmetic find them in L2.
-template <int ND, typename T, int NR, int TC, int ZB, bool ASYNC = false, bool PF = false>
-__global__ void __launch_bounds__(TE_TR * TC) k_asm_apply(BlkArgs<ND, T> a, const T* __restrict__ tab) {
+//
+// TG: the table is read from global memory through the L1 cache instead of being copied into
+// shared memory (the staging loads then bypass L1 so that they do not evict it), which leaves
+// the shared memory to the planes and allows MINB CTAs per SM.
+template <int ND, typename T, int NR, int TC, int ZB, bool ASYNC = false, bool PF = false, bool TG = false, int MINB = 1>
+__global__ void __launch_bounds__(TE_TR * TC, MINB) k_asm_apply(BlkArgs<ND, T> a, const T* __restrict__ tab) {
   using Lo = AsmLayout<ND, T, NR>;
   using V = typename Lo::V;
   constexpr int NW = Lo::NW;
@@ -126,9 +131,10 @@ __global__ void __launch_bounds__(TE_TR * TC) k_asm_apply(BlkArgs<ND, T> a, cons
   for (int k = 0; k < NR; k++) all_done = all_done && a.sc[k].done;
   if (all_done) return;
   T* sT = reinterpret_cast<T*>(smem_raw);
-  T* sP = sT + ASM_NBLK * Lo::BS;  // ASM_NBLK * BS words keep 16-byte alignment (416 = 16 * 26)
+  T* sP = TG ? sT : sT + ASM_NBLK * Lo::BS;  // ASM_NBLK * BS words keep 16-byte alignment (416 = 16 * 26)
   const int tid = threadIdx.x + TE_TR * threadIdx.y;
-  for (int i = tid; i < ASM_NBLK * Lo::BS; i += NT) sT[i] = tab[i];
+  if constexpr (!TG)
+    for (int i = tid; i < ASM_NBLK * Lo::BS; i += NT) sT[i] = tab[i];
   if (tid < NR) { sbeta[tid] = T(a.sc[tid].beta); sdone[tid] = a.sc[tid].done; }
   __syncthreads();
   const int R = a.R, C = a.C, L = a.L;
@@ -198,7 +204,8 @@ __global__ void __launch_bounds__(TE_TR * TC) k_asm_apply(BlkArgs<ND, T> a, cons
 #pragma unroll
           for (int c = 0; c < ND; c++) {
             const size_t j = (size_t)k * n + node * ND + c;
-            dst[p * PS + c * NR + k] = fma(beta[k], a.dold[j], a.s[j]);
+            if constexpr (TG) dst[p * PS + c * NR + k] = fma(beta[k], __ldcg(a.dold + j), __ldcg(a.s + j));
+            else dst[p * PS + c * NR + k] = fma(beta[k], a.dold[j], a.s[j]);
           }
       }
     }
@@ -264,7 +271,8 @@ __global__ void __launch_bounds__(TE_TR * TC) k_asm_apply(BlkArgs<ND, T> a, cons
               if constexpr (Lo::PAIRS) out[z][ci][ww] = make_float2(0.f, 0.f);
               else out[z][ci][ww] = T(0);
             }
-        asm_positions<ND, T, NR, ZB>(std::make_integer_sequence<int, 9 * (ZB + 2)>{}, pl, ctr, sT, m, out);
+        if constexpr (TG) asm_positions<ND, T, NR, ZB>(std::make_integer_sequence<int, 9 * (ZB + 2)>{}, pl, ctr, tab, m, out);
+        else asm_positions<ND, T, NR, ZB>(std::make_integer_sequence<int, 9 * (ZB + 2)>{}, pl, ctr, sT, m, out);
 #pragma unroll
         for (int z = 0; z < ZB; z++) {
           if (l + z >= l1) break;

@@ -329,4 +329,121 @@ __global__ void __launch_bounds__(PW_NT) k_blk_point(BlkPw<ND, T> a) {
   }
 }
 
+// The same pass with each thread on 4 consecutive unknowns of every right-hand side (16-byte
+// vector loads and stores of whole warps' contiguous 512-byte runs) instead of one node's ND
+// unknowns at a stride of ND words, which made each warp access touch ND times the sectors it
+// used.  The Jacobi diagonal of the (at most two) nodes the 4 unknowns belong to comes from
+// their keys.  Requires n % 4 == 0 (every right-hand side's vectors start 16-byte aligned).
+template <typename T>
+__device__ __forceinline__ void blk_ld4(const T* p, T (&v)[4]) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 t = __ldcs(reinterpret_cast<const float4*>(p));
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+  } else {
+    const double2 a = __ldcs(reinterpret_cast<const double2*>(p)), b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  }
+}
+template <typename T>
+__device__ __forceinline__ void blk_st4(T* p, const T (&v)[4]) {
+  if constexpr (sizeof(T) == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  } else {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+  }
+}
+
+template <int ND, typename T, int NR, bool MAXN>
+__global__ void __launch_bounds__(PW_NT) k_blk_point4(BlkPw<ND, T> a) {
+  constexpr int ED = 8 * ND;
+  constexpr int NV = MAXN ? 4 : 1;
+  __shared__ double sred[PW_NT / 32];
+  __shared__ T sD[4 * 8 * ND];
+  __shared__ double salpha[NR];
+  __shared__ int sdone[NR];
+  bool all_done = true;
+#pragma unroll
+  for (int k = 0; k < NR; k++) all_done = all_done && a.sc[k].done;
+  if (all_done) return;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 4 * 8 * ND; i += PW_NT) {
+    const int m = i / (8 * ND), kk = i % (8 * ND);
+    sD[i] = (m < a.nmat) ? a.Kd[(size_t)m * ED * ED + (size_t)kk * ED + kk] : T(1);
+  }
+  if (tid < NR) { salpha[tid] = a.sc[tid].alpha; sdone[tid] = a.sc[tid].done; }
+  __syncthreads();
+  double vals[NV * NR];
+#pragma unroll
+  for (int k = 0; k < NV * NR; k++) vals[k] = 0.0;
+  const long n4 = a.n / 4;
+  for (long t = blockIdx.x * (long)PW_NT + tid; t < n4; t += (long)gridDim.x * PW_NT) {
+    const long j0 = 4 * t;
+    T inv[4];
+    if (a.cfg.precond) {
+      // the 4 unknowns span nodes j0 / ND .. (j0 + 3) / ND (at most 2 for ND = 3, 4 for ND = 1)
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const long node = (j0 + i) / ND;
+        const int c = (int)(j0 + i - node * ND);
+        if (ND == 1 || i == 0 || c == 0) {  // first unknown of a node in this chunk: its diagonal
+          T iv[ND];
+          te_invdiag<ND, T>(sD, a.keys[node], iv);
+#pragma unroll
+          for (int q = i; q < 4; q++) {
+            const int cq = (int)(j0 + q - node * ND);
+            if (cq < ND) inv[q] = iv[cq];
+          }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; i++) inv[i] = T(1);
+    }
+#pragma unroll
+    for (int k = 0; k < NR; k++) {
+      if (sdone[k]) continue;
+      const double al64 = salpha[k];
+      const T al = T(al64);
+      const long j = (long)k * a.n + j0;
+      T dv[4], qv[4], rv[4], sv[4];
+      blk_ld4(a.d + j, dv);
+      blk_ld4(a.q + j, qv);
+      blk_ld4(a.r + j, rv);
+      const double2 x01 = __ldcs(reinterpret_cast<const double2*>(a.x + j)), x23 = __ldcs(reinterpret_cast<const double2*>(a.x + j) + 1);
+      double xv[4] = {x01.x, x01.y, x23.x, x23.y};
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        xv[i] = fma(al64, (double)dv[i], xv[i]);
+        rv[i] = fma(-al, qv[i], rv[i]);
+        sv[i] = rv[i] * inv[i];
+        vals[NV * k] += (double)rv[i] * (double)sv[i];
+        if constexpr (MAXN) {
+          vals[NV * k + 1] = fmax(vals[NV * k + 1], fabs((double)rv[i]));
+          vals[NV * k + 2] = fmax(vals[NV * k + 2], fabs((double)dv[i]));
+          vals[NV * k + 3] = fmax(vals[NV * k + 3], fabs(xv[i]));
+        }
+      }
+      reinterpret_cast<double2*>(a.x + j)[0] = make_double2(xv[0], xv[1]);
+      reinterpret_cast<double2*>(a.x + j)[1] = make_double2(xv[2], xv[3]);
+      blk_st4(a.r + j, rv);
+      blk_st4(a.s + j, sv);
+    }
+  }
+  bool ismax[NV * NR];
+#pragma unroll
+  for (int k = 0; k < NV * NR; k++) ismax[k] = (k % NV) != 0;
+  double out[NV * NR];
+  if (grid_reduce<PW_NT, NV * NR>(vals, ismax, a.rc, blockIdx.x, out, sred) && tid == 0) {
+#pragma unroll
+    for (int k = 0; k < NR; k++) {
+      if (sdone[k]) continue;
+      double s4[4] = {out[NV * k], 0.0, 0.0, 0.0};
+      if constexpr (MAXN) { s4[1] = out[NV * k + 1]; s4[2] = out[NV * k + 2]; s4[3] = out[NV * k + 3]; }
+      for (int t = 0; t < 4; t++) a.sc[k].red[t] = s4[t];
+      pcg_finish(PW_PCG, s4, a.sc + k, a.cfg);
+    }
+  }
+}
+
 }  // namespace chfem

@@ -19,6 +19,7 @@
 #include <utility>
 #include "common.cuh"
 #include "asm_table.cuh"
+#include "pointwise.cuh"
 
 namespace chfem {
 
@@ -29,7 +30,13 @@ constexpr int TE_PR = TE_TR + 2;       // plane pitch (rows incl. halo)
 constexpr int TE_PC = TE_TC + 2;
 constexpr int TE_PP = TE_PR * TE_PC;   // points per plane incl. halo
 
-enum TeMode : int { TE_PLAIN = 0, TE_PCG = 1, TE_MR = 2 };
+// TE_DIRDOT and TE_UPD are the two passes of the 3-vector PCG (x, r and the direction's two
+// buffers; chfem/src/femhmg/cudapcg/solvers/pcg3.cu:28-227 keeps the same vectors and applies
+// the operator twice per iteration):
+//   TE_DIRDOT  v = M^-1 in0 + beta in1 = M^-1 r + beta d_old, written to vout; d.Ad -> alpha
+//   TE_UPD     v = in0 = d; r (vout) -= alpha A v, x += alpha v; r.M^-1 r, max-norms -> the
+//              PCG finisher (delta, beta, stopping test) -- A v itself is never stored
+enum TeMode : int { TE_PLAIN = 0, TE_PCG = 1, TE_MR = 2, TE_DIRDOT = 3, TE_UPD = 4 };
 // Finishers run by the last CTA on the grid-reduced sums.
 enum TeFinish : int {
   FIN_NONE = 0, FIN_ALPHA = 1, FIN_STORE = 2, FIN_MR_INIT = 3, FIN_MR_X0 = 4, FIN_MR_STEP = 5,
@@ -235,15 +242,16 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a, const T* __
     // 4 material slots always (keys carry 2 bits per voxel); slots past nmat are zero.
     for (int i = tid; i < 4 * ED * ED; i += TE_NT) sK[(i / (ED * ED)) * kstride + i % (ED * ED)] = (i < a.nmat * ED * ED) ? a.Kd[i] : T(0);
   }
-  if (MODE == TE_MR) {
+  if (MODE == TE_MR || MODE == TE_DIRDOT || MODE == TE_UPD) {
     for (int i = tid; i < 4 * 8 * ND; i += TE_NT) {
       const int m = i / (8 * ND), k = i % (8 * ND);
       sD[i] = (m < a.nmat) ? a.Kd[(size_t)m * ED * ED + (size_t)k * ED + k] : T(1);
     }
     __syncthreads();
   }
-  const T beta = (MODE == TE_PCG) ? T(a.sc->beta) : T(0);
+  const T beta = (MODE == TE_PCG || MODE == TE_DIRDOT) ? T(a.sc->beta) : T(0);
   const T alpha = (MODE == TE_MR && mr_steps(a.finish)) ? T(a.sc->alpha) : T(0);
+  const double alpha64 = (MODE == TE_UPD) ? a.sc->alpha : 0.0;
   const bool pre = a.cfg.precond != 0;
   const int R = a.R, C = a.C, L = a.L;
   const size_t RC = (size_t)R * C;
@@ -258,7 +266,7 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a, const T* __
       const int gr = wrap(r0 + hr - 1, R), gc = wrap(c0 + hc - 1, C);
       const size_t node = (size_t)gr + (size_t)gc * R + (size_t)lw * RC;
       T inv[ND];
-      if (MODE == TE_MR) {
+      if (MODE == TE_MR || MODE == TE_DIRDOT) {
         if (pre) te_invdiag<ND, T>(sD, a.keys[node], inv);
         else {
 #pragma unroll
@@ -270,6 +278,7 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a, const T* __
         T v = a.in0[node * ND + c];
         if (MODE == TE_PCG) v = fma(beta, a.in1[node * ND + c], v);
         if (MODE == TE_MR) v = fma(-alpha, a.in1[node * ND + c], v) * inv[c];
+        if (MODE == TE_DIRDOT) v = fma(beta, a.in1[node * ND + c], v * inv[c]);
         dst[p * ND + c] = v;
       }
     }
@@ -302,12 +311,30 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a, const T* __
       T out[ND];
       if constexpr (ASM) asm_te_node<ND, T>(std::make_integer_sequence<int, 27>{}, sK, key, pm, p0, pp, ctr, out);
       else te_node<ND, T>(sK, kstride, key, pm, p0, pp, ctr, out);
+      [[maybe_unused]] T own_inv[ND];
+      if constexpr (MODE == TE_UPD) {
+        if (pre) te_invdiag<ND, T>(sD, key, own_inv);
+        else {
+#pragma unroll
+          for (int cc = 0; cc < ND; cc++) own_inv[cc] = T(1);
+        }
+      }
 #pragma unroll
       for (int cc = 0; cc < ND; cc++) {
         const size_t j = node * ND + cc;
         const T v = p0[ctr * ND + cc];
-        a.y[j] = out[cc];
-        if (MODE == TE_PCG) a.vout[j] = v;
+        if (MODE != TE_DIRDOT && MODE != TE_UPD) a.y[j] = out[cc];
+        if (MODE == TE_PCG || MODE == TE_DIRDOT) a.vout[j] = v;
+        if (MODE == TE_UPD) {
+          const T rn = fma(-T(alpha64), out[cc], a.vout[j]);
+          a.vout[j] = rn;
+          const double xv = fma(alpha64, (double)v, a.x[j]);
+          a.x[j] = xv;
+          acc_rz += (double)rn * (double)(rn * own_inv[cc]);
+          mr = fmax(mr, fabs((double)rn));
+          md = fmax(md, fabs((double)v));
+          mx = fmax(mx, fabs(xv));
+        }
         if (MODE == TE_MR) {
           const T rn = fma(-alpha, a.in1[j], a.in0[j]);
           a.vout[j] = rn;
@@ -328,7 +355,16 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a, const T* __
   }
   if (a.finish == FIN_NONE) return;
   const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-  if (MODE == TE_MR) {
+  if (MODE == TE_UPD) {
+    const double vals[4] = {acc_rz, mr, md, mx};
+    const bool ismax[4] = {false, true, true, true};
+    double out[4];
+    if (grid_reduce<TE_NT, 4>(vals, ismax, a.rc, bid, out, sred) && tid == 0) {
+      for (int k = 0; k < 4; k++) a.sc->red[k] = out[k];
+      const SolveCfg cfg{a.cfg.tol, a.cfg.maxit, a.cfg.norm, a.cfg.precond, a.cfg.nhmg};
+      pcg_finish(PW_PCG, out, a.sc, cfg);
+    }
+  } else if (MODE == TE_MR) {
     const double vals[5] = {acc, acc_rz, mr, md, mx};
     const bool ismax[5] = {false, false, true, true, true};
     double out[5];
