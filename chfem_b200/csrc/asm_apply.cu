@@ -12,7 +12,7 @@ namespace {
 // cp.async staging at one CTA per SM 0.447 ms, the table read through L1 0.378 ms).
 // (FP64 elastic planes of 19 doubles per node leave room for one CTA per SM: no cap there.)
 template <int ND, typename T, int NR, int TC, int ZB>
-constexpr auto asm_kernel = k_asm_apply<ND, T, NR, TC, ZB, false, true, false, (ND == 3 && sizeof(T) == 8) ? 1 : 2>;
+constexpr auto asm_kernel = k_asm_apply<ND, T, NR, TC, ZB, (ND == 3 && sizeof(T) == 8) ? 1 : 2>;
 
 template <int ND, typename T, int NR, int TC, int ZB>
 int ctas_of(int R, int C, int L, int num_sms) {
@@ -99,6 +99,14 @@ CHFEM_ASM_TE_INSTANTIATE(3, float, TE_MR)
 CHFEM_ASM_TE_INSTANTIATE(3, double, TE_PLAIN)
 CHFEM_ASM_TE_INSTANTIATE(3, double, TE_PCG)
 CHFEM_ASM_TE_INSTANTIATE(3, double, TE_MR)
+CHFEM_ASM_TE_INSTANTIATE(1, float, TE_DIRDOT)
+CHFEM_ASM_TE_INSTANTIATE(1, float, TE_UPD)
+CHFEM_ASM_TE_INSTANTIATE(1, double, TE_DIRDOT)
+CHFEM_ASM_TE_INSTANTIATE(1, double, TE_UPD)
+CHFEM_ASM_TE_INSTANTIATE(3, float, TE_DIRDOT)
+CHFEM_ASM_TE_INSTANTIATE(3, float, TE_UPD)
+CHFEM_ASM_TE_INSTANTIATE(3, double, TE_DIRDOT)
+CHFEM_ASM_TE_INSTANTIATE(3, double, TE_UPD)
 
 #define CHFEM_ASM_INSTANTIATE(ND, T, NR)                                              \
   template int asm_block_ctas<ND, T, NR>(int, int, int, int, int);                    \

@@ -144,11 +144,28 @@ __device__ __forceinline__ void asm_block(const T* __restrict__ sT, unsigned m, 
   }
 }
 
+// After the blocks the table holds the inverse Jacobi diagonal of each of the 256 node
+// configurations (ND values each): the Jacobi preconditioner's M^-1 of a node from its
+// configuration alone (the diagonal of its centre block, matrix_free.cu:167-188 and :388-408
+// sum it from the 8 voxels' element-matrix diagonals).
+constexpr int ASM_NCFG = 256;
+__host__ __device__ constexpr int asm_table_words(int nd, int bs) { return ASM_NBLK * bs + ASM_NCFG * nd; }
+
 // Host: the 416 assembled blocks of a model from its dense element matrices Kd [nmat][8ND][8ND]
-// (row-major), summed in FP64; block (o, v) at (asm_base(o) + v) * bs.
+// (row-major), summed in FP64; block (o, v) at (asm_base(o) + v) * bs; then the inverse
+// diagonals at ASM_NBLK * bs + m * nd.
 inline void asm_build_table(int nd, int nmat, const double* Kd, int bs, double* tab) {
   const int ED = 8 * nd;
-  for (int i = 0; i < ASM_NBLK * bs; i++) tab[i] = 0.0;
+  for (int i = 0; i < asm_table_words(nd, bs); i++) tab[i] = 0.0;
+  for (int m = 0; m < ASM_NCFG; m++)
+    for (int c = 0; c < nd; c++) {
+      double d = 0.0;
+      for (int p = 0; p < 8; p++) {
+        const int e = asm_eloc(p), mat = std::min((m >> p) & 1, nmat - 1);
+        d += Kd[(size_t)mat * ED * ED + (size_t)(e * nd + c) * ED + e * nd + c];
+      }
+      tab[ASM_NBLK * bs + m * nd + c] = 1.0 / d;
+    }
   for (int o = 0; o < 27; o++) {
     const int dr = o % 3 - 1, dc = (o / 3) % 3 - 1, dl = o / 9 - 1;
     const int cnt = asm_count(o);

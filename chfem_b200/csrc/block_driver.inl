@@ -38,7 +38,10 @@ static bool block_alloc(int nr) {
   B = new BlockState();
   B->nr = nr; B->prec = p; B->n = S->nvars;
   const size_t tot = (size_t)nr * std::max<long>(S->nvars, 1);
-  void** vs[] = {&B->r, &B->s, &B->d0, &B->d1, &B->q};
+  // thermal / elastic: r, the direction's two buffers and q (s = M^-1 r is formed by the
+  // operator pass); Stokes (P)MINRES also keeps s
+  std::vector<void**> vs = {&B->r, &B->d0, &B->d1, &B->q};
+  if (S->analysis == CUDAPCG_FLUID_3D) vs.push_back(&B->s);
   for (void** v : vs) { CKV(cudaMalloc(v, tot * sizeof(T))); CKV(cudaMemset(*v, 0, tot * sizeof(T))); }
   CKV(cudaMalloc(&B->x, tot * 8));
   CKV(cudaMalloc(&B->b64, tot * 8));
@@ -73,29 +76,31 @@ static int asm_tile_choice() {
 
 // The assembled-stencil block operator pass (stencil_asm.cuh, launched from asm_apply.cu).
 template <int ND, typename T, int NR>
-static bool launch_asm_block(T* dold, T* dnew) {
+static bool launch_asm_block(T* dold, T* dnew, int precond) {
   const int tile = asm_tile_choice();
   const int nb = asm_block_ctas<ND, T, NR>(S->R, S->C, S->L, num_sms(), tile);
   if (nb < 1) { set_err("assembled block operator", "launch configuration"); return false; }
   if (!ensure_reduction(nb)) return false;
-  BlkArgs<ND, T> a{(const T*)B->s, dold, dnew, (T*)B->q, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->nvars, B->sc, redctl(nb)};
+  BlkArgs<ND, T> a{(const T*)B->r, dold, dnew, (T*)B->q, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->nvars, B->sc, redctl(nb), precond};
   const cudaError_t e = asm_block_launch<ND, T, NR>(a, tabdev<T>(), nb, tile, S->stream);
   S->launches++;
   if (e != cudaSuccess) { set_err("assembled block operator", cudaGetErrorString(e)); return false; }
   return true;
 }
 
+// plain: the bare operator (M = I in the direction), for cudapcgB200ApplyBlockOperator
 template <int ND, typename T, int NR>
-static bool launch_blk_apply(int parity) {
+static bool launch_blk_apply(int parity, bool plain = false) {
   const long n = S->nvars;
   T* dold = (T*)(parity ? B->d1 : B->d0);
   T* dnew = (T*)(parity ? B->d0 : B->d1);
-  if (asm_applies()) return launch_asm_block<ND, T, NR>(dold, dnew);
+  const int precond = plain ? 0 : S->precond;
+  if (asm_applies()) return launch_asm_block<ND, T, NR>(dold, dnew, precond);
   const dim3 block(TE_TR, TE_TC);
   if (!blk_prepare<ND, T, NR>()) return false;
   const int nb = te_ctas(k_blk_apply<ND, T, NR>, blk_smem_bytes<ND, T, NR>());
   if (!ensure_reduction(nb)) return false;
-  BlkArgs<ND, T> a{(const T*)B->s, dold, dnew, (T*)B->q, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, n, B->sc, redctl(nb)};
+  BlkArgs<ND, T> a{(const T*)B->r, dold, dnew, (T*)B->q, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, n, B->sc, redctl(nb), precond};
   k_blk_apply<ND, T, NR><<<nb, block, blk_smem_bytes<ND, T, NR>(), S->stream>>>(a);
   S->launches++;
   return cudaPeekAtLastError() == cudaSuccess;
@@ -109,7 +114,7 @@ static bool launch_blk_point(int parity) {
   const bool chunks = n % 4 == 0;
   const int g = pw_grid(chunks ? n / 4 : S->N);
   if (!ensure_reduction(g)) return false;
-  BlkPw<ND, T> p{B->x, dnew, (T*)B->r, (const T*)B->q, (T*)B->s, S->d_keys, Kdev<T>(), S->nmat, S->N, n, B->sc, redctl(g), solvecfg()};
+  BlkPw<ND, T> p{B->x, dnew, (T*)B->r, (const T*)B->q, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->N, n, B->sc, redctl(g), solvecfg()};
   if (chunks) {
     if (S->resnorm == CUDAPCG_L2_NORM) k_blk_point4<ND, T, NR, false><<<g, PW_NT, 0, S->stream>>>(p);
     else k_blk_point4<ND, T, NR, true><<<g, PW_NT, 0, S->stream>>>(p);
@@ -196,10 +201,10 @@ static bool solve_block_device(const bool* has_x0) {
   CKV(cudaEventRecord(S->ev0, S->stream));
   for (int k = 0; k < NR; k++) {
     S->cur_sc = B->sc + k;
-    if (!launch_point<T, PW_INIT>(slice<double>(B->x, k), nullptr, slice<T>(B->r, k), nullptr, slice<T>(B->s, k), nullptr)) { S->cur_sc = S->d_sc; return false; }
+    if (!launch_point<T, PW_INIT>(slice<double>(B->x, k), nullptr, slice<T>(B->r, k), nullptr, nullptr, nullptr)) { S->cur_sc = S->d_sc; return false; }
     if (has_x0[k]) {
       if (!residual_from_x<T>(true, slice<double>(B->x, k), slice<double>(B->b64, k), slice<T>(B->r, k)) ||
-          !launch_point<T, PW_X0R>(slice<double>(B->x, k), nullptr, slice<T>(B->r, k), nullptr, slice<T>(B->s, k), nullptr)) { S->cur_sc = S->d_sc; return false; }
+          !launch_point<T, PW_X0R>(slice<double>(B->x, k), nullptr, slice<T>(B->r, k), nullptr, nullptr, nullptr)) { S->cur_sc = S->d_sc; return false; }
     }
   }
   S->cur_sc = S->d_sc;
@@ -231,7 +236,7 @@ static bool solve_block_device(const bool* has_x0) {
           checks[k]++;
           S->cur_sc = B->sc + k;
           bool ok = residual_from_x<T>(false, slice<double>(B->x, k), slice<double>(B->b64, k), slice<T>(B->r, k)) &&
-                    launch_point<T, PW_CHECK>(slice<double>(B->x, k), nullptr, slice<T>(B->r, k), nullptr, slice<T>(B->s, k), nullptr);
+                    launch_point<T, PW_CHECK>(slice<double>(B->x, k), nullptr, slice<T>(B->r, k), nullptr, nullptr, nullptr);
           S->cur_sc = S->d_sc;
           if (!ok) return false;
           checked[k] = true;
@@ -244,7 +249,7 @@ static bool solve_block_device(const bool* has_x0) {
       if (mixed && ((unsigned)h.iteration >= next_replace[k] || fabs(h.delta) < S->replace_drop * repl_delta[k])) {
         S->cur_sc = B->sc + k;
         bool ok = residual_from_x<T>(true, slice<double>(B->x, k), slice<double>(B->b64, k), slice<T>(B->r, k)) &&
-                  launch_point<T, PW_REPL>(slice<double>(B->x, k), nullptr, slice<T>(B->r, k), nullptr, slice<T>(B->s, k), nullptr);
+                  launch_point<T, PW_REPL>(slice<double>(B->x, k), nullptr, slice<T>(B->r, k), nullptr, nullptr, nullptr);
         S->cur_sc = S->d_sc;
         if (!ok) return false;
         next_replace[k] = (unsigned)h.iteration + S->replace_every;
@@ -540,8 +545,8 @@ static bool solve_block_T(int nr, const double* const* rhs, const double* const*
 }
 
 // y_k = A v_k for nr host vectors through the block operator pass of the block solver (the
-// assembled-stencil pass for two-material models): direction formed with beta = 0, so
-// d_new = v and q = A v.
+// assembled-stencil pass for two-material models): v goes into r, and the direction is formed
+// with beta = 0 and M = I, so d_new = v and q = A v.
 template <typename T>
 static bool apply_block_T(int nr, const double* const* v, double* const* y) {
   if (!ensure_vectors<T>() || !ensure_K<T>() || !block_alloc<T>(nr)) return false;
@@ -550,8 +555,8 @@ static bool apply_block_T(int nr, const double* const* v, double* const* y) {
   const long n = S->nvars;
   for (int k = 0; k < nr; k++) {
     CKV(cudaMemcpyAsync(slice<double>(B->b64, k), v[k], n * 8, cudaMemcpyHostToDevice, S->stream));
-    if (sizeof(T) == 8) CKV(cudaMemcpyAsync(slice<double>(B->s, k), slice<double>(B->b64, k), n * 8, cudaMemcpyDeviceToDevice, S->stream));
-    else k_convert<double, float><<<pw_grid(n), PW_NT, 0, S->stream>>>(slice<double>(B->b64, k), slice<float>(B->s, k), n);
+    if (sizeof(T) == 8) CKV(cudaMemcpyAsync(slice<double>(B->r, k), slice<double>(B->b64, k), n * 8, cudaMemcpyDeviceToDevice, S->stream));
+    else k_convert<double, float><<<pw_grid(n), PW_NT, 0, S->stream>>>(slice<double>(B->b64, k), slice<float>(B->r, k), n);
   }
   CKV(cudaMemsetAsync(B->d0, 0, (size_t)nr * n * sizeof(T), S->stream));
   for (int k = 0; k < nr; k++) {
@@ -562,9 +567,9 @@ static bool apply_block_T(int nr, const double* const* v, double* const* y) {
   CKV(cudaMemcpyAsync(B->sc, B->h_sc, nr * sizeof(DevScalars), cudaMemcpyHostToDevice, S->stream));
   CKV(cudaMemsetAsync(S->d_ticket, 0, sizeof(unsigned), S->stream));
   bool ok;
-  if (S->nd == 1 && nr == 3) ok = launch_blk_apply<1, T, 3>(0);
-  else if (S->nd == 3 && nr == 6) ok = launch_blk_apply<3, T, 6>(0);
-  else if (S->nd == 3 && nr == 3) ok = launch_blk_apply<3, T, 3>(0);
+  if (S->nd == 1 && nr == 3) ok = launch_blk_apply<1, T, 3>(0, true);
+  else if (S->nd == 3 && nr == 6) ok = launch_blk_apply<3, T, 6>(0, true);
+  else if (S->nd == 3 && nr == 3) ok = launch_blk_apply<3, T, 3>(0, true);
   else { set_err("cudapcgB200ApplyBlockOperator", "block sizes are 3 (thermal, elastic) and 6 (elastic)"); return false; }
   if (!ok) { set_err("cudapcgB200ApplyBlockOperator", cudaGetErrorString(cudaGetLastError())); return false; }
   for (int k = 0; k < nr; k++) {

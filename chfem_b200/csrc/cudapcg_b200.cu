@@ -24,6 +24,7 @@
 #include "stencil_block.cuh"
 #include "stencil_asm.cuh"
 #include "asm_apply.h"
+#include "pore_maps.h"
 #include "stencil_fluid_block.cuh"
 #include "loadcase.cuh"
 #include "fields.cuh"
@@ -109,6 +110,7 @@ struct Solver {
   float* d_tab32 = nullptr;
   // Krylov work vectors, typed for the precision in use
   int vec_prec = -1;
+  int vec_layout = -1;  // which work vectors ensure_vectors allocated (precision, solver kind)
   void* r = nullptr; void* r2 = nullptr; void* d0 = nullptr; void* d1 = nullptr;
   void* q = nullptr; void* s = nullptr; void* q2 = nullptr;
   // FP64 in every mode: the solution, the right-hand side, an operator output and staging
@@ -175,6 +177,7 @@ static void free_work_vectors() {
   free_ptr(S->q); free_ptr(S->s); free_ptr(S->q2);
   S->r = S->r2 = S->d0 = S->d1 = S->q = S->s = S->q2 = nullptr;
   S->vec_prec = -1;
+  S->vec_layout = -1;
   if (S->gexec) { cudaGraphExecDestroy(S->gexec); S->gexec = nullptr; S->graph_key = -1; }
 }
 static void free_vectors() {
@@ -197,32 +200,67 @@ static void free_model_dev() {
   S->have_K = S->have_keys = S->have_maps = false;
 }
 
-// Work vectors for precision T (the right-hand side is carried across a precision change
-// through its FP64 copy); the FP64 vectors are allocated once per model.
+static bool minres_solver() { return S->solver_flag == CUDAPCG_MINRES_SOLVER || S->solver_flag == CUDAPCG_MINRES3_SOLVER; }
+// CG3 on thermal / elastic models: the 3-vector PCG (x, r and the direction's two buffers)
+static bool pcg3_solver() { return S->solver_flag == CUDAPCG_CG3_SOLVER && S->analysis != CUDAPCG_FLUID_3D; }
+
+// An FP64 vector of nvars entries allocated on first use (staging and scratch; never called
+// while a stream capture is open).
+static bool ensure_scratch64(double*& p) {
+  if (p) return true;
+  CKV(cudaMalloc(&p, std::max<size_t>((size_t)S->nvars, 1) * 8));
+  return true;
+}
+
+// Work vectors for precision T, as many as the selected solver reads:
+//   every solver      x (FP64), r, the direction's two buffers d0 / d1
+//   PCG / MINRES      q = A d
+//   Stokes, MINRES    s (Stokes PCG reads a stored M^-1 r; (P)MINRES keeps A M^-1 r)
+//   MINRES            r2, q2 (the residual's second buffer, the q recursion)
+//   b64 (FP64 right-hand side): kept except for FP64 PCG3, whose r is the only copy of b (as
+//   in the reference's 3-vector solvers, chfem/src/femhmg/cudapcg/solvers/pcg3.cu:28-60)
+// The right-hand side is carried across a change of precision or solver.
 template <typename T>
 static bool ensure_vectors() {
   const int p = prec_of<T>();
   const size_t n = std::max<size_t>((size_t)S->nvars, 1);
+  const int layout = p | (minres_solver() ? 0x10 : 0) | (pcg3_solver() ? 0x20 : 0) | (S->analysis == CUDAPCG_FLUID_3D ? 0x40 : 0);
+  const bool want_b64 = !(pcg3_solver() && p == CHFEM_B200_FP64);
   if (!S->x) {
-    double** v64[] = {&S->x, &S->b64, &S->y64, &S->x64};
-    for (double** v : v64) {
-      CKV(cudaMalloc(v, n * 8));
-      CKV(cudaMemsetAsync(*v, 0, n * 8, S->stream));
-    }
+    CKV(cudaMalloc(&S->x, n * 8));
+    CKV(cudaMemsetAsync(S->x, 0, n * 8, S->stream));
     S->arrays_alloc = true;
   }
-  if (S->vec_prec == p && S->r) return true;
+  if (S->vec_prec == p && S->r && S->vec_layout == layout && (S->b64 != nullptr) == want_b64) return true;
+  // the right-hand side: from b64, or from an FP64 r that is its only copy
+  if (S->rhs_set && !S->b64 && S->r && S->vec_prec == CHFEM_B200_FP64) {
+    CKV(cudaMalloc(&S->b64, n * 8));
+    CKV(cudaMemcpyAsync(S->b64, S->r, n * 8, cudaMemcpyDeviceToDevice, S->stream));
+  }
+  if (want_b64 && !S->b64) {
+    CKV(cudaMalloc(&S->b64, n * 8));
+    CKV(cudaMemsetAsync(S->b64, 0, n * 8, S->stream));
+  }
   free_work_vectors();
-  void** vs[] = {&S->r, &S->r2, &S->d0, &S->d1, &S->q, &S->s, &S->q2};
+  std::vector<void**> vs = {&S->r, &S->d0, &S->d1};
+  if (!pcg3_solver()) vs.push_back(&S->q);
+  if (S->analysis == CUDAPCG_FLUID_3D || minres_solver()) vs.push_back(&S->s);
+  if (minres_solver()) { vs.push_back(&S->r2); vs.push_back(&S->q2); }
   for (void** v : vs) {
     CKV(cudaMalloc(v, n * sizeof(T)));
     CKV(cudaMemsetAsync(*v, 0, n * sizeof(T), S->stream));
   }
   S->vec_prec = p;
-  if (S->rhs_set) {  // re-derive the working right-hand side from its FP64 copy
+  S->vec_layout = layout;
+  if (S->rhs_set && S->b64) {  // re-derive the working right-hand side from its FP64 copy
     if (sizeof(T) == 8) CKV(cudaMemcpyAsync(S->r, S->b64, n * 8, cudaMemcpyDeviceToDevice, S->stream));
     else k_convert<double, float><<<std::max<long>(1, std::min<long>((n + 255) / 256, 8 * 148)), 256, 0, S->stream>>>(S->b64, (float*)S->r, (long)n);
   }
+  if (!want_b64 && S->b64) { CKV(cudaStreamSynchronize(S->stream)); free_ptr(S->b64); S->b64 = nullptr; }
+  if (p == CHFEM_B200_MIXED && !ensure_scratch64(S->y64)) return false;  // residual replacement
+  if (getenv("CHFEM_B200_TRACE"))
+    fprintf(stderr, "[vectors] precision %d layout 0x%x: r %d r2 %d d0 %d d1 %d q %d s %d q2 %d | x %d b64 %d y64 %d x64 %d\n", p, layout,
+            !!S->r, !!S->r2, !!S->d0, !!S->d1, !!S->q, !!S->s, !!S->q2, !!S->x, !!S->b64, !!S->y64, !!S->x64);
   return true;
 }
 
@@ -241,7 +279,7 @@ static bool ensure_tab() {
   if (tabdev<T>()) return true;
   if (!S->have_K) { set_err("solve", "local matrices were not set (cudapcgSetLclMtxs)"); return false; }
   const int bs = S->nd == 1 ? 1 : (sizeof(T) == 4 ? 12 : 9);  // AsmLayout<ND, T, NR>::BS
-  std::vector<double> t64((size_t)ASM_NBLK * bs);
+  std::vector<double> t64((size_t)asm_table_words(S->nd, bs));
   asm_build_table(S->nd, S->nmat, S->Kd.data(), bs, t64.data());
   std::vector<T> t(t64.begin(), t64.end());
   T* d = nullptr;
@@ -406,12 +444,71 @@ static bool launch_mr_op(const T* rin, T* rout, int fin, bool skip_if_done);
 // finishes alpha = delta / (d_new . A d_new); pass 2 updates x, r, s and finishes delta,
 // beta and the stopping test.  Buffers: d_old/d_new alternate, so a chunk has an even
 // number of iterations.
+// Thermal / elastic PCG forms s = M^-1 r inside the operator pass from r and the node keys and
+// stores no s; the Stokes operator (a gather through the DOF map) reads a stored s.
+static bool keeps_s() { return S->analysis == CUDAPCG_FLUID_3D; }
+template <typename T> static T* s_or_null() { return keeps_s() ? (T*)S->s : nullptr; }
+template <typename T> static const T* pcg_dir_in() { return keeps_s() ? (const T*)S->s : (const T*)S->r; }
+
+// A thermal / elastic operator pass of the given mode (TE_DIRDOT, TE_UPD: the 3-vector PCG)
+// on the model, with the assembled blocks where they apply.
+template <typename T, int MODE>
+static bool launch_te_mode(const T* in0, const T* in1, T* vout, double* x, int finish) {
+  const SolveCfg sc = solvecfg();
+  const MrCfg cfg{sc.tol, sc.maxit, sc.norm, sc.precond, sc.nhmg};
+  cudaError_t e = cudaSuccess;
+  if (asm_applies()) {
+    if (S->nd == 1) {
+      const int nb = asm_te_ctas<1, T, MODE>(S->R, S->C, S->L, num_sms());
+      if (nb < 1 || !ensure_reduction(nb)) return false;
+      TeArgs<1, T> a{in0, in1, vout, nullptr, x, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->cur_sc, redctl(nb), finish, 1, cfg};
+      e = asm_te_launch<1, T, MODE>(a, tabdev<T>(), nb, S->stream);
+    } else {
+      const int nb = asm_te_ctas<3, T, MODE>(S->R, S->C, S->L, num_sms());
+      if (nb < 1 || !ensure_reduction(nb)) return false;
+      TeArgs<3, T> a{in0, in1, vout, nullptr, x, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->cur_sc, redctl(nb), finish, 1, cfg};
+      e = asm_te_launch<3, T, MODE>(a, tabdev<T>(), nb, S->stream);
+    }
+  } else {
+    const dim3 block(TE_TR, TE_TC);
+    if (S->nd == 1) {
+      const size_t sm = te_smem_bytes<1, T>(S->nmat);
+      const int nb = te_ctas(k_te_apply<1, T, MODE>, sm);
+      if (!ensure_reduction(nb)) return false;
+      TeArgs<1, T> a{in0, in1, vout, nullptr, x, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->cur_sc, redctl(nb), finish, 1, cfg};
+      k_te_apply<1, T, MODE><<<nb, block, sm, S->stream>>>(a);
+    } else {
+      const size_t sm = te_smem_bytes<3, T>(S->nmat);
+      const int nb = te_ctas(k_te_apply<3, T, MODE>, sm);
+      if (!ensure_reduction(nb)) return false;
+      TeArgs<3, T> a{in0, in1, vout, nullptr, x, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->cur_sc, redctl(nb), finish, 1, cfg};
+      k_te_apply<3, T, MODE><<<nb, block, sm, S->stream>>>(a);
+    }
+    e = cudaGetLastError();
+  }
+  S->launches++;
+  if (e != cudaSuccess) { set_err("operator pass", cudaGetErrorString(e)); return false; }
+  return true;
+}
+
+// One 3-vector PCG iteration (CG3 on thermal / elastic models; pcg3.cu:163-208 applies the
+// operator twice per iteration on x, r, d): pass 1 forms d_new = M^-1 r + beta d_old and
+// finishes alpha = delta / (d_new . A d_new); pass 2 applies A to d_new again and updates
+// r -= alpha A d_new, x += alpha d_new, then finishes delta, beta and the stopping test.
+template <typename T>
+static bool enqueue_pcg3_iteration(int parity) {
+  T* dold = (T*)(parity ? S->d1 : S->d0);
+  T* dnew = (T*)(parity ? S->d0 : S->d1);
+  return launch_te_mode<T, TE_DIRDOT>((const T*)S->r, dold, dnew, nullptr, FIN_ALPHA) &&
+         launch_te_mode<T, TE_UPD>(dnew, nullptr, (T*)S->r, S->x, FIN_STORE);
+}
+
 template <typename T>
 static bool enqueue_pcg_iteration(int parity) {
   T* dold = (T*)(parity ? S->d1 : S->d0);
   T* dnew = (T*)(parity ? S->d0 : S->d1);
-  if (!launch_apply<T>((const T*)S->s, dold, dnew, (T*)S->q, true, FIN_ALPHA, true)) return false;
-  return launch_point<T, PW_PCG>(S->x, dnew, (T*)S->r, (const T*)S->q, (T*)S->s, nullptr);
+  if (!launch_apply<T>(pcg_dir_in<T>(), dold, dnew, (T*)S->q, true, FIN_ALPHA, true)) return false;
+  return launch_point<T, PW_PCG>(S->x, dnew, (T*)S->r, (const T*)S->q, s_or_null<T>(), nullptr);
 }
 
 // r = b - A x with the operator applied in FP64 to the FP64 solution (initial guesses and
@@ -421,7 +518,8 @@ __global__ void k_residual_replace(const double* b, const double* Ax, T* r, long
 template <typename T>
 static bool residual_from_x(bool skip_if_done = true, double* x = nullptr, const double* b = nullptr, T* r = nullptr) {
   if (!x) { x = S->x; b = S->b64; r = (T*)S->r; }
-  if (!ensure_K<double>()) return false;
+  if (!b) b = (const double*)r;  // FP64 without a copy of b: r still holds it (set-up only)
+  if (!ensure_K<double>() || !ensure_scratch64(S->y64)) return false;
   if (!launch_apply<double>(x, nullptr, nullptr, S->y64, false, FIN_NONE, skip_if_done)) return false;
   const long n = S->nvars;
   k_residual_replace<T><<<pw_grid(n), PW_NT, 0, S->stream>>>(b, S->y64, r, n);
@@ -447,6 +545,7 @@ static bool build_graph(int key, int chunk, bool minres) {
   const unsigned long long l0 = S->launches;
   for (int it = 0; it < chunk && ok; it++) {
     if (minres) ok = enqueue_minres_iteration<T>(it & 1);
+    else if (pcg3_solver()) ok = enqueue_pcg3_iteration<T>(it & 1);
     else ok = enqueue_pcg_iteration<T>(it & 1);
   }
   S->launches = l0;
@@ -470,7 +569,8 @@ static bool read_scalars() {
 template <typename T>
 static bool run_chunks(bool minres) {
   const int chunk = std::max(2u, S->iters_per_launch & ~1u);
-  const int key = (prec_of<T>() << 8) | (minres ? 0x80 : 0) | (chunk & 0x7f) | (S->resnorm << 16) | (S->precond << 20);
+  const int key = (prec_of<T>() << 8) | (minres ? 0x80 : 0) | (chunk & 0x7f) | (S->resnorm << 16) | (S->precond << 20) |
+                  (pcg3_solver() ? 1 << 24 : 0);
   if (!build_graph<T>(key, chunk, minres)) return false;
   const bool mixed = sizeof(T) == 4 && S->replace_every > 0;
   unsigned next_replace = S->replace_every;
@@ -495,7 +595,7 @@ static bool run_chunks(bool minres) {
         checks++;
         if (!residual_from_x<T>(false)) return false;
         if (minres) { if (!launch_mr_op<T>((const T*)S->r, (T*)S->r2, FIN_MR_CHECK, false)) return false; }
-        else if (!launch_point<T, PW_CHECK>(S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
+        else if (!launch_point<T, PW_CHECK>(S->x, nullptr, (T*)S->r, nullptr, s_or_null<T>(), nullptr)) return false;
         if (!read_scalars()) return false;
         if (trace) fprintf(stderr, "[single] true-residual check %d: done %d metric %.6e\n", checks, S->h_sc->done, S->h_sc->metric);
         if (S->h_sc->done) break;
@@ -515,7 +615,7 @@ static bool run_chunks(bool minres) {
         // both are refreshed, q by an apply of the current direction
         if (!launch_mr_op<T>((const T*)S->r, (T*)S->r2, FIN_MR_REPL, true)) return false;
         if (!launch_apply<T>((const T*)S->d0, nullptr, nullptr, (T*)S->q, false, FIN_NONE, true)) return false;
-      } else if (!launch_point<T, PW_REPL>(S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
+      } else if (!launch_point<T, PW_REPL>(S->x, nullptr, (T*)S->r, nullptr, s_or_null<T>(), nullptr)) return false;
       next_replace = (unsigned)S->h_sc->iteration + S->replace_every;
       repl_ref = progress();
       if (trace) fprintf(stderr, "[single] residual replacement at %d\n", S->h_sc->iteration);
@@ -535,15 +635,15 @@ static bool solve_pcg_device() {
   CKV(cudaMemsetAsync(S->d_sc, 0, sizeof(DevScalars), S->stream));
   const size_t n = (size_t)S->nvars;
   if (!S->x0_set) CKV(cudaMemsetAsync(S->x, 0, n * 8, S->stream));
-  CKV(cudaMemsetAsync(S->q, 0, n * sizeof(T), S->stream));
+  if (S->q) CKV(cudaMemsetAsync(S->q, 0, n * sizeof(T), S->stream));
   CKV(cudaMemsetAsync(S->d0, 0, n * sizeof(T), S->stream));
   CKV(cudaMemsetAsync(S->d1, 0, n * sizeof(T), S->stream));
   CKV(cudaEventRecord(S->ev0, S->stream));
   // zero-guess reference: s = M^-1 r, delta0 = r.s   (pcg.cu:61-81)
-  if (!launch_point<T, PW_INIT>(S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
+  if (!launch_point<T, PW_INIT>(S->x, nullptr, (T*)S->r, nullptr, s_or_null<T>(), nullptr)) return false;
   if (S->x0_set) {  // pcg.cu:83-99: r = b - A x0 (FP64 apply), then the initial-guess test
     if (!residual_from_x<T>()) return false;
-    if (!launch_point<T, PW_X0R>(S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
+    if (!launch_point<T, PW_X0R>(S->x, nullptr, (T*)S->r, nullptr, s_or_null<T>(), nullptr)) return false;
   }
   CKV(cudaEventRecord(S->ev1, S->stream));
   if (!run_chunks<T>(false)) return false;
@@ -730,7 +830,9 @@ cudapcgFlag_t cudapcgSetSolver(cudapcgFlag_t flag) {
     S->rhs_set = false;
     S->x0_set = false;
   }
-  S->solver_flag = flag;  // CG3/MINRES3 run the same iterates as CG/MINRES
+  // CG3 on thermal / elastic models: the 3-vector PCG (same iterates as CG, two operator passes
+  // per iteration, no q); MINRES3 runs the iterates of MINRES
+  S->solver_flag = flag;
   if (S->gexec) { cudaGraphExecDestroy(S->gexec); S->gexec = nullptr; S->graph_key = -1; }
   return CUDAPCG_TRUE;
 }
@@ -758,8 +860,11 @@ static bool upload_vec(const double* host, void* dst_T) {
   if (S->vec_prec == CHFEM_B200_FP64) {
     CKV(cudaMemcpyAsync(dst_T, host, n * 8, cudaMemcpyHostToDevice, S->stream));
   } else {
-    CKV(cudaMemcpyAsync(S->x64, host, n * 8, cudaMemcpyHostToDevice, S->stream));
-    k_convert<double, float><<<pw_grid(n), PW_NT, 0, S->stream>>>(S->x64, (float*)dst_T, n);
+    // staged in FP64 scratch: the residual-replacement scratch of mixed mode when it exists
+    double*& stage = S->y64 ? S->y64 : S->x64;
+    if (!ensure_scratch64(stage)) return false;
+    CKV(cudaMemcpyAsync(stage, host, n * 8, cudaMemcpyHostToDevice, S->stream));
+    k_convert<double, float><<<pw_grid(n), PW_NT, 0, S->stream>>>(stage, (float*)dst_T, n);
   }
   return true;
 }
@@ -778,7 +883,7 @@ cudapcgFlag_t cudapcgSetRHS(cudapcgVar_t* RHS) {
     return CUDAPCG_TRUE;
   }
   if (!upload_vec(RHS, S->r)) return CUDAPCG_FALSE;
-  CK(cudaMemcpyAsync(S->b64, RHS, S->nvars * 8, cudaMemcpyHostToDevice, S->stream));
+  if (S->b64) CK(cudaMemcpyAsync(S->b64, RHS, S->nvars * 8, cudaMemcpyHostToDevice, S->stream));
   CK(cudaStreamSynchronize(S->stream));
   S->rhs_set = true;
   return CUDAPCG_TRUE;
@@ -828,6 +933,7 @@ extern "C" {
 static bool interp_into(const double* coarse_host, double* target) {
   const int rows = S->R, cols = S->C, lays = S->L, nd = (int)(S->nvars / S->N);
   const size_t ncoarse = (size_t)nd * (cols / 2) * (rows / 2) * (lays / 2 + (lays < 2));
+  if (!ensure_scratch64(S->x64)) return false;
   CKV(cudaMemcpyAsync(S->x64, coarse_host, ncoarse * 8, cudaMemcpyHostToDevice, S->stream));
   CKV(cudaMemsetAsync(target, 0, S->nvars * 8, S->stream));
   const int g = pw_grid(S->N);
@@ -960,6 +1066,73 @@ cudapcgFlag_t cudapcgB200SetImageColors(const uint8_t* colors, unsigned int rows
   if (bad) { set_err(who, "the image holds a colour without a material (or a material index above 3)"); return CUDAPCG_FALSE; }
   S->have_keys = true;
   invalidate_graphs();
+  return CUDAPCG_TRUE;
+}
+// Stokes DOF-number maps built on the device from the image's colours (pore_maps.cu): the
+// node -> DOF map, the DOF -> node map and the interface keys, numbered as
+// femhmg_fluid_3D.c:370-491 does (pore nodes, then interface nodes, each in node order).  The
+// current model's unknown counts (and the caller's model struct) are set from the numbering.
+cudapcgFlag_t cudapcgB200SetPoreImageColors(const uint8_t* colors, unsigned int rows, unsigned int cols, unsigned int slices,
+                                            unsigned int refinement, const int* material_of_color, unsigned int* npore,
+                                            unsigned int* nborder) {
+  const char* who = "cudapcgB200SetPoreImageColors";
+  if (!S || !S->model || !colors || !material_of_color || refinement < 1) { set_err(who, "bad arguments"); return CUDAPCG_FALSE; }
+  if (S->analysis != CUDAPCG_FLUID_3D) { set_err(who, "FLUID_3D models only (thermal / elastic: cudapcgB200SetImageColors)"); return CUDAPCG_FALSE; }
+  if ((long)rows * refinement != S->R || (long)cols * refinement != S->C || (long)slices * refinement != S->L) {
+    set_err(who, "image size times refinement differs from the model's");
+    return CUDAPCG_FALSE;
+  }
+  PoreColorMap cm;
+  for (int c = 0; c < 256; c++) cm.mat[c] = (int16_t)(material_of_color[c] < 0 ? -1 : material_of_color[c]);
+  const long N = S->N, nchunks = pore_maps_chunks(N);
+  const size_t nimg = (size_t)rows * cols * slices;
+  uint8_t *d_col = nullptr, *d_fk = nullptr;
+  unsigned* d_cnt = nullptr;
+  unsigned long long* d_tot = nullptr;
+  int* d_bad = nullptr;
+  auto cleanup = [&]() { cudaFree(d_col); cudaFree(d_fk); cudaFree(d_cnt); cudaFree(d_tot); cudaFree(d_bad); };
+  cudaError_t e = cudaMalloc(&d_col, nimg);
+  if (e == cudaSuccess) e = cudaMalloc(&d_fk, N);
+  if (e == cudaSuccess) e = cudaMalloc(&d_cnt, 2 * sizeof(unsigned) * nchunks);
+  if (e == cudaSuccess) e = cudaMalloc(&d_tot, 2 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&d_bad, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_col, colors, nimg, cudaMemcpyHostToDevice, S->stream);
+  if (e != cudaSuccess) { cleanup(); set_err(who, cudaGetErrorString(e)); return CUDAPCG_FALSE; }
+  unsigned long long nV = 0, nB = 0;
+  const char* msg = nullptr;
+  if (!pore_maps_count(d_col, cm, S->R, S->C, S->L, (int)refinement, d_fk, d_cnt, d_tot, d_bad, &nV, &nB, S->stream, &msg)) {
+    cleanup(); set_err(who, msg); return CUDAPCG_FALSE;
+  }
+  if (nV + nB >= 0xffffffffull || 4 * nV + nB >= 0xffffffffull) { cleanup(); set_err(who, "too many Stokes unknowns for 32-bit DOF ids"); return CUDAPCG_FALSE; }
+  // the maps take the sizes of this numbering
+  free_vectors();
+  block_free();
+  free_ptr(S->d_node_of_dof); free_ptr(S->d_bkeys);
+  S->d_node_of_dof = nullptr; S->d_bkeys = nullptr;
+  e = cudaMalloc(&S->d_node_of_dof, sizeof(uint32_t) * std::max<unsigned long long>(1, nV + nB));
+  if (e == cudaSuccess) e = cudaMalloc(&S->d_bkeys, std::max<unsigned long long>(1, nB));
+  if (e != cudaSuccess) { cleanup(); set_err(who, cudaGetErrorString(e)); return CUDAPCG_FALSE; }
+  if (!pore_maps_number(d_fk, S->R, S->C, S->L, d_cnt, (unsigned)nV, S->d_dof_of_node, S->d_node_of_dof, S->d_bkeys, S->stream, &msg)) {
+    cleanup(); set_err(who, msg); return CUDAPCG_FALSE;
+  }
+  e = cudaStreamSynchronize(S->stream);
+  cleanup();
+  if (e != cudaSuccess) { set_err(who, cudaGetErrorString(e)); return CUDAPCG_FALSE; }
+  S->nV = (long)nV; S->nB = (long)nB; S->nvars = 4 * S->nV + S->nB;
+  S->model->nporenodes = (unsigned)nV; S->model->nbordernodes = (unsigned)nB;
+  S->model->nvars = (unsigned)S->nvars; S->model->nhmgvars = (unsigned)(3 * nV);
+  S->have_maps = true;
+  invalidate_graphs();
+  if (npore) *npore = (unsigned)nV;
+  if (nborder) *nborder = (unsigned)nB;
+  return CUDAPCG_TRUE;
+}
+// The current Stokes model's maps copied to the host (N, nV + nB and nB entries); for tests.
+cudapcgFlag_t cudapcgB200GetPoreMaps(uint32_t* dof_of_node, uint32_t* node_of_dof, uint8_t* border_keys) {
+  if (!S || !S->model || S->analysis != CUDAPCG_FLUID_3D || !S->have_maps) { set_err("cudapcgB200GetPoreMaps", "no Stokes maps"); return CUDAPCG_FALSE; }
+  if (dof_of_node) CK(cudaMemcpy(dof_of_node, S->d_dof_of_node, sizeof(uint32_t) * S->N, cudaMemcpyDeviceToHost));
+  if (node_of_dof && S->nV + S->nB) CK(cudaMemcpy(node_of_dof, S->d_node_of_dof, sizeof(uint32_t) * (S->nV + S->nB), cudaMemcpyDeviceToHost));
+  if (border_keys && S->nB) CK(cudaMemcpy(border_keys, S->d_bkeys, S->nB, cudaMemcpyDeviceToHost));
   return CUDAPCG_TRUE;
 }
 cudapcgFlag_t cudapcgSetParametricDensityField(parametricScalarField_t*, double, double) {
@@ -1096,24 +1269,26 @@ template <typename T>
 static bool apply_host_T(const double* xh, double* yh, bool precond_only) {
   if (!ensure_vectors<T>() || !ensure_K<T>()) return false;
   const size_t n = (size_t)S->nvars;
-  // use q2 as input, q as output (solver state in x, r stays untouched)
-  if (!upload_vec(xh, S->q2)) return false;
+  // the direction buffers are free between solves: d0 takes the input, d1 the output (the
+  // solver state in x and r stays untouched)
+  if (!upload_vec(xh, S->d0)) return false;
   if (!ensure_reduction(8 * num_sms())) return false;
   CKV(cudaMemsetAsync(S->d_sc, 0, sizeof(DevScalars), S->stream));
   if (precond_only) {
-    // s = M^-1 q2 via the INIT pass on a copy: r <- q2 temporarily
-    CKV(cudaMemcpyAsync(S->q, S->r, n * sizeof(T), cudaMemcpyDeviceToDevice, S->stream));  // save r in q
-    CKV(cudaMemcpyAsync(S->r, S->q2, n * sizeof(T), cudaMemcpyDeviceToDevice, S->stream));
-    if (!launch_point<T, PW_INIT>(S->x, nullptr, (T*)S->r, nullptr, (T*)S->s, nullptr)) return false;
-    CKV(cudaMemcpyAsync(S->r, S->q, n * sizeof(T), cudaMemcpyDeviceToDevice, S->stream));  // restore r
-    CKV(cudaMemcpyAsync(S->q, S->s, n * sizeof(T), cudaMemcpyDeviceToDevice, S->stream));
+    // M^-1 d0 via the INIT pass on r <- d0 (r saved in x64 meanwhile, as FP64 bits of n T words)
+    if (!ensure_scratch64(S->x64)) return false;
+    CKV(cudaMemcpyAsync(S->x64, S->r, n * sizeof(T), cudaMemcpyDeviceToDevice, S->stream));
+    CKV(cudaMemcpyAsync(S->r, S->d0, n * sizeof(T), cudaMemcpyDeviceToDevice, S->stream));
+    if (!launch_point<T, PW_INIT>(S->x, nullptr, (T*)S->r, nullptr, (T*)S->d1, nullptr)) return false;
+    CKV(cudaMemcpyAsync(S->r, S->x64, n * sizeof(T), cudaMemcpyDeviceToDevice, S->stream));
   } else {
-    if (!launch_apply<T>((const T*)S->q2, nullptr, nullptr, (T*)S->q, false, FIN_STORE, false)) return false;
+    if (!launch_apply<T>((const T*)S->d0, nullptr, nullptr, (T*)S->d1, false, FIN_STORE, false)) return false;
   }
   if (sizeof(T) == 8) {
-    CKV(cudaMemcpyAsync(yh, S->q, n * 8, cudaMemcpyDeviceToHost, S->stream));
+    CKV(cudaMemcpyAsync(yh, S->d1, n * 8, cudaMemcpyDeviceToHost, S->stream));
   } else {
-    k_convert<float, double><<<pw_grid(n), PW_NT, 0, S->stream>>>((const float*)S->q, S->x64, n);
+    if (!ensure_scratch64(S->x64)) return false;
+    k_convert<float, double><<<pw_grid(n), PW_NT, 0, S->stream>>>((const float*)S->d1, S->x64, n);
     CKV(cudaMemcpyAsync(yh, S->x64, n * 8, cudaMemcpyDeviceToHost, S->stream));
   }
   CKV(cudaStreamSynchronize(S->stream));
@@ -1148,9 +1323,9 @@ static double time_op_T(unsigned reps) {
   if (!ensure_vectors<T>() || !ensure_K<T>()) return -1.0;
   if (!ensure_reduction(8 * num_sms())) return -1.0;
   cudaMemsetAsync(S->d_sc, 0, sizeof(DevScalars), S->stream);
-  for (int w = 0; w < 3; w++) launch_apply<T>((const T*)S->s, nullptr, nullptr, (T*)S->q2, false, FIN_NONE, false);
+  for (int w = 0; w < 3; w++) launch_apply<T>((const T*)S->d0, nullptr, nullptr, (T*)S->d1, false, FIN_NONE, false);
   cudaEventRecord(S->ev0, S->stream);
-  for (unsigned i = 0; i < reps; i++) launch_apply<T>((const T*)S->s, nullptr, nullptr, (T*)S->q2, false, FIN_NONE, false);
+  for (unsigned i = 0; i < reps; i++) launch_apply<T>((const T*)S->d0, nullptr, nullptr, (T*)S->d1, false, FIN_NONE, false);
   cudaEventRecord(S->ev1, S->stream);
   if (cudaEventSynchronize(S->ev1) != cudaSuccess) return -1.0;
   float ms = 0;
@@ -1162,6 +1337,7 @@ extern "C" {
 template <typename T>
 static double time_kernel_T(int which, unsigned reps) {
   if (!ensure_vectors<T>() || !ensure_K<T>()) return -1.0;
+  if (!S->q || ((which == 3 || which == 4) && !S->r2)) { set_err("cudapcgB200TimeKernel", "kernel not used by the selected solver"); return -1.0; }
   if (!ensure_reduction(needed_blocks())) return -1.0;
   // each repetition resets the scalars (so no pass exits early) and brackets only the launch
   float total = 0.f;
@@ -1172,9 +1348,9 @@ static double time_kernel_T(int which, unsigned reps) {
     cudaEventRecord(S->ev0, S->stream);
     bool ok;
     switch (which) {
-      case 0: ok = launch_apply<T>((const T*)S->s, nullptr, nullptr, (T*)S->q2, false, FIN_NONE, false); break;
-      case 1: ok = launch_apply<T>((const T*)S->s, (const T*)S->d0, (T*)S->d1, (T*)S->q, true, FIN_ALPHA, false); break;
-      case 2: ok = launch_point<T, PW_PCG>(S->x, (T*)S->d1, (T*)S->r, (const T*)S->q, (T*)S->s, nullptr); break;
+      case 0: ok = launch_apply<T>((const T*)S->d0, nullptr, nullptr, (T*)S->q, false, FIN_NONE, false); break;
+      case 1: ok = launch_apply<T>(pcg_dir_in<T>(), (const T*)S->d0, (T*)S->d1, (T*)S->q, true, FIN_ALPHA, false); break;
+      case 2: ok = launch_point<T, PW_PCG>(S->x, (T*)S->d1, (T*)S->r, (const T*)S->q, s_or_null<T>(), nullptr); break;
       case 3: ok = launch_mr_op<T>((const T*)S->r, (T*)S->r2, FIN_MR_STEP, false); break;
       case 4: ok = launch_mr_dir<T>((const T*)S->r); break;
       default: ok = false;
@@ -1202,11 +1378,23 @@ double cudapcgB200TimeOperator(unsigned int reps) {
 }
 unsigned long long cudapcgB200DeviceBytes(void) {
   if (!S) return 0;
-  const size_t es = S->vec_prec == CHFEM_B200_FP64 ? 8 : 4;
+  const unsigned long long n = (unsigned long long)S->nvars;
   unsigned long long b = 0;
-  if (S->x) b += 7ull * S->nvars * es + 32ull * S->nvars;
-  // the 2-vector solvers: r and d, the reduction accumulator and the per-step sums
-  if (S->vec_prec == VEC_LEAN) b += 16ull * S->nvars + 8ull * (S->xa_cap + S->hist_cap);
+  if (S->vec_prec == VEC_LEAN) {  // the 2-vector solvers: r and d, the accumulator, the per-step sums
+    b += 16ull * n + 8ull * (S->xa_cap + S->hist_cap);
+  } else {
+    const unsigned long long es = S->vec_prec == CHFEM_B200_FP64 ? 8 : 4;
+    const void* work[] = {S->r, S->r2, S->d0, S->d1, S->q, S->s, S->q2};
+    for (const void* v : work) b += v ? es * n : 0;
+    const double* v64[] = {S->x, S->b64, S->y64, S->x64};
+    for (const double* v : v64) b += v ? 8ull * n : 0;
+  }
+  if (B) {  // the block solver's vectors: r, s, d0, d1, q in the work precision, x and b in FP64
+    const unsigned long long es = B->prec == CHFEM_B200_FP64 ? 8 : 4, tot = (unsigned long long)B->nr * B->n;
+    const void* work[] = {B->r, B->s, B->d0, B->d1, B->q};
+    for (const void* v : work) b += v ? es * tot : 0;
+    b += (B->x ? 8ull * tot : 0) + (B->b64 ? 8ull * tot : 0);
+  }
   if (S->analysis == CUDAPCG_FLUID_3D) b += 4ull * S->N + 4ull * (S->nV + S->nB) + S->nB;
   else b += 2ull * S->N;
   return b;
@@ -1247,7 +1435,8 @@ extern "C" cudapcgFlag_t cudapcgB200ComputeFields(int block_index, int axis, int
 template <typename T>
 static bool load_case_rhs_T(int axis, int comp, double jump, const double* CB) {
   const long n = S->nvars;
-  double* b = lean_solver() ? (double*)S->r : S->b64;  // the 2-vector solvers keep no copy of b
+  // the 2-vector solvers and FP64 PCG3 keep no copy of b: their FP64 r is it
+  double* b = (lean_solver() || !S->b64) ? (double*)S->r : S->b64;
   if (S->analysis == CUDAPCG_FLUID_3D) {
     double w = 0.0;
     for (int a = 0; a < 8; a++) w += CB[72 + a];

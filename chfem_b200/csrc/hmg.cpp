@@ -304,6 +304,15 @@ bool setup_solver(Model& m, bool coarse = false) {
     } else {
       ok = ensure_host_maps(m) && cudapcgSetImage(g_par == CUDAPCG_EBE ? m.elem_mat.data() : m.keys.data());
     }
+  } else if (!m.host_maps) {
+    int lut[256];
+    for (int c = 0; c < 256; c++) lut[c] = m.props_keys[c];
+    unsigned nv = 0, nb = 0;
+    ok = cudapcgB200SetPoreImageColors(m.colors.data(), m.frows, m.fcols, m.fslices, m.refinement, lut, &nv, &nb);
+    if (ok && ((long)nv != m.nV || (long)nb != m.nB)) {
+      fail("device DOF numbering disagrees with the host's counts");
+      return false;
+    }
   } else {
     ok = cudapcgSetPeriodic2DOFMap(m.dof_of_node.data()) && cudapcgSetPoreMap(m.border_keys.data()) &&
          cudapcgSetDOF2PeriodicMap(m.node_of_dof.data());
@@ -339,10 +348,11 @@ logical hmgInit(char* data_filename, char* elem_filename, char* sdf_filename, ui
   m->C_dim = m->analysis == ELASTIC ? 36 : 9;
   if (!read_colors(*m, data, elem_filename)) { delete m; return 0; }
   if (m->analysis == FLUID) {
+    // the sizes of the DOF numbering here; the numbering itself on the device at upload
+    // (cudapcgB200SetPoreImageColors), or on the host for the paths that read the maps
     build_elem_mat(*m);
     std::string err;
-    if (!build_maps(*m, err)) { fail(err); delete m; return 0; }
-    m->host_maps = true;
+    if (!count_pore_nodes(*m, err)) { fail(err); delete m; return 0; }
   } else {
     // the node keys are built on the device from the colours (cudapcgB200SetImageColors)
     if (m->nmat > 4) { fail("more than 4 materials cannot be encoded in 16-bit node keys"); delete m; return 0; }

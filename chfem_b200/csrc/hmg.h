@@ -61,6 +61,7 @@ struct Model {
 
 // physics (hmg_physics.cpp)
 bool build_maps(Model& m, std::string& err);
+bool count_pore_nodes(Model& m, std::string& err);
 void build_local_matrices(Model& m);
 void assemble_rhs(const Model& m, int direction, double* rhs);
 void update_C(Model& m, int direction, const double* x);

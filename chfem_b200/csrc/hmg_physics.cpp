@@ -70,6 +70,32 @@ static void shape(int a, const double* p, double& phi, double* grad, bool zflip)
 }
 
 // ---- maps -----------------------------------------------------------------------------
+// Stokes: the fluid key of every node (bit e: the voxel in which the node is local node e is
+// pore, material index 0), the pore voxels, and the counts of pore nodes (key 255) and
+// interface nodes (0 < key < 255) -- the sizes of the DOF numbering (femhmg_fluid_3D.c:370-424),
+// which itself runs in build_maps or on the device (cudapcgB200SetPoreImageColors).
+bool count_pore_nodes(Model& m, std::string& err) {
+  const long R = m.ny, C = m.nx, L = m.nz, N = m.N;
+  m.fluid_keys.assign(N, 0);
+  long pores = 0, nv = 0, nb = 0;
+#pragma omp parallel for reduction(+ : pores, nv, nb) schedule(static)
+  for (long i = 0; i < N; i++) {
+    const long r = i % R, c = (i / R) % C, l = i / (R * C);
+    unsigned k = 0;
+    for (int e = 0; e < 8; e++) k |= (unsigned)(m.elem_mat[node_elem(r, c, l, e, R, C, L)] == 0) << e;
+    m.fluid_keys[i] = (uint8_t)k;
+    pores += (m.elem_mat[i] == 0);
+    nv += (k == 255);
+    nb += (k != 0 && k != 255);
+  }
+  m.nporeelem = pores;
+  if (nv + nb >= (long)0xffffffffL || 4 * nv + nb >= (long)0xffffffffL) { err = "too many Stokes unknowns for 32-bit DOF ids"; return false; }
+  m.nV = nv;
+  m.nB = nb;
+  m.ndof = 4 * nv + nb;
+  return true;
+}
+
 bool build_maps(Model& m, std::string& err) {
   const long R = m.ny, C = m.nx, L = m.nz, N = m.N;
   if (m.analysis != FLUID) {
@@ -85,18 +111,7 @@ bool build_maps(Model& m, std::string& err) {
     m.ndof = N * m.nd;
     return true;
   }
-  // Stokes: bit e of a node's fluid key = voxel e of that node is pore (material index 0)
-  m.fluid_keys.assign(N, 0);
-  long pores = 0;
-#pragma omp parallel for reduction(+ : pores) schedule(static)
-  for (long i = 0; i < N; i++) {
-    const long r = i % R, c = (i / R) % C, l = i / (R * C);
-    unsigned k = 0;
-    for (int e = 0; e < 8; e++) k |= (unsigned)(m.elem_mat[node_elem(r, c, l, e, R, C, L)] == 0) << e;
-    m.fluid_keys[i] = (uint8_t)k;
-    pores += (m.elem_mat[i] == 0);
-  }
-  m.nporeelem = pores;
+  if (!count_pore_nodes(m, err)) return false;
   m.dof_of_node.assign(N, 0);
   long id = 0;
   for (long i = 0; i < N; i++)

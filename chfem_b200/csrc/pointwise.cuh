@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(PW_NT) k_te_point(TePw<ND, T> a) {
         mx = fmax(mx, fabs((double)xv));
       }
       const T sv = rv * inv[c];
-      a.s[j] = sv;
+      if (a.s) a.s[j] = sv;  // thermal / elastic PCG keeps no s (formed from r where it is used)
       sum += (double)rv * (double)sv;
       mr = fmax(mr, fabs((double)rv));
     }

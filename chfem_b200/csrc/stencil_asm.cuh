@@ -15,34 +15,18 @@
 
 namespace chfem {
 
-// raw staging record of a point (ASYNC): s then d_old for every right-hand side in global order,
-// an odd word count so that consecutive lanes' records fall on distinct banks
-template <int ND, int NR>
-__host__ __device__ constexpr int asm_raw_stride() { return 2 * NR * ND + 1; }
-
-template <int ND, typename T, int NR, int TC, int ZB, bool ASYNC = false, bool TG = false>
+template <int ND, typename T, int NR, int TC, int ZB>
 inline size_t asm_smem_bytes() {
   using Lo = AsmLayout<ND, T, NR>;
   const size_t pp = (size_t)(TE_TR + 2) * (TC + 2);
-  return ((TG ? 0 : (size_t)ASM_NBLK * Lo::BS) + (size_t)(ZB + 2) * pp * Lo::PS + (ASYNC ? (size_t)ZB * pp * asm_raw_stride<ND, NR>() : 0)) *
-         sizeof(T);
+  return ((size_t)asm_table_words(ND, Lo::BS) + (size_t)(ZB + 2) * pp * Lo::PS) * sizeof(T);
 }
 
-// 4-byte (or 8-byte) asynchronous global -> shared copy (sm_80+ cp.async; completion by
-// cp.async.wait_all of the issuing thread)
-template <typename T>
-__device__ __forceinline__ void asm_cp_async(T* dst, const T* src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  if constexpr (sizeof(T) == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
-  else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
-}
 // L2 prefetch of [p, p + bytes) rounded out to 16-byte boundaries (sm_90+ bulk prefetch)
 __device__ __forceinline__ void asm_prefetch_l2(const void* p, size_t bytes) {
   const size_t a0 = (size_t)p & ~(size_t)15, a1 = ((size_t)p + bytes + 15) & ~(size_t)15;
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a0), "r"((unsigned)(a1 - a0)) : "memory");
 }
-__device__ __forceinline__ void asm_cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void asm_cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // does any of the ZB nodes use the neighbour position (Q plane, DR row, DC column)?
 template <int ND, int ZB>
@@ -94,25 +78,16 @@ __device__ __forceinline__ void asm_positions(std::integer_sequence<int, Ps...>,
   (asm_position<ND, T, NR, ZB, Ps>(pl, ctr, sT, m, out), ...);
 }
 
-// The block PCG operator pass (same contract as k_blk_apply): d_new_k = s_k + beta_k d_old_k,
-// q_k = A d_new_k, and per right-hand side the sum d_new_k . q_k reduced over the grid, whose
-// last CTA sets alpha_k = delta_k / (d_new_k . q_k).  A CTA owns a 32 x TC column of nodes and
-// marches through its run of layers ZB at a time, with ZB + 2 halo'd planes of d_new staged in
-// shared memory (d_new is formed while staging).  Requires node keys of materials 0 and 1 only.
-//
-// ASYNC: the input planes of the next step are copied (s and d_old as they are) by cp.async
-// into a raw buffer while the current step computes, and d_new is formed from it afterwards
-// shared memory to shared memory, so the global-memory latency of the staging overlaps the
-// arithmetic within the CTA.
-//
-// PF: at the start of a step the CTA asks L2 to prefetch (bulk prefetch, one request per
-// contiguous column segment of every input vector) the planes it will stage after the step, so
-// the staging loads that follow the arithmetic find them in L2.
-//
-// TG: the table is read from global memory through the L1 cache instead of being copied into
-// shared memory (the staging loads then bypass L1 so that they do not evict it), which leaves
-// the shared memory to the planes and allows MINB CTAs per SM.
-template <int ND, typename T, int NR, int TC, int ZB, bool ASYNC = false, bool PF = false, bool TG = false, int MINB = 1>
+// The block PCG operator pass: d_new_k = M^-1 r_k + beta_k d_old_k (the Jacobi diagonal from
+// the node keys; a.s holds r), q_k = A d_new_k, and per right-hand side the sum d_new_k . q_k
+// reduced over the grid, whose last CTA sets alpha_k = delta_k / (d_new_k . q_k).  A CTA owns a
+// 32 x TC column of nodes and marches through its run of layers ZB at a time, with ZB + 2
+// halo'd planes of d_new staged in shared memory (d_new is formed while staging).  At the start
+// of a step the CTA asks L2 to prefetch (bulk prefetch, one request per contiguous column
+// segment of every input vector) the planes it stages after the step, so that those loads find
+// them in L2.  MINB: CTAs per SM the registers are capped for.  Requires node keys of materials
+// 0 and 1 only.
+template <int ND, typename T, int NR, int TC, int ZB, int MINB = 1>
 __global__ void __launch_bounds__(TE_TR * TC, MINB) k_asm_apply(BlkArgs<ND, T> a, const T* __restrict__ tab) {
   using Lo = AsmLayout<ND, T, NR>;
   using V = typename Lo::V;
@@ -130,67 +105,24 @@ __global__ void __launch_bounds__(TE_TR * TC, MINB) k_asm_apply(BlkArgs<ND, T> a
 #pragma unroll
   for (int k = 0; k < NR; k++) all_done = all_done && a.sc[k].done;
   if (all_done) return;
+  constexpr int TW = asm_table_words(ND, Lo::BS);  // a multiple of 4 words: 16-byte alignment kept
   T* sT = reinterpret_cast<T*>(smem_raw);
-  T* sP = TG ? sT : sT + ASM_NBLK * Lo::BS;  // ASM_NBLK * BS words keep 16-byte alignment (416 = 16 * 26)
+  const T* sInv = sT + ASM_NBLK * Lo::BS;  // inverse Jacobi diagonal by node configuration
+  T* sP = sT + TW;
   const int tid = threadIdx.x + TE_TR * threadIdx.y;
-  if constexpr (!TG)
-    for (int i = tid; i < ASM_NBLK * Lo::BS; i += NT) sT[i] = tab[i];
+  for (int i = tid; i < TW; i += NT) sT[i] = tab[i];
   if (tid < NR) { sbeta[tid] = T(a.sc[tid].beta); sdone[tid] = a.sc[tid].done; }
   __syncthreads();
   const int R = a.R, C = a.C, L = a.L;
   const size_t RC = (size_t)R * C;
   const long n = a.n;
+  const bool pre = a.precond != 0;
   T beta[NR];
 #pragma unroll
   for (int k = 0; k < NR; k++) beta[k] = sbeta[k];
   int r0 = 0, c0 = 0;
   size_t poff[PPT];  // in-layer node index of this thread's staged points (for the current tile)
-  constexpr int RS = asm_raw_stride<ND, NR>();
-  T* sRaw = sP + NPL * PP * PS;  // ASYNC: ZB raw planes
   auto slot_of = [&](int l) { return ((l % NPL) + NPL) % NPL; };
-  // PF: L2 prefetch of plane l of the current tile: per input vector and tile column, the rows
-  // of the tile and its halo that are contiguous in memory (a wrapped halo row is left out)
-  auto prefetch_plane = [&](int l) {
-    const size_t lo = (size_t)wrap(l, L) * RC;
-    const int ra = max(r0 - 1, 0), rb = min(r0 + TE_TR, R - 1);
-    for (int i = tid; i < 2 * NR * (TC + 2); i += NT) {
-      const int k = i % NR, arr = (i / NR) % 2, hc = i / (2 * NR);
-      const size_t node = (size_t)ra + (size_t)wrap(c0 + hc - 1, C) * R + lo;
-      const T* base = (arr ? a.dold : a.s) + (size_t)k * n + node * ND;
-      asm_prefetch_l2(base, (size_t)(rb - ra + 1) * ND * sizeof(T));
-    }
-  };
-  // ASYNC: copy plane l into raw slot i
-  auto issue_plane = [&](int l, int i) {
-    const size_t lo = (size_t)wrap(l, L) * RC;
-    T* dst = sRaw + (size_t)i * PP * RS;
-#pragma unroll
-    for (int pi = 0; pi < PPT; pi++) {
-      const int p = tid + pi * NT;
-      if (PP % NT == 0 || p < PP) {
-        const size_t node = poff[pi] + lo;
-#pragma unroll
-        for (int k = 0; k < NR; k++)
-#pragma unroll
-          for (int c = 0; c < ND; c++) {
-            const size_t j = (size_t)k * n + node * ND + c;
-            asm_cp_async(dst + p * RS + k * ND + c, a.s + j);
-            asm_cp_async(dst + p * RS + NR * ND + k * ND + c, a.dold + j);
-          }
-      }
-    }
-  };
-  // ASYNC: d_new of plane l from raw slot i into its ring slot
-  auto form_plane = [&](int l, int i) {
-    const T* src = sRaw + (size_t)i * PP * RS;
-    T* dst = sP + slot_of(l) * PP * PS;
-    for (int p = tid; p < PP; p += NT) {
-#pragma unroll
-      for (int c = 0; c < ND; c++)
-#pragma unroll
-        for (int k = 0; k < NR; k++) dst[p * PS + c * NR + k] = fma(beta[k], src[p * RS + NR * ND + k * ND + c], src[p * RS + k * ND + c]);
-    }
-  };
   auto load_plane = [&](int l) {
     const size_t lo = (size_t)wrap(l, L) * RC;
     T* dst = sP + slot_of(l) * PP * PS;
@@ -199,15 +131,35 @@ __global__ void __launch_bounds__(TE_TR * TC, MINB) k_asm_apply(BlkArgs<ND, T> a
       const int p = tid + i * NT;
       if (PP % NT == 0 || p < PP) {
         const size_t node = poff[i] + lo;
+        T inv[ND];
+        if (pre) {
+          const unsigned m = asm_config(a.keys[node]);
+#pragma unroll
+          for (int c = 0; c < ND; c++) inv[c] = sInv[m * ND + c];
+        } else {
+#pragma unroll
+          for (int c = 0; c < ND; c++) inv[c] = T(1);
+        }
 #pragma unroll
         for (int k = 0; k < NR; k++)
 #pragma unroll
           for (int c = 0; c < ND; c++) {
             const size_t j = (size_t)k * n + node * ND + c;
-            if constexpr (TG) dst[p * PS + c * NR + k] = fma(beta[k], __ldcg(a.dold + j), __ldcg(a.s + j));
-            else dst[p * PS + c * NR + k] = fma(beta[k], a.dold[j], a.s[j]);
+            dst[p * PS + c * NR + k] = fma(beta[k], a.dold[j], a.s[j] * inv[c]);
           }
       }
+    }
+  };
+  // L2 prefetch of plane l of the current tile: per input vector and tile column, the rows of
+  // the tile and its halo that are contiguous in memory (a wrapped halo row is left out)
+  auto prefetch_plane = [&](int l) {
+    const size_t lo = (size_t)wrap(l, L) * RC;
+    const int ra = max(r0 - 1, 0), rb = min(r0 + TE_TR, R - 1);
+    for (int i = tid; i < 2 * NR * (TC + 2); i += NT) {
+      const int k = i % NR, arr = (i / NR) % 2, hc = i / (2 * NR);
+      const size_t node = (size_t)ra + (size_t)wrap(c0 + hc - 1, C) * R + lo;
+      const T* base = (arr ? a.dold : a.s) + (size_t)k * n + node * ND;
+      asm_prefetch_l2(base, (size_t)(rb - ra + 1) * ND * sizeof(T));
     }
   };
   double acc[NR];
@@ -236,20 +188,11 @@ __global__ void __launch_bounds__(TE_TR * TC, MINB) k_asm_apply(BlkArgs<ND, T> a
     __syncthreads();  // the previous run's planes are no longer read
 #pragma unroll
     for (int q = -1; q <= ZB; q++) load_plane(l0 + q);
-    if constexpr (ASYNC) {
-      if (l0 + ZB < l1) {
-#pragma unroll
-        for (int q = 1; q <= ZB; q++) issue_plane(l0 + ZB + q, q - 1);
-        asm_cp_commit();
-      }
-    }
     __syncthreads();
     for (int l = l0; l < l1; l += ZB) {
-      if constexpr (PF) {
-        if (l + ZB < l1) {
+      if (l + ZB < l1) {
 #pragma unroll
-          for (int q = 1; q <= ZB; q++) prefetch_plane(l + ZB + q);
-        }
+        for (int q = 1; q <= ZB; q++) prefetch_plane(l + ZB + q);
       }
       unsigned kn[ZB];
 #pragma unroll
@@ -271,8 +214,7 @@ __global__ void __launch_bounds__(TE_TR * TC, MINB) k_asm_apply(BlkArgs<ND, T> a
               if constexpr (Lo::PAIRS) out[z][ci][ww] = make_float2(0.f, 0.f);
               else out[z][ci][ww] = T(0);
             }
-        if constexpr (TG) asm_positions<ND, T, NR, ZB>(std::make_integer_sequence<int, 9 * (ZB + 2)>{}, pl, ctr, tab, m, out);
-        else asm_positions<ND, T, NR, ZB>(std::make_integer_sequence<int, 9 * (ZB + 2)>{}, pl, ctr, sT, m, out);
+        asm_positions<ND, T, NR, ZB>(std::make_integer_sequence<int, 9 * (ZB + 2)>{}, pl, ctr, sT, m, out);
 #pragma unroll
         for (int z = 0; z < ZB; z++) {
           if (l + z >= l1) break;
@@ -296,23 +238,10 @@ __global__ void __launch_bounds__(TE_TR * TC, MINB) k_asm_apply(BlkArgs<ND, T> a
 #pragma unroll
       for (int z = 0; z < ZB; z++) kc[z] = kn[z];
       if (l + ZB < l1) {
-        if constexpr (ASYNC) {
-          asm_cp_wait_all();
-          __syncthreads();  // the raw planes have landed; planes l - 1 .. l + ZB - 2 are no longer read
+        __syncthreads();  // planes l - 1 .. l + ZB - 2 are no longer read
 #pragma unroll
-          for (int q = 1; q <= ZB; q++) form_plane(l + ZB + q, q - 1);
-          __syncthreads();  // the raw slots are free again
-          if (l + 2 * ZB < l1) {
-#pragma unroll
-            for (int q = 1; q <= ZB; q++) issue_plane(l + 2 * ZB + q, q - 1);
-            asm_cp_commit();
-          }
-        } else {
-          __syncthreads();  // planes l - 1 .. l + ZB - 2 are no longer read
-#pragma unroll
-          for (int q = 1; q <= ZB; q++) load_plane(l + ZB + q);
-          __syncthreads();
-        }
+        for (int q = 1; q <= ZB; q++) load_plane(l + ZB + q);
+        __syncthreads();
       }
     }
     w += l1 - l0;

@@ -24,7 +24,7 @@ constexpr int BLK_MAX = 6;
 
 template <int ND, typename T>
 struct BlkArgs {
-  const T* s;       // [NR][n]: s_k = M^-1 r_k
+  const T* s;       // [NR][n]: r_k (the direction is formed from M^-1 r_k, M^-1 from the keys)
   const T* dold;    // [NR][n]
   T* dnew;          // [NR][n]
   T* q;             // [NR][n]
@@ -35,6 +35,7 @@ struct BlkArgs {
   long n;           // unknowns per right-hand side
   DevScalars* sc;   // [NR]
   RedCtl rc;
+  int precond;      // 0: M = I (plain CG, and the bare operator apply)
 };
 
 // point stride in the staged planes: NR*ND values padded to an odd count (conflict-free
@@ -165,12 +166,18 @@ __global__ void __launch_bounds__(TE_NT) k_blk_apply(BlkArgs<ND, T> a) {
   } else {
     for (int i = tid; i < 4 * ED * ED; i += TE_NT) sK[(i / (ED * ED)) * kstride + i % (ED * ED)] = (i < a.nmat * ED * ED) ? a.Kd[i] : T(0);
   }
+  __shared__ T sD[4 * 8 * ND];
+  for (int i = tid; i < 4 * 8 * ND; i += TE_NT) {
+    const int m = i / (8 * ND), kk = i % (8 * ND);
+    sD[i] = (m < a.nmat) ? a.Kd[(size_t)m * ED * ED + (size_t)kk * ED + kk] : T(1);
+  }
   if (tid < NR) { sbeta[tid] = T(a.sc[tid].beta); sdone[tid] = a.sc[tid].done; }
   __syncthreads();
   const int R = a.R, C = a.C, L = a.L;
   const size_t RC = (size_t)R * C;
   int r0 = 0, c0 = 0;  // column tile of the current run
   const long n = a.n;
+  const bool pre = a.precond != 0;
   auto slot_of = [&](int l) { return ((l % 3) + 3) % 3; };
   auto load_plane = [&](int l) {
     const int lw = wrap(l, L);
@@ -179,12 +186,18 @@ __global__ void __launch_bounds__(TE_NT) k_blk_apply(BlkArgs<ND, T> a) {
       const int hr = p % TE_PR, hc = p / TE_PR;
       const int gr = wrap(r0 + hr - 1, R), gc = wrap(c0 + hc - 1, C);
       const size_t node = (size_t)gr + (size_t)gc * R + (size_t)lw * RC;
+      T inv[ND];
+      if (pre) te_invdiag<ND, T>(sD, a.keys[node], inv);
+      else {
+#pragma unroll
+        for (int c = 0; c < ND; c++) inv[c] = T(1);
+      }
 #pragma unroll
       for (int k = 0; k < NR; k++)
 #pragma unroll
         for (int c = 0; c < ND; c++) {
           const size_t j = (size_t)k * n + node * ND + c;
-          dst[p * PS + k * ND + c] = fma(sbeta[k], a.dold[j], a.s[j]);
+          dst[p * PS + k * ND + c] = fma(sbeta[k], a.dold[j], a.s[j] * inv[c]);
         }
     }
   };
@@ -245,8 +258,9 @@ __global__ void __launch_bounds__(TE_NT) k_blk_apply(BlkArgs<ND, T> a) {
   }
 }
 
-// Pointwise pass for all right-hand sides: x_k += a_k d_k, r_k -= a_k q_k, s_k = M^-1 r_k,
-// delta_k and the max-norms, then each right-hand side's own finisher (pcg_finish).
+// Pointwise pass for all right-hand sides: x_k += a_k d_k, r_k -= a_k q_k, s_k = M^-1 r_k (not
+// stored when a.s is null: the operator pass forms it), delta_k and the max-norms, then each
+// right-hand side's own finisher (pcg_finish).
 template <int ND, typename T>
 struct BlkPw {
   double* x; const T* d; T* r; const T* q; T* s;   // [NR][n]
@@ -303,7 +317,7 @@ __global__ void __launch_bounds__(PW_NT) k_blk_point(BlkPw<ND, T> a) {
         const T rv = fma(-al, a.q[j], a.r[j]);
         a.r[j] = rv;
         const T sv = rv * inv[c];
-        a.s[j] = sv;
+        if (a.s) a.s[j] = sv;
         vals[NV * k] += (double)rv * (double)sv;
         if constexpr (MAXN) {
           vals[NV * k + 1] = fmax(vals[NV * k + 1], fabs((double)rv));
@@ -427,7 +441,7 @@ __global__ void __launch_bounds__(PW_NT) k_blk_point4(BlkPw<ND, T> a) {
       reinterpret_cast<double2*>(a.x + j)[0] = make_double2(xv[0], xv[1]);
       reinterpret_cast<double2*>(a.x + j)[1] = make_double2(xv[2], xv[3]);
       blk_st4(a.r + j, rv);
-      blk_st4(a.s + j, sv);
+      if (a.s) blk_st4(a.s + j, sv);
     }
   }
   bool ismax[NV * NR];

@@ -13,7 +13,8 @@
 // constant cache).  The input field is formed while it is staged, which fuses the vector
 // update that precedes the operator in each Krylov recurrence:
 //   TE_PLAIN  v = in0                                  (plain apply)
-//   TE_PCG    v = in0 + beta*in1 = s + beta d_old       (PCG direction; written once)
+//   TE_PCG    v = M^-1 in0 + beta*in1 = M^-1 r + beta d_old   (PCG direction; written once;
+//             the preconditioned residual s = M^-1 r is formed here and never stored)
 //   TE_MR     r' = in0 - alpha*in1 = r - alpha q, v = M^-1 r'   (PMINRES; r', x updated)
 #pragma once
 #include <utility>
@@ -233,8 +234,19 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a, const T* __
   if (a.skip_if_done && a.sc->done) return;
   T* sK = reinterpret_cast<T*>(smem_raw);
   const int kstride = ED * ED + 1;  // padded material stride spreads materials over banks
-  constexpr int TAB = ASM_NBLK * AsmLayout<ND, T, 1>::BS;
+  constexpr int TAB = asm_table_words(ND, AsmLayout<ND, T, 1>::BS);
   T* sP = sK + (ASM ? TAB : 4 * kstride);
+  // ASM: the inverse Jacobi diagonal by node configuration follows the blocks
+  [[maybe_unused]] const T* sInv = sK + ASM_NBLK * AsmLayout<ND, T, 1>::BS;
+  auto invdiag = [&](unsigned key, T (&inv)[ND]) {
+    if constexpr (ASM) {
+      const unsigned m = asm_config(key);
+#pragma unroll
+      for (int c = 0; c < ND; c++) inv[c] = sInv[m * ND + c];
+    } else {
+      te_invdiag<ND, T>(sD, key, inv);
+    }
+  };
   const int tid = threadIdx.x + TE_TR * threadIdx.y;
   if constexpr (ASM) {
     for (int i = tid; i < TAB; i += TE_NT) sK[i] = tab[i];
@@ -242,7 +254,7 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a, const T* __
     // 4 material slots always (keys carry 2 bits per voxel); slots past nmat are zero.
     for (int i = tid; i < 4 * ED * ED; i += TE_NT) sK[(i / (ED * ED)) * kstride + i % (ED * ED)] = (i < a.nmat * ED * ED) ? a.Kd[i] : T(0);
   }
-  if (MODE == TE_MR || MODE == TE_DIRDOT || MODE == TE_UPD) {
+  if (MODE == TE_MR || MODE == TE_PCG || MODE == TE_DIRDOT || MODE == TE_UPD) {
     for (int i = tid; i < 4 * 8 * ND; i += TE_NT) {
       const int m = i / (8 * ND), k = i % (8 * ND);
       sD[i] = (m < a.nmat) ? a.Kd[(size_t)m * ED * ED + (size_t)k * ED + k] : T(1);
@@ -266,8 +278,8 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a, const T* __
       const int gr = wrap(r0 + hr - 1, R), gc = wrap(c0 + hc - 1, C);
       const size_t node = (size_t)gr + (size_t)gc * R + (size_t)lw * RC;
       T inv[ND];
-      if (MODE == TE_MR || MODE == TE_DIRDOT) {
-        if (pre) te_invdiag<ND, T>(sD, a.keys[node], inv);
+      if (MODE == TE_MR || MODE == TE_PCG || MODE == TE_DIRDOT) {
+        if (pre) invdiag(a.keys[node], inv);
         else {
 #pragma unroll
           for (int c = 0; c < ND; c++) inv[c] = T(1);
@@ -276,7 +288,7 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a, const T* __
 #pragma unroll
       for (int c = 0; c < ND; c++) {
         T v = a.in0[node * ND + c];
-        if (MODE == TE_PCG) v = fma(beta, a.in1[node * ND + c], v);
+        if (MODE == TE_PCG) v = fma(beta, a.in1[node * ND + c], v * inv[c]);
         if (MODE == TE_MR) v = fma(-alpha, a.in1[node * ND + c], v) * inv[c];
         if (MODE == TE_DIRDOT) v = fma(beta, a.in1[node * ND + c], v * inv[c]);
         dst[p * ND + c] = v;
@@ -313,7 +325,7 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a, const T* __
       else te_node<ND, T>(sK, kstride, key, pm, p0, pp, ctr, out);
       [[maybe_unused]] T own_inv[ND];
       if constexpr (MODE == TE_UPD) {
-        if (pre) te_invdiag<ND, T>(sD, key, own_inv);
+        if (pre) invdiag(key, own_inv);
         else {
 #pragma unroll
           for (int cc = 0; cc < ND; cc++) own_inv[cc] = T(1);
@@ -385,7 +397,7 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a, const T* __
 
 template <int ND, typename T>
 inline size_t te_asm_smem_bytes() {
-  return (size_t)ASM_NBLK * AsmLayout<ND, T, 1>::BS * sizeof(T) + (size_t)3 * TE_PP * ND * sizeof(T) + 16;
+  return (size_t)asm_table_words(ND, AsmLayout<ND, T, 1>::BS) * sizeof(T) + (size_t)3 * TE_PP * ND * sizeof(T) + 16;
 }
 
 template <int ND, typename T>

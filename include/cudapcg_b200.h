@@ -234,6 +234,18 @@ cudapcgFlag_t cudapcgB200VolumeTerm(const double *CB, unsigned int ns, double *m
    crosses PCIe instead of two. */
 cudapcgFlag_t cudapcgB200SetImageColors(const uint8_t *colors, unsigned int rows, unsigned int cols, unsigned int slices,
                                         unsigned int refinement, const int *material_of_color);
+/* Stokes (FLUID_3D) DOF-number maps built on the device from the image's colours, in place of
+   building them on the host and cudapcgSetPeriodic2DOFMap / SetPoreMap / SetDOF2PeriodicMap
+   (femhmg_fluid_3D.c:370-491 numbers them on the host): material_of_color as for
+   cudapcgB200SetImageColors, pore = material 0; pore nodes are numbered first, then interface
+   nodes, each in node order.  The model's nporenodes, nbordernodes, nvars and nhmgvars are set
+   from the numbering (also in the caller's model struct), and *npore, *nborder return them. */
+cudapcgFlag_t cudapcgB200SetPoreImageColors(const uint8_t *colors, unsigned int rows, unsigned int cols, unsigned int slices,
+                                            unsigned int refinement, const int *material_of_color, unsigned int *npore,
+                                            unsigned int *nborder);
+/* The current Stokes model's node->DOF (N), DOF->node (nporenodes + nbordernodes) and interface
+   key (nbordernodes) maps copied to host buffers (any may be NULL); for tests. */
+cudapcgFlag_t cudapcgB200GetPoreMaps(uint32_t *dof_of_node, uint32_t *node_of_dof, uint8_t *border_keys);
 /* Initial guess of the next cudapcgSolve from a device vector of nvars doubles (the device
    counterpart of cudapcgSetX0(x0, 0); cleared by cudapcgSetX0(NULL, 0)). */
 cudapcgFlag_t cudapcgB200SetX0Device(const double *x0);
