@@ -52,6 +52,12 @@ WORKLOADS = {
     "elastic128_grf_mixed_block": dict(analysis=1, shape=(128, 128, 128), gen="grf", corr=6.0, fraction=0.40, seed=2000,
                                        props={0: (1.0, 0.30), 255: (10.0, 0.20)}, tol=1e-6, maxit=20000,
                                        precision="mixed", multirhs=True),
+    # the thermal operator above L2 (256^3: 16.8 M nodes, 570 MB per FP64 operator pass);
+    # overlapping balls (non-overlapping placement jams below 0.30 at this size)
+    "thermal256_spheres_fp64": dict(analysis=0, shape=(256, 256, 256), gen="spheres", vf=0.30, seed=1100, overlap=True,
+                                    props={0: 1.0, 255: 10.0}, tol=1e-6, maxit=20000, precision="fp64"),
+    "thermal256_spheres_mixed": dict(analysis=0, shape=(256, 256, 256), gen="spheres", vf=0.30, seed=1100, overlap=True,
+                                     props={0: 1.0, 255: 10.0}, tol=1e-6, maxit=20000, precision="mixed"),
     "thermal64_spheres_fp64_block": dict(analysis=0, shape=(64, 64, 64), gen="spheres", vf=0.30, seed=1000,
                                          props={0: 1.0, 255: 10.0}, tol=1e-6, maxit=20000, precision="fp64",
                                          multirhs=True),
@@ -78,7 +84,7 @@ def make_image(w, rank):
     if w["gen"] == "grf":
         return synthetic.grf(w["shape"], corr=w["corr"], fraction=w["fraction"], seed=seed)
     if w["gen"] == "spheres":
-        return synthetic.spheres(w["shape"], vf=w["vf"], seed=seed)
+        return synthetic.spheres(w["shape"], vf=w["vf"], seed=seed, overlap=w.get("overlap", False))
     return synthetic.pore_grf(w["shape"], corr=w["corr"], porosity=w["porosity"], seed=seed)
 
 
@@ -260,6 +266,18 @@ class Resident:
     def close(self):
         self.c.cudapcgEnd()
         self.h.hmgEnd()
+
+
+def kernel_only(w, workload, which):
+    """One kernel of the workload's model launched 10 times after warm-up, its mean CUDA-event time
+    printed: the command the ncu captures under profiles/ run."""
+    img = make_image(w, 0)
+    wd = tempfile.mkdtemp()
+    nf, raw = write_case(wd, w, img)
+    m = Resident(nf, raw, w)
+    t = m.kernel_time(which, reps=10)
+    print(json.dumps({"workload": workload, "kernel": which, "ms": t * 1e3, "nodes": m.N, "ndof": m.ndof}))
+    m.close()
 
 
 def e2e_step(img, nf, w):
@@ -549,8 +567,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-check", action="store_true", help="skip the untimed reference run (tensor error, same-precision ratio)")
     ap.add_argument("--no-north-star", action="store_true", help="skip the 256^3 north-star sub-record of the default workload")
+    ap.add_argument("--kernel", type=int, default=0,
+                    help="only time one kernel of the workload's resident model, 10 launches (for ncu captures): "
+                         "1 operator pass (PCG), 2 pointwise pass (PCG), 3 operator pass ((P)MINRES), "
+                         "5 block operator pass, 6 block pointwise pass")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
+    if args.kernel:
+        kernel_only(w, args.workload, args.kernel)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -729,8 +754,12 @@ def dominant_kernel_roofline(model, w, block, workload):
     es = 4 if w["precision"] == "mixed" else 8
     if w["analysis"] == 2:
         kern_which, kname = 3, "k_fl_apply<MR> (Stokes operator + PMINRES step, one right-hand side)"
-        per_unit = 4 * es * 4 + 4 * 2  # per DOF row set, approximate
-        units = model.ndof
+        # per DOF: r, q, d in, q', r' out (5 es) and the FP64 x read and written (16 B); per row
+        # set (pore node: 4 DOFs, interface node: 1) its DOF->node and node->DOF entries (8 B) and
+        # an interface node's fluid key (1 B); units = row sets, bytes_per_unit their mean
+        nV, nB = model.info[5], model.info[6]
+        units = nV + nB
+        per_unit = (nV * (4 * (5 * es + 16) + 8) + nB * ((5 * es + 16) + 9)) / max(1, units)
     else:
         nd = 3 if w["analysis"] == 1 else 1
         tn = 'float' if es == 4 else 'double'

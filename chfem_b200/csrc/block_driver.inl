@@ -481,6 +481,7 @@ static bool moments_on_device(const LoadCases& lc, int nr) {
 template <typename T>
 static bool solve_block_T(int nr, const double* const* rhs, const double* const* x0, int x0_mode, double* const* x_out,
                           unsigned* iters, double* resid, const LoadCases* lc = nullptr) {
+  if (S->d_sdf) { set_err("cudapcgB200SolveBlock", "a scalar density field is solved one load case at a time"); return false; }
   if (!ensure_vectors<T>() || !ensure_K<T>() || !block_alloc<T>(nr)) return false;
   if (asm_applies() && !ensure_tab<T>()) return false;
   const long n = S->nvars;

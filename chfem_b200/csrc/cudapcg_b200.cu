@@ -108,6 +108,11 @@ struct Solver {
   // assembled neighbour blocks of a two-material model (stencil_asm.cuh), per precision
   double* d_tab64 = nullptr;
   float* d_tab32 = nullptr;
+  // scalar density field (cudapcgSetParametricDensityField): 16-bit code per voxel and its
+  // range; the inverse Jacobi diagonal it implies, per unknown (FP64, built at solve set-up)
+  uint16_t* d_sdf = nullptr;
+  double sdf_min = 0.0, sdf_max = 0.0;
+  double* d_invd = nullptr;
   // Krylov work vectors, typed for the precision in use
   int vec_prec = -1;
   int vec_layout = -1;  // which work vectors ensure_vectors allocated (precision, solver kind)
@@ -195,8 +200,10 @@ static void free_model_dev() {
   if (!S) return;
   free_ptr(S->d_keys); free_ptr(S->d_dof_of_node); free_ptr(S->d_node_of_dof); free_ptr(S->d_bkeys);
   free_ptr(S->d_K64); free_ptr(S->d_K32); free_ptr(S->d_tab64); free_ptr(S->d_tab32);
+  free_ptr(S->d_sdf); free_ptr(S->d_invd);
   S->d_keys = nullptr; S->d_dof_of_node = S->d_node_of_dof = nullptr; S->d_bkeys = nullptr;
   S->d_K64 = nullptr; S->d_K32 = nullptr; S->d_tab64 = nullptr; S->d_tab32 = nullptr;
+  S->d_sdf = nullptr; S->d_invd = nullptr;
   S->have_K = S->have_keys = S->have_maps = false;
 }
 
@@ -267,7 +274,7 @@ static bool ensure_vectors() {
 // Assembled neighbour blocks (stencil_asm.cuh) of a thermal/elastic model of at most two
 // materials; CHFEM_B200_BLOCK_OP=element keeps the element-by-element block operator.
 static bool asm_applies() {
-  if (S->analysis == CUDAPCG_FLUID_3D || S->nmat > 2) return false;
+  if (S->analysis == CUDAPCG_FLUID_3D || S->nmat > 2 || S->d_sdf) return false;
   const char* e = getenv("CHFEM_B200_BLOCK_OP");
   return !(e && !strcmp(e, "element"));
 }
@@ -289,13 +296,62 @@ static bool ensure_tab() {
   return true;
 }
 
+// Inverse Jacobi diagonal under a scalar density field: sum over the node's 8 voxels of the
+// scaled diagonal of its element matrix (matrix_free.cu:2270-2306 and the elastic counterpart
+// compute it per application; here once per model).
+template <int ND>
+__global__ void k_sdf_invdiag(const uint16_t* keys, const uint16_t* sdf, double fmin, double frng, const double* Kd, int R, int C,
+                              int L, double* invd) {
+  constexpr int ED = 8 * ND;
+  const long N = (long)R * C * L;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const int r = (int)(i % R), c = (int)((i / R) % C), l = (int)(i / ((long)R * C));
+    const unsigned key = keys[i];
+    double d[ND];
+#pragma unroll
+    for (int cc = 0; cc < ND; cc++) d[cc] = 0.0;
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      const double f = fmin + frng * (double)sdf[te_voxel(r, c, l, e, R, C, L)] * (1.0 / 65535.0);
+      const double* K = Kd + (size_t)((key >> (2 * e)) & 3u) * ED * ED;
+#pragma unroll
+      for (int cc = 0; cc < ND; cc++) d[cc] += f * K[(e * ND + cc) * ED + e * ND + cc];
+    }
+#pragma unroll
+    for (int cc = 0; cc < ND; cc++) invd[i * ND + cc] = 1.0 / d[cc];
+  }
+}
+static bool ensure_K64_only();
+static bool ensure_invd() {
+  if (S->d_invd || !S->d_sdf) return true;
+  if (!ensure_K64_only()) return false;
+  CKV(cudaMalloc(&S->d_invd, sizeof(double) * S->N * S->nd));
+  const long g = std::max(1L, std::min<long>((S->N + 255) / 256, 8L * num_sms()));
+  if (S->nd == 1) k_sdf_invdiag<1><<<(int)g, 256, 0, S->stream>>>(S->d_keys, S->d_sdf, S->sdf_min, S->sdf_max - S->sdf_min, S->d_K64, S->R, S->C, S->L, S->d_invd);
+  else k_sdf_invdiag<3><<<(int)g, 256, 0, S->stream>>>(S->d_keys, S->d_sdf, S->sdf_min, S->sdf_max - S->sdf_min, S->d_K64, S->R, S->C, S->L, S->d_invd);
+  CKV(cudaGetLastError());
+  return true;
+}
+// the scalar-density-field arguments of a thermal / elastic operator pass
+template <int ND, typename T>
+static void sdf_args(TeArgs<ND, T>& a) {
+  a.sdf = S->d_sdf;
+  a.sdf_min = S->sdf_min;
+  a.sdf_rng = S->sdf_max - S->sdf_min;
+  a.invd = S->d_invd;
+}
+
 template <typename T> static T* Kdev();
 template <> double* Kdev<double>() { return S->d_K64; }
 template <> float* Kdev<float>() { return S->d_K32; }
 
 template <typename T>
 static bool ensure_K() {
-  if (Kdev<T>()) return true;
+  if (Kdev<T>()) {  // the derived tables may have been dropped since (new density field, new model)
+    if (asm_applies() && !ensure_tab<T>()) return false;
+    if (S->d_sdf && !ensure_invd()) return false;
+    return true;
+  }
   if (!S->have_K) { set_err("solve", "local matrices were not set (cudapcgSetLclMtxs)"); return false; }
   std::vector<T> kt(S->Kd.size());
   for (size_t i = 0; i < kt.size(); i++) kt[i] = (T)S->Kd[i];
@@ -304,10 +360,19 @@ static bool ensure_K() {
   CKV(cudaMemcpy(dk, kt.data(), kt.size() * sizeof(T), cudaMemcpyHostToDevice));
   if (sizeof(T) == 8) S->d_K64 = (double*)dk; else S->d_K32 = (float*)dk;
   if (asm_applies() && !ensure_tab<T>()) return false;
+  if (S->d_sdf && !ensure_invd()) return false;
   if (S->analysis == CUDAPCG_FLUID_3D) {
     if (sizeof(T) == 8) CKV(cudaMemcpyToSymbol(c_flK64, kt.data(), 1024 * sizeof(double)));
     else CKV(cudaMemcpyToSymbol(c_flK32, kt.data(), 1024 * sizeof(float)));
   }
+  return true;
+}
+
+static bool ensure_K64_only() {
+  if (S->d_K64) return true;
+  if (!S->have_K) { set_err("solve", "local matrices were not set (cudapcgSetLclMtxs)"); return false; }
+  CKV(cudaMalloc(&S->d_K64, S->Kd.size() * sizeof(double)));
+  CKV(cudaMemcpy(S->d_K64, S->Kd.data(), S->Kd.size() * sizeof(double), cudaMemcpyHostToDevice));
   return true;
 }
 
@@ -395,6 +460,7 @@ static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, i
       const int nb = fuse ? te_ctas(k_te_apply<1, T, TE_PCG>, sm) : te_ctas(k_te_apply<1, T, TE_PLAIN>, sm);
       if (!ensure_reduction(nb)) return false;
       TeArgs<1, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->cur_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
+      sdf_args(a);
       if (fuse) k_te_apply<1, T, TE_PCG><<<nb, block, sm, S->stream>>>(a);
       else k_te_apply<1, T, TE_PLAIN><<<nb, block, sm, S->stream>>>(a);
     } else {
@@ -402,6 +468,7 @@ static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, i
       const int nb = fuse ? te_ctas(k_te_apply<3, T, TE_PCG>, sm) : te_ctas(k_te_apply<3, T, TE_PLAIN>, sm);
       if (!ensure_reduction(nb)) return false;
       TeArgs<3, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->cur_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
+      sdf_args(a);
       if (fuse) k_te_apply<3, T, TE_PCG><<<nb, block, sm, S->stream>>>(a);
       else k_te_apply<3, T, TE_PLAIN><<<nb, block, sm, S->stream>>>(a);
     }
@@ -423,10 +490,10 @@ static bool launch_point(double* x, T* d, T* r, const T* q, T* s, const T* dold)
     const int g = pw_grid(S->N);
     if (!ensure_reduction(g)) return false;
     if (S->nd == 1) {
-      TePw<1, T> a{x, d, r, q, s, dold, S->d_keys, Kdev<T>(), S->nmat, S->N, S->cur_sc, redctl(g), cfg};
+      TePw<1, T> a{x, d, r, q, s, dold, S->d_keys, Kdev<T>(), S->nmat, S->N, S->cur_sc, redctl(g), cfg, S->d_invd};
       k_te_point<1, T, MODE><<<g, PW_NT, 0, S->stream>>>(a);
     } else {
-      TePw<3, T> a{x, d, r, q, s, dold, S->d_keys, Kdev<T>(), S->nmat, S->N, S->cur_sc, redctl(g), cfg};
+      TePw<3, T> a{x, d, r, q, s, dold, S->d_keys, Kdev<T>(), S->nmat, S->N, S->cur_sc, redctl(g), cfg, S->d_invd};
       k_te_point<3, T, MODE><<<g, PW_NT, 0, S->stream>>>(a);
     }
   }
@@ -476,12 +543,14 @@ static bool launch_te_mode(const T* in0, const T* in1, T* vout, double* x, int f
       const int nb = te_ctas(k_te_apply<1, T, MODE>, sm);
       if (!ensure_reduction(nb)) return false;
       TeArgs<1, T> a{in0, in1, vout, nullptr, x, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->cur_sc, redctl(nb), finish, 1, cfg};
+      sdf_args(a);
       k_te_apply<1, T, MODE><<<nb, block, sm, S->stream>>>(a);
     } else {
       const size_t sm = te_smem_bytes<3, T>(S->nmat);
       const int nb = te_ctas(k_te_apply<3, T, MODE>, sm);
       if (!ensure_reduction(nb)) return false;
       TeArgs<3, T> a{in0, in1, vout, nullptr, x, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->cur_sc, redctl(nb), finish, 1, cfg};
+      sdf_args(a);
       k_te_apply<3, T, MODE><<<nb, block, sm, S->stream>>>(a);
     }
     e = cudaGetLastError();
@@ -691,6 +760,7 @@ template <typename T>
 static bool solve_T(double* res_x) {
   if (!ensure_vectors<T>() || !ensure_K<T>()) return false;
   const bool minres = (S->solver_flag == CUDAPCG_MINRES_SOLVER || S->solver_flag == CUDAPCG_MINRES3_SOLVER);
+  if (minres && S->d_sdf) { set_err("cudapcgSolve", "a scalar density field is solved by CG / PCG (-s 0, 2)"); return false; }
   bool ok = minres ? solve_minres_device<T>() : solve_pcg_device<T>();
   if (!ok) return false;
   collect_results(minres);
@@ -761,7 +831,6 @@ cudapcgModel_t* cudapcgNewModel(void) {
 
 static cudapcgFlag_t adopt_model() {
   cudapcgModel_t* m = S->model;
-  if (m->parametric_density_field_flag) { set_err("model", "scalar density fields are not provided by chfem_b200"); return CUDAPCG_FALSE; }
   if (S->analysis == CUDAPCG_FLUID_3D && m->poremap_flag != CUDAPCG_POREMAP_NUM) {
     set_err("model", "only the DOF-number pore map (-pm 1) is provided by chfem_b200");
     return CUDAPCG_FALSE;
@@ -1135,9 +1204,26 @@ cudapcgFlag_t cudapcgB200GetPoreMaps(uint32_t* dof_of_node, uint32_t* node_of_do
   if (border_keys && S->nB) CK(cudaMemcpy(border_keys, S->d_bkeys, S->nB, cudaMemcpyDeviceToHost));
   return CUDAPCG_TRUE;
 }
-cudapcgFlag_t cudapcgSetParametricDensityField(parametricScalarField_t*, double, double) {
-  set_err("cudapcgSetParametricDensityField", "scalar density fields are not provided by chfem_b200");
-  return CUDAPCG_FALSE;
+// cudapcg.cu:327-334: the density codes of every voxel (row-fastest model order) and their
+// range; voxel v's element matrix is then scaled by fmin + (fmax - fmin) field[v] / 65535.  A
+// thermal model has one material (femhmg.c:256-262 normalises it): without an image, its keys
+// are zero.  PCG / CG and the 3-vector PCG solve such models, one load case at a time.
+cudapcgFlag_t cudapcgSetParametricDensityField(parametricScalarField_t* field, double fmin, double fmax) {
+  const char* who = "cudapcgSetParametricDensityField";
+  if (!S || !S->model || !field) { set_err(who, "bad arguments"); return CUDAPCG_FALSE; }
+  if (S->analysis == CUDAPCG_FLUID_3D) { set_err(who, "not used for FLUID analysis"); return CUDAPCG_FALSE; }
+  if (!S->d_sdf) CK(cudaMalloc(&S->d_sdf, sizeof(uint16_t) * S->N));
+  CK(cudaMemcpy(S->d_sdf, field, sizeof(uint16_t) * S->N, cudaMemcpyHostToDevice));
+  S->sdf_min = fmin;
+  S->sdf_max = fmax;
+  if (!S->have_keys) {
+    CK(cudaMemset(S->d_keys, 0, sizeof(uint16_t) * S->N));
+    S->have_keys = true;
+  }
+  free_ptr(S->d_invd); S->d_invd = nullptr;
+  free_ptr(S->d_tab64); free_ptr(S->d_tab32); S->d_tab64 = nullptr; S->d_tab32 = nullptr;
+  invalidate_graphs();
+  return CUDAPCG_TRUE;
 }
 cudapcgFlag_t cudapcgSetPoreMap(cudapcgFlag_t* pores) {
   if (!S || !S->model || !pores) return CUDAPCG_FALSE;
@@ -1191,6 +1277,7 @@ cudapcgFlag_t cudapcgSetLclMtxs(cudapcgVar_t* Lm) {
   S->have_K = true;
   free_ptr(S->d_K64); free_ptr(S->d_K32); S->d_K64 = nullptr; S->d_K32 = nullptr;
   free_ptr(S->d_tab64); free_ptr(S->d_tab32); S->d_tab64 = nullptr; S->d_tab32 = nullptr;
+  free_ptr(S->d_invd); S->d_invd = nullptr;
   invalidate_graphs();  // captured launches hold the old matrix pointers
   if (S->analysis == CUDAPCG_FLUID_3D && !set_fluid_diag()) return CUDAPCG_FALSE;
   return CUDAPCG_TRUE;

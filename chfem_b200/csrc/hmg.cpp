@@ -145,9 +145,10 @@ bool read_nf(Model& m, const char* fn) {
         for (unsigned i = 0; i < m.nmat; i++) if (fscanf(f, "%lf", &m.alpha[i]) != 1) break;
         m.has_thermal_expansion = true;
       }
-    } else if (!strcmp(tok, "%data_type")) {
+    } else if (!strcmp(tok, "%data_type")) {  // femhmg.c:1550-1561
       char buf[64]; if (fscanf(f, "%63s", buf) != 1) break;
       count++;
+      m.data_type = (!strcmp(buf, "float64") || !strcmp(buf, "double")) ? 1 : 0;
     } else if (!strcmp(tok, "%xreduce_scale_factor")) {
       double v; if (fscanf(f, "%lf", &v) != 1) break;
       m.xreduce_stab = v;
@@ -209,6 +210,61 @@ void build_elem_mat(Model& m) {
       }
 }
 
+// Scalar density field (femhmg.c:1760-1835): the file holds float32 or float64 values (as
+// %data_type says), x fastest; each value times its voxel's conductivity (thermal) or Young's
+// modulus (elastic) is quantised to 16 bits between the smallest and largest product, and the
+// properties are then normalised (thermal: one material of conductivity 1; elastic: E = 1,
+// Poisson's ratios kept), so that voxel e's element matrix is scale_e times the normalised one.
+// As the reference: the file must hold as many values as the refined model has voxels (only the
+// image's count is used), the range pairs value i with the material of the model's voxel i, and
+// a voxel's product reads the material at model index (row + col R + layer R C) x refinement.
+bool read_density_field(Model& m, const char* fn) {
+  const unsigned ref = m.refinement, rows = m.frows, cols = m.fcols, slices = m.fslices;
+  const size_t R = m.ny, C = m.nx, N = (size_t)m.N, nfile = (size_t)rows * cols * slices;
+  const size_t sz = m.data_type ? 8 : 4;
+  std::vector<unsigned char> raw(sz * N);
+  FILE* f = fopen(fn, "rb");
+  if (!f) { fail(std::string("failed to open ") + fn); return false; }
+  const size_t got = fread(raw.data(), sz, N, f);
+  fclose(f);
+  if (got < N) { fail(std::string("failed to read the scalar density field from ") + fn); return false; }
+  auto value = [&](size_t i) -> double {
+    if (m.data_type) { double v; memcpy(&v, raw.data() + 8 * i, 8); return v; }
+    float v; memcpy(&v, raw.data() + 4 * i, 4); return (double)v;
+  };
+  const int stride = m.analysis == ELASTIC ? 2 : 1;
+  build_elem_mat(m);
+  double vmax = value(0) * m.props[m.elem_mat[0] * stride], vmin = vmax;
+  for (size_t i = 1; i < nfile; i++) {
+    const double v = value(i) * m.props[m.elem_mat[i] * stride];
+    vmax = v > vmax ? v : vmax;
+    vmin = v < vmin ? v : vmin;
+  }
+  if (vmax == vmin) vmin = vmax - 1.0;
+  const double dv = vmax - vmin;
+  m.sdf_range[0] = vmin;
+  m.sdf_range[1] = vmax;
+  m.sdf.assign(N, 0);
+  for (size_t k = 0; k < slices; k++)
+    for (size_t i = 0; i < rows; i++)
+      for (size_t j = 0; j < cols; j++) {
+        const double v = value(j + i * cols + k * rows * cols) * m.props[m.elem_mat[(i + j * R + k * R * C) * ref] * stride];
+        const uint16_t q = (uint16_t)(65535 * (v - vmin) / dv);
+        for (size_t kk = ref * k; kk < ref * (k + 1); kk++)
+          for (size_t ii = ref * i; ii < ref * (i + 1); ii++)
+            for (size_t jj = ref * j; jj < ref * (j + 1); jj++) m.sdf[ii + jj * R + kk * R * C] = q;
+      }
+  if (m.analysis == THERMAL) {  // one material of conductivity 1 (femhmg.c:256-262)
+    for (int c = 0; c < 256; c++) if (m.props_keys[c] >= 0) m.props_keys[c] = 0;
+    m.nmat = 1;
+    m.props[0] = 1.0;
+    build_elem_mat(m);
+  } else {
+    for (unsigned j = 0; j < m.nmat; j++) m.props[2 * j] = 1.0;
+  }
+  return true;
+}
+
 // The host maps of a thermal / elastic model, for the paths that read them (one-by-one
 // right-hand sides and tensor updates, coarse levels, EBE input, the model-array hooks).
 bool ensure_host_maps(Model& m) {
@@ -229,7 +285,7 @@ cudapcgFlag_t model_ctor(cudapcgModel_t** ptr, const void* data) {
   strcpy(p->name, m.nf_noext.c_str());
   p->parStrategy_flag = (cudapcgFlag_t)g_par;
   p->poremap_flag = (cudapcgFlag_t)g_poremap;
-  p->parametric_density_field_flag = 0;
+  p->parametric_density_field_flag = m.sdf.empty() ? 0 : 1;  // femhmg.c:67
   p->nrows = m.ny; p->ncols = m.nx; p->nlayers = m.nz;
   p->nelem = (unsigned)m.N;
   p->nvars = (unsigned)m.ndof;
@@ -318,6 +374,7 @@ bool setup_solver(Model& m, bool coarse = false) {
          cudapcgSetDOF2PeriodicMap(m.node_of_dof.data());
   }
   ok = ok && cudapcgSetLclMtxs(m.lcl.data()) && cudapcgAllocateArrays();
+  if (ok && !m.sdf.empty()) ok = cudapcgSetParametricDensityField(m.sdf.data(), m.sdf_range[0], m.sdf_range[1]);  // femhmg.c:971-976
   if (!ok) { fail(std::string("model upload: ") + cudapcgB200LastError()); return false; }
   return true;
 }
@@ -332,7 +389,6 @@ logical hmgInit(char* data_filename, char* elem_filename, char* sdf_filename, ui
   hmgEnd();
   g_err.clear();
   if (!data_filename) { fail("no .nf file"); return 0; }
-  if (sdf_filename) { fail("scalar density field input is not provided by chfem_b200"); return 0; }
   SAY("Initializing femhmg...\n");
   Model* m = new Model();
   m->nf = data_filename;
@@ -357,7 +413,9 @@ logical hmgInit(char* data_filename, char* elem_filename, char* sdf_filename, ui
     // the node keys are built on the device from the colours (cudapcgB200SetImageColors)
     if (m->nmat > 4) { fail("more than 4 materials cannot be encoded in 16-bit node keys"); delete m; return 0; }
     m->ndof = m->N * m->nd;
+    if (sdf_filename && !read_density_field(*m, sdf_filename)) { delete m; return 0; }
   }
+  if (sdf_filename && m->analysis == FLUID) SAY("WARNING: Scalar density field input is not supported for permeability analysis.\n");
   build_local_matrices(*m);
   g_m = m;
   g_dir_set = 0;
@@ -403,6 +461,10 @@ void hmgFindInitialGuesses(unsigned int nlevels) {
   g_have_coarse = false;
   if (!nlevels || !g_m) return;
   Model& fine = *g_m;
+  if (!fine.sdf.empty()) {  // a coarse level would need a coarsened density field
+    fail("recursive initial guesses (-r) are not provided with a scalar density field");
+    return;
+  }
   if (fine.analysis == FLUID) {  // femhmg.c:565-570
     SAY("WARNING: Initial guess estimation is not yet available for permeability analysis.\n");
     SAY("         Null initial guess will be considered (x0 = [0]).\n");
@@ -470,6 +532,10 @@ void hmgSetHomogenizationFlag(hmgFlag_t flag) {
 void hmgSolveHomogenization(void) {
   if (!g_m) return;
   Model& m = *g_m;
+  if (!m.sdf.empty() && (g_export_fields || m.has_thermal_expansion)) {
+    fail("field export and thermal expansion are not provided with a scalar density field");
+    return;
+  }
   const auto t_all = std::chrono::steady_clock::now();
   memset(&g_stats, 0, sizeof(g_stats));
   int dirs[6], nd = 0;
@@ -496,7 +562,9 @@ void hmgSolveHomogenization(void) {
   g_stats.ndof = (unsigned)m.ndof;
   // Block multi-RHS path: all load cases of the analysis advance together (one operator pass
   // per iteration for all of them).  Same per-case recurrence, stopping test and results.
-  const bool block = g_multirhs && !two_vector && ((m.analysis != FLUID && !(g_solver & 1) &&
+  // (a scalar density field runs the one-by-one host path: right-hand sides and tensor terms
+  // scaled per voxel on the host)
+  const bool block = g_multirhs && !two_vector && m.sdf.empty() && ((m.analysis != FLUID && !(g_solver & 1) &&
                                      ((m.analysis == THERMAL && nd == 3) || (m.analysis == ELASTIC && (nd == 6 || nd == 3)))) ||
                                     (m.analysis == FLUID && (g_solver & 1) && nd == 3));
   if (block) {
@@ -565,7 +633,7 @@ void hmgSolveHomogenization(void) {
   }
   // One-by-one path: right-hand side, solution and tensor volume term stay on the device unless
   // x must come back to the host (-xo, -e: the solution files are written from it).
-  const bool on_device = !g_export_x && !g_export_fields;
+  const bool on_device = !g_export_x && !g_export_fields && m.sdf.empty();
   if (!block) {  // host vectors (and, for the host path, maps) of the one-by-one path
     if (!on_device && !ensure_host_maps(m)) { cudapcgEnd(); return; }
     m.rhs.assign(on_device ? 0 : m.ndof, 0.0);
@@ -861,6 +929,8 @@ unsigned long long chfemB200ModelArraySize(int which) {
     case 5: return m.rhs.size() * 8;
     case 6: return m.elem_mat.size() * 2;
     case 7: return m.CB.size() * 8;
+    case 8: return m.sdf.size() * 2;
+    case 9: return m.sdf.empty() ? 0 : 16;
   }
   return 0;
 }
@@ -877,6 +947,8 @@ int chfemB200CopyModelArray(int which, void* dst, unsigned long long bytes) {
     case 5: src = m.rhs.data(); break;
     case 6: src = m.elem_mat.data(); break;
     case 7: src = m.CB.data(); break;
+    case 8: src = m.sdf.data(); break;
+    case 9: src = m.sdf_range; break;  // min, max
     default: return 0;
   }
   const unsigned long long have = chfemB200ModelArraySize(which);

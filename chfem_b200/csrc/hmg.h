@@ -54,10 +54,20 @@ struct Model {
   std::vector<double> lcl;           // thermal 40/mat, elastic 576/mat, Stokes 1024
   std::vector<double> CB;            // thermal 8x3 (avg gradient)*k per mat, elastic 6x24 per mat, Stokes 3x24
   std::vector<double> Kdense;        // dense element matrices (8nd x 8nd per material; Stokes 32x32)
+  // scalar density field (-f): per model voxel a 16-bit code q; the voxel's element matrix is
+  // scaled by sdf_min + (sdf_max - sdf_min) q / 65535 (femhmg.c:1760-1835); empty without one
+  int data_type = 0;                 // %data_type of the field file: 0 float32, 1 float64
+  std::vector<uint16_t> sdf;
+  double sdf_range[2] = {0.0, 0.0};  // [min, max] of the quantised products
   // results
   double C[36] = {0};
   std::vector<double> rhs;
 };
+
+// scale of voxel e's element matrix (1 without a density field)
+inline double sdf_scale(const Model& m, long e) {
+  return m.sdf.empty() ? 1.0 : (double)m.sdf[e] * (1.0 / 65535.0) * (m.sdf_range[1] - m.sdf_range[0]) + m.sdf_range[0];
+}
 
 // physics (hmg_physics.cpp)
 bool build_maps(Model& m, std::string& err);

@@ -288,12 +288,13 @@ void assemble_rhs(const Model& m, int dir, double* rhs) {
   for_boundary_voxels(m, axis, [&](long r, long c, long l) {
     const long e = r + c * R + l * R * C;
     const double* K = m.Kdense.data() + (size_t)m.elem_mat[e] * ed * ed;
+    const double f_e = sdf_scale(m, e);
     for (int a = 0; a < 8; a++) {
       const long n = elem_node(r, c, l, a, R, C, L);
       for (int ci = 0; ci < nd; ci++) {
         double s = 0.0;
         for (int f = 0; f < 4; f++) s += K[(a * nd + ci) * ed + FACE[axis][f] * nd + comp];
-        rhs[n * nd + ci] -= s * jump;
+        rhs[n * nd + ci] -= f_e * s * jump;
       }
     }
   });
@@ -332,10 +333,11 @@ void update_C(Model& m, int dir, const double* x) {
     for (long e = 0; e < N; e++) {
       const long r = e % R, c = (e / R) % C, l = e / (R * C);
       const double* CB = m.CB.data() + (size_t)m.elem_mat[e] * ns * ec;
+      const double f_e = sdf_scale(m, e);
       for (int a = 0; a < 8; a++) {
         const long n = elem_node(r, c, l, a, R, C, L);
         for (int ci = 0; ci < nd; ci++) {
-          const double v = x[n * nd + ci];
+          const double v = f_e * x[n * nd + ci];
           for (int s = 0; s < ns; s++) loc[s] += CB[s * ec + a * nd + ci] * v;
         }
       }
@@ -344,9 +346,11 @@ void update_C(Model& m, int dir, const double* x) {
     for (int s = 0; s < ns; s++) acc[s] += loc[s];
   }
   for_boundary_voxels(m, axis, [&](long r, long c, long l) {
-    const double* CB = m.CB.data() + (size_t)m.elem_mat[r + c * R + l * R * C] * ns * ec;
+    const long e = r + c * R + l * R * C;
+    const double* CB = m.CB.data() + (size_t)m.elem_mat[e] * ns * ec;
+    const double f_e = sdf_scale(m, e);
     for (int f = 0; f < 4; f++)
-      for (int s = 0; s < ns; s++) acc[s] += CB[s * ec + FACE[axis][f] * nd + comp] * jump;
+      for (int s = 0; s < ns; s++) acc[s] += f_e * CB[s * ec + FACE[axis][f] * nd + comp] * jump;
   });
   for (int s = 0; s < ns; s++) m.C[s * ns + dir] = acc[s] / (double)N;
 }

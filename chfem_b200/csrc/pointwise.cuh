@@ -111,6 +111,7 @@ struct TePw {
   DevScalars* sc;
   RedCtl rc;
   SolveCfg cfg;
+  const double* invd = nullptr;  // precomputed inverse Jacobi diagonal (scalar density field)
 };
 
 template <int ND, typename T, int MODE>
@@ -136,7 +137,10 @@ __global__ void __launch_bounds__(PW_NT) k_te_point(TePw<ND, T> a) {
       continue;
     }
     T inv[ND];
-    if (a.cfg.precond) {
+    if (a.cfg.precond && a.invd) {
+#pragma unroll
+      for (int c = 0; c < ND; c++) inv[c] = T(a.invd[i * ND + c]);
+    } else if (a.cfg.precond) {
       const unsigned key = a.keys[i];
       T dg[ND];
 #pragma unroll

@@ -107,17 +107,32 @@ struct TeArgs {
   int finish;          // TeFinish
   int skip_if_done;
   MrCfg cfg;
+  // scalar density field: voxel v's element matrix scaled by sdf_min + sdf_rng sdf[v] / 65535
+  // (cudapcg.cu:327-334); and then the node's inverse Jacobi diagonal, precomputed (FP64)
+  const uint16_t* sdf = nullptr;
+  double sdf_min = 0.0, sdf_rng = 0.0;
+  const double* invd = nullptr;
 };
+
+// Index of the voxel in which node (r, c, l) is local node e: (r - drow(e) - 1, c - dcol(e),
+// l - dlay(e)), periodic (the 8 voxels around a node in the order of
+// matrix_free.cu:2283-2295).
+__device__ __forceinline__ size_t te_voxel(int r, int c, int l, int e, int R, int C, int L) {
+  return (size_t)wrap(r - drow(e) - 1, R) + (size_t)wrap(c - dcol(e), C) * R + (size_t)wrap(l - dlay(e), L) * R * C;
+}
 
 template <int ND, typename T>
 __device__ __forceinline__ void te_node(const T* __restrict__ sK, int kstride, unsigned key,
-                                        const T* pm, const T* p0, const T* pp, int ctr, T (&out)[ND]) {
+                                        const T* pm, const T* p0, const T* pp, int ctr, T (&out)[ND], const T* scl = nullptr) {
   constexpr int ED = 8 * ND;
 #pragma unroll
   for (int c = 0; c < ND; c++) out[c] = T(0);
 #pragma unroll
   for (int e = 0; e < 8; e++) {
     const T* K = sK + ((key >> (2 * e)) & 3u) * kstride + e * ND * ED;
+    T oe[ND];
+#pragma unroll
+    for (int ci = 0; ci < ND; ci++) oe[ci] = T(0);
 #pragma unroll
     for (int b = 0; b < 8; b++) {
       if (ND == 1 && shares_edge(e, b)) continue;  // structural zero of the Q1 conductivity matrix
@@ -126,11 +141,16 @@ __device__ __forceinline__ void te_node(const T* __restrict__ sK, int kstride, u
       const T* v = P + (ctr + dr + dc * TE_PR) * ND;
 #pragma unroll
       for (int ci = 0; ci < ND; ci++) {
-        T s = out[ci];
+        T s = scl ? oe[ci] : out[ci];
 #pragma unroll
         for (int cj = 0; cj < ND; cj++) s = fma(K[ci * ED + b * ND + cj], v[cj], s);
-        out[ci] = s;
+        if (scl) oe[ci] = s;
+        else out[ci] = s;
       }
+    }
+    if (scl) {
+#pragma unroll
+      for (int ci = 0; ci < ND; ci++) out[ci] = fma(scl[e], oe[ci], out[ci]);
     }
   }
 }
@@ -238,7 +258,12 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a, const T* __
   T* sP = sK + (ASM ? TAB : 4 * kstride);
   // ASM: the inverse Jacobi diagonal by node configuration follows the blocks
   [[maybe_unused]] const T* sInv = sK + ASM_NBLK * AsmLayout<ND, T, 1>::BS;
-  auto invdiag = [&](unsigned key, T (&inv)[ND]) {
+  auto invdiag = [&](size_t node, unsigned key, T (&inv)[ND]) {
+    if (a.invd) {
+#pragma unroll
+      for (int c = 0; c < ND; c++) inv[c] = T(a.invd[node * ND + c]);
+      return;
+    }
     if constexpr (ASM) {
       const unsigned m = asm_config(key);
 #pragma unroll
@@ -279,7 +304,7 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a, const T* __
       const size_t node = (size_t)gr + (size_t)gc * R + (size_t)lw * RC;
       T inv[ND];
       if (MODE == TE_MR || MODE == TE_PCG || MODE == TE_DIRDOT) {
-        if (pre) invdiag(a.keys[node], inv);
+        if (pre) invdiag(node, a.invd ? 0u : (unsigned)a.keys[node], inv);
         else {
 #pragma unroll
           for (int c = 0; c < ND; c++) inv[c] = T(1);
@@ -321,11 +346,19 @@ __global__ void __launch_bounds__(TE_NT) k_te_apply(TeArgs<ND, T> a, const T* __
       const T* p0 = sP + slot_of(l) * TE_PP * ND;
       const T* pp = sP + slot_of(l + 1) * TE_PP * ND;
       T out[ND];
-      if constexpr (ASM) asm_te_node<ND, T>(std::make_integer_sequence<int, 27>{}, sK, key, pm, p0, pp, ctr, out);
-      else te_node<ND, T>(sK, kstride, key, pm, p0, pp, ctr, out);
+      if constexpr (ASM) {
+        asm_te_node<ND, T>(std::make_integer_sequence<int, 27>{}, sK, key, pm, p0, pp, ctr, out);
+      } else if (a.sdf) {
+        T scl[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) scl[e] = T(a.sdf_min + a.sdf_rng * (double)a.sdf[te_voxel(r, c, l, e, R, C, L)] * (1.0 / 65535.0));
+        te_node<ND, T>(sK, kstride, key, pm, p0, pp, ctr, out, scl);
+      } else {
+        te_node<ND, T>(sK, kstride, key, pm, p0, pp, ctr, out);
+      }
       [[maybe_unused]] T own_inv[ND];
       if constexpr (MODE == TE_UPD) {
-        if (pre) invdiag(key, own_inv);
+        if (pre) invdiag(node, key, own_inv);
         else {
 #pragma unroll
           for (int cc = 0; cc < ND; cc++) own_inv[cc] = T(1);

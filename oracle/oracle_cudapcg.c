@@ -82,17 +82,24 @@ typedef struct {
   unsigned int ed;   /* element matrix dimension: 8, 24 or 32 */
   unsigned int nkeys;
   unsigned short *keys; /* per-node material key (NBN form), derived for EBE */
+  /* scalar density field (cudapcgSetParametricDensityField): per voxel a 16-bit code q, the
+     voxel's element matrix scaled by fmin + (fmax - fmin) q / 65535 */
+  parametricScalarField_t *sdf;
+  double sdf_min, sdf_max;
 } oracle_solver_t;
 
 static oracle_solver_t *S = NULL;
 static cudapcgFlag_t (*model_ctor)(cudapcgModel_t **, const void *) = NULL;
 static int g_quiet = 0;
 
-/* captured inputs (checker access) */
-static void *cap_ptr[7] = {0};
-static unsigned int cap_n[7] = {0};
-static size_t cap_elsz[7] = {sizeof(cudapcgMap_t), sizeof(cudapcgIdMap_t), sizeof(cudapcgIdMap_t),
-                             sizeof(cudapcgFlag_t), sizeof(double), sizeof(double), sizeof(double)};
+/* captured inputs (checker access): 0 image/keys, 1 node->DOF, 2 DOF->node, 3 pore map,
+   4 local matrices, 5 right-hand side, 6 solution, 7 density codes, 8 density range */
+#define CAP_SLOTS 9
+static void *cap_ptr[CAP_SLOTS] = {0};
+static unsigned int cap_n[CAP_SLOTS] = {0};
+static size_t cap_elsz[CAP_SLOTS] = {sizeof(cudapcgMap_t), sizeof(cudapcgIdMap_t), sizeof(cudapcgIdMap_t),
+                                     sizeof(cudapcgFlag_t), sizeof(double), sizeof(double), sizeof(double),
+                                     sizeof(parametricScalarField_t), sizeof(double)};
 static double *hist = NULL;
 static unsigned int hist_n = 0, hist_cap = 0;
 #define LOG_CAP 4096
@@ -179,6 +186,16 @@ static void keys_from_elements(const cudapcgMap_t *em, unsigned int R, unsigned 
 
 /* ------------------------------------------------------------------------------------ */
 /* Operator y = A x (reference formulation, FP64).                                        */
+/* Scale of the voxel in which node (r, c, l) is local node e: 1 without a density field;
+   with one, fmin + (fmax - fmin) q / 65535 of that voxel, the voxel at (r - DROW[e] - 1,
+   c - DCOL[e], l - DLAY[e]) (matrix_free.cu:2283-2295 lists the 8 voxels around a node in this
+   order, kernel_applyPreConditioner_thermal_3D_ElemByElem_ScalarDensityField). */
+static double sdf_scale(int r, int c, int l, int e, unsigned int R, unsigned int C, unsigned int L) {
+  if (!S->sdf) return 1.0;
+  const unsigned int v = pnum(r - DROW[e] - 1, c - DCOL[e], l - DLAY[e], R, C, L);
+  return S->sdf_min + (S->sdf_max - S->sdf_min) * (double)S->sdf[v] * (1.0 / 65535.0);
+}
+
 static void apply_thermal_elastic(const double *v, double *y) {
   cudapcgModel_t *m = S->model;
   const unsigned int R = m->nrows, C = m->ncols, L = m->nlayers, N = R * C * L;
@@ -193,13 +210,14 @@ static void apply_thermal_elastic(const double *v, double *y) {
     double acc[3] = {0, 0, 0};
     for (int e = 0; e < 8; e++) {
       const double *K = S->Kd + (size_t)((key >> (2 * e)) & 3u) * ed * ed;
+      const double f = sdf_scale(r, c, l, e, R, C, L);
       for (int b = 0; b < 8; b++) {
         unsigned int j = nb[NBIDX(e, b)];
         for (unsigned int ci = 0; ci < nd; ci++) {
           const double *row = K + (size_t)(e * nd + ci) * ed + b * nd;
           double s = 0.0;
           for (unsigned int cj = 0; cj < nd; cj++) s += row[cj] * v[(size_t)j * nd + cj];
-          acc[ci] += s;
+          acc[ci] += f * s;
         }
       }
     }
@@ -285,14 +303,16 @@ static void inv_diag(double *dinv) {
   }
   const unsigned int N = m->nrows * m->ncols * m->nlayers;
   const unsigned int nd = (S->analysis == CUDAPCG_ELASTIC_3D) ? 3 : 1, ed = 8 * nd;
+  const unsigned int R = m->nrows, C = m->ncols, L = m->nlayers;
 #pragma omp parallel for schedule(static)
   for (long i = 0; i < (long)N; i++) {
     unsigned int key = S->keys[i];
+    const int r = (int)(i % R), c = (int)((i / R) % C), l = (int)(i / ((long)R * C));
     for (unsigned int ci = 0; ci < nd; ci++) {
       double s = 0.0;
       for (int e = 0; e < 8; e++) {
         const double *K = S->Kd + (size_t)((key >> (2 * e)) & 3u) * ed * ed;
-        s += K[(e * nd + ci) * ed + e * nd + ci];
+        s += sdf_scale(r, c, l, e, R, C, L) * K[(e * nd + ci) * ed + e * nd + ci];
       }
       dinv[(size_t)i * nd + ci] = 1.0 / s;
     }
@@ -407,7 +427,7 @@ cudapcgModel_t *cudapcgNewModel(void) {
 cudapcgFlag_t cudapcgEnd(void) {
   if (!S) return CUDAPCG_FALSE;
   if (S->model && S->model->freeAllowed_flag) free_model(S->model);
-  free(S->x); free(S->r); free(S->d); free(S->q); free(S->s); free(S->Kd); free(S->keys); free(S->header);
+  free(S->x); free(S->r); free(S->d); free(S->q); free(S->s); free(S->Kd); free(S->keys); free(S->sdf); free(S->header);
   free(g_dinv); g_dinv = NULL;
   free(S); S = NULL;
   return CUDAPCG_TRUE;  /* the oracle never resets a device */
@@ -460,10 +480,6 @@ cudapcgFlag_t cudapcgBuildModel(const void *data) {
   if (!model_ctor(&S->model, data)) return CUDAPCG_FALSE;
   if (S->analysis == CUDAPCG_FLUID_3D && S->model->poremap_flag != CUDAPCG_POREMAP_NUM) {
     fprintf(stderr, "oracle: only the DOF-number pore map is supported\n");
-    return CUDAPCG_FALSE;
-  }
-  if (S->model->parametric_density_field_flag) {
-    fprintf(stderr, "oracle: scalar density fields are outside the hot path\n");
     return CUDAPCG_FALSE;
   }
   free_arrays();
@@ -552,7 +568,22 @@ cudapcgFlag_t cudapcgSetImage(cudapcgMap_t *img) {
   else for (unsigned int i = 0; i < m->nelem; i++) S->keys[i] = img[i];
   return 1;
 }
-cudapcgFlag_t cudapcgSetParametricDensityField(parametricScalarField_t *f, double a, double b) { (void)f; (void)a; (void)b; return 0; }
+/* cudapcg.cu:327-334: the density codes of every voxel and their range; a thermal model has one
+   material (femhmg.c:256-262 normalises it), whose key is zero everywhere. */
+cudapcgFlag_t cudapcgSetParametricDensityField(parametricScalarField_t *f, double fmin, double fmax) {
+  if (!S || !S->model || !f) return 0;
+  cudapcgModel_t *m = S->model;
+  free(S->sdf);
+  S->sdf = (parametricScalarField_t *)malloc(sizeof(parametricScalarField_t) * m->nelem);
+  memcpy(S->sdf, f, sizeof(parametricScalarField_t) * m->nelem);
+  S->sdf_min = fmin;
+  S->sdf_max = fmax;
+  if (!S->keys) S->keys = (unsigned short *)calloc(m->nelem, sizeof(unsigned short));
+  capture(7, f, m->nelem);
+  const double range[2] = {fmin, fmax};
+  capture(8, range, 2);
+  return 1;
+}
 cudapcgFlag_t cudapcgSetPoreMap(cudapcgFlag_t *pores) {
   if (!S || !S->model) return 0;
   memcpy(S->model->border_pore_map, pores, S->model->nbordernodes);
@@ -1130,9 +1161,9 @@ int oracle_precond(const double *x, double *y) {
   return 1;
 }
 unsigned int oracle_nvars(void) { return (S && S->model) ? S->model->nvars : 0; }
-unsigned int oracle_captured_count(int which) { return (which >= 0 && which < 7) ? cap_n[which] : 0; }
+unsigned int oracle_captured_count(int which) { return (which >= 0 && which < CAP_SLOTS) ? cap_n[which] : 0; }
 int oracle_copy_captured(int which, void *dst, unsigned int bytes) {
-  if (which < 0 || which >= 7 || !cap_ptr[which]) return 0;
+  if (which < 0 || which >= CAP_SLOTS || !cap_ptr[which]) return 0;
   size_t have = (size_t)cap_n[which] * cap_elsz[which];
   memcpy(dst, cap_ptr[which], bytes < have ? bytes : have);
   return 1;
