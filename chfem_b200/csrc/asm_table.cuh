@@ -118,7 +118,8 @@ template <int ND, typename T, int O, typename V, int NW>
 __device__ __forceinline__ void asm_block(const T* __restrict__ sT, unsigned m, const V (&val)[ND][NW], V (&out)[ND][NW]) {
   if constexpr (asm_used<ND>(O)) {
     constexpr int BS = ND == 1 ? 1 : ((std::is_same<T, float>::value && ND == 3) ? 12 : ND * ND);
-    const T* tb = sT + (asm_base(O) + asm_variant<O>(m)) * BS;
+    constexpr int kBase = asm_base(O);  // evaluated at compile time, not per node
+    const T* tb = sT + (kBase + asm_variant<O>(m)) * BS;
     T blk[ND * ND];
     if constexpr (std::is_same<T, float>::value && ND == 3) {
       const float4 q0 = *reinterpret_cast<const float4*>(tb);

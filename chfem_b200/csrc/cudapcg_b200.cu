@@ -24,6 +24,7 @@
 #include "stencil_block.cuh"
 #include "stencil_asm.cuh"
 #include "asm_apply.h"
+#include "stencil_2d.cuh"
 #include "pore_maps.h"
 #include "stencil_fluid_block.cuh"
 #include "loadcase.cuh"
@@ -80,6 +81,7 @@ static void sparseq1_to_dense(const double* sp, double* dense) {
 struct Solver {
   // configuration (cudapcg.cu:108-183 defaults)
   int analysis = 0, par = 0;
+  bool dim2 = false;  // 2D thermal / elastic (pixel images, one layer, 4-bit key fields)
   double tol = 0.00001;
   unsigned maxit = 100000;
   int solver_flag = CUDAPCG_CG_SOLVER;
@@ -274,7 +276,7 @@ static bool ensure_vectors() {
 // Assembled neighbour blocks (stencil_asm.cuh) of a thermal/elastic model of at most two
 // materials; CHFEM_B200_BLOCK_OP=element keeps the element-by-element block operator.
 static bool asm_applies() {
-  if (S->analysis == CUDAPCG_FLUID_3D || S->nmat > 2 || S->d_sdf) return false;
+  if (S->analysis == CUDAPCG_FLUID_3D || S->dim2 || S->nmat > 2 || S->d_sdf) return false;
   const char* e = getenv("CHFEM_B200_BLOCK_OP");
   return !(e && !strcmp(e, "element"));
 }
@@ -323,11 +325,14 @@ __global__ void k_sdf_invdiag(const uint16_t* keys, const uint16_t* sdf, double 
 }
 static bool ensure_K64_only();
 static bool ensure_invd() {
-  if (S->d_invd || !S->d_sdf) return true;
+  if (S->d_invd || !(S->d_sdf || S->dim2)) return true;
   if (!ensure_K64_only()) return false;
   CKV(cudaMalloc(&S->d_invd, sizeof(double) * S->N * S->nd));
   const long g = std::max(1L, std::min<long>((S->N + 255) / 256, 8L * num_sms()));
-  if (S->nd == 1) k_sdf_invdiag<1><<<(int)g, 256, 0, S->stream>>>(S->d_keys, S->d_sdf, S->sdf_min, S->sdf_max - S->sdf_min, S->d_K64, S->R, S->C, S->L, S->d_invd);
+  if (S->dim2) {
+    if (S->nd == 1) k_2d_invdiag<1><<<(int)g, 256, 0, S->stream>>>(S->d_keys, S->d_K64, S->N, S->d_invd);
+    else k_2d_invdiag<2><<<(int)g, 256, 0, S->stream>>>(S->d_keys, S->d_K64, S->N, S->d_invd);
+  } else if (S->nd == 1) k_sdf_invdiag<1><<<(int)g, 256, 0, S->stream>>>(S->d_keys, S->d_sdf, S->sdf_min, S->sdf_max - S->sdf_min, S->d_K64, S->R, S->C, S->L, S->d_invd);
   else k_sdf_invdiag<3><<<(int)g, 256, 0, S->stream>>>(S->d_keys, S->d_sdf, S->sdf_min, S->sdf_max - S->sdf_min, S->d_K64, S->R, S->C, S->L, S->d_invd);
   CKV(cudaGetLastError());
   return true;
@@ -349,7 +354,7 @@ template <typename T>
 static bool ensure_K() {
   if (Kdev<T>()) {  // the derived tables may have been dropped since (new density field, new model)
     if (asm_applies() && !ensure_tab<T>()) return false;
-    if (S->d_sdf && !ensure_invd()) return false;
+    if ((S->d_sdf || S->dim2) && !ensure_invd()) return false;
     return true;
   }
   if (!S->have_K) { set_err("solve", "local matrices were not set (cudapcgSetLclMtxs)"); return false; }
@@ -360,7 +365,7 @@ static bool ensure_K() {
   CKV(cudaMemcpy(dk, kt.data(), kt.size() * sizeof(T), cudaMemcpyHostToDevice));
   if (sizeof(T) == 8) S->d_K64 = (double*)dk; else S->d_K32 = (float*)dk;
   if (asm_applies() && !ensure_tab<T>()) return false;
-  if (S->d_sdf && !ensure_invd()) return false;
+  if ((S->d_sdf || S->dim2) && !ensure_invd()) return false;
   if (S->analysis == CUDAPCG_FLUID_3D) {
     if (sizeof(T) == 8) CKV(cudaMemcpyToSymbol(c_flK64, kt.data(), 1024 * sizeof(double)));
     else CKV(cudaMemcpyToSymbol(c_flK32, kt.data(), 1024 * sizeof(float)));
@@ -422,6 +427,12 @@ static SolveCfg solvecfg() {
 }
 
 // y = A v (+ fused direction form and dot finisher).  in1/vout only with fuse.
+// CTAs of a 2D operator pass: the tiles, at most 8 per SM
+static int d2_ctas() {
+  const long tiles = (long)((S->R + T2_TR - 1) / T2_TR) * ((S->C + T2_TC - 1) / T2_TC);
+  return (int)std::max(1L, std::min(tiles, 8L * num_sms()));
+}
+
 template <typename T>
 static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, int finish, bool skip_if_done) {
   if (S->analysis == CUDAPCG_FLUID_3D) {
@@ -436,6 +447,21 @@ static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, i
     a.rc = redctl(g);
     if (fuse) k_fl_apply<T, TE_PCG><<<g, FL_NT, 0, S->stream>>>(a);
     else k_fl_apply<T, TE_PLAIN><<<g, FL_NT, 0, S->stream>>>(a);
+  } else if (S->dim2) {
+    const int nb = d2_ctas();
+    if (!ensure_reduction(nb)) return false;
+    const MrCfg cfg{S->tol, 0, S->resnorm, S->precond, 0};
+    if (S->nd == 1) {
+      TeArgs<1, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, 1, S->cur_sc, redctl(nb), finish, skip_if_done, cfg};
+      a.invd = S->d_invd;
+      if (fuse) k_2d_apply<1, T, TE_PCG><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<1, T>(), S->stream>>>(a);
+      else k_2d_apply<1, T, TE_PLAIN><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<1, T>(), S->stream>>>(a);
+    } else {
+      TeArgs<2, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, 1, S->cur_sc, redctl(nb), finish, skip_if_done, cfg};
+      a.invd = S->d_invd;
+      if (fuse) k_2d_apply<2, T, TE_PCG><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<2, T>(), S->stream>>>(a);
+      else k_2d_apply<2, T, TE_PLAIN><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<2, T>(), S->stream>>>(a);
+    }
   } else if (asm_applies()) {
     int nb;
     cudaError_t e;
@@ -489,8 +515,11 @@ static bool launch_point(double* x, T* d, T* r, const T* q, T* s, const T* dold)
   } else {
     const int g = pw_grid(S->N);
     if (!ensure_reduction(g)) return false;
-    if (S->nd == 1) {
-      TePw<1, T> a{x, d, r, q, s, dold, S->d_keys, Kdev<T>(), S->nmat, S->N, S->cur_sc, redctl(g), cfg, S->d_invd};
+    if (S->dim2 && S->nd == 2) {  // 2D elastic: the Jacobi diagonal from invd only
+      TePw<2, T> a{x, d, r, q, s, dold, S->d_keys, Kdev<T>(), 0, S->N, S->cur_sc, redctl(g), cfg, S->d_invd};
+      k_te_point<2, T, MODE><<<g, PW_NT, 0, S->stream>>>(a);
+    } else if (S->nd == 1) {
+      TePw<1, T> a{x, d, r, q, s, dold, S->d_keys, Kdev<T>(), S->dim2 ? 0 : S->nmat, S->N, S->cur_sc, redctl(g), cfg, S->d_invd};
       k_te_point<1, T, MODE><<<g, PW_NT, 0, S->stream>>>(a);
     } else {
       TePw<3, T> a{x, d, r, q, s, dold, S->d_keys, Kdev<T>(), S->nmat, S->N, S->cur_sc, redctl(g), cfg, S->d_invd};
@@ -524,7 +553,20 @@ static bool launch_te_mode(const T* in0, const T* in1, T* vout, double* x, int f
   const SolveCfg sc = solvecfg();
   const MrCfg cfg{sc.tol, sc.maxit, sc.norm, sc.precond, sc.nhmg};
   cudaError_t e = cudaSuccess;
-  if (asm_applies()) {
+  if (S->dim2) {
+    const int nb = d2_ctas();
+    if (!ensure_reduction(nb)) return false;
+    if (S->nd == 1) {
+      TeArgs<1, T> a{in0, in1, vout, nullptr, x, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, 1, S->cur_sc, redctl(nb), finish, 1, cfg};
+      a.invd = S->d_invd;
+      k_2d_apply<1, T, MODE><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<1, T>(), S->stream>>>(a);
+    } else {
+      TeArgs<2, T> a{in0, in1, vout, nullptr, x, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, 1, S->cur_sc, redctl(nb), finish, 1, cfg};
+      a.invd = S->d_invd;
+      k_2d_apply<2, T, MODE><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<2, T>(), S->stream>>>(a);
+    }
+    e = cudaGetLastError();
+  } else if (asm_applies()) {
     if (S->nd == 1) {
       const int nb = asm_te_ctas<1, T, MODE>(S->R, S->C, S->L, num_sms());
       if (nb < 1 || !ensure_reduction(nb)) return false;
@@ -760,7 +802,6 @@ template <typename T>
 static bool solve_T(double* res_x) {
   if (!ensure_vectors<T>() || !ensure_K<T>()) return false;
   const bool minres = (S->solver_flag == CUDAPCG_MINRES_SOLVER || S->solver_flag == CUDAPCG_MINRES3_SOLVER);
-  if (minres && S->d_sdf) { set_err("cudapcgSolve", "a scalar density field is solved by CG / PCG (-s 0, 2)"); return false; }
   bool ok = minres ? solve_minres_device<T>() : solve_pcg_device<T>();
   if (!ok) return false;
   collect_results(minres);
@@ -794,10 +835,8 @@ cudapcgFlag_t cudapcgEnd(void) {
 cudapcgFlag_t cudapcgInit(cudapcgFlag_t analysis_flag, cudapcgFlag_t parStrategy_flag) {
   cudapcgEnd();
   g_err.clear();
-  if (analysis_flag != CUDAPCG_THERMAL_3D && analysis_flag != CUDAPCG_ELASTIC_3D && analysis_flag != CUDAPCG_FLUID_3D) {
-    set_err("cudapcgInit", analysis_flag <= CUDAPCG_FLUID_3D ? "2D analyses are not provided by chfem_b200" : "invalid analysis flag");
-    return CUDAPCG_FALSE;
-  }
+  if (analysis_flag > CUDAPCG_FLUID_3D) { set_err("cudapcgInit", "invalid analysis flag"); return CUDAPCG_FALSE; }
+  if (analysis_flag == CUDAPCG_FLUID_2D) { set_err("cudapcgInit", "2D permeability analysis is not provided by chfem_b200"); return CUDAPCG_FALSE; }
   if (analysis_flag == CUDAPCG_FLUID_3D && parStrategy_flag != CUDAPCG_NBN) {
     printf("ERROR: EBE solver is unavailable for FLUID analysis.\n");
     set_err("cudapcgInit", "EBE is unavailable for FLUID analysis");
@@ -806,7 +845,8 @@ cudapcgFlag_t cudapcgInit(cudapcgFlag_t analysis_flag, cudapcgFlag_t parStrategy
   S = new Solver();
   S->analysis = analysis_flag;
   S->par = parStrategy_flag;
-  S->nd = (analysis_flag == CUDAPCG_ELASTIC_3D) ? 3 : 1;
+  S->dim2 = analysis_flag == CUDAPCG_THERMAL_2D || analysis_flag == CUDAPCG_ELASTIC_2D;
+  S->nd = (analysis_flag == CUDAPCG_ELASTIC_3D) ? 3 : (analysis_flag == CUDAPCG_ELASTIC_2D ? 2 : 1);
   if (const char* e = getenv("CHFEM_B200_PRECISION")) cudapcgB200SetPrecision((!strcmp(e, "mixed") || !strcmp(e, "fp32")) ? CHFEM_B200_MIXED : CHFEM_B200_FP64);
   if (!g_ctor) g_ctor = ctor_simple;
   CK(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
@@ -838,12 +878,15 @@ static cudapcgFlag_t adopt_model() {
   free_vectors();
   free_model_dev();
   block_free();
-  S->R = (int)m->nrows; S->C = (int)m->ncols; S->L = (int)m->nlayers;
+  S->R = (int)m->nrows; S->C = (int)m->ncols; S->L = S->dim2 ? 1 : (int)m->nlayers;
   S->N = (long)S->R * S->C * S->L;
   S->nvars = m->nvars; S->nV = m->nporenodes; S->nB = m->nbordernodes;
   S->nmat = (int)m->nkeys;
   if (S->N <= 0 || S->nvars <= 0) { set_err("model", "empty model"); return CUDAPCG_FALSE; }
-  if (S->analysis != CUDAPCG_FLUID_3D && (S->nmat < 1 || S->nmat > 4)) { set_err("model", "1 to 4 materials are supported with 16-bit keys"); return CUDAPCG_FALSE; }
+  if (S->analysis != CUDAPCG_FLUID_3D && (S->nmat < 1 || S->nmat > (S->dim2 ? T2_NMAT : 4))) {
+    set_err("model", S->dim2 ? "1 to 16 materials are supported with 16-bit 2D keys" : "1 to 4 materials are supported with 16-bit keys");
+    return CUDAPCG_FALSE;
+  }
   if (S->analysis == CUDAPCG_FLUID_3D) {
     CK(cudaMalloc(&S->d_dof_of_node, sizeof(uint32_t) * S->N));
     CK(cudaMalloc(&S->d_node_of_dof, sizeof(uint32_t) * std::max<long>(1, S->nV + S->nB)));
@@ -1092,13 +1135,15 @@ cudapcgFlag_t cudapcgSetImage(cudapcgMap_t* img) {
     uint16_t* tmp = nullptr;
     CK(cudaMalloc(&tmp, sizeof(uint16_t) * S->N));
     CK(cudaMemcpy(tmp, img, sizeof(uint16_t) * S->N, cudaMemcpyHostToDevice));
-    k_keys_from_elements<<<pw_grid(S->N), PW_NT, 0, S->stream>>>(tmp, S->d_keys, S->R, S->C, S->L);
+    if (S->dim2) k_keys_from_elements_2d<<<pw_grid(S->N), PW_NT, 0, S->stream>>>(tmp, S->d_keys, S->R, S->C);
+    else k_keys_from_elements<<<pw_grid(S->N), PW_NT, 0, S->stream>>>(tmp, S->d_keys, S->R, S->C, S->L);
     CK(cudaStreamSynchronize(S->stream));
     cudaFree(tmp);
   } else {
     CK(cudaMemcpy(S->d_keys, img, sizeof(uint16_t) * S->N, cudaMemcpyHostToDevice));
   }
   S->have_keys = true;
+  if (S->dim2) { free_ptr(S->d_invd); S->d_invd = nullptr; invalidate_graphs(); }  // a 2D Jacobi diagonal follows the keys
   return CUDAPCG_TRUE;
 }
 cudapcgFlag_t cudapcgB200SetImageColors(const uint8_t* colors, unsigned int rows, unsigned int cols, unsigned int slices,
@@ -1106,6 +1151,7 @@ cudapcgFlag_t cudapcgB200SetImageColors(const uint8_t* colors, unsigned int rows
   const char* who = "cudapcgB200SetImageColors";
   if (!S || !S->model || !colors || !material_of_color || refinement < 1) { set_err(who, "bad arguments"); return CUDAPCG_FALSE; }
   if (S->analysis == CUDAPCG_FLUID_3D) { set_err(who, "not used for FLUID analysis"); return CUDAPCG_FALSE; }
+  if (S->dim2) { set_err(who, "2D node keys are set with cudapcgSetImage"); return CUDAPCG_FALSE; }
   if ((long)rows * refinement != S->R || (long)cols * refinement != S->C || (long)slices * refinement != S->L) {
     set_err(who, "image dimensions times refinement differ from the model's");
     return CUDAPCG_FALSE;
@@ -1266,7 +1312,9 @@ static bool set_fluid_diag() {
 cudapcgFlag_t cudapcgSetLclMtxs(cudapcgVar_t* Lm) {
   if (!S || !S->model || !Lm) return CUDAPCG_FALSE;
   const int nk = S->analysis == CUDAPCG_FLUID_3D ? 1 : S->nmat;
-  if (S->analysis == CUDAPCG_THERMAL_3D) {
+  if (S->dim2) {  // dense (4 nd) x (4 nd) per material (femhmg_thermal_2D.c:42-90, femhmg_elastic_2D.c:56-146)
+    S->Kd.assign(Lm, Lm + (size_t)16 * S->nd * S->nd * nk);
+  } else if (S->analysis == CUDAPCG_THERMAL_3D) {
     S->Kd.assign((size_t)64 * nk, 0.0);
     for (int k = 0; k < nk; k++) sparseq1_to_dense(Lm + 40 * k, S->Kd.data() + 64 * k);
   } else if (S->analysis == CUDAPCG_ELASTIC_3D) {
@@ -1493,6 +1541,7 @@ extern "C" cudapcgFlag_t cudapcgB200ComputeFields(int block_index, int axis, int
                                                   double* field_out) {
   const char* who = "cudapcgB200ComputeFields";
   if (!S || !S->model || !props || !field_out) { set_err(who, "bad arguments"); return CUDAPCG_FALSE; }
+  if (S->dim2) { set_err(who, "not provided for 2D models"); return CUDAPCG_FALSE; }
   if (S->analysis == CUDAPCG_FLUID_3D) { set_err(who, "Stokes fields are the solution itself (velocity, pressure)"); return CUDAPCG_FALSE; }
   if (axis < 0 || axis > 2 || comp < 0 || comp >= S->nd) { set_err(who, "bad load case"); return CUDAPCG_FALSE; }
   const double* x = nullptr;
@@ -1543,6 +1592,7 @@ static bool load_case_rhs_T(int axis, int comp, double jump, const double* CB) {
 extern "C" cudapcgFlag_t cudapcgB200SetLoadCaseRHS(int axis, int comp, double jump, const double* CB) {
   const char* who = "cudapcgB200SetLoadCaseRHS";
   if (!S || !S->model || axis < 0 || axis > 2) { set_err(who, "bad arguments"); return CUDAPCG_FALSE; }
+  if (S->dim2) { set_err(who, "not provided for 2D models"); return CUDAPCG_FALSE; }
   const bool fluid = S->analysis == CUDAPCG_FLUID_3D;
   if (fluid ? !CB : (comp < 0 || comp >= S->nd)) { set_err(who, "bad load case"); return CUDAPCG_FALSE; }
   if (!fluid && !S->have_keys) { set_err(who, "the model's keys were not set"); return CUDAPCG_FALSE; }
@@ -1556,6 +1606,7 @@ extern "C" cudapcgFlag_t cudapcgB200SetLoadCaseRHS(int axis, int comp, double ju
 extern "C" cudapcgFlag_t cudapcgB200VolumeTerm(const double* CB, unsigned int ns, double* moments) {
   const char* who = "cudapcgB200VolumeTerm";
   if (!S || !S->model || !CB || !moments || !S->x) { set_err(who, "bad arguments or no solution on the device"); return CUDAPCG_FALSE; }
+  if (S->dim2) { set_err(who, "not provided for 2D models"); return CUDAPCG_FALSE; }
   const bool fluid = S->analysis == CUDAPCG_FLUID_3D;
   if (ns != (fluid ? 3u : (S->nd == 3 ? 6u : 3u))) { set_err(who, "ns must be 3 (thermal, Stokes) or 6 (elastic)"); return CUDAPCG_FALSE; }
   if (!S->d_vt) CK(cudaMalloc(&S->d_vt, (8 + 4 * 6 * 24) * sizeof(double)));
@@ -1585,6 +1636,7 @@ extern "C" cudapcgFlag_t cudapcgB200SolveLoadCases(unsigned int nrhs, const int*
                                                    double* residuals) {
   const char* who = "cudapcgB200SolveLoadCases";
   if (!S || !S->model || !axis || !CB || !moments || nrhs < 1 || nrhs > BLK_MAX) { set_err(who, "bad arguments"); return CUDAPCG_FALSE; }
+  if (S->dim2) { set_err(who, "not provided for 2D models"); return CUDAPCG_FALSE; }
   if (lean_solver()) { set_err(who, "block solves run CG/MINRES(3); the 2-vector solvers reduce one load case at a time"); return CUDAPCG_FALSE; }
   const bool fluid = S->analysis == CUDAPCG_FLUID_3D;
   if (fluid != ((S->solver_flag & 1) != 0)) {
@@ -1612,6 +1664,7 @@ extern "C" cudapcgFlag_t cudapcgB200SolveLoadCases(unsigned int nrhs, const int*
 
 extern "C" cudapcgFlag_t cudapcgB200ApplyBlockOperator(unsigned int nrhs, const double* const* v, double* const* y) {
   if (!S || !S->model || !v || !y || nrhs < 1 || nrhs > BLK_MAX) { set_err("cudapcgB200ApplyBlockOperator", "bad arguments"); return CUDAPCG_FALSE; }
+  if (S->dim2) { set_err("cudapcgB200ApplyBlockOperator", "not provided for 2D models"); return CUDAPCG_FALSE; }
   if (S->analysis == CUDAPCG_FLUID_3D) { set_err("cudapcgB200ApplyBlockOperator", "thermal and elastic models only"); return CUDAPCG_FALSE; }
   for (unsigned k = 0; k < nrhs; k++) if (!v[k] || !y[k]) { set_err("cudapcgB200ApplyBlockOperator", "null buffer"); return CUDAPCG_FALSE; }
   const bool ok = (S->precision == CHFEM_B200_FP64) ? apply_block_T<double>((int)nrhs, v, y) : apply_block_T<float>((int)nrhs, v, y);
@@ -1622,6 +1675,7 @@ extern "C" cudapcgFlag_t cudapcgB200SolveBlock(unsigned int nrhs, const double* 
                                                int x0_interpolate, double* const* x_out, unsigned int* iterations,
                                                double* residuals) {
   if (!S || !S->model || !rhs || !x_out || nrhs < 1 || nrhs > BLK_MAX) { set_err("cudapcgB200SolveBlock", "bad arguments"); return CUDAPCG_FALSE; }
+  if (S->dim2) { set_err("cudapcgB200SolveBlock", "not provided for 2D models"); return CUDAPCG_FALSE; }
   if (lean_solver()) { set_err("cudapcgB200SolveBlock", "block solves run CG/MINRES(3), not the 2-vector solvers"); return CUDAPCG_FALSE; }
   const bool fluid = S->analysis == CUDAPCG_FLUID_3D;
   if (fluid != ((S->solver_flag & 1) != 0)) {

@@ -1,4 +1,4 @@
-// hmg.cpp -- femhmg-compatible host API of chfem_b200 (3D): settings and image input,
+// hmg.cpp -- femhmg-compatible host API of chfem_b200 (3D; 2D thermal / elastic): settings and image input,
 // model set-up, the load-case loop over the cudapcg C ABI, output.
 //
 // Follows chfem/src/femhmg/femhmg.c: hmgInit :135-394, readData :1456-1586 (tag grammar and
@@ -158,13 +158,14 @@ bool read_nf(Model& m, const char* fn) {
   fclose(f);
   if (!ok) return false;
   if (nx <= 0 || ny <= 0) { fail("%image_dimensions missing or invalid"); return false; }
-  if (nz <= 0) { fail("2D images are not provided by chfem_b200 (3D only)"); return false; }
+  if (nz < 0) { fail("%image_dimensions missing or invalid"); return false; }
+  m.dim2 = nz == 0;  // femhmg.c:1496-1504: zero layers make a 2D (pixel) model
   if (m.analysis < 0) { fail("%type_of_analysis missing"); return false; }
   if (m.nmat == 0) { fail("no materials"); return false; }
   if (m.refinement > 1) m.voxel /= m.refinement;
   // femhmg.c:1583-1584: the x-reduce stabilisation factor defaults to tol^2, or 1e-12 below 5e-7
   if (m.xreduce_stab < 0) m.xreduce_stab = m.tol >= 0.0000005 ? m.tol * m.tol : 0.000000000001;
-  m.nx = (unsigned)nx * m.refinement; m.ny = (unsigned)ny * m.refinement; m.nz = (unsigned)nz * m.refinement;
+  m.nx = (unsigned)nx * m.refinement; m.ny = (unsigned)ny * m.refinement; m.nz = m.dim2 ? 1u : (unsigned)nz * m.refinement;
   return true;
 }
 
@@ -172,7 +173,7 @@ bool read_nf(Model& m, const char* fn) {
 // The image's colour bytes (file order, x fastest), checked against the .nf material list.
 bool read_colors(Model& m, const uint8_t* data, const char* raw) {
   const unsigned ref = m.refinement;
-  m.frows = m.ny / ref; m.fcols = m.nx / ref; m.fslices = m.nz / ref;
+  m.frows = m.ny / ref; m.fcols = m.nx / ref; m.fslices = m.dim2 ? 1u : m.nz / ref;
   const size_t nvox_file = (size_t)m.frows * m.fcols * m.fslices;
   m.colors.resize(nvox_file);
   if (data) {
@@ -204,7 +205,8 @@ void build_elem_mat(Model& m) {
     for (size_t i = 0; i < rows; i++)
       for (size_t j = 0; j < cols; j++) {
         const int mat = m.props_keys[src[(size_t)k * rows * cols + i * cols + j]];  // x fastest in the file
-        for (unsigned kk = ref * k; kk < ref * (k + 1); kk++)
+        const unsigned kref = m.dim2 ? 1u : ref;  // a 2D image is refined in its plane only
+        for (unsigned kk = kref * k; kk < kref * (k + 1); kk++)
           for (unsigned ii = ref * i; ii < ref * (i + 1); ii++)
             for (unsigned jj = ref * j; jj < ref * (j + 1); jj++) m.elem_mat[ii + jj * R + (size_t)kk * R * C] = (uint16_t)mat;
       }
@@ -286,19 +288,22 @@ cudapcgFlag_t model_ctor(cudapcgModel_t** ptr, const void* data) {
   p->parStrategy_flag = (cudapcgFlag_t)g_par;
   p->poremap_flag = (cudapcgFlag_t)g_poremap;
   p->parametric_density_field_flag = m.sdf.empty() ? 0 : 1;  // femhmg.c:67
-  p->nrows = m.ny; p->ncols = m.nx; p->nlayers = m.nz;
+  p->nrows = m.ny; p->ncols = m.nx; p->nlayers = m.dim2 ? 0 : m.nz;
   p->nelem = (unsigned)m.N;
   p->nvars = (unsigned)m.ndof;
   p->nvarspernode = 3;
   p->nkeys = m.analysis == FLUID ? 1 : m.nmat;
-  p->localmtxdim = m.analysis == THERMAL ? 40 : (m.analysis == ELASTIC ? 576 : 1024);
+  p->localmtxdim = m.dim2 ? (m.analysis == THERMAL ? 16 : 64) : (m.analysis == THERMAL ? 40 : (m.analysis == ELASTIC ? 576 : 1024));
   p->nporenodes = (unsigned)m.nV;
   p->nbordernodes = (unsigned)m.nB;
   p->nhmgvars = m.analysis == FLUID ? (unsigned)(3 * m.nV) : (unsigned)m.ndof;
   return CUDAPCG_TRUE;
 }
 
-int pcg_flag_of(const Model& m) { return m.analysis == THERMAL ? CUDAPCG_THERMAL_3D : (m.analysis == ELASTIC ? CUDAPCG_ELASTIC_3D : CUDAPCG_FLUID_3D); }
+int pcg_flag_of(const Model& m) {
+  if (m.dim2) return m.analysis == THERMAL ? CUDAPCG_THERMAL_2D : (m.analysis == ELASTIC ? CUDAPCG_ELASTIC_2D : CUDAPCG_FLUID_2D);
+  return m.analysis == THERMAL ? CUDAPCG_THERMAL_3D : (m.analysis == ELASTIC ? CUDAPCG_ELASTIC_3D : CUDAPCG_FLUID_3D);
+}
 
 const char* DIR_STR[6] = {"X", "Y", "Z", "YZ (shear)", "XZ (shear)", "XY (shear)"};
 
@@ -353,7 +358,7 @@ bool setup_solver(Model& m, bool coarse = false) {
   if (m.analysis != FLUID) {
     // femhmg.c:1000-1004: node keys for NBN, the per-voxel material map for EBE; without host
     // maps the device builds the keys from the colours
-    if (g_par == CUDAPCG_NBN && !m.host_maps) {
+    if (g_par == CUDAPCG_NBN && !m.host_maps && !m.dim2) {
       int lut[256];
       for (int c = 0; c < 256; c++) lut[c] = m.props_keys[c];
       ok = cudapcgB200SetImageColors(m.colors.data(), m.frows, m.fcols, m.fslices, m.refinement, lut);
@@ -400,10 +405,15 @@ logical hmgInit(char* data_filename, char* elem_filename, char* sdf_filename, ui
     const size_t L = strlen(elem_filename);
     if (L < 4 || strcmp(elem_filename + L - 4, ".raw")) { fail(std::string("file ") + elem_filename + " is not in a valid format (.raw)"); delete m; return 0; }
   }
-  m->nd = m->analysis == ELASTIC ? 3 : 1;
-  m->C_dim = m->analysis == ELASTIC ? 36 : 9;
+  m->nd = m->analysis == ELASTIC ? (m->dim2 ? 2 : 3) : 1;
+  m->C_dim = (unsigned)(tensor_dim(*m) * tensor_dim(*m));
   if (!read_colors(*m, data, elem_filename)) { delete m; return 0; }
-  if (m->analysis == FLUID) {
+  if (m->dim2) {
+    // 2D: the node keys (4 bits per pixel) are built on the host
+    if (m->analysis == FLUID) { fail("2D permeability analysis is not provided by chfem_b200"); delete m; return 0; }
+    if (sdf_filename) { fail("a scalar density field is not provided for 2D images"); delete m; return 0; }
+    if (!ensure_host_maps(*m)) { delete m; return 0; }
+  } else if (m->analysis == FLUID) {
     // the sizes of the DOF numbering here; the numbering itself on the device at upload
     // (cudapcgB200SetPoreImageColors), or on the host for the paths that read the maps
     build_elem_mat(*m);
@@ -465,6 +475,11 @@ void hmgFindInitialGuesses(unsigned int nlevels) {
     fail("recursive initial guesses (-r) are not provided with a scalar density field");
     return;
   }
+  if (fine.dim2) {
+    SAY("WARNING: Initial guess estimation is not provided by chfem_b200 for 2D images.\n");
+    SAY("         Null initial guess will be considered (x0 = [0]).\n");
+    return;
+  }
   if (fine.analysis == FLUID) {  // femhmg.c:565-570
     SAY("WARNING: Initial guess estimation is not yet available for permeability analysis.\n");
     SAY("         Null initial guess will be considered (x0 = [0]).\n");
@@ -523,8 +538,9 @@ void hmgFindInitialGuesses(unsigned int nlevels) {
 }
 void hmgSetHomogenizationFlag(hmgFlag_t flag) {
   if (!g_m) return;
-  const int maxdir = g_m->analysis == ELASTIC ? 5 : 2;
+  const int maxdir = g_m->analysis == ELASTIC ? 5 : (g_m->dim2 ? 1 : 2);
   if (flag > maxdir) { g_dir_set = 0; return; }
+  if (g_m->dim2 && g_m->analysis == ELASTIC && flag > 1 && flag != 5) { g_dir_set = 0; return; }  // femhmg.c:536-541
   g_dir_set = 1;
   g_dir = flag;
 }
@@ -534,6 +550,10 @@ void hmgSolveHomogenization(void) {
   Model& m = *g_m;
   if (!m.sdf.empty() && (g_export_fields || m.has_thermal_expansion)) {
     fail("field export and thermal expansion are not provided with a scalar density field");
+    return;
+  }
+  if (m.dim2 && (g_export_fields || m.has_thermal_expansion)) {
+    fail("field export and thermal expansion are not provided for 2D images");
     return;
   }
   const auto t_all = std::chrono::steady_clock::now();
@@ -564,7 +584,7 @@ void hmgSolveHomogenization(void) {
   // per iteration for all of them).  Same per-case recurrence, stopping test and results.
   // (a scalar density field runs the one-by-one host path: right-hand sides and tensor terms
   // scaled per voxel on the host)
-  const bool block = g_multirhs && !two_vector && m.sdf.empty() && ((m.analysis != FLUID && !(g_solver & 1) &&
+  const bool block = g_multirhs && !two_vector && m.sdf.empty() && !m.dim2 && ((m.analysis != FLUID && !(g_solver & 1) &&
                                      ((m.analysis == THERMAL && nd == 3) || (m.analysis == ELASTIC && (nd == 6 || nd == 3)))) ||
                                     (m.analysis == FLUID && (g_solver & 1) && nd == 3));
   if (block) {
@@ -633,7 +653,7 @@ void hmgSolveHomogenization(void) {
   }
   // One-by-one path: right-hand side, solution and tensor volume term stay on the device unless
   // x must come back to the host (-xo, -e: the solution files are written from it).
-  const bool on_device = !g_export_x && !g_export_fields && m.sdf.empty();
+  const bool on_device = !g_export_x && !g_export_fields && m.sdf.empty() && !m.dim2;
   if (!block) {  // host vectors (and, for the host path, maps) of the one-by-one path
     if (!on_device && !ensure_host_maps(m)) { cudapcgEnd(); return; }
     m.rhs.assign(on_device ? 0 : m.ndof, 0.0);
@@ -750,9 +770,9 @@ void hmgSolveHomogenization(void) {
 void hmgPrintModelData(void) {
   if (!g_m || g_quiet) return;
   const Model& m = *g_m;
-  static const char* AN[3] = {"THERMAL_3D", "ELASTIC_3D", "FLUID_3D"};
+  static const char* AN[6] = {"THERMAL_3D", "ELASTIC_3D", "FLUID_3D", "THERMAL_2D", "ELASTIC_2D", "FLUID_2D"};
   static const char* SO[6] = {"CG", "MINRES", "CG3", "MINRES3", "CG2", "MINRES2"};
-  printf("*******************************************************\nMODEL DATA:\nAnalysis: %s\n", AN[m.analysis]);
+  printf("*******************************************************\nMODEL DATA:\nAnalysis: %s\n", AN[m.analysis + (m.dim2 ? 3 : 0)]);
   printf("Number of voxels (x,y,z): [%u,%u,%u]\nNumber of voxels (total): %ld\n", m.nx, m.ny, m.nz, m.N);
   if (m.analysis == FLUID)
     printf("  | porosity: %05.2f%%\n  | within pores: %ld\n  | at interfaces: %ld\n", 100.0 * m.nporeelem / (double)m.N, m.nV, m.nB);
@@ -766,7 +786,7 @@ void hmgPrintConstitutiveMtx(void) {
   if (!g_m) return;
   const Model& m = *g_m;
   static const char* NAME[3] = {"Thermal Conductivity", "Elasticity", "Permeability"};
-  const int n = m.analysis == ELASTIC ? 6 : 3;
+  const int n = tensor_dim(m);
   printf("-------------------------------------------------------\nHomogenized Constitutive Matrix (%s):\n", NAME[m.analysis]);
   for (int i = 0; i < n; i++) {
     for (int j = 0; j < n; j++) printf("  %.8e", m.C[i * n + j]);
@@ -912,7 +932,7 @@ int chfemB200Run(const uint8_t* voxels, const char* nf, int direction, int solve
   hmgPrintModelData();
   hmgSolveHomogenization();
   if (!g_err.empty()) return 0;
-  const int n = g_m->analysis == ELASTIC ? 6 : 3;
+  const int n = tensor_dim(*g_m);
   memcpy(C_out, g_m->C, sizeof(double) * n * n);
   return n;
 }

@@ -1,4 +1,5 @@
-// hmg.h -- internal model of the chfem_b200 host layer (3D thermal / elastic / Stokes).
+// hmg.h -- internal model of the chfem_b200 host layer (3D thermal / elastic / Stokes, 2D
+// thermal / elastic).
 //
 // Index conventions are chfem's (chfem/src/femhmg/femhmg.c:1644-1709,
 // physical_phenomena/femhmg_3D.c:4-75): voxel and node index i = row + col*ny + layer*ny*nx,
@@ -18,6 +19,7 @@ enum Analysis { THERMAL = 0, ELASTIC = 1, FLUID = 2 };
 struct Model {
   // settings (.nf, femhmg.c:1456-1586)
   int analysis = -1;
+  bool dim2 = false;                 // 2D image (%image_dimensions with 0 layers): pixels, nz = 1
   int solver_flag = 0;
   double voxel = 1.0;
   double tol = 1e-6;
@@ -35,7 +37,7 @@ struct Model {
   // sizes
   long N = 0;                        // voxels = periodic nodes
   long ndof = 0;
-  unsigned nd = 1;                   // DOF per node (thermal 1, elastic 3; Stokes layout is special)
+  unsigned nd = 1;                   // DOF per node (thermal 1, elastic 3 (2D: 2); Stokes layout is special)
   unsigned C_dim = 9;
   // the image as read: one colour byte per voxel of the file, x fastest (refinement not applied)
   std::vector<uint8_t> colors;
@@ -51,7 +53,7 @@ struct Model {
   std::vector<uint8_t> border_keys;  // Stokes: fluid keys of interface nodes
   long nV = 0, nB = 0, nporeelem = 0;
   // local matrices in the cudapcg formats, and the stress (flux, velocity) averaging matrices
-  std::vector<double> lcl;           // thermal 40/mat, elastic 576/mat, Stokes 1024
+  std::vector<double> lcl;           // thermal 40/mat, elastic 576/mat, Stokes 1024; 2D: dense 16 / 64 per mat
   std::vector<double> CB;            // thermal 8x3 (avg gradient)*k per mat, elastic 6x24 per mat, Stokes 3x24
   std::vector<double> Kdense;        // dense element matrices (8nd x 8nd per material; Stokes 32x32)
   // scalar density field (-f): per model voxel a 16-bit code q; the voxel's element matrix is
@@ -85,6 +87,10 @@ void update_C_from_volume(Model& m, int direction, const double* volume);
 void case_axis(const Model& m, int direction, int& axis, int& comp);
 long axis_len(const Model& m, int axis);
 int load_case_count(const Model& m);
+// number of flux / stress components of the tensor (thermal 3, elastic 6; 2D: 2, 3)
+int tensor_dim(const Model& m);
+// column of the effective tensor that load case `direction` fills (2D elastic XY: 2)
+int tensor_column(const Model& m, int direction);
 void load_case_list(const Model& m, int* dirs);
 
 }  // namespace chfem_host

@@ -1,5 +1,5 @@
-// hmg_physics.cpp -- 3D physics of the chfem_b200 host layer: node keys and pore maps,
-// element matrices, right-hand sides and effective-tensor updates.
+// hmg_physics.cpp -- physics of the chfem_b200 host layer: node keys and pore maps, element
+// matrices, right-hand sides and effective-tensor updates (3D; 2D thermal and elastic at the end).
 //
 // Reference behaviour followed (chfem/src/femhmg/physical_phenomena/):
 //   node keys ................. femhmg_3D.c:19-75
@@ -21,6 +21,7 @@
 #include "hmg.h"
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <omp.h>
 
@@ -96,7 +97,13 @@ bool count_pore_nodes(Model& m, std::string& err) {
   return true;
 }
 
+static bool build_maps_2d(Model& m, std::string& err);
+static void build_local_matrices_2d(Model& m);
+static void assemble_rhs_2d(const Model& m, int dir, double* rhs);
+static void update_C_2d(Model& m, int dir, const double* x);
+
 bool build_maps(Model& m, std::string& err) {
+  if (m.dim2) return build_maps_2d(m, err);
   const long R = m.ny, C = m.nx, L = m.nz, N = m.N;
   if (m.analysis != FLUID) {
     if (m.nmat > 4) { err = "more than 4 materials cannot be encoded in 16-bit node keys"; return false; }
@@ -136,6 +143,7 @@ bool build_maps(Model& m, std::string& err) {
 
 // ---- element matrices -------------------------------------------------------------------
 void build_local_matrices(Model& m) {
+  if (m.dim2) { build_local_matrices_2d(m); return; }
   QP q[8];
   gauss(q);
   double phi[8][8], grad[8][8][3];  // [qp][node]
@@ -243,13 +251,18 @@ void build_local_matrices(Model& m) {
 }
 
 // ---- load cases -----------------------------------------------------------------------
-int load_case_count(const Model& m) { return m.analysis == ELASTIC ? 6 : 3; }
+// 2D: thermal X, Y; elastic X, Y, XY (direction flags 0, 1, 5; femhmg.c:868-896)
+int load_case_count(const Model& m) { return m.dim2 ? (m.analysis == ELASTIC ? 3 : 2) : (m.analysis == ELASTIC ? 6 : 3); }
 void load_case_list(const Model& m, int* dirs) {
   for (int i = 0; i < load_case_count(m); i++) dirs[i] = i;
+  if (m.dim2 && m.analysis == ELASTIC) dirs[2] = 5;
 }
+int tensor_dim(const Model& m) { return m.dim2 ? (m.analysis == ELASTIC ? 3 : 2) : (m.analysis == ELASTIC ? 6 : 3); }
+int tensor_column(const Model& m, int dir) { return (m.dim2 && dir == 5) ? 2 : dir; }
 // (axis of the jump, displaced component) of a load case; X Y Z YZ XZ XY
 void case_axis(const Model& m, int dir, int& axis, int& comp) {
   if (m.analysis != ELASTIC) { axis = dir; comp = 0; return; }
+  if (m.dim2) { axis = dir == 0 ? 0 : 1; comp = dir == 1 ? 1 : 0; return; }
   static const int AX[6] = {0, 1, 2, 1, 2, 1}, CO[6] = {0, 1, 2, 2, 0, 0};
   axis = AX[dir]; comp = CO[dir];
 }
@@ -267,6 +280,7 @@ static void for_boundary_voxels(const Model& m, int axis, F f) {
 }
 
 void assemble_rhs(const Model& m, int dir, double* rhs) {
+  if (m.dim2) { assemble_rhs_2d(m, dir, rhs); return; }
   std::memset(rhs, 0, sizeof(double) * m.ndof);
   const long R = m.ny, C = m.nx, L = m.nz;
   if (m.analysis == FLUID) {  // unit body force along dir: int(phi_a) at every pore-node velocity
@@ -301,6 +315,7 @@ void assemble_rhs(const Model& m, int dir, double* rhs) {
 }
 
 void update_C(Model& m, int dir, const double* x) {
+  if (m.dim2) { update_C_2d(m, dir, x); return; }
   const long R = m.ny, C = m.nx, L = m.nz, N = m.N;
   if (m.analysis == FLUID) {
     double c0 = 0, c1 = 0, c2 = 0;
@@ -449,6 +464,151 @@ void update_C_from_volume(Model& m, int dir, const double* volume) {
       for (int s = 0; s < ns; s++) acc[s] += CB[s * ec + FACE[axis][f] * nd + comp] * jump;
   });
   for (int s = 0; s < ns; s++) m.C[s * ns + dir] = acc[s] / (double)m.N;
+}
+
+// ---- 2D: pixel images (femhmg_2D.c, femhmg_thermal_2D.c, femhmg_elastic_2D.c) ----------
+// A pixel (r, c) has its local node k at node (r + 1 + drow(k), c + dcol(k)), k = 0..3 (left
+// bottom, right bottom, right top, left top; x = +col, y = -row); node (r, c) is local node e of
+// pixel (r - drow(e) - 1, c - dcol(e)).  Node keys hold a pixel's material in 4 bits per local
+// index (16 materials).  Element matrices are integrated with 2 x 2 Gauss points on the unit
+// square; elasticity is plane strain (the reference's default build) unless
+// CHFEM_B200_PLANE_STRESS=1 (its ELASTIC_2D_PLANESTRESS build).
+static inline long elem_node_2d(long r, long c, int k, long R, long C) { return wrapl(r + 1 + drow(k), R) + wrapl(c + dcol(k), C) * R; }
+static inline long node_elem_2d(long r, long c, int e, long R, long C) { return wrapl(r - drow(e) - 1, R) + wrapl(c - dcol(e), C) * R; }
+static const int FACE2D[2][2] = {{1, 2}, {2, 3}};  // local nodes on the +x and +y sides
+
+static bool build_maps_2d(Model& m, std::string& err) {
+  const long R = m.ny, C = m.nx, N = m.N;
+  if (m.analysis == FLUID) { err = "2D permeability analysis is not provided by chfem_b200"; return false; }
+  if (m.nmat > 16) { err = "more than 16 materials cannot be encoded in 16-bit 2D node keys"; return false; }
+  m.keys.assign(N, 0);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < N; i++) {
+    const long r = i % R, c = i / R;
+    unsigned k = 0;
+    for (int e = 0; e < 4; e++) k |= ((unsigned)m.elem_mat[node_elem_2d(r, c, e, R, C)] & 15u) << (4 * e);
+    m.keys[i] = (uint16_t)k;
+  }
+  m.ndof = N * m.nd;
+  return true;
+}
+
+static void build_local_matrices_2d(Model& m) {
+  const double g[2] = {0.5 - 0.5 / std::sqrt(3.0), 0.5 + 0.5 / std::sqrt(3.0)};
+  double grad[4][4][2];  // [qp][node][x, y]
+  for (int q = 0; q < 4; q++) {
+    const double px = g[q & 1], py = g[q >> 1];
+    for (int a = 0; a < 4; a++) {
+      const int cx = nxi(a), cy = neta(a);
+      grad[q][a][0] = df1(cx) * f1(cy, py);
+      grad[q][a][1] = f1(cx, px) * df1(cy);
+    }
+  }
+  const int nd = m.nd, ed = 4 * nd;
+  m.lcl.assign((size_t)ed * ed * m.nmat, 0.0);
+  if (m.analysis == THERMAL) {
+    m.CB.assign((size_t)8 * m.nmat, 0.0);  // [mat][flux s][node a]
+    for (unsigned k = 0; k < m.nmat; k++) {
+      const double kp = m.props[k];
+      for (int q = 0; q < 4; q++)
+        for (int a = 0; a < 4; a++) {
+          for (int b = 0; b < 4; b++)
+            m.lcl[16 * k + 4 * a + b] += 0.25 * kp * (grad[q][a][0] * grad[q][b][0] + grad[q][a][1] * grad[q][b][1]);
+          for (int s = 0; s < 2; s++) m.CB[8 * k + 4 * s + a] += 0.25 * kp * grad[q][a][s];
+        }
+    }
+  } else {
+    const char* ps = getenv("CHFEM_B200_PLANE_STRESS");
+    const bool stress = ps && ps[0] == '1';
+    m.CB.assign((size_t)24 * m.nmat, 0.0);  // [mat][stress s (xx, yy, xy)][dof]
+    for (unsigned k = 0; k < m.nmat; k++) {
+      const double E = m.props[2 * k], nu = m.props[2 * k + 1];
+      double D[3][3] = {{0}};
+      if (stress) {
+        const double f = E / (1.0 - nu * nu);
+        D[0][0] = D[1][1] = f; D[0][1] = D[1][0] = f * nu; D[2][2] = f * 0.5 * (1.0 - nu);
+      } else {
+        const double lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), mu = E / (2.0 * (1.0 + nu));
+        D[0][0] = D[1][1] = lam + 2.0 * mu; D[0][1] = D[1][0] = lam; D[2][2] = mu;
+      }
+      for (int q = 0; q < 4; q++) {
+        double B[3][8] = {{0}};
+        for (int a = 0; a < 4; a++) {
+          B[0][2 * a] = grad[q][a][0];
+          B[1][2 * a + 1] = grad[q][a][1];
+          B[2][2 * a] = grad[q][a][1]; B[2][2 * a + 1] = grad[q][a][0];
+        }
+        double DB[3][8];
+        for (int r = 0; r < 3; r++)
+          for (int c = 0; c < 8; c++) DB[r][c] = D[r][0] * B[0][c] + D[r][1] * B[1][c] + D[r][2] * B[2][c];
+        for (int i = 0; i < 8; i++)
+          for (int j = 0; j < 8; j++) m.lcl[64 * k + 8 * i + j] += 0.25 * (B[0][i] * DB[0][j] + B[1][i] * DB[1][j] + B[2][i] * DB[2][j]);
+        for (int r = 0; r < 3; r++)
+          for (int c = 0; c < 8; c++) m.CB[24 * k + 8 * r + c] += 0.25 * DB[r][c];
+      }
+    }
+  }
+  m.Kdense = m.lcl;
+}
+
+// Pixels whose +axis side is the cell's +axis boundary: last column (x), first row (y)
+// (femhmg_thermal_2D.c:101-140)
+template <typename F>
+static void for_boundary_pixels(const Model& m, int axis, F f) {
+  const long R = m.ny, C = m.nx;
+  if (axis == 0) { for (long r = 0; r < R; r++) f(r, C - 1); }
+  else { for (long c = 0; c < C; c++) f(0, c); }
+}
+
+static void assemble_rhs_2d(const Model& m, int dir, double* rhs) {
+  std::memset(rhs, 0, sizeof(double) * m.ndof);
+  const long R = m.ny, C = m.nx;
+  int axis, comp;
+  case_axis(m, dir, axis, comp);
+  const double jump = (double)(axis == 0 ? m.nx : m.ny);
+  const int nd = m.nd, ed = 4 * nd;
+  for_boundary_pixels(m, axis, [&](long r, long c) {
+    const double* K = m.Kdense.data() + (size_t)m.elem_mat[r + c * R] * ed * ed;
+    for (int a = 0; a < 4; a++) {
+      const long n = elem_node_2d(r, c, a, R, C);
+      for (int ci = 0; ci < nd; ci++) {
+        double s = 0.0;
+        for (int f = 0; f < 2; f++) s += K[(a * nd + ci) * ed + FACE2D[axis][f] * nd + comp];
+        rhs[n * nd + ci] -= s * jump;
+      }
+    }
+  });
+}
+
+static void update_C_2d(Model& m, int dir, const double* x) {
+  const long R = m.ny, C = m.nx, N = m.N;
+  int axis, comp;
+  case_axis(m, dir, axis, comp);
+  const double jump = (double)(axis == 0 ? m.nx : m.ny);
+  const int nd = m.nd, ns = tensor_dim(m), ec = 4 * nd, col = tensor_column(m, dir);
+  double acc[3] = {0, 0, 0};
+#pragma omp parallel
+  {
+    double loc[3] = {0, 0, 0};
+#pragma omp for schedule(static)
+    for (long e = 0; e < N; e++) {
+      const long r = e % R, c = e / R;
+      const double* CB = m.CB.data() + (size_t)m.elem_mat[e] * ns * ec;
+      for (int a = 0; a < 4; a++) {
+        const long n = elem_node_2d(r, c, a, R, C);
+        for (int ci = 0; ci < nd; ci++)
+          for (int s = 0; s < ns; s++) loc[s] += CB[s * ec + a * nd + ci] * x[n * nd + ci];
+      }
+    }
+#pragma omp critical
+    for (int s = 0; s < ns; s++) acc[s] += loc[s];
+  }
+  for_boundary_pixels(m, axis, [&](long r, long c) {
+    const double* CB = m.CB.data() + (size_t)m.elem_mat[r + c * R] * ns * ec;
+    for (int f = 0; f < 2; f++)
+      for (int s = 0; s < ns; s++) acc[s] += CB[s * ec + FACE2D[axis][f] * nd + comp] * jump;
+  });
+  for (int s = 0; s < ns; s++) m.C[s * ns + col] = acc[s] / (double)N;
 }
 
 }  // namespace chfem_host

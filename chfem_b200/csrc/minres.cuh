@@ -22,6 +22,7 @@ struct MrDirTe {
   const uint16_t* keys; const T* Kd; int nmat;
   long N;
   DevScalars* sc; RedCtl rc; int precond;
+  const double* invd = nullptr;  // precomputed inverse Jacobi diagonal (density field, 2D models)
 };
 
 template <int ND, typename T>
@@ -39,7 +40,10 @@ __global__ void __launch_bounds__(PW_NT) k_te_mr_dir(MrDirTe<ND, T> a) {
   double sum = 0.0;
   for (long i = blockIdx.x * (long)PW_NT + threadIdx.x; i < a.N; i += (long)gridDim.x * PW_NT) {
     T inv[ND];
-    if (a.precond) te_invdiag<ND, T>(sD, a.keys[i], inv);
+    if (a.precond && a.invd) {
+#pragma unroll
+      for (int c = 0; c < ND; c++) inv[c] = T(a.invd[i * ND + c]);
+    } else if (a.precond) te_invdiag<ND, T>(sD, a.keys[i], inv);
     else {
 #pragma unroll
       for (int c = 0; c < ND; c++) inv[c] = T(1);

@@ -26,6 +26,18 @@ static bool launch_mr_op_buf(const T* rin, T* rout, const T* q, T* s, double* x,
     if (!ensure_reduction(g)) return false;
     a.rc = redctl(g);
     k_fl_apply<T, TE_MR><<<g, FL_NT, 0, S->stream>>>(a);
+  } else if (S->dim2) {
+    const int nb = d2_ctas();
+    if (!ensure_reduction(nb)) return false;
+    if (S->nd == 1) {
+      TeArgs<1, T> a{rin, q, rout, s, x, d, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, 1, S->cur_sc, redctl(nb), fin, skip_if_done, cfg};
+      a.invd = S->d_invd;
+      k_2d_apply<1, T, TE_MR><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<1, T>(), S->stream>>>(a);
+    } else {
+      TeArgs<2, T> a{rin, q, rout, s, x, d, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, 1, S->cur_sc, redctl(nb), fin, skip_if_done, cfg};
+      a.invd = S->d_invd;
+      k_2d_apply<2, T, TE_MR><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<2, T>(), S->stream>>>(a);
+    }
   } else if (asm_applies()) {
     int nb;
     cudaError_t e;
@@ -51,6 +63,7 @@ static bool launch_mr_op_buf(const T* rin, T* rout, const T* q, T* s, double* x,
       if (!ensure_reduction(nb)) return false;
       TeArgs<1, T> a{rin, q, rout, s, x, d, S->d_keys, Kdev<T>(), S->nmat,
                      S->R, S->C, S->L, S->cur_sc, redctl(nb), fin, skip_if_done, cfg};
+      sdf_args(a);
       k_te_apply<1, T, TE_MR><<<nb, block, sm, S->stream>>>(a);
     } else {
       const size_t sm = te_smem_bytes<3, T>(S->nmat);
@@ -58,6 +71,7 @@ static bool launch_mr_op_buf(const T* rin, T* rout, const T* q, T* s, double* x,
       if (!ensure_reduction(nb)) return false;
       TeArgs<3, T> a{rin, q, rout, s, x, d, S->d_keys, Kdev<T>(), S->nmat,
                      S->R, S->C, S->L, S->cur_sc, redctl(nb), fin, skip_if_done, cfg};
+      sdf_args(a);
       k_te_apply<3, T, TE_MR><<<nb, block, sm, S->stream>>>(a);
     }
   }
@@ -79,11 +93,14 @@ static bool launch_mr_dir(const T* rcur) {
   } else {
     const int g = pw_grid(S->N);
     if (!ensure_reduction(g)) return false;
-    if (S->nd == 1) {
-      MrDirTe<1, T> a{(T*)S->d0, (T*)S->q, rcur, (const T*)S->s, S->d_keys, Kdev<T>(), S->nmat, S->N, S->cur_sc, redctl(g), S->precond};
+    if (S->dim2 && S->nd == 2) {  // 2D elastic: the Jacobi diagonal from invd only
+      MrDirTe<2, T> a{(T*)S->d0, (T*)S->q, rcur, (const T*)S->s, S->d_keys, Kdev<T>(), 0, S->N, S->cur_sc, redctl(g), S->precond, S->d_invd};
+      k_te_mr_dir<2, T><<<g, PW_NT, 0, S->stream>>>(a);
+    } else if (S->nd == 1) {
+      MrDirTe<1, T> a{(T*)S->d0, (T*)S->q, rcur, (const T*)S->s, S->d_keys, Kdev<T>(), S->dim2 ? 0 : S->nmat, S->N, S->cur_sc, redctl(g), S->precond, S->d_invd};
       k_te_mr_dir<1, T><<<g, PW_NT, 0, S->stream>>>(a);
     } else {
-      MrDirTe<3, T> a{(T*)S->d0, (T*)S->q, rcur, (const T*)S->s, S->d_keys, Kdev<T>(), S->nmat, S->N, S->cur_sc, redctl(g), S->precond};
+      MrDirTe<3, T> a{(T*)S->d0, (T*)S->q, rcur, (const T*)S->s, S->d_keys, Kdev<T>(), S->nmat, S->N, S->cur_sc, redctl(g), S->precond, S->d_invd};
       k_te_mr_dir<3, T><<<g, PW_NT, 0, S->stream>>>(a);
     }
   }

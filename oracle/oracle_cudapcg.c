@@ -11,8 +11,8 @@
  * Each function cites the reference file:line it follows (paths inside cortezpedro/chfem).
  * Scope: 3D thermal (1 DOF/node), 3D elastic (3 DOF/node), 3D Stokes with the DOF-number
  * pore map (CUDAPCG_POREMAP_NUM), including the 2-vector solvers with on-the-fly reduction of
- * the solution (CG2/PCG2/MINRES2/PMINRES2, Stokes).  2D analyses and the scalar-density-field
- * input are outside the hot path and rejected with an error.
+ * the solution (CG2/PCG2/MINRES2/PMINRES2, Stokes); the scalar density field (3D); 2D thermal
+ * (1 DOF/node) and 2D elastic (2 DOF/node) on pixel images.  2D Stokes is rejected.
  *
  * Operator restatement.  The reference applies A node-by-node: for node i and each of the
  * 8 voxels (elements) around it, i is local node e of element e, and the row block of the
@@ -60,7 +60,8 @@ static inline void neighbours27(int r, int c, int l, unsigned int R, unsigned in
 /* ------------------------------------------------------------------------------------ */
 typedef struct {
   cudapcgModel_t *model;
-  unsigned int analysis;   /* CUDAPCG_THERMAL_3D / ELASTIC_3D / FLUID_3D */
+  unsigned int analysis;   /* CUDAPCG_THERMAL_2D / 3D, ELASTIC_2D / 3D, FLUID_3D */
+  int dim2;                /* 2D analysis: pixel images, 4-node elements, 4-bit key fields */
   unsigned int par;        /* NBN / EBE */
   cudapcgTol_t tol;
   unsigned int maxit;
@@ -264,8 +265,59 @@ static void apply_fluid(const double *v, double *y) {
   }
 }
 
+/* 2D thermal / elastic (matrix_free.cu:70-95, :353-385): node i = (row, col) is local node e of
+   the pixel (row - DROW[e] - 1, col - DCOL[e]) and that pixel's local node b sits at
+   (row - DROW[e] + DROW[b], col - DCOL[e] + DCOL[b]); the key holds the pixel's material in bits
+   [4e, 4e + 4) (femhmg_2D.c:14-46); element matrices are dense (4 nd) x (4 nd), row-major. */
+static void apply_2d(const double *v, double *y) {
+  cudapcgModel_t *m = S->model;
+  const unsigned int R = m->nrows, C = m->ncols, N = R * C;
+  const unsigned int nd = (S->analysis == CUDAPCG_ELASTIC_2D) ? 2 : 1, ed = 4 * nd;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < (long)N; i++) {
+    const int r = (int)(i % R), c = (int)(i / R);
+    const unsigned int key = S->keys[i];
+    double acc[2] = {0, 0};
+    for (int e = 0; e < 4; e++) {
+      const double *K = S->Kd + (size_t)((key >> (4 * e)) & 15u) * ed * ed;
+      for (int b = 0; b < 4; b++) {
+        const unsigned int j = wrapi(r - DROW[e] + DROW[b], R) + wrapi(c - DCOL[e] + DCOL[b], C) * R;
+        for (unsigned int ci = 0; ci < nd; ci++)
+          for (unsigned int cj = 0; cj < nd; cj++) acc[ci] += K[(e * nd + ci) * ed + b * nd + cj] * v[(size_t)j * nd + cj];
+      }
+    }
+    for (unsigned int ci = 0; ci < nd; ci++) y[(size_t)i * nd + ci] = acc[ci];
+  }
+}
+/* 2D Jacobi (matrix_free.cu:51-68, :325-346): the node's diagonal entries over its 4 pixels */
+static void inv_diag_2d(double *dinv) {
+  cudapcgModel_t *m = S->model;
+  const unsigned int N = m->nrows * m->ncols;
+  const unsigned int nd = (S->analysis == CUDAPCG_ELASTIC_2D) ? 2 : 1, ed = 4 * nd;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < (long)N; i++) {
+    const unsigned int key = S->keys[i];
+    for (unsigned int ci = 0; ci < nd; ci++) {
+      double s = 0.0;
+      for (int e = 0; e < 4; e++) s += S->Kd[(size_t)((key >> (4 * e)) & 15u) * ed * ed + (e * nd + ci) * ed + e * nd + ci];
+      dinv[(size_t)i * nd + ci] = 1.0 / s;
+    }
+  }
+}
+/* 2D node key from a per-pixel material map (EBE input) */
+static void keys_from_elements_2d(const cudapcgMap_t *em, unsigned int R, unsigned int C, unsigned short *keys) {
+  for (long i = 0; i < (long)R * C; i++) {
+    const int r = (int)(i % R), c = (int)(i / R);
+    unsigned int k = 0;
+    for (int e = 0; e < 4; e++) k |= ((unsigned int)em[wrapi(r - DROW[e] - 1, R) + wrapi(c - DCOL[e], C) * R] & 15u) << (4 * e);
+    keys[i] = (unsigned short)k;
+  }
+}
+
 static void Aprod(const double *v, double *y) {
-  if (S->analysis == CUDAPCG_FLUID_3D) apply_fluid(v, y); else apply_thermal_elastic(v, y);
+  if (S->dim2) apply_2d(v, y);
+  else if (S->analysis == CUDAPCG_FLUID_3D) apply_fluid(v, y);
+  else apply_thermal_elastic(v, y);
 }
 /* Aprod with the reference's (scl, scl_prev) form: y = scl*A v + scl_prev*y (wrappers.cu:711-906). */
 static void Aprod_scl(const double *v, double scl, double scl_prev, double *y, double *tmp) {
@@ -279,6 +331,7 @@ static void Aprod_scl(const double *v, double scl, double scl_prev, double *y, d
 /* (matrix_free.cu:167-188 thermal, :388-408 elastic, :663-672 and :912-925 Stokes).       */
 static void inv_diag(double *dinv) {
   cudapcgModel_t *m = S->model;
+  if (S->dim2) { inv_diag_2d(dinv); return; }
   if (S->analysis == CUDAPCG_FLUID_3D) {
     const unsigned int nV = m->nporenodes, nB = m->nbordernodes;
     const double *K = S->Kd;
@@ -435,8 +488,9 @@ cudapcgFlag_t cudapcgEnd(void) {
 
 cudapcgFlag_t cudapcgInit(cudapcgFlag_t analysis_flag, cudapcgFlag_t par) {
   cudapcgEnd();
-  if (analysis_flag != CUDAPCG_THERMAL_3D && analysis_flag != CUDAPCG_ELASTIC_3D && analysis_flag != CUDAPCG_FLUID_3D) {
-    fprintf(stderr, "oracle: analysis %d is outside the 3D hot path\n", analysis_flag);
+  if (analysis_flag != CUDAPCG_THERMAL_3D && analysis_flag != CUDAPCG_ELASTIC_3D && analysis_flag != CUDAPCG_FLUID_3D &&
+      analysis_flag != CUDAPCG_THERMAL_2D && analysis_flag != CUDAPCG_ELASTIC_2D) {
+    fprintf(stderr, "oracle: analysis %d is not restated\n", analysis_flag);
     return CUDAPCG_FALSE;
   }
   if (analysis_flag == CUDAPCG_FLUID_3D && par != CUDAPCG_NBN) {
@@ -446,6 +500,7 @@ cudapcgFlag_t cudapcgInit(cudapcgFlag_t analysis_flag, cudapcgFlag_t par) {
   S = (oracle_solver_t *)calloc(1, sizeof(oracle_solver_t));
   if (!S) return CUDAPCG_FALSE;
   S->analysis = analysis_flag; S->par = par;
+  S->dim2 = (analysis_flag == CUDAPCG_THERMAL_2D || analysis_flag == CUDAPCG_ELASTIC_2D);
   S->tol = CUDAPCG_TOLERANCE; S->maxit = CUDAPCG_MAX_ITERATIONS;
   S->solver_flag = CUDAPCG_CG_SOLVER; S->precond = 1; S->resnorm = CUDAPCG_L2_NORM;
   S->xr_mode = CUDAPCG_XREDUCE_FULL; S->xr_shift = 0; S->xr_scale = 1.0;  /* cudapcg.cu:154-156 */
@@ -564,14 +619,15 @@ cudapcgFlag_t cudapcgSetImage(cudapcgMap_t *img) {
   capture(0, img, m->nelem);
   free(S->keys);
   S->keys = (unsigned short *)malloc(sizeof(unsigned short) * m->nelem);
-  if (S->par == CUDAPCG_EBE) keys_from_elements(img, m->nrows, m->ncols, m->nlayers, S->keys);
+  if (S->par == CUDAPCG_EBE && S->dim2) keys_from_elements_2d(img, m->nrows, m->ncols, S->keys);
+  else if (S->par == CUDAPCG_EBE) keys_from_elements(img, m->nrows, m->ncols, m->nlayers, S->keys);
   else for (unsigned int i = 0; i < m->nelem; i++) S->keys[i] = img[i];
   return 1;
 }
 /* cudapcg.cu:327-334: the density codes of every voxel and their range; a thermal model has one
    material (femhmg.c:256-262 normalises it), whose key is zero everywhere. */
 cudapcgFlag_t cudapcgSetParametricDensityField(parametricScalarField_t *f, double fmin, double fmax) {
-  if (!S || !S->model || !f) return 0;
+  if (!S || !S->model || !f || S->dim2) return 0;
   cudapcgModel_t *m = S->model;
   free(S->sdf);
   S->sdf = (parametricScalarField_t *)malloc(sizeof(parametricScalarField_t) * m->nelem);
@@ -609,7 +665,11 @@ cudapcgFlag_t cudapcgSetLclMtxs(cudapcgVar_t *L) {
   S->nkeys = m->nkeys;
   capture(4, L, m->nkeys * m->localmtxdim);
   free(S->Kd);
-  if (S->analysis == CUDAPCG_THERMAL_3D) {
+  if (S->analysis == CUDAPCG_THERMAL_2D || S->analysis == CUDAPCG_ELASTIC_2D) {  /* dense 4x4 / 8x8 */
+    S->ed = S->analysis == CUDAPCG_THERMAL_2D ? 4 : 8;
+    S->Kd = (double *)malloc(sizeof(double) * S->ed * S->ed * m->nkeys);
+    memcpy(S->Kd, L, sizeof(double) * S->ed * S->ed * m->nkeys);
+  } else if (S->analysis == CUDAPCG_THERMAL_3D) {
     S->ed = 8;
     S->Kd = (double *)malloc(sizeof(double) * 64 * m->nkeys);
     for (unsigned int k = 0; k < m->nkeys; k++) expand_sparseq1(L + 40 * k, S->Kd + 64 * k);

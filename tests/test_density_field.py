@@ -121,7 +121,13 @@ def test_density_of_ones_is_the_two_phase_model(tmp_path, analysis):
 
 
 @pytest.mark.gpu
-def test_density_field_rejects_minres(tmp_path):
-    nf, raw, fb = make_case(tmp_path, 0, (6, 6, 6), 1, "float32")
-    with pytest.raises(RuntimeError):
-        H.run_exec(H.CHFEM_EXEC, nf, raw, "-f", fb, "-s", "1")
+@pytest.mark.parametrize("analysis", [0, 1])
+def test_density_field_minres(tmp_path, analysis):
+    """(P)MINRES under a density field: the solutions of every load case equal the oracle's."""
+    nf, raw, fb = make_case(tmp_path, analysis, (6, 7, 8), 1, "float32")
+    Cref, xref, logref = _x_of(H.ORACLE_EXEC, nf, raw, fb, ["-s", "1"])
+    C, xs, log = _x_of(H.CHFEM_EXEC, nf, raw, fb, ["-s", "1"])
+    for a, b in zip(xs, xref):
+        assert H.rel_to_max(a, b) < 1e-6
+    its, its_ref = H.parse_iterations(log), H.parse_iterations(logref)
+    assert all(abs(a - b) <= 1 for a, b in zip(its, its_ref)), (its, its_ref)

@@ -1,0 +1,104 @@
+"""2D thermal and elastic homogenization on pixel images (chfem's femhmg_2D.c,
+femhmg_thermal_2D.c, femhmg_elastic_2D.c; operators matrix_free.cu:51-95, :325-385).
+
+The B200 path (k_2d_apply) against the reference's golden 2D tensors (test/input/2D, the
+reference's bar 1e-4) and against the oracle (the reference's host code with the CPU restatement
+of its 2D operators) on the same inputs: tensors 1e-6 in FP64 and 1e-4 in mixed precision,
+iteration counts within one, across the solvers, stopping norms, Jacobi on/off, node-by-node
+and element-by-element input, %refinement, thin images and 12 materials.
+"""
+import zlib
+
+import numpy as np
+import pytest
+
+from tests import helpers as H
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not H.oracle_available(), reason="oracle/_ref not built")]
+
+
+def _its_close(log, logref):
+    its, its_ref = H.parse_iterations(log), H.parse_iterations(logref)
+    assert len(its) == len(its_ref) and all(abs(a - b) <= 1 for a, b in zip(its, its_ref)), (its, its_ref)
+
+
+@pytest.mark.parametrize("name", ["thermal_2d", "elastic_2d"])
+@pytest.mark.parametrize("par", ["0", "1"])
+def test_2d_golden(tmp_path, name, par):
+    nf, raw, meta = H.golden_case_files(name, str(tmp_path))
+    C, log = H.run_exec(H.CHFEM_EXEC, nf, raw, "-p", par)
+    assert H.rel_to_max(C, meta["tensor"]) < meta["reference_tolerance"]
+    Cref, logref = H.run_exec(H.ORACLE_EXEC, nf, raw, "-p", par)
+    assert H.rel_to_max(C, Cref) < 1e-6
+    _its_close(log, logref)
+
+
+CASES = [
+    # name, analysis, shape (y, x), nmat, flags
+    ("t2_pcg", 0, (37, 45), 3, []),
+    ("t2_cg", 0, (20, 33), 2, ["-j", "0"]),
+    ("t2_minres", 0, (16, 40), 4, ["-s", "1"]),
+    ("t2_cg3_inf", 0, (24, 24), 2, ["-s", "2", "-c", "1"]),
+    ("t2_thin", 0, (1, 50), 2, []),
+    ("e2_pcg", 1, (33, 29), 2, []),
+    ("e2_minres", 1, (18, 22), 3, ["-s", "1"]),
+    ("e2_cg3_err", 1, (26, 20), 2, ["-s", "2", "-c", "2"]),
+    ("e2_many", 1, (30, 31), 12, []),
+    ("e2_ebe", 1, (21, 17), 3, ["-p", "1"]),
+]
+
+
+def _case(tmp_path, name, analysis, shape, nmat, refinement=1):
+    codes = list(range(0, 256, 256 // nmat))[:nmat] if nmat > 4 else None
+    img = H.small_image(shape, nmat, seed=zlib.crc32(name.encode()) % 10000, codes=codes)
+    props = None
+    if nmat > 4:
+        cs = sorted(np.unique(img).tolist())
+        props = {c: ((1.0 + i, 0.2 + 0.01 * i) if analysis == 1 else 1.0 + i) for i, c in enumerate(cs)}
+    return H.write_small_case(str(tmp_path), name, img, analysis, tol=1e-8, maxit=20000, refinement=refinement, props=props)
+
+
+@pytest.mark.parametrize("name,analysis,shape,nmat,flags", CASES)
+def test_2d_models_fp64(tmp_path, name, analysis, shape, nmat, flags):
+    nf, raw = _case(tmp_path, name, analysis, shape, nmat)
+    Cref, logref = H.run_exec(H.ORACLE_EXEC, nf, raw, *flags)
+    C, log = H.run_exec(H.CHFEM_EXEC, nf, raw, *flags)
+    assert H.rel_to_max(C, Cref) < 1e-6
+    _its_close(log, logref)
+
+
+@pytest.mark.parametrize("name,analysis,shape,nmat,flags", [c for c in CASES if c[0] in ("t2_pcg", "e2_pcg", "e2_minres")])
+def test_2d_models_mixed(tmp_path, name, analysis, shape, nmat, flags):
+    nf, raw = _case(tmp_path, name, analysis, shape, nmat)
+    Cref, _ = H.run_exec(H.ORACLE_EXEC, nf, raw, *flags)
+    C, _ = H.run_exec(H.CHFEM_EXEC, nf, raw, *flags, "--precision", "mixed")
+    assert H.rel_to_max(C, Cref) < 1e-4
+
+
+def test_2d_refinement_and_solution_files(tmp_path):
+    """%refinement 2 in the plane; -xo writes every load case's solution (2D elastic: X, Y, XY =
+    files _0, _1, _5) equal to the oracle's, and -xi of those files converges at once."""
+    nf, raw = _case(tmp_path, "e2_ref", 1, (9, 12), 2, refinement=2)
+    Cref, _ = H.run_exec(H.ORACLE_EXEC, nf, raw, "-xo")
+    xref = {d: np.fromfile(nf[:-3] + f"_X_{d}.bin") for d in (0, 1, 5)}
+    C, _ = H.run_exec(H.CHFEM_EXEC, nf, raw, "-xo")
+    assert H.rel_to_max(C, Cref) < 1e-6
+    for d in (0, 1, 5):
+        x = np.fromfile(nf[:-3] + f"_X_{d}.bin")
+        assert x.size == 2 * 18 * 24
+        assert H.rel_to_max(x, xref[d]) < 1e-6
+    C2, log = H.run_exec(H.CHFEM_EXEC, nf, raw, "-xi", nf[:-3] + "_X")
+    assert H.rel_to_max(C2, C) < 1e-6
+    assert all(i <= 1 for i in H.parse_iterations(log))
+
+
+def test_2d_compute_property():
+    """The Python API on a 2D array: tensors of the 2D shapes, symmetric stiffness."""
+    from chfem_b200 import compute_property
+    img = H.small_image((40, 36), 2, seed=11)
+    Kt = np.array(compute_property("conductivity", img, mat_props={0: 1.0, 255: 5.0}, solver_tolerance=1e-8))
+    assert Kt.shape == (2, 2)
+    Ce = np.array(compute_property("elasticity", img, mat_props={0: (1.0, 0.3), 255: (5.0, 0.2)}, solver_tolerance=1e-8))
+    assert Ce.shape == (3, 3)
+    assert np.allclose(Ce, Ce.T, rtol=1e-5, atol=1e-7 * np.abs(Ce).max())
+    assert Kt[0, 0] > 1.0 and Kt[1, 1] > 1.0

@@ -74,6 +74,35 @@ def test_thermal_elastic_maps_rhs_updateC(tmp_path, name, analysis, shape, nmat,
         assert H.rel_to_max(col_mine, col_ref) < 1e-12
 
 
+CASES_2D = [
+    # name, analysis, shape (y, x), nmat, directions (2D elastic: X, Y, XY = 0, 1, 5)
+    ("th2d2", 0, (9, 11), 2, [0, 1]),
+    ("th2d4", 0, (6, 5), 4, [1]),
+    ("el2d2", 1, (7, 10), 2, [0, 1, 5]),
+    ("el2d3", 1, (5, 4), 3, [5]),
+]
+
+
+@pytest.mark.parametrize("name,analysis,shape,nmat,dirs", CASES_2D)
+def test_2d_maps_rhs_updateC(tmp_path, name, analysis, shape, nmat, dirs):
+    """2D pixel models (femhmg_2D.c, femhmg_thermal_2D.c, femhmg_elastic_2D.c): 4-bit node keys
+    bit-exact, element matrices (dense 4x4 / 8x8, plane strain) and right-hand sides to round-off,
+    the tensor column from the reference's solution vector."""
+    img = H.small_image(shape, nmat, seed=zlib.crc32(name.encode()) % 1000)
+    nf, raw = H.write_small_case(str(tmp_path), name, img, analysis, tol=1e-6, maxit=50)
+    for d in dirs:
+        ref = H.oracle_capture(nf, raw, d)
+        lib, mine = host_arrays(nf, raw, d)
+        assert mine["info"][2] == 1
+        assert np.array_equal(mine[0], ref["0"]), "node material keys differ"
+        np.testing.assert_allclose(mine[4], ref["4"], rtol=1e-12, atol=1e-12 * np.abs(ref["4"]).max())
+        np.testing.assert_allclose(mine["rhs"], ref["5"], rtol=1e-11, atol=1e-11 * np.abs(ref["5"]).max())
+        C = updateC(lib, d, ref["6"])
+        k = 3 if analysis == 1 else 2
+        col = 2 if d == 5 else d
+        assert H.rel_to_max(C[: k * k].reshape(k, k)[:, col], ref["C"][: k * k].reshape(k, k)[:, col]) < 1e-12
+
+
 def test_fluid_maps_rhs_updateC(tmp_path):
     from chfem_b200.synthetic import pore_grf
     img = pore_grf((10, 12, 14), corr=2.0, porosity=0.45, seed=7)

@@ -1,5 +1,5 @@
 """The oracle (reference host code + CPU restatement of its solver) reproduces the reference's
-own golden effective-tensor columns (test/input/3D/*_result.bin) within the reference's
+own golden effective tensors (test/input/3D/*_result.bin, test/input/2D/*_result.bin) within the reference's
 regression tolerance of 1e-4 relative to the largest entry (test/test_chfem.c:5,340-351)."""
 import os
 
@@ -17,6 +17,15 @@ def test_oracle_matches_golden(tmp_path, name):
     C, out = H.run_exec(H.ORACLE_EXEC, nf, raw, "-d", meta["direction"], env={"OMP_NUM_THREADS": str(os.cpu_count() or 4)})
     col = C[:, meta["direction"]]
     assert H.rel_to_max(col, meta["column"]) < meta["reference_tolerance"]
+
+
+@pytest.mark.parametrize("name", ["thermal_2d", "elastic_2d"])
+@pytest.mark.parametrize("par", ["0", "1"])
+def test_oracle_matches_golden_2d(tmp_path, name, par):
+    """2D pixel models (test/input/2D): every load case, node-by-node and element-by-element."""
+    nf, raw, meta = H.golden_case_files(name, str(tmp_path))
+    C, out = H.run_exec(H.ORACLE_EXEC, nf, raw, "-p", par, env={"OMP_NUM_THREADS": str(os.cpu_count() or 4)})
+    assert H.rel_to_max(C, meta["tensor"]) < meta["reference_tolerance"]
 
 
 def test_oracle_standalone_builds():
