@@ -567,13 +567,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-check", action="store_true", help="skip the untimed reference run (tensor error, same-precision ratio)")
     ap.add_argument("--no-north-star", action="store_true", help="skip the 256^3 north-star sub-record of the default workload")
-    ap.add_argument("--kernel", type=int, default=0,
+    ap.add_argument("--kernel", type=int, default=None,
                     help="only time one kernel of the workload's resident model, 10 launches (for ncu captures): "
-                         "1 operator pass (PCG), 2 pointwise pass (PCG), 3 operator pass ((P)MINRES), "
-                         "5 block operator pass, 6 block pointwise pass")
+                         "0 plain operator pass, 1 operator pass (PCG), 2 pointwise pass (PCG), 3 operator pass "
+                         "((P)MINRES), 5 block operator pass, 6 block pointwise pass")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
-    if args.kernel:
+    if args.kernel is not None:
         kernel_only(w, args.workload, args.kernel)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))

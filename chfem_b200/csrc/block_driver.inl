@@ -41,7 +41,7 @@ static bool block_alloc(int nr) {
   // thermal / elastic: r, the direction's two buffers and q (s = M^-1 r is formed by the
   // operator pass); Stokes (P)MINRES also keeps s
   std::vector<void**> vs = {&B->r, &B->d0, &B->d1, &B->q};
-  if (S->analysis == CUDAPCG_FLUID_3D) vs.push_back(&B->s);
+  if (S->fluid) vs.push_back(&B->s);
   for (void** v : vs) { CKV(cudaMalloc(v, tot * sizeof(T))); CKV(cudaMemset(*v, 0, tot * sizeof(T))); }
   CKV(cudaMalloc(&B->x, tot * 8));
   CKV(cudaMalloc(&B->b64, tot * 8));
@@ -433,7 +433,7 @@ struct LoadCases {
 template <typename T>
 static bool rhs_on_device(const LoadCases& lc, int k) {
   const long n = S->nvars;
-  if (S->analysis == CUDAPCG_FLUID_3D) {
+  if (S->fluid) {
     double w = 0.0;
     for (int a = 0; a < 8; a++) w += lc.CB[72 + a];
     k_fl_rhs<T><<<pw_grid(n), PW_NT, 0, S->stream>>>(S->nV, n, lc.axis[k], w, slice<double>(B->b64, k), slice<T>(B->r, k));
@@ -454,9 +454,9 @@ static bool rhs_on_device(const LoadCases& lc, int k) {
 static bool moments_on_device(const LoadCases& lc, int nr) {
   if (!B->d_mom) CKV(cudaMalloc(&B->d_mom, (size_t)BLK_MAX * 8 * sizeof(double) + 4 * 6 * 24 * sizeof(double)));
   double* d_cb = B->d_mom + BLK_MAX * 8;
-  const int g = pw_grid(S->analysis == CUDAPCG_FLUID_3D ? S->nV : S->N);
+  const int g = pw_grid(S->fluid ? S->nV : S->N);
   if (!ensure_reduction(g)) return false;
-  if (S->analysis == CUDAPCG_FLUID_3D) {
+  if (S->fluid) {
     double w[3] = {0, 0, 0};
     for (int a = 0; a < 8; a++) { w[0] += lc.CB[3 * a]; w[1] += lc.CB[24 + 3 * a + 1]; w[2] += lc.CB[48 + 3 * a + 2]; }
     for (int k = 0; k < nr; k++) k_fl_moments<<<g, PW_NT, 0, S->stream>>>(slice<double>(B->x, k), S->nV, w[0], w[1], w[2], redctl(g), B->d_mom + 8 * k);
@@ -501,7 +501,7 @@ static bool solve_block_T(int nr, const double* const* rhs, const double* const*
     else CKV(cudaMemsetAsync(slice<double>(B->x, k), 0, n * 8, S->stream));
   }
   bool ok;
-  if (S->analysis == CUDAPCG_FLUID_3D) {
+  if (S->fluid) {
     if (nr != 3) { set_err("cudapcgB200SolveBlock", "Stokes blocks hold the 3 flow directions"); return false; }
     ok = solve_block_minres_device<T, 3>(has_x0);
   } else if (S->nd == 1 && nr == 3) ok = solve_block_device<1, T, 3>(has_x0);
@@ -512,7 +512,7 @@ static bool solve_block_T(int nr, const double* const* rhs, const double* const*
   if (!blk_read()) return false;
   for (int k = 0; k < nr; k++) {
     // a null right-hand side under (P)MINRES returns x = 0 as cudapcgSolve does
-    if (S->analysis == CUDAPCG_FLUID_3D && B->h_sc[k].status == 1) CKV(cudaMemsetAsync(slice<double>(B->x, k), 0, n * 8, S->stream));
+    if (S->fluid && B->h_sc[k].status == 1) CKV(cudaMemsetAsync(slice<double>(B->x, k), 0, n * 8, S->stream));
     if (x_out && x_out[k]) CKV(cudaMemcpyAsync(x_out[k], slice<double>(B->x, k), n * 8, cudaMemcpyDeviceToHost, S->stream));
   }
   if (lc && !moments_on_device(*lc, nr)) return false;
@@ -525,12 +525,12 @@ static bool solve_block_T(int nr, const double* const* rhs, const double* const*
     int found;
     if (h.status == 1) { res = 0.0; found = 1; }
     else if (h.status == 2) { res = h.metric; found = 1; }
-    else if (S->resnorm == CUDAPCG_L2_NORM && S->analysis != CUDAPCG_FLUID_3D) { res = sqrt(fabs(h.delta) / fabs(h.delta0)); found = !(fabs(h.delta) > S->tol * S->tol * fabs(h.delta0)); }
+    else if (S->resnorm == CUDAPCG_L2_NORM && !S->fluid) { res = sqrt(fabs(h.delta) / fabs(h.delta0)); found = !(fabs(h.delta) > S->tol * S->tol * fabs(h.delta0)); }
     else { res = h.metric; found = res <= S->tol; }
     if (iters) iters[k] = (unsigned)h.iteration;
     if (resid) resid[k] = res;
     // per right-hand side, the messages cudapcgSolve prints for a single solve
-    const char* name = S->analysis == CUDAPCG_FLUID_3D ? "MINRES" : (S->precond ? "PCG" : "CG");
+    const char* name = S->fluid ? "MINRES" : (S->precond ? "PCG" : "CG");
     if (h.status == 1) printf("%s[%d] Null solution satisfied %s.\n", S->header.c_str(), k, name);
     else if (h.status == 2) printf("%s[%d] Initial guess satisfied %s.\n", S->header.c_str(), k, name);
     else if (!getenv("CHFEM_B200_QUIET")) {

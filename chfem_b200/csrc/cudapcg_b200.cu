@@ -82,6 +82,8 @@ struct Solver {
   // configuration (cudapcg.cu:108-183 defaults)
   int analysis = 0, par = 0;
   bool dim2 = false;  // 2D thermal / elastic (pixel images, one layer, 4-bit key fields)
+  bool fluid = false; // Stokes (FLUID_3D or FLUID_2D)
+  int fdim = 3;       // Stokes: 3 (voxels) or 2 (pixels, one layer)
   double tol = 0.00001;
   unsigned maxit = 100000;
   int solver_flag = CUDAPCG_CG_SOLVER;
@@ -209,9 +211,12 @@ static void free_model_dev() {
   S->have_K = S->have_keys = S->have_maps = false;
 }
 
+// any 2D model (thermal, elastic or Stokes): the block, field, device load-case and
+// device-numbering entry points are 3D only
+static bool is2d() { return S->dim2 || (S->fluid && S->fdim == 2); }
 static bool minres_solver() { return S->solver_flag == CUDAPCG_MINRES_SOLVER || S->solver_flag == CUDAPCG_MINRES3_SOLVER; }
 // CG3 on thermal / elastic models: the 3-vector PCG (x, r and the direction's two buffers)
-static bool pcg3_solver() { return S->solver_flag == CUDAPCG_CG3_SOLVER && S->analysis != CUDAPCG_FLUID_3D; }
+static bool pcg3_solver() { return S->solver_flag == CUDAPCG_CG3_SOLVER && !S->fluid; }
 
 // An FP64 vector of nvars entries allocated on first use (staging and scratch; never called
 // while a stream capture is open).
@@ -233,7 +238,7 @@ template <typename T>
 static bool ensure_vectors() {
   const int p = prec_of<T>();
   const size_t n = std::max<size_t>((size_t)S->nvars, 1);
-  const int layout = p | (minres_solver() ? 0x10 : 0) | (pcg3_solver() ? 0x20 : 0) | (S->analysis == CUDAPCG_FLUID_3D ? 0x40 : 0);
+  const int layout = p | (minres_solver() ? 0x10 : 0) | (pcg3_solver() ? 0x20 : 0) | (S->fluid ? 0x40 : 0);
   const bool want_b64 = !(pcg3_solver() && p == CHFEM_B200_FP64);
   if (!S->x) {
     CKV(cudaMalloc(&S->x, n * 8));
@@ -253,7 +258,7 @@ static bool ensure_vectors() {
   free_work_vectors();
   std::vector<void**> vs = {&S->r, &S->d0, &S->d1};
   if (!pcg3_solver()) vs.push_back(&S->q);
-  if (S->analysis == CUDAPCG_FLUID_3D || minres_solver()) vs.push_back(&S->s);
+  if (S->fluid || minres_solver()) vs.push_back(&S->s);
   if (minres_solver()) { vs.push_back(&S->r2); vs.push_back(&S->q2); }
   for (void** v : vs) {
     CKV(cudaMalloc(v, n * sizeof(T)));
@@ -276,7 +281,7 @@ static bool ensure_vectors() {
 // Assembled neighbour blocks (stencil_asm.cuh) of a thermal/elastic model of at most two
 // materials; CHFEM_B200_BLOCK_OP=element keeps the element-by-element block operator.
 static bool asm_applies() {
-  if (S->analysis == CUDAPCG_FLUID_3D || S->dim2 || S->nmat > 2 || S->d_sdf) return false;
+  if (S->fluid || S->dim2 || S->nmat > 2 || S->d_sdf) return false;
   const char* e = getenv("CHFEM_B200_BLOCK_OP");
   return !(e && !strcmp(e, "element"));
 }
@@ -366,9 +371,9 @@ static bool ensure_K() {
   if (sizeof(T) == 8) S->d_K64 = (double*)dk; else S->d_K32 = (float*)dk;
   if (asm_applies() && !ensure_tab<T>()) return false;
   if ((S->d_sdf || S->dim2) && !ensure_invd()) return false;
-  if (S->analysis == CUDAPCG_FLUID_3D) {
-    if (sizeof(T) == 8) CKV(cudaMemcpyToSymbol(c_flK64, kt.data(), 1024 * sizeof(double)));
-    else CKV(cudaMemcpyToSymbol(c_flK32, kt.data(), 1024 * sizeof(float)));
+  if (S->fluid) {
+    if (sizeof(T) == 8) CKV(cudaMemcpyToSymbol(c_flK64, kt.data(), kt.size() * sizeof(double)));
+    else CKV(cudaMemcpyToSymbol(c_flK32, kt.data(), kt.size() * sizeof(float)));
   }
   return true;
 }
@@ -413,16 +418,16 @@ static int pw_grid(long n) {
 // Largest grid any pass of the current model launches (reduction partials are sized once,
 // before graph capture, which must not allocate).
 static int needed_blocks() {
-  long nb = pw_grid(S->analysis == CUDAPCG_FLUID_3D ? S->nV + S->nB : S->N);
+  long nb = pw_grid(S->fluid ? S->nV + S->nB : S->N);
   // stencil passes: at most 8 resident CTAs of TE_NT = 256 threads per SM
-  if (S->analysis != CUDAPCG_FLUID_3D) nb = std::max<long>(nb, 8L * num_sms());
+  if (!S->fluid) nb = std::max<long>(nb, 8L * num_sms());
   return (int)nb;
 }
 static RedCtl redctl(int nblocks) { return RedCtl{S->d_part, S->d_ticket, nblocks}; }
 static SolveCfg solvecfg() {
   SolveCfg c;
   c.tol = S->tol; c.maxit = (int)std::min<unsigned>(S->maxit, 0x7fffffffu); c.norm = S->resnorm; c.precond = S->precond;
-  c.nhmg = (S->analysis == CUDAPCG_FLUID_3D) ? 3 * S->nV : S->nvars;
+  c.nhmg = (S->fluid) ? (long)S->fdim * S->nV : S->nvars;
   return c;
 }
 
@@ -435,7 +440,7 @@ static int d2_ctas() {
 
 template <typename T>
 static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, int finish, bool skip_if_done) {
-  if (S->analysis == CUDAPCG_FLUID_3D) {
+  if (S->fluid) {
     FlArgs<T> a;
     a.v = in0; a.vd = in1; a.vout = vout; a.y = y; a.x = nullptr; a.d = nullptr;
     a.dof_of_node = S->d_dof_of_node; a.node_of_dof = S->d_node_of_dof; a.bkeys = S->d_bkeys;
@@ -445,8 +450,13 @@ static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, i
     const int g = pw_grid(S->nV + S->nB);
     if (!ensure_reduction(g)) return false;
     a.rc = redctl(g);
-    if (fuse) k_fl_apply<T, TE_PCG><<<g, FL_NT, 0, S->stream>>>(a);
-    else k_fl_apply<T, TE_PLAIN><<<g, FL_NT, 0, S->stream>>>(a);
+    if (S->fdim == 2) {
+      if (fuse) k_fl_apply<T, TE_PCG, 2><<<g, FL_NT, 0, S->stream>>>(a);
+      else k_fl_apply<T, TE_PLAIN, 2><<<g, FL_NT, 0, S->stream>>>(a);
+    } else {
+      if (fuse) k_fl_apply<T, TE_PCG><<<g, FL_NT, 0, S->stream>>>(a);
+      else k_fl_apply<T, TE_PLAIN><<<g, FL_NT, 0, S->stream>>>(a);
+    }
   } else if (S->dim2) {
     const int nb = d2_ctas();
     if (!ensure_reduction(nb)) return false;
@@ -507,11 +517,12 @@ static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, i
 template <typename T, int MODE>
 static bool launch_point(double* x, T* d, T* r, const T* q, T* s, const T* dold) {
   const SolveCfg cfg = solvecfg();
-  if (S->analysis == CUDAPCG_FLUID_3D) {
+  if (S->fluid) {
     const int g = pw_grid(S->nV + S->nB);
     if (!ensure_reduction(g)) return false;
     FlPw<T> a{x, d, r, q, s, dold, S->d_bkeys, S->nV, S->nB, S->cur_sc, redctl(g), cfg};
-    k_fl_point<T, MODE><<<g, PW_NT, 0, S->stream>>>(a);
+    if (S->fdim == 2) k_fl_point<T, MODE, 2><<<g, PW_NT, 0, S->stream>>>(a);
+    else k_fl_point<T, MODE><<<g, PW_NT, 0, S->stream>>>(a);
   } else {
     const int g = pw_grid(S->N);
     if (!ensure_reduction(g)) return false;
@@ -542,7 +553,7 @@ static bool launch_mr_op(const T* rin, T* rout, int fin, bool skip_if_done);
 // number of iterations.
 // Thermal / elastic PCG forms s = M^-1 r inside the operator pass from r and the node keys and
 // stores no s; the Stokes operator (a gather through the DOF map) reads a stored s.
-static bool keeps_s() { return S->analysis == CUDAPCG_FLUID_3D; }
+static bool keeps_s() { return S->fluid; }
 template <typename T> static T* s_or_null() { return keeps_s() ? (T*)S->s : nullptr; }
 template <typename T> static const T* pcg_dir_in() { return keeps_s() ? (const T*)S->s : (const T*)S->r; }
 
@@ -836,8 +847,7 @@ cudapcgFlag_t cudapcgInit(cudapcgFlag_t analysis_flag, cudapcgFlag_t parStrategy
   cudapcgEnd();
   g_err.clear();
   if (analysis_flag > CUDAPCG_FLUID_3D) { set_err("cudapcgInit", "invalid analysis flag"); return CUDAPCG_FALSE; }
-  if (analysis_flag == CUDAPCG_FLUID_2D) { set_err("cudapcgInit", "2D permeability analysis is not provided by chfem_b200"); return CUDAPCG_FALSE; }
-  if (analysis_flag == CUDAPCG_FLUID_3D && parStrategy_flag != CUDAPCG_NBN) {
+  if ((analysis_flag == CUDAPCG_FLUID_3D || analysis_flag == CUDAPCG_FLUID_2D) && parStrategy_flag != CUDAPCG_NBN) {
     printf("ERROR: EBE solver is unavailable for FLUID analysis.\n");
     set_err("cudapcgInit", "EBE is unavailable for FLUID analysis");
     return CUDAPCG_FALSE;
@@ -846,6 +856,8 @@ cudapcgFlag_t cudapcgInit(cudapcgFlag_t analysis_flag, cudapcgFlag_t parStrategy
   S->analysis = analysis_flag;
   S->par = parStrategy_flag;
   S->dim2 = analysis_flag == CUDAPCG_THERMAL_2D || analysis_flag == CUDAPCG_ELASTIC_2D;
+  S->fluid = analysis_flag == CUDAPCG_FLUID_3D || analysis_flag == CUDAPCG_FLUID_2D;
+  S->fdim = analysis_flag == CUDAPCG_FLUID_2D ? 2 : 3;
   S->nd = (analysis_flag == CUDAPCG_ELASTIC_3D) ? 3 : (analysis_flag == CUDAPCG_ELASTIC_2D ? 2 : 1);
   if (const char* e = getenv("CHFEM_B200_PRECISION")) cudapcgB200SetPrecision((!strcmp(e, "mixed") || !strcmp(e, "fp32")) ? CHFEM_B200_MIXED : CHFEM_B200_FP64);
   if (!g_ctor) g_ctor = ctor_simple;
@@ -871,23 +883,23 @@ cudapcgModel_t* cudapcgNewModel(void) {
 
 static cudapcgFlag_t adopt_model() {
   cudapcgModel_t* m = S->model;
-  if (S->analysis == CUDAPCG_FLUID_3D && m->poremap_flag != CUDAPCG_POREMAP_NUM) {
+  if (S->fluid && m->poremap_flag != CUDAPCG_POREMAP_NUM) {
     set_err("model", "only the DOF-number pore map (-pm 1) is provided by chfem_b200");
     return CUDAPCG_FALSE;
   }
   free_vectors();
   free_model_dev();
   block_free();
-  S->R = (int)m->nrows; S->C = (int)m->ncols; S->L = S->dim2 ? 1 : (int)m->nlayers;
+  S->R = (int)m->nrows; S->C = (int)m->ncols; S->L = std::max(1, (int)m->nlayers);  // 2D: one layer
   S->N = (long)S->R * S->C * S->L;
   S->nvars = m->nvars; S->nV = m->nporenodes; S->nB = m->nbordernodes;
   S->nmat = (int)m->nkeys;
   if (S->N <= 0 || S->nvars <= 0) { set_err("model", "empty model"); return CUDAPCG_FALSE; }
-  if (S->analysis != CUDAPCG_FLUID_3D && (S->nmat < 1 || S->nmat > (S->dim2 ? T2_NMAT : 4))) {
+  if (!S->fluid && (S->nmat < 1 || S->nmat > (S->dim2 ? T2_NMAT : 4))) {
     set_err("model", S->dim2 ? "1 to 16 materials are supported with 16-bit 2D keys" : "1 to 4 materials are supported with 16-bit keys");
     return CUDAPCG_FALSE;
   }
-  if (S->analysis == CUDAPCG_FLUID_3D) {
+  if (S->fluid) {
     CK(cudaMalloc(&S->d_dof_of_node, sizeof(uint32_t) * S->N));
     CK(cudaMalloc(&S->d_node_of_dof, sizeof(uint32_t) * std::max<long>(1, S->nV + S->nB)));
     CK(cudaMalloc(&S->d_bkeys, std::max<long>(1, S->nB)));
@@ -936,6 +948,7 @@ cudapcgFlag_t cudapcgSetReduceStabFactor(double) { return S ? CUDAPCG_TRUE : CUD
 cudapcgFlag_t cudapcgSetSolver(cudapcgFlag_t flag) {
   if (!S) return CUDAPCG_FALSE;
   if (flag > CUDAPCG_MINRES2_SOLVER) { printf("ERROR: Invalid \"solverFlag\" (%d).\n", flag); return CUDAPCG_FALSE; }
+  if (flag >= CUDAPCG_CG2_SOLVER && is2d()) { set_err("cudapcgSetSolver", "the 2-vector solvers are provided for 3D Stokes models"); return CUDAPCG_FALSE; }
   // the 2-vector solvers keep another set of device vectors: a switch drops the old set
   if ((flag >= CUDAPCG_CG2_SOLVER) != (S->solver_flag >= CUDAPCG_CG2_SOLVER) && S->r) {
     free_vectors();
@@ -1130,7 +1143,7 @@ extern "C" {
 
 cudapcgFlag_t cudapcgSetImage(cudapcgMap_t* img) {
   if (!S || !S->model || !img) return CUDAPCG_FALSE;
-  if (S->analysis == CUDAPCG_FLUID_3D) { set_err("cudapcgSetImage", "not used for FLUID analysis"); return CUDAPCG_FALSE; }
+  if (S->fluid) { set_err("cudapcgSetImage", "not used for FLUID analysis"); return CUDAPCG_FALSE; }
   if (S->par == CUDAPCG_EBE) {
     uint16_t* tmp = nullptr;
     CK(cudaMalloc(&tmp, sizeof(uint16_t) * S->N));
@@ -1150,7 +1163,7 @@ cudapcgFlag_t cudapcgB200SetImageColors(const uint8_t* colors, unsigned int rows
                                          unsigned int refinement, const int* material_of_color) {
   const char* who = "cudapcgB200SetImageColors";
   if (!S || !S->model || !colors || !material_of_color || refinement < 1) { set_err(who, "bad arguments"); return CUDAPCG_FALSE; }
-  if (S->analysis == CUDAPCG_FLUID_3D) { set_err(who, "not used for FLUID analysis"); return CUDAPCG_FALSE; }
+  if (S->fluid) { set_err(who, "not used for FLUID analysis"); return CUDAPCG_FALSE; }
   if (S->dim2) { set_err(who, "2D node keys are set with cudapcgSetImage"); return CUDAPCG_FALSE; }
   if ((long)rows * refinement != S->R || (long)cols * refinement != S->C || (long)slices * refinement != S->L) {
     set_err(who, "image dimensions times refinement differ from the model's");
@@ -1192,7 +1205,7 @@ cudapcgFlag_t cudapcgB200SetPoreImageColors(const uint8_t* colors, unsigned int 
                                             unsigned int* nborder) {
   const char* who = "cudapcgB200SetPoreImageColors";
   if (!S || !S->model || !colors || !material_of_color || refinement < 1) { set_err(who, "bad arguments"); return CUDAPCG_FALSE; }
-  if (S->analysis != CUDAPCG_FLUID_3D) { set_err(who, "FLUID_3D models only (thermal / elastic: cudapcgB200SetImageColors)"); return CUDAPCG_FALSE; }
+  if (!S->fluid || is2d()) { set_err(who, "FLUID_3D models only (thermal / elastic: cudapcgB200SetImageColors)"); return CUDAPCG_FALSE; }
   if ((long)rows * refinement != S->R || (long)cols * refinement != S->C || (long)slices * refinement != S->L) {
     set_err(who, "image size times refinement differs from the model's");
     return CUDAPCG_FALSE;
@@ -1244,7 +1257,7 @@ cudapcgFlag_t cudapcgB200SetPoreImageColors(const uint8_t* colors, unsigned int 
 }
 // The current Stokes model's maps copied to the host (N, nV + nB and nB entries); for tests.
 cudapcgFlag_t cudapcgB200GetPoreMaps(uint32_t* dof_of_node, uint32_t* node_of_dof, uint8_t* border_keys) {
-  if (!S || !S->model || S->analysis != CUDAPCG_FLUID_3D || !S->have_maps) { set_err("cudapcgB200GetPoreMaps", "no Stokes maps"); return CUDAPCG_FALSE; }
+  if (!S || !S->model || !S->fluid || !S->have_maps) { set_err("cudapcgB200GetPoreMaps", "no Stokes maps"); return CUDAPCG_FALSE; }
   if (dof_of_node) CK(cudaMemcpy(dof_of_node, S->d_dof_of_node, sizeof(uint32_t) * S->N, cudaMemcpyDeviceToHost));
   if (node_of_dof && S->nV + S->nB) CK(cudaMemcpy(node_of_dof, S->d_node_of_dof, sizeof(uint32_t) * (S->nV + S->nB), cudaMemcpyDeviceToHost));
   if (border_keys && S->nB) CK(cudaMemcpy(border_keys, S->d_bkeys, S->nB, cudaMemcpyDeviceToHost));
@@ -1257,7 +1270,7 @@ cudapcgFlag_t cudapcgB200GetPoreMaps(uint32_t* dof_of_node, uint32_t* node_of_do
 cudapcgFlag_t cudapcgSetParametricDensityField(parametricScalarField_t* field, double fmin, double fmax) {
   const char* who = "cudapcgSetParametricDensityField";
   if (!S || !S->model || !field) { set_err(who, "bad arguments"); return CUDAPCG_FALSE; }
-  if (S->analysis == CUDAPCG_FLUID_3D) { set_err(who, "not used for FLUID analysis"); return CUDAPCG_FALSE; }
+  if (S->fluid) { set_err(who, "not used for FLUID analysis"); return CUDAPCG_FALSE; }
   if (!S->d_sdf) CK(cudaMalloc(&S->d_sdf, sizeof(uint16_t) * S->N));
   CK(cudaMemcpy(S->d_sdf, field, sizeof(uint16_t) * S->N, cudaMemcpyHostToDevice));
   S->sdf_min = fmin;
@@ -1273,18 +1286,18 @@ cudapcgFlag_t cudapcgSetParametricDensityField(parametricScalarField_t* field, d
 }
 cudapcgFlag_t cudapcgSetPoreMap(cudapcgFlag_t* pores) {
   if (!S || !S->model || !pores) return CUDAPCG_FALSE;
-  if (S->analysis != CUDAPCG_FLUID_3D) return CUDAPCG_FALSE;
+  if (!S->fluid) return CUDAPCG_FALSE;
   if (S->nB) CK(cudaMemcpy(S->d_bkeys, pores, S->nB, cudaMemcpyHostToDevice));
   return CUDAPCG_TRUE;
 }
 cudapcgFlag_t cudapcgSetPeriodic2DOFMap(cudapcgIdMap_t* vars) {
-  if (!S || !S->model || !vars || S->analysis != CUDAPCG_FLUID_3D) return CUDAPCG_FALSE;
+  if (!S || !S->model || !vars || !S->fluid) return CUDAPCG_FALSE;
   CK(cudaMemcpy(S->d_dof_of_node, vars, sizeof(uint32_t) * S->N, cudaMemcpyHostToDevice));
   S->have_maps = true;
   return CUDAPCG_TRUE;
 }
 cudapcgFlag_t cudapcgSetDOF2PeriodicMap(cudapcgIdMap_t* nodes) {
-  if (!S || !S->model || !nodes || S->analysis != CUDAPCG_FLUID_3D) return CUDAPCG_FALSE;
+  if (!S || !S->model || !nodes || !S->fluid) return CUDAPCG_FALSE;
   CK(cudaMemcpy(S->d_node_of_dof, nodes, sizeof(uint32_t) * (S->nV + S->nB), cudaMemcpyHostToDevice));
   return CUDAPCG_TRUE;
 }
@@ -1293,16 +1306,18 @@ cudapcgFlag_t cudapcgSetDOF2PeriodicMap(cudapcgIdMap_t* nodes) {
 static bool set_fluid_diag() {
   FlDiag dg;
   const double* K = S->Kd.data();
+  const int D = S->fdim, NE = 1 << D, ED = (D + 1) * NE, PC = D * NE;
   double dv[3] = {0, 0, 0}, dp = 0.0;
-  for (int e = 0; e < 8; e++) {
-    for (int c = 0; c < 3; c++) dv[c] += K[(3 * e + c) * 33];
-    dp -= K[(24 + e) * 33];
+  for (int e = 0; e < NE; e++) {
+    for (int c = 0; c < D; c++) dv[c] += K[(D * e + c) * (ED + 1)];
+    dp -= K[(PC + e) * (ED + 1)];
   }
-  for (int c = 0; c < 3; c++) dg.pore[c] = 1.0 / dv[c];
-  dg.pore[3] = 1.0 / dp;
+  for (int c = 0; c < 4; c++) dg.pore[c] = 0.0;
+  for (int c = 0; c < D; c++) dg.pore[c] = 1.0 / dv[c];
+  dg.pore[D] = 1.0 / dp;
   for (int k = 0; k < 256; k++) {
     double sum = 0.0;
-    for (int e = 0; e < 8; e++) sum -= K[(24 + e) * 33] * (double)((k >> e) & 1);
+    for (int e = 0; e < NE; e++) sum -= K[(PC + e) * (ED + 1)] * (double)((k >> e) & 1);
     dg.border[k] = (sum != 0.0) ? 1.0 / sum : 0.0;
   }
   CKV(cudaMemcpyToSymbol(c_fldiag, &dg, sizeof(FlDiag)));
@@ -1311,7 +1326,7 @@ static bool set_fluid_diag() {
 
 cudapcgFlag_t cudapcgSetLclMtxs(cudapcgVar_t* Lm) {
   if (!S || !S->model || !Lm) return CUDAPCG_FALSE;
-  const int nk = S->analysis == CUDAPCG_FLUID_3D ? 1 : S->nmat;
+  const int nk = S->fluid ? 1 : S->nmat;
   if (S->dim2) {  // dense (4 nd) x (4 nd) per material (femhmg_thermal_2D.c:42-90, femhmg_elastic_2D.c:56-146)
     S->Kd.assign(Lm, Lm + (size_t)16 * S->nd * S->nd * nk);
   } else if (S->analysis == CUDAPCG_THERMAL_3D) {
@@ -1320,14 +1335,14 @@ cudapcgFlag_t cudapcgSetLclMtxs(cudapcgVar_t* Lm) {
   } else if (S->analysis == CUDAPCG_ELASTIC_3D) {
     S->Kd.assign(Lm, Lm + (size_t)576 * nk);
   } else {
-    S->Kd.assign(Lm, Lm + 1024);
+    S->Kd.assign(Lm, Lm + (S->fdim == 2 ? 144 : 1024));  // one (DIM + 1) 2^DIM square matrix
   }
   S->have_K = true;
   free_ptr(S->d_K64); free_ptr(S->d_K32); S->d_K64 = nullptr; S->d_K32 = nullptr;
   free_ptr(S->d_tab64); free_ptr(S->d_tab32); S->d_tab64 = nullptr; S->d_tab32 = nullptr;
   free_ptr(S->d_invd); S->d_invd = nullptr;
   invalidate_graphs();  // captured launches hold the old matrix pointers
-  if (S->analysis == CUDAPCG_FLUID_3D && !set_fluid_diag()) return CUDAPCG_FALSE;
+  if (S->fluid && !set_fluid_diag()) return CUDAPCG_FALSE;
   return CUDAPCG_TRUE;
 }
 
@@ -1388,7 +1403,7 @@ cudapcgFlag_t cudapcgB200SetPrecision(int mode) {
   // diagonal that is negative on the pressure rows) comes close to breaking down on the
   // indefinite saddle-point system -- z.Az changes sign and beta jumps by orders of magnitude
   // even in FP64 -- and FP32 rounding at those points sends it into stagnation.
-  S->precision = (S->analysis == CUDAPCG_FLUID_3D) ? CHFEM_B200_FP64 : mode;
+  S->precision = (S->fluid) ? CHFEM_B200_FP64 : mode;
   return CUDAPCG_TRUE;
 }
 cudapcgFlag_t cudapcgB200SetResidualReplacement(unsigned int k) { if (!S) return CUDAPCG_FALSE; S->replace_every = k; return CUDAPCG_TRUE; }
@@ -1502,7 +1517,7 @@ extern "C" {
 double cudapcgB200TimeKernel(int which, unsigned int reps) {
   if (!S || !S->model) return -1.0;
   if (which == 5 || which == 6) {
-    if (S->analysis == CUDAPCG_FLUID_3D) return -1.0;
+    if (S->fluid) return -1.0;
     return (S->precision == CHFEM_B200_FP64) ? time_block_kernel_T<double>(which, reps) : time_block_kernel_T<float>(which, reps);
   }
   return (S->precision == CHFEM_B200_FP64) ? time_kernel_T<double>(which, reps) : time_kernel_T<float>(which, reps);
@@ -1530,7 +1545,7 @@ unsigned long long cudapcgB200DeviceBytes(void) {
     for (const void* v : work) b += v ? es * tot : 0;
     b += (B->x ? 8ull * tot : 0) + (B->b64 ? 8ull * tot : 0);
   }
-  if (S->analysis == CUDAPCG_FLUID_3D) b += 4ull * S->N + 4ull * (S->nV + S->nB) + S->nB;
+  if (S->fluid) b += 4ull * S->N + 4ull * (S->nV + S->nB) + S->nB;
   else b += 2ull * S->N;
   return b;
 }
@@ -1541,8 +1556,8 @@ extern "C" cudapcgFlag_t cudapcgB200ComputeFields(int block_index, int axis, int
                                                   double* field_out) {
   const char* who = "cudapcgB200ComputeFields";
   if (!S || !S->model || !props || !field_out) { set_err(who, "bad arguments"); return CUDAPCG_FALSE; }
-  if (S->dim2) { set_err(who, "not provided for 2D models"); return CUDAPCG_FALSE; }
-  if (S->analysis == CUDAPCG_FLUID_3D) { set_err(who, "Stokes fields are the solution itself (velocity, pressure)"); return CUDAPCG_FALSE; }
+  if (is2d()) { set_err(who, "not provided for 2D models"); return CUDAPCG_FALSE; }
+  if (S->fluid) { set_err(who, "Stokes fields are the solution itself (velocity, pressure)"); return CUDAPCG_FALSE; }
   if (axis < 0 || axis > 2 || comp < 0 || comp >= S->nd) { set_err(who, "bad load case"); return CUDAPCG_FALSE; }
   const double* x = nullptr;
   if (block_index < 0) x = S->x;
@@ -1573,7 +1588,7 @@ static bool load_case_rhs_T(int axis, int comp, double jump, const double* CB) {
   const long n = S->nvars;
   // the 2-vector solvers and FP64 PCG3 keep no copy of b: their FP64 r is it
   double* b = (lean_solver() || !S->b64) ? (double*)S->r : S->b64;
-  if (S->analysis == CUDAPCG_FLUID_3D) {
+  if (S->fluid) {
     double w = 0.0;
     for (int a = 0; a < 8; a++) w += CB[72 + a];
     k_fl_rhs<T><<<pw_grid(n), PW_NT, 0, S->stream>>>(S->nV, n, axis, w, b, (T*)S->r);
@@ -1592,8 +1607,8 @@ static bool load_case_rhs_T(int axis, int comp, double jump, const double* CB) {
 extern "C" cudapcgFlag_t cudapcgB200SetLoadCaseRHS(int axis, int comp, double jump, const double* CB) {
   const char* who = "cudapcgB200SetLoadCaseRHS";
   if (!S || !S->model || axis < 0 || axis > 2) { set_err(who, "bad arguments"); return CUDAPCG_FALSE; }
-  if (S->dim2) { set_err(who, "not provided for 2D models"); return CUDAPCG_FALSE; }
-  const bool fluid = S->analysis == CUDAPCG_FLUID_3D;
+  if (is2d()) { set_err(who, "not provided for 2D models"); return CUDAPCG_FALSE; }
+  const bool fluid = S->fluid;
   if (fluid ? !CB : (comp < 0 || comp >= S->nd)) { set_err(who, "bad load case"); return CUDAPCG_FALSE; }
   if (!fluid && !S->have_keys) { set_err(who, "the model's keys were not set"); return CUDAPCG_FALSE; }
   if (!ensure_vectors_current()) return CUDAPCG_FALSE;
@@ -1606,8 +1621,8 @@ extern "C" cudapcgFlag_t cudapcgB200SetLoadCaseRHS(int axis, int comp, double ju
 extern "C" cudapcgFlag_t cudapcgB200VolumeTerm(const double* CB, unsigned int ns, double* moments) {
   const char* who = "cudapcgB200VolumeTerm";
   if (!S || !S->model || !CB || !moments || !S->x) { set_err(who, "bad arguments or no solution on the device"); return CUDAPCG_FALSE; }
-  if (S->dim2) { set_err(who, "not provided for 2D models"); return CUDAPCG_FALSE; }
-  const bool fluid = S->analysis == CUDAPCG_FLUID_3D;
+  if (is2d()) { set_err(who, "not provided for 2D models"); return CUDAPCG_FALSE; }
+  const bool fluid = S->fluid;
   if (ns != (fluid ? 3u : (S->nd == 3 ? 6u : 3u))) { set_err(who, "ns must be 3 (thermal, Stokes) or 6 (elastic)"); return CUDAPCG_FALSE; }
   if (!S->d_vt) CK(cudaMalloc(&S->d_vt, (8 + 4 * 6 * 24) * sizeof(double)));
   double* d_cb = S->d_vt + 8;
@@ -1636,9 +1651,9 @@ extern "C" cudapcgFlag_t cudapcgB200SolveLoadCases(unsigned int nrhs, const int*
                                                    double* residuals) {
   const char* who = "cudapcgB200SolveLoadCases";
   if (!S || !S->model || !axis || !CB || !moments || nrhs < 1 || nrhs > BLK_MAX) { set_err(who, "bad arguments"); return CUDAPCG_FALSE; }
-  if (S->dim2) { set_err(who, "not provided for 2D models"); return CUDAPCG_FALSE; }
+  if (is2d()) { set_err(who, "not provided for 2D models"); return CUDAPCG_FALSE; }
   if (lean_solver()) { set_err(who, "block solves run CG/MINRES(3); the 2-vector solvers reduce one load case at a time"); return CUDAPCG_FALSE; }
-  const bool fluid = S->analysis == CUDAPCG_FLUID_3D;
+  const bool fluid = S->fluid;
   if (fluid != ((S->solver_flag & 1) != 0)) {
     set_err(who, "load-case blocks are provided for thermal and elastic CG/PCG and Stokes MINRES/PMINRES");
     return CUDAPCG_FALSE;
@@ -1664,8 +1679,8 @@ extern "C" cudapcgFlag_t cudapcgB200SolveLoadCases(unsigned int nrhs, const int*
 
 extern "C" cudapcgFlag_t cudapcgB200ApplyBlockOperator(unsigned int nrhs, const double* const* v, double* const* y) {
   if (!S || !S->model || !v || !y || nrhs < 1 || nrhs > BLK_MAX) { set_err("cudapcgB200ApplyBlockOperator", "bad arguments"); return CUDAPCG_FALSE; }
-  if (S->dim2) { set_err("cudapcgB200ApplyBlockOperator", "not provided for 2D models"); return CUDAPCG_FALSE; }
-  if (S->analysis == CUDAPCG_FLUID_3D) { set_err("cudapcgB200ApplyBlockOperator", "thermal and elastic models only"); return CUDAPCG_FALSE; }
+  if (is2d()) { set_err("cudapcgB200ApplyBlockOperator", "not provided for 2D models"); return CUDAPCG_FALSE; }
+  if (S->fluid) { set_err("cudapcgB200ApplyBlockOperator", "thermal and elastic models only"); return CUDAPCG_FALSE; }
   for (unsigned k = 0; k < nrhs; k++) if (!v[k] || !y[k]) { set_err("cudapcgB200ApplyBlockOperator", "null buffer"); return CUDAPCG_FALSE; }
   const bool ok = (S->precision == CHFEM_B200_FP64) ? apply_block_T<double>((int)nrhs, v, y) : apply_block_T<float>((int)nrhs, v, y);
   return ok ? CUDAPCG_TRUE : CUDAPCG_FALSE;
@@ -1675,9 +1690,9 @@ extern "C" cudapcgFlag_t cudapcgB200SolveBlock(unsigned int nrhs, const double* 
                                                int x0_interpolate, double* const* x_out, unsigned int* iterations,
                                                double* residuals) {
   if (!S || !S->model || !rhs || !x_out || nrhs < 1 || nrhs > BLK_MAX) { set_err("cudapcgB200SolveBlock", "bad arguments"); return CUDAPCG_FALSE; }
-  if (S->dim2) { set_err("cudapcgB200SolveBlock", "not provided for 2D models"); return CUDAPCG_FALSE; }
+  if (is2d()) { set_err("cudapcgB200SolveBlock", "not provided for 2D models"); return CUDAPCG_FALSE; }
   if (lean_solver()) { set_err("cudapcgB200SolveBlock", "block solves run CG/MINRES(3), not the 2-vector solvers"); return CUDAPCG_FALSE; }
-  const bool fluid = S->analysis == CUDAPCG_FLUID_3D;
+  const bool fluid = S->fluid;
   if (fluid != ((S->solver_flag & 1) != 0)) {
     set_err("cudapcgB200SolveBlock", "block solves are provided for thermal and elastic CG/PCG and Stokes MINRES/PMINRES");
     return CUDAPCG_FALSE;

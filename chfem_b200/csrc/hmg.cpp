@@ -293,10 +293,11 @@ cudapcgFlag_t model_ctor(cudapcgModel_t** ptr, const void* data) {
   p->nvars = (unsigned)m.ndof;
   p->nvarspernode = 3;
   p->nkeys = m.analysis == FLUID ? 1 : m.nmat;
-  p->localmtxdim = m.dim2 ? (m.analysis == THERMAL ? 16 : 64) : (m.analysis == THERMAL ? 40 : (m.analysis == ELASTIC ? 576 : 1024));
+  p->localmtxdim = m.dim2 ? (m.analysis == THERMAL ? 16 : (m.analysis == ELASTIC ? 64 : 144))
+                          : (m.analysis == THERMAL ? 40 : (m.analysis == ELASTIC ? 576 : 1024));
   p->nporenodes = (unsigned)m.nV;
   p->nbordernodes = (unsigned)m.nB;
-  p->nhmgvars = m.analysis == FLUID ? (unsigned)(3 * m.nV) : (unsigned)m.ndof;
+  p->nhmgvars = m.analysis == FLUID ? (unsigned)((m.dim2 ? 2 : 3) * m.nV) : (unsigned)m.ndof;
   return CUDAPCG_TRUE;
 }
 
@@ -409,9 +410,8 @@ logical hmgInit(char* data_filename, char* elem_filename, char* sdf_filename, ui
   m->C_dim = (unsigned)(tensor_dim(*m) * tensor_dim(*m));
   if (!read_colors(*m, data, elem_filename)) { delete m; return 0; }
   if (m->dim2) {
-    // 2D: the node keys (4 bits per pixel) are built on the host
-    if (m->analysis == FLUID) { fail("2D permeability analysis is not provided by chfem_b200"); delete m; return 0; }
-    if (sdf_filename) { fail("a scalar density field is not provided for 2D images"); delete m; return 0; }
+    // 2D: the node keys (4 bits per pixel) or the Stokes DOF numbering are built on the host
+    if (sdf_filename && m->analysis != FLUID) { fail("a scalar density field is not provided for 2D images"); delete m; return 0; }
     if (!ensure_host_maps(*m)) { delete m; return 0; }
   } else if (m->analysis == FLUID) {
     // the sizes of the DOF numbering here; the numbering itself on the device at upload
@@ -569,6 +569,7 @@ void hmgSolveHomogenization(void) {
   }
   // the 2-vector solvers never form the solution: its exports have nothing to write
   const bool two_vector = g_solver >= CUDAPCG_CG2_SOLVER;
+  if (two_vector && m.dim2) { fail("the 2-vector solvers (CG2/MINRES2) are provided for 3D Stokes models"); return; }
   if (two_vector && (g_export_fields || g_export_x))
     SAY("WARNING: the 2-vector solvers (CG2/MINRES2) reduce the solution on the fly; fields and x are not exported.\n");
   SAY("Running homogenization...\n");

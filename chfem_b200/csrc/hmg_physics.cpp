@@ -75,7 +75,9 @@ static void shape(int a, const double* p, double& phi, double* grad, bool zflip)
 // pore, material index 0), the pore voxels, and the counts of pore nodes (key 255) and
 // interface nodes (0 < key < 255) -- the sizes of the DOF numbering (femhmg_fluid_3D.c:370-424),
 // which itself runs in build_maps or on the device (cudapcgB200SetPoreImageColors).
+static bool count_pore_nodes_2d(Model& m, std::string& err);
 bool count_pore_nodes(Model& m, std::string& err) {
+  if (m.dim2) return count_pore_nodes_2d(m, err);
   const long R = m.ny, C = m.nx, L = m.nz, N = m.N;
   m.fluid_keys.assign(N, 0);
   long pores = 0, nv = 0, nb = 0;
@@ -479,7 +481,25 @@ static const int FACE2D[2][2] = {{1, 2}, {2, 3}};  // local nodes on the +x and 
 
 static bool build_maps_2d(Model& m, std::string& err) {
   const long R = m.ny, C = m.nx, N = m.N;
-  if (m.analysis == FLUID) { err = "2D permeability analysis is not provided by chfem_b200"; return false; }
+  if (m.analysis == FLUID) {  // femhmg_fluid_2D.c:370-460: pore nodes (key 15) first, then interface nodes
+    if (!count_pore_nodes_2d(m, err)) return false;
+    m.dof_of_node.assign(N, 0);
+    long id = 0;
+    for (long i = 0; i < N; i++)
+      if (m.fluid_keys[i] == 15) m.dof_of_node[i] = (uint32_t)id++;
+    for (long i = 0; i < N; i++)
+      if (m.fluid_keys[i] != 15 && m.fluid_keys[i] != 0) m.dof_of_node[i] = (uint32_t)id++;
+    m.node_of_dof.assign(m.nV + m.nB, 0);
+    m.border_keys.assign(m.nB, 0);
+    for (long i = 0; i < N; i++) {
+      const uint8_t k = m.fluid_keys[i];
+      if (!k) continue;
+      const uint32_t d = m.dof_of_node[i];
+      m.node_of_dof[d] = (uint32_t)i;
+      if (k != 15) m.border_keys[d - m.nV] = k;
+    }
+    return true;
+  }
   if (m.nmat > 16) { err = "more than 16 materials cannot be encoded in 16-bit 2D node keys"; return false; }
   m.keys.assign(N, 0);
 #pragma omp parallel for schedule(static)
@@ -493,6 +513,30 @@ static bool build_maps_2d(Model& m, std::string& err) {
   return true;
 }
 
+// Stokes: fluid key of every node (bit e: the pixel in which the node is local node e is pore,
+// material 0), pore nodes (key 15) and interface nodes (0 < key < 15); DOFs 3 per pore node
+// (2 velocities, pressure) and 1 per interface node
+static bool count_pore_nodes_2d(Model& m, std::string& err) {
+  const long R = m.ny, C = m.nx, N = m.N;
+  m.fluid_keys.assign(N, 0);
+  long pores = 0, nv = 0, nb = 0;
+  for (long i = 0; i < N; i++) {
+    const long r = i % R, c = i / R;
+    unsigned k = 0;
+    for (int e = 0; e < 4; e++) k |= (unsigned)(m.elem_mat[node_elem_2d(r, c, e, R, C)] == 0) << e;
+    m.fluid_keys[i] = (uint8_t)k;
+    pores += (m.elem_mat[i] == 0);
+    nv += (k == 15);
+    nb += (k != 0 && k != 15);
+  }
+  if (3 * nv + nb >= (long)0xffffffffL) { err = "too many Stokes unknowns for 32-bit DOF ids"; return false; }
+  m.nporeelem = pores;
+  m.nV = nv;
+  m.nB = nb;
+  m.ndof = 3 * nv + nb;
+  return true;
+}
+
 static void build_local_matrices_2d(Model& m) {
   const double g[2] = {0.5 - 0.5 / std::sqrt(3.0), 0.5 + 0.5 / std::sqrt(3.0)};
   double grad[4][4][2];  // [qp][node][x, y]
@@ -503,6 +547,33 @@ static void build_local_matrices_2d(Model& m) {
       grad[q][a][0] = df1(cx) * f1(cy, py);
       grad[q][a][1] = f1(cx, px) * df1(cy);
     }
+  }
+  if (m.analysis == FLUID) {
+    // unit pixel, mu = 1 (femhmg_fluid_2D.c:41-80): [K G; G^T Stab], K = int(grad u : grad v +
+    // grad u^T : grad v), G = int(d_i phi_a psi_b), Stab = (1/6) * Q1 Laplacian; CB: the velocity
+    // average (2 x 8) and the body-force load (4)
+    double phi[4][4];
+    for (int q = 0; q < 4; q++)
+      for (int a = 0; a < 4; a++) phi[q][a] = f1(nxi(a), g[q & 1]) * f1(neta(a), g[q >> 1]);
+    m.lcl.assign(144, 0.0);
+    m.CB.assign(20, 0.0);
+    for (int q = 0; q < 4; q++)
+      for (int a = 0; a < 4; a++) {
+        for (int b = 0; b < 4; b++) {
+          const double kl = grad[q][a][0] * grad[q][b][0] + grad[q][a][1] * grad[q][b][1];
+          for (int i = 0; i < 2; i++) {
+            for (int j = 0; j < 2; j++) m.lcl[(2 * a + i) * 12 + 2 * b + j] += 0.25 * ((i == j ? kl : 0.0) + grad[q][a][j] * grad[q][b][i]);
+            const double gp = 0.25 * grad[q][a][i] * phi[q][b];
+            m.lcl[(2 * a + i) * 12 + 8 + b] += gp;
+            m.lcl[(8 + b) * 12 + 2 * a + i] += gp;
+          }
+          m.lcl[(8 + a) * 12 + 8 + b] += 0.25 * kl / 6.0;
+        }
+        for (int i = 0; i < 2; i++) m.CB[8 * i + 2 * a + i] += 0.25 * phi[q][a];
+        m.CB[16 + a] += 0.25 * phi[q][a];
+      }
+    m.Kdense = m.lcl;
+    return;
   }
   const int nd = m.nd, ed = 4 * nd;
   m.lcl.assign((size_t)ed * ed * m.nmat, 0.0);
@@ -563,6 +634,17 @@ static void for_boundary_pixels(const Model& m, int axis, F f) {
 static void assemble_rhs_2d(const Model& m, int dir, double* rhs) {
   std::memset(rhs, 0, sizeof(double) * m.ndof);
   const long R = m.ny, C = m.nx;
+  if (m.analysis == FLUID) {  // unit body force along dir at every pore-node velocity (femhmg_fluid_2D.c:84-124)
+    for (long e = 0; e < m.N; e++) {
+      if (m.elem_mat[e] != 0) continue;
+      const long r = e % R, c = e / R;
+      for (int a = 0; a < 4; a++) {
+        const uint32_t d = m.dof_of_node[elem_node_2d(r, c, a, R, C)];
+        if (d < (uint32_t)m.nV) rhs[2 * (size_t)d + dir] += m.CB[16 + a];
+      }
+    }
+    return;
+  }
   int axis, comp;
   case_axis(m, dir, axis, comp);
   const double jump = (double)(axis == 0 ? m.nx : m.ny);
@@ -582,6 +664,24 @@ static void assemble_rhs_2d(const Model& m, int dir, double* rhs) {
 
 static void update_C_2d(Model& m, int dir, const double* x) {
   const long R = m.ny, C = m.nx, N = m.N;
+  if (m.analysis == FLUID) {  // femhmg_fluid_2D.c:245-300: mean velocity times h^2
+    double c0 = 0, c1 = 0;
+    for (long e = 0; e < N; e++) {
+      if (m.elem_mat[e] != 0) continue;
+      const long r = e % R, c = e / R;
+      for (int a = 0; a < 4; a++) {
+        const uint32_t d = m.dof_of_node[elem_node_2d(r, c, a, R, C)];
+        if (d < (uint32_t)m.nV) {
+          c0 += m.CB[2 * a] * x[2 * (size_t)d];
+          c1 += m.CB[8 + 2 * a + 1] * x[2 * (size_t)d + 1];
+        }
+      }
+    }
+    const double scl = m.voxel * m.voxel / (double)N;
+    m.C[0 + dir] = c0 * scl;
+    m.C[2 + dir] = c1 * scl;
+    return;
+  }
   int axis, comp;
   case_axis(m, dir, axis, comp);
   const double jump = (double)(axis == 0 ? m.nx : m.ny);

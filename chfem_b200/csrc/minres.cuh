@@ -74,7 +74,7 @@ struct MrDirFl {
   DevScalars* sc; RedCtl rc; int precond;
 };
 
-template <typename T>
+template <typename T, int DIM = 3>
 __global__ void __launch_bounds__(PW_NT) k_fl_mr_dir(MrDirFl<T> a) {
   __shared__ double sred[PW_NT / 32];
   if (a.sc->done) return;
@@ -83,9 +83,9 @@ __global__ void __launch_bounds__(PW_NT) k_fl_mr_dir(MrDirFl<T> a) {
   double sum = 0.0;
   for (long t = blockIdx.x * (long)PW_NT + threadIdx.x; t < nT; t += (long)gridDim.x * PW_NT) {
     const bool pore = t < nV;
-    const int cnt = pore ? 4 : 1;
+    const int cnt = pore ? DIM + 1 : 1;
     for (int k = 0; k < cnt; k++) {
-      const long j = pore ? (k < 3 ? 3 * t + k : 3 * nV + t) : 3 * nV + t;
+      const long j = pore ? (k < DIM ? DIM * t + k : DIM * nV + t) : DIM * nV + t;
       T inv = T(1);
       if (a.precond) inv = pore ? T(c_fldiag.pore[k]) : T(c_fldiag.border[a.bkeys[t - nV]]);
       const T z = a.r[j] * inv;

@@ -16,7 +16,7 @@ static MrCfg mrcfg() {
 template <typename T>
 static bool launch_mr_op_buf(const T* rin, T* rout, const T* q, T* s, double* x, const T* d, int fin, bool skip_if_done) {
   const MrCfg cfg = mrcfg();
-  if (S->analysis == CUDAPCG_FLUID_3D) {
+  if (S->fluid) {
     FlArgs<T> a;
     a.v = rin; a.vd = q; a.vout = rout; a.y = s; a.x = x; a.d = d;
     a.dof_of_node = S->d_dof_of_node; a.node_of_dof = S->d_node_of_dof; a.bkeys = S->d_bkeys;
@@ -25,7 +25,8 @@ static bool launch_mr_op_buf(const T* rin, T* rout, const T* q, T* s, double* x,
     const int g = pw_grid(S->nV + S->nB);
     if (!ensure_reduction(g)) return false;
     a.rc = redctl(g);
-    k_fl_apply<T, TE_MR><<<g, FL_NT, 0, S->stream>>>(a);
+    if (S->fdim == 2) k_fl_apply<T, TE_MR, 2><<<g, FL_NT, 0, S->stream>>>(a);
+    else k_fl_apply<T, TE_MR><<<g, FL_NT, 0, S->stream>>>(a);
   } else if (S->dim2) {
     const int nb = d2_ctas();
     if (!ensure_reduction(nb)) return false;
@@ -85,11 +86,12 @@ static bool launch_mr_op(const T* rin, T* rout, int fin, bool skip_if_done) {
 
 template <typename T>
 static bool launch_mr_dir(const T* rcur) {
-  if (S->analysis == CUDAPCG_FLUID_3D) {
+  if (S->fluid) {
     const int g = pw_grid(S->nV + S->nB);
     if (!ensure_reduction(g)) return false;
     MrDirFl<T> a{(T*)S->d0, (T*)S->q, rcur, (const T*)S->s, S->d_bkeys, S->nV, S->nB, S->cur_sc, redctl(g), S->precond};
-    k_fl_mr_dir<T><<<g, PW_NT, 0, S->stream>>>(a);
+    if (S->fdim == 2) k_fl_mr_dir<T, 2><<<g, PW_NT, 0, S->stream>>>(a);
+    else k_fl_mr_dir<T><<<g, PW_NT, 0, S->stream>>>(a);
   } else {
     const int g = pw_grid(S->N);
     if (!ensure_reduction(g)) return false;

@@ -56,7 +56,7 @@ struct FlDiag {
 };
 __constant__ FlDiag c_fldiag;
 
-// Value of the operator's input at DOF `dof` (component comp: 0..2 velocity, 3 pressure),
+// Value of the operator's input at DOF `dof` (component comp: 0..DIM-1 velocity, DIM pressure),
 // formed per MODE.  `off` is the vector offset of that entry.
 template <typename T, int MODE>
 __device__ __forceinline__ T fl_in(const FlArgs<T>& a, size_t off, T beta, T alpha, T inv) {
@@ -66,8 +66,14 @@ __device__ __forceinline__ T fl_in(const FlArgs<T>& a, size_t off, T beta, T alp
   return v;
 }
 
-template <typename T, int MODE>
+// DIM = 3: voxels, 8 elements, 27 neighbours, element matrix 32 x 32 (3 velocities + pressure
+// per node); DIM = 2: pixels (one layer), 4 elements, 9 neighbours, 12 x 12 (2 velocities +
+// pressure; matrix_free.cu:484-518 pore rows, :628-660 interface rows).  Vector layout
+// [DIM nVel interleaved velocities | nVel + nBorder pressures].
+template <typename T, int MODE, int DIM = 3>
 __global__ void __launch_bounds__(FL_NT) k_fl_apply(FlArgs<T> a) {
+  constexpr int NE = 1 << DIM, ED = (DIM + 1) * NE, PC = DIM * NE, NO = DIM == 3 ? 27 : 9;
+  constexpr unsigned FULL = (1u << NE) - 1u;
   __shared__ double sred[FL_NT / 32];
   if (a.skip_if_done && a.sc->done) return;
   const long nV = a.nV, nT = a.nV + a.nB;
@@ -75,64 +81,81 @@ __global__ void __launch_bounds__(FL_NT) k_fl_apply(FlArgs<T> a) {
   const T beta = (MODE == TE_PCG) ? T(a.sc->beta) : T(0);
   const T alpha = (MODE == TE_MR && mr_steps(a.finish)) ? T(a.sc->alpha) : T(0);
   const bool pre = a.cfg.precond != 0;
-  const T ivv0 = pre ? T(c_fldiag.pore[0]) : T(1), ivv1 = pre ? T(c_fldiag.pore[1]) : T(1), ivv2 = pre ? T(c_fldiag.pore[2]) : T(1);
-  const T ivp = pre ? T(c_fldiag.pore[3]) : T(1);
+  T ivv[DIM];
+#pragma unroll
+  for (int k = 0; k < DIM; k++) ivv[k] = pre ? T(c_fldiag.pore[k]) : T(1);
+  const T ivp = pre ? T(c_fldiag.pore[DIM]) : T(1);
   double acc = 0.0, acc_rz = 0.0, mr = 0.0, md = 0.0, mx = 0.0;
   for (long t = blockIdx.x * (long)FL_NT + threadIdx.x; t < nT; t += (long)gridDim.x * FL_NT) {
     const uint32_t node = a.node_of_dof[t];
     const int r = (int)(node % (uint32_t)R), c = (int)((node / (uint32_t)R) % (uint32_t)C), l = (int)(node / ((uint32_t)R * (uint32_t)C));
     const bool pore = t < nV;
-    const unsigned fk = pore ? 255u : a.bkeys[t - nV];
+    const unsigned fk = pore ? FULL : a.bkeys[t - nV];
     const int rr[3] = {wrap(r - 1, R), r, wrap(r + 1, R)};
     const int cc[3] = {wrap(c - 1, C), c, wrap(c + 1, C)};
     const int ll[3] = {wrap(l - 1, L), l, wrap(l + 1, L)};
-    T ov0 = 0, ov1 = 0, ov2 = 0, op = 0;
+    T ov[DIM], op = 0;
 #pragma unroll
-    for (int o = 0; o < 27; o++) {
-      const int orr = o % 3 - 1, occ = (o / 3) % 3 - 1, oll = o / 9 - 1;
-      // voxels of this node that also contain the neighbour
+    for (int k = 0; k < DIM; k++) ov[k] = 0;
+#pragma unroll
+    for (int o = 0; o < NO; o++) {
+      const int orr = o % 3 - 1, occ = (o / 3) % 3 - 1, oll = DIM == 3 ? o / 9 - 1 : 0;
+      // elements of this node that also contain the neighbour
       unsigned emask = 0;
 #pragma unroll
-      for (int e = 0; e < 8; e++)
+      for (int e = 0; e < NE; e++)
 #pragma unroll
-        for (int b = 0; b < 8; b++)
+        for (int b = 0; b < NE; b++)
           if (drow(b) - drow(e) == orr && dcol(b) - dcol(e) == occ && dlay(b) - dlay(e) == oll) emask |= 1u << e;
       if (!(fk & emask)) continue;
       const uint32_t nb = (uint32_t)rr[orr + 1] + (uint32_t)cc[occ + 1] * (uint32_t)R + (uint32_t)ll[oll + 1] * (uint32_t)R * (uint32_t)C;
       const uint32_t dof = a.dof_of_node[nb];
-      T vx = 0, vy = 0, vz = 0;
+      T vv[DIM];
+#pragma unroll
+      for (int k = 0; k < DIM; k++) vv[k] = 0;
       const bool vel = dof < (uint32_t)nV;
       if (vel) {
-        vx = fl_in<T, MODE>(a, 3 * (size_t)dof, beta, alpha, ivv0);
-        vy = fl_in<T, MODE>(a, 3 * (size_t)dof + 1, beta, alpha, ivv1);
-        vz = fl_in<T, MODE>(a, 3 * (size_t)dof + 2, beta, alpha, ivv2);
+#pragma unroll
+        for (int k = 0; k < DIM; k++) vv[k] = fl_in<T, MODE>(a, DIM * (size_t)dof + k, beta, alpha, ivv[k]);
       }
       T ip = ivp;
       if (MODE == TE_MR && pre && !vel) ip = T(c_fldiag.border[a.bkeys[dof - (uint32_t)nV]]);
-      const T vp = fl_in<T, MODE>(a, 3 * (size_t)nV + dof, beta, alpha, ip);
+      const T vp = fl_in<T, MODE>(a, DIM * (size_t)nV + dof, beta, alpha, ip);
 #pragma unroll
-      for (int e = 0; e < 8; e++) {
+      for (int e = 0; e < NE; e++) {
 #pragma unroll
-        for (int b = 0; b < 8; b++) {
+        for (int b = 0; b < NE; b++) {
           if (!(drow(b) - drow(e) == orr && dcol(b) - dcol(e) == occ && dlay(b) - dlay(e) == oll)) continue;
           if (!((fk >> e) & 1u)) continue;
           if (pore) {
-            ov0 += flK<T>((3 * e + 0) * 32 + 3 * b) * vx + flK<T>((3 * e + 0) * 32 + 3 * b + 1) * vy + flK<T>((3 * e + 0) * 32 + 3 * b + 2) * vz + flK<T>((3 * e + 0) * 32 + 24 + b) * vp;
-            ov1 += flK<T>((3 * e + 1) * 32 + 3 * b) * vx + flK<T>((3 * e + 1) * 32 + 3 * b + 1) * vy + flK<T>((3 * e + 1) * 32 + 3 * b + 2) * vz + flK<T>((3 * e + 1) * 32 + 24 + b) * vp;
-            ov2 += flK<T>((3 * e + 2) * 32 + 3 * b) * vx + flK<T>((3 * e + 2) * 32 + 3 * b + 1) * vy + flK<T>((3 * e + 2) * 32 + 3 * b + 2) * vz + flK<T>((3 * e + 2) * 32 + 24 + b) * vp;
+#pragma unroll
+            for (int ci = 0; ci < DIM; ci++) {
+              T sum = flK<T>((DIM * e + ci) * ED + DIM * b) * vv[0];
+#pragma unroll
+              for (int cj = 1; cj < DIM; cj++) sum += flK<T>((DIM * e + ci) * ED + DIM * b + cj) * vv[cj];
+              ov[ci] += sum + flK<T>((DIM * e + ci) * ED + PC + b) * vp;
+            }
           }
-          op += flK<T>((24 + e) * 32 + 3 * b) * vx + flK<T>((24 + e) * 32 + 3 * b + 1) * vy + flK<T>((24 + e) * 32 + 3 * b + 2) * vz - flK<T>((24 + e) * 32 + 24 + b) * vp;
+          T sp = flK<T>((PC + e) * ED + DIM * b) * vv[0];
+#pragma unroll
+          for (int cj = 1; cj < DIM; cj++) sp += flK<T>((PC + e) * ED + DIM * b + cj) * vv[cj];
+          op += sp - flK<T>((PC + e) * ED + PC + b) * vp;
         }
       }
     }
     // own rows: formed input (dot), ping-pong outputs, MR updates
-    const int cnt = pore ? 4 : 1;
-    const T outv[4] = {pore ? ov0 : op, ov1, ov2, op};
-    const size_t offs[4] = {pore ? 3 * (size_t)t : 3 * (size_t)nV + t, 3 * (size_t)t + 1, 3 * (size_t)t + 2, 3 * (size_t)nV + t};
+    const int cnt = pore ? DIM + 1 : 1;
+    T outv[DIM + 1];
+    size_t offs[DIM + 1];
+#pragma unroll
+    for (int k = 0; k < DIM; k++) { outv[k] = ov[k]; offs[k] = DIM * (size_t)t + k; }
+    outv[DIM] = op;
+    offs[DIM] = DIM * (size_t)nV + t;
+    if (!pore) { outv[0] = op; offs[0] = DIM * (size_t)nV + t; }
     for (int k = 0; k < cnt; k++) {
       const size_t j = offs[k];
       T iv = T(1);
-      if (MODE == TE_MR && pre) iv = pore ? (k == 3 ? ivp : (k == 0 ? ivv0 : (k == 1 ? ivv1 : ivv2))) : T(c_fldiag.border[fk]);
+      if (MODE == TE_MR && pre) iv = pore ? (k == DIM ? ivp : ivv[k < DIM ? k : 0]) : T(c_fldiag.border[fk]);
       const T v = fl_in<T, MODE>(a, j, beta, alpha, iv);
       a.y[j] = outv[k];
       if (MODE == TE_PCG) a.vout[j] = v;
@@ -179,7 +202,7 @@ struct FlPw {
   SolveCfg cfg;
 };
 
-template <typename T, int MODE>
+template <typename T, int MODE, int DIM = 3>
 __global__ void __launch_bounds__(PW_NT) k_fl_point(FlPw<T> a) {
   __shared__ double sred[PW_NT / 32];
   if (MODE != PW_INIT && MODE != PW_CHECK && a.sc->done) return;
@@ -194,10 +217,12 @@ __global__ void __launch_bounds__(PW_NT) k_fl_point(FlPw<T> a) {
     double inv[4];
     int cnt;
     if (pore) {
-      idx[0] = 3 * t; idx[1] = 3 * t + 1; idx[2] = 3 * t + 2; idx[3] = 3 * nV + t; cnt = 4;
-      for (int k = 0; k < 4; k++) inv[k] = c_fldiag.pore[k];
+      for (int k = 0; k < DIM; k++) idx[k] = DIM * t + k;
+      idx[DIM] = DIM * nV + t;
+      cnt = DIM + 1;
+      for (int k = 0; k <= DIM; k++) inv[k] = c_fldiag.pore[k];
     } else {
-      idx[0] = 3 * nV + t; cnt = 1;
+      idx[0] = DIM * nV + t; cnt = 1;
       inv[0] = c_fldiag.border[a.bkeys[t - nV]];
     }
     for (int k = 0; k < cnt; k++) {

@@ -153,7 +153,7 @@ static bool finish_two_vector(double* res_x, bool write_metrics) {
 }
 
 static bool solve_two_vector(double* res_x) {
-  if (S->analysis != CUDAPCG_FLUID_3D) {
+  if (!S->fluid) {
     set_err("cudapcgSolve", "the 2-vector solvers (CG2/MINRES2) reduce Stokes velocities; use CG3/MINRES3 for other analyses");
     return false;
   }

@@ -12,7 +12,7 @@
  * Scope: 3D thermal (1 DOF/node), 3D elastic (3 DOF/node), 3D Stokes with the DOF-number
  * pore map (CUDAPCG_POREMAP_NUM), including the 2-vector solvers with on-the-fly reduction of
  * the solution (CG2/PCG2/MINRES2/PMINRES2, Stokes); the scalar density field (3D); 2D thermal
- * (1 DOF/node) and 2D elastic (2 DOF/node) on pixel images.  2D Stokes is rejected.
+ * (1 DOF/node), 2D elastic (2 DOF/node) and 2D Stokes (2 velocities + pressure) on pixel images.
  *
  * Operator restatement.  The reference applies A node-by-node: for node i and each of the
  * 8 voxels (elements) around it, i is local node e of element e, and the row block of the
@@ -60,7 +60,7 @@ static inline void neighbours27(int r, int c, int l, unsigned int R, unsigned in
 /* ------------------------------------------------------------------------------------ */
 typedef struct {
   cudapcgModel_t *model;
-  unsigned int analysis;   /* CUDAPCG_THERMAL_2D / 3D, ELASTIC_2D / 3D, FLUID_3D */
+  unsigned int analysis;   /* CUDAPCG_THERMAL_2D / 3D, ELASTIC_2D / 3D, FLUID_2D / 3D */
   int dim2;                /* 2D analysis: pixel images, 4-node elements, 4-bit key fields */
   unsigned int par;        /* NBN / EBE */
   cudapcgTol_t tol;
@@ -90,6 +90,7 @@ typedef struct {
 } oracle_solver_t;
 
 static oracle_solver_t *S = NULL;
+static int is_fluid(void) { return S->analysis == CUDAPCG_FLUID_3D || S->analysis == CUDAPCG_FLUID_2D; }
 static cudapcgFlag_t (*model_ctor)(cudapcgModel_t **, const void *) = NULL;
 static int g_quiet = 0;
 
@@ -314,8 +315,70 @@ static void keys_from_elements_2d(const cudapcgMap_t *em, unsigned int R, unsign
   }
 }
 
+/* 2D Stokes, DOF-number pore map (matrix_free.cu:484-518 pore rows, :628-660 interface rows):
+   the 12 x 12 element matrix [K G; G^T Stab] enters as [K G; G^T -Stab] over the node's fluid
+   pixels; velocity columns of non-pore neighbours are dropped (no slip); vector layout
+   [2 nVel interleaved velocities | nVel + nBorder pressures]. */
+static void apply_fluid_2d(const double *v, double *y) {
+  cudapcgModel_t *m = S->model;
+  const unsigned int R = m->nrows, C = m->ncols;
+  const unsigned int nV = m->nporenodes, nB = m->nbordernodes;
+  const double *K = S->Kd;
+  const cudapcgIdMap_t *dmap = m->periodic2DOF_map, *nmap = m->DOF2periodic_map;
+#pragma omp parallel for schedule(static)
+  for (long id = 0; id < (long)(nV + nB); id++) {
+    const unsigned int node = nmap[id];
+    const int r = (int)(node % R), c = (int)(node / R);
+    const int pore = id < (long)nV;
+    const unsigned int fkey = pore ? 15u : m->border_pore_map[id - nV];
+    double rv[2] = {0, 0}, rp = 0.0;
+    for (int e = 0; e < 4; e++) {
+      if (!((fkey >> e) & 1u)) continue;
+      for (int b = 0; b < 4; b++) {
+        const unsigned int dof = dmap[wrapi(r - DROW[e] + DROW[b], R) + wrapi(c - DCOL[e] + DCOL[b], C) * R];
+        if (dof < nV) {
+          const double *vv = v + 2 * (size_t)dof;
+          if (pore)
+            for (int ci = 0; ci < 2; ci++) rv[ci] += K[(2 * e + ci) * 12 + 2 * b] * vv[0] + K[(2 * e + ci) * 12 + 2 * b + 1] * vv[1];
+          rp += K[(8 + e) * 12 + 2 * b] * vv[0] + K[(8 + e) * 12 + 2 * b + 1] * vv[1];
+        }
+        const double vp = v[2 * (size_t)nV + dof];
+        if (pore)
+          for (int ci = 0; ci < 2; ci++) rv[ci] += K[(2 * e + ci) * 12 + 8 + b] * vp;
+        rp -= K[(8 + e) * 12 + 8 + b] * vp;
+      }
+    }
+    if (pore) { y[2 * id] = rv[0]; y[2 * id + 1] = rv[1]; }
+    y[2 * (size_t)nV + id] = rp;
+  }
+}
+/* 2D Stokes Jacobi (matrix_free.cu:461-469, :608-616) */
+static void inv_diag_fluid_2d(double *dinv) {
+  cudapcgModel_t *m = S->model;
+  const unsigned int nV = m->nporenodes, nB = m->nbordernodes;
+  const double *K = S->Kd;
+  double dv[2] = {0, 0}, dp = 0.0;
+  for (int e = 0; e < 4; e++) {
+    for (int ci = 0; ci < 2; ci++) dv[ci] += K[(2 * e + ci) * 13];
+    dp -= K[(8 + e) * 13];
+  }
+#pragma omp parallel for schedule(static)
+  for (long id = 0; id < (long)nV; id++) {
+    for (int ci = 0; ci < 2; ci++) dinv[2 * id + ci] = 1.0 / dv[ci];
+    dinv[2 * (size_t)nV + id] = 1.0 / dp;
+  }
+#pragma omp parallel for schedule(static)
+  for (long b = 0; b < (long)nB; b++) {
+    const unsigned int fk = m->border_pore_map[b];
+    double s = 0.0;
+    for (int e = 0; e < 4; e++) s -= K[(8 + e) * 13] * (double)((fk >> e) & 1u);
+    dinv[3 * (size_t)nV + b] = 1.0 / s;
+  }
+}
+
 static void Aprod(const double *v, double *y) {
-  if (S->dim2) apply_2d(v, y);
+  if (S->analysis == CUDAPCG_FLUID_2D) apply_fluid_2d(v, y);
+  else if (S->dim2) apply_2d(v, y);
   else if (S->analysis == CUDAPCG_FLUID_3D) apply_fluid(v, y);
   else apply_thermal_elastic(v, y);
 }
@@ -331,6 +394,7 @@ static void Aprod_scl(const double *v, double scl, double scl_prev, double *y, d
 /* (matrix_free.cu:167-188 thermal, :388-408 elastic, :663-672 and :912-925 Stokes).       */
 static void inv_diag(double *dinv) {
   cudapcgModel_t *m = S->model;
+  if (S->analysis == CUDAPCG_FLUID_2D) { inv_diag_fluid_2d(dinv); return; }
   if (S->dim2) { inv_diag_2d(dinv); return; }
   if (S->analysis == CUDAPCG_FLUID_3D) {
     const unsigned int nV = m->nporenodes, nB = m->nbordernodes;
@@ -383,6 +447,11 @@ static void apply_precond(const double *v1, const double *v2, double scl1, doubl
 /* thermal/elastic versions are warnings that leave res untouched (wrappers.cu:635-648).  */
 static void apply_invprecond(const double *v1, double scl1, double *res) {
   cudapcgModel_t *m = S->model;
+  if (S->analysis == CUDAPCG_FLUID_2D) {  /* the 2D stencil constants are the diagonal's (4, -4/9, -n/9) */
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)m->nvars; i++) res[i] = scl1 * v1[i] / g_dinv[i];
+    return;
+  }
   if (S->analysis != CUDAPCG_FLUID_3D) return;
   const unsigned int nV = m->nporenodes, nB = m->nbordernodes;
 #pragma omp parallel for schedule(static)
@@ -489,18 +558,18 @@ cudapcgFlag_t cudapcgEnd(void) {
 cudapcgFlag_t cudapcgInit(cudapcgFlag_t analysis_flag, cudapcgFlag_t par) {
   cudapcgEnd();
   if (analysis_flag != CUDAPCG_THERMAL_3D && analysis_flag != CUDAPCG_ELASTIC_3D && analysis_flag != CUDAPCG_FLUID_3D &&
-      analysis_flag != CUDAPCG_THERMAL_2D && analysis_flag != CUDAPCG_ELASTIC_2D) {
+      analysis_flag != CUDAPCG_THERMAL_2D && analysis_flag != CUDAPCG_ELASTIC_2D && analysis_flag != CUDAPCG_FLUID_2D) {
     fprintf(stderr, "oracle: analysis %d is not restated\n", analysis_flag);
     return CUDAPCG_FALSE;
   }
-  if (analysis_flag == CUDAPCG_FLUID_3D && par != CUDAPCG_NBN) {
+  if ((analysis_flag == CUDAPCG_FLUID_3D || analysis_flag == CUDAPCG_FLUID_2D) && par != CUDAPCG_NBN) {
     printf("ERROR: EBE solver is unavailable for FLUID analysis.\n");
     return CUDAPCG_FALSE;
   }
   S = (oracle_solver_t *)calloc(1, sizeof(oracle_solver_t));
   if (!S) return CUDAPCG_FALSE;
   S->analysis = analysis_flag; S->par = par;
-  S->dim2 = (analysis_flag == CUDAPCG_THERMAL_2D || analysis_flag == CUDAPCG_ELASTIC_2D);
+  S->dim2 = (analysis_flag == CUDAPCG_THERMAL_2D || analysis_flag == CUDAPCG_ELASTIC_2D || analysis_flag == CUDAPCG_FLUID_2D);
   S->tol = CUDAPCG_TOLERANCE; S->maxit = CUDAPCG_MAX_ITERATIONS;
   S->solver_flag = CUDAPCG_CG_SOLVER; S->precond = 1; S->resnorm = CUDAPCG_L2_NORM;
   S->xr_mode = CUDAPCG_XREDUCE_FULL; S->xr_shift = 0; S->xr_scale = 1.0;  /* cudapcg.cu:154-156 */
@@ -519,7 +588,7 @@ cudapcgFlag_t cudapcgSetModelConstructorFcn(cudapcgFlag_t (*fcn)(cudapcgModel_t 
 static void alloc_model_arrays(void) {
   cudapcgModel_t *m = S->model;
   free(S->r); S->r = (double *)calloc(m->nvars, sizeof(double));
-  if (S->analysis != CUDAPCG_FLUID_3D) {
+  if (!is_fluid()) {
     if (!m->image) m->image = (cudapcgMap_t *)calloc(m->nelem, sizeof(cudapcgMap_t));
   } else {
     if (!m->periodic2DOF_map) m->periodic2DOF_map = (cudapcgIdMap_t *)calloc(m->nelem, sizeof(cudapcgIdMap_t));
@@ -533,7 +602,7 @@ cudapcgFlag_t cudapcgBuildModel(const void *data) {
   if (!S->model) S->model = cudapcgNewModel();
   else if (S->model->freeAllowed_flag) { free_model(S->model); S->model = cudapcgNewModel(); }
   if (!model_ctor(&S->model, data)) return CUDAPCG_FALSE;
-  if (S->analysis == CUDAPCG_FLUID_3D && S->model->poremap_flag != CUDAPCG_POREMAP_NUM) {
+  if (is_fluid() && S->model->poremap_flag != CUDAPCG_POREMAP_NUM) {
     fprintf(stderr, "oracle: only the DOF-number pore map is supported\n");
     return CUDAPCG_FALSE;
   }
@@ -665,7 +734,11 @@ cudapcgFlag_t cudapcgSetLclMtxs(cudapcgVar_t *L) {
   S->nkeys = m->nkeys;
   capture(4, L, m->nkeys * m->localmtxdim);
   free(S->Kd);
-  if (S->analysis == CUDAPCG_THERMAL_2D || S->analysis == CUDAPCG_ELASTIC_2D) {  /* dense 4x4 / 8x8 */
+  if (S->analysis == CUDAPCG_FLUID_2D) {  /* one 12 x 12 matrix (femhmg_fluid_2D.c:41-80) */
+    S->ed = 12;
+    S->Kd = (double *)malloc(sizeof(double) * 144);
+    memcpy(S->Kd, L, sizeof(double) * 144);
+  } else if (S->analysis == CUDAPCG_THERMAL_2D || S->analysis == CUDAPCG_ELASTIC_2D) {  /* dense 4x4 / 8x8 */
     S->ed = S->analysis == CUDAPCG_THERMAL_2D ? 4 : 8;
     S->Kd = (double *)malloc(sizeof(double) * S->ed * S->ed * m->nkeys);
     memcpy(S->Kd, L, sizeof(double) * S->ed * S->ed * m->nkeys);
@@ -1146,7 +1219,7 @@ cudapcgFlag_t cudapcgSolve(cudapcgVar_t *res_x) {
   S->count++;
   if (S->solver_flag >= CUDAPCG_CG2_SOLVER) {
     if (S->analysis != CUDAPCG_FLUID_3D) {
-      printf("ERROR: the 2-vector solvers reduce Stokes velocities; use CG3/MINRES3.\n");
+      printf("ERROR: the 2-vector solvers are restated for 3D Stokes; use CG3/MINRES3.\n");
       if (must_free) free_arrays();
       return 0;
     }
@@ -1205,7 +1278,7 @@ cudapcgFlag_t cudapcgPrintSolverReport2(char *dest) {
 /* Oracle-only entry points.                                                              */
 int oracle_apply(const double *x, double *y) {
   if (!S || !S->model || !S->Kd) return 0;
-  if (S->analysis != CUDAPCG_FLUID_3D && !S->keys) return 0;
+  if (!is_fluid() && !S->keys) return 0;
   Aprod(x, y);
   return 1;
 }

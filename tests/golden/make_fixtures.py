@@ -2,7 +2,7 @@
 
 The reference's own regression data (its test/input/3D directory: two voxel images, their
 .nf settings files and the golden effective-tensor columns; test/input/2D: a pixel image and
-the golden thermal and elastic tensors) is copied here so that the parity tests can run where
+the golden thermal, elastic and permeability tensors) is copied here so that the parity tests can run where
 the reference tree is absent.  Images are stored gzip-compressed.
 
 Usage:  python tests/golden/make_fixtures.py [/path/to/chfem]
@@ -30,6 +30,7 @@ CASES = {
 CASES_2D = {
     "thermal_2d": ("2D/100x100.raw", (100, 100), "2D/thermal/100x100.nf", "2D/thermal/100x100_result.bin", 2),
     "elastic_2d": ("2D/100x100.raw", (100, 100), "2D/elastic/100x100.nf", "2D/elastic/100x100_result.bin", 3),
+    "fluid_2d": ("2D/100x100.raw", (100, 100), "2D/fluid/100x100.nf", "2D/fluid/100x100_result.bin", 2),
 }
 
 

@@ -40,11 +40,12 @@ def test_errors_are_reported_not_fatal(tmp_path):
     lib = _native.chfem()
     lib.chfemB200SetQuiet(1)
     nf = tmp_path / "bad.nf"
-    nf.write_text("%type_of_analysis\n2\n%image_dimensions\n4 4 0\n%number_of_materials\n1\n%properties_of_materials\n0\n")
+    nf.write_text("%type_of_analysis\n0\n%image_dimensions\n4 4 0\n%number_of_materials\n1\n%properties_of_materials\n0 1.0\n")
     raw = tmp_path / "bad.raw"
     raw.write_bytes(bytes(16))
-    assert lib.hmgInit(str(nf).encode(), str(raw).encode(), None, None) == 0  # 2D Stokes
-    assert b"2D permeability" in lib.chfemB200LastError()
+    sdf = str(tmp_path / "field.bin").encode()
+    assert lib.hmgInit(str(nf).encode(), str(raw).encode(), sdf, None) == 0  # density field on a 2D image
+    assert b"2D" in lib.chfemB200LastError()
     # 2D with more than 16 materials for 16-bit keys of 4 bits per pixel
     mats = "".join(f"{i} {i + 1}\n" for i in range(17))
     nf.write_text(f"%type_of_analysis\n0\n%image_dimensions\n4 4 0\n%number_of_materials\n17\n%properties_of_materials\n{mats}")
@@ -69,8 +70,9 @@ def test_errors_are_reported_not_fatal(tmp_path):
 def test_cudapcg_rejects_out_of_scope():
     from chfem_b200 import _native
     lib = _native.cudapcg()
-    assert lib.cudapcgInit(4, 0) == 0            # 2D Stokes
-    assert b"2D" in lib.cudapcgB200LastError()
+    assert lib.cudapcgInit(6, 0) == 0            # no such analysis
+    assert b"invalid analysis" in lib.cudapcgB200LastError()
+    assert lib.cudapcgInit(4, 1) == 0            # 2D Stokes with EBE
     assert lib.cudapcgInit(5, 1) == 0            # Stokes with EBE
 
 

@@ -123,11 +123,16 @@ def test_density_of_ones_is_the_two_phase_model(tmp_path, analysis):
 @pytest.mark.gpu
 @pytest.mark.parametrize("analysis", [0, 1])
 def test_density_field_minres(tmp_path, analysis):
-    """(P)MINRES under a density field: the solutions of every load case equal the oracle's."""
+    """MINRES under a density field: the solutions of every load case equal the oracle's
+    (unpreconditioned: the reference's thermal / elastic PMINRES iterates with a stub inverse
+    Jacobi, wrappers.cu:635-648); PMINRES gives the PCG solution."""
     nf, raw, fb = make_case(tmp_path, analysis, (6, 7, 8), 1, "float32")
-    Cref, xref, logref = _x_of(H.ORACLE_EXEC, nf, raw, fb, ["-s", "1"])
-    C, xs, log = _x_of(H.CHFEM_EXEC, nf, raw, fb, ["-s", "1"])
+    Cref, xref, logref = _x_of(H.ORACLE_EXEC, nf, raw, fb, ["-s", "1", "-j", "0"])
+    C, xs, log = _x_of(H.CHFEM_EXEC, nf, raw, fb, ["-s", "1", "-j", "0"])
     for a, b in zip(xs, xref):
         assert H.rel_to_max(a, b) < 1e-6
     its, its_ref = H.parse_iterations(log), H.parse_iterations(logref)
-    assert all(abs(a - b) <= 1 for a, b in zip(its, its_ref)), (its, its_ref)
+    assert all(abs(a - b) <= max(1, 0.01 * b) for a, b in zip(its, its_ref)), (its, its_ref)
+    Cp, _ = H.run_exec(H.CHFEM_EXEC, nf, raw, "-f", fb)
+    Cm, _ = H.run_exec(H.CHFEM_EXEC, nf, raw, "-f", fb, "-s", "1")
+    assert H.rel_to_max(Cm, Cp) < 1e-6

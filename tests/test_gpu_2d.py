@@ -1,7 +1,8 @@
-"""2D thermal and elastic homogenization on pixel images (chfem's femhmg_2D.c,
-femhmg_thermal_2D.c, femhmg_elastic_2D.c; operators matrix_free.cu:51-95, :325-385).
+"""2D thermal, elastic and Stokes homogenization on pixel images (chfem's femhmg_2D.c,
+femhmg_thermal_2D.c, femhmg_elastic_2D.c, femhmg_fluid_2D.c; operators matrix_free.cu:51-95,
+:325-385, :461-660).
 
-The B200 path (k_2d_apply) against the reference's golden 2D tensors (test/input/2D, the
+The B200 path (k_2d_apply; k_fl_apply<.., 2> for Stokes) against the reference's golden 2D tensors (test/input/2D, the
 reference's bar 1e-4) and against the oracle (the reference's host code with the CPU restatement
 of its 2D operators) on the same inputs: tensors 1e-6 in FP64 and 1e-4 in mixed precision,
 iteration counts within one, across the solvers, stopping norms, Jacobi on/off, node-by-node
@@ -22,26 +23,30 @@ def _its_close(log, logref):
     assert len(its) == len(its_ref) and all(abs(a - b) <= 1 for a, b in zip(its, its_ref)), (its, its_ref)
 
 
-@pytest.mark.parametrize("name", ["thermal_2d", "elastic_2d"])
-@pytest.mark.parametrize("par", ["0", "1"])
+@pytest.mark.parametrize("name,par", [("thermal_2d", "0"), ("thermal_2d", "1"), ("elastic_2d", "0"), ("elastic_2d", "1"),
+                                      ("fluid_2d", "0")])
 def test_2d_golden(tmp_path, name, par):
     nf, raw, meta = H.golden_case_files(name, str(tmp_path))
     C, log = H.run_exec(H.CHFEM_EXEC, nf, raw, "-p", par)
     assert H.rel_to_max(C, meta["tensor"]) < meta["reference_tolerance"]
     Cref, logref = H.run_exec(H.ORACLE_EXEC, nf, raw, "-p", par)
     assert H.rel_to_max(C, Cref) < 1e-6
-    _its_close(log, logref)
+    # the reference's 2D Stokes case runs CG on the indefinite saddle-point system, whose stopping
+    # iteration moves with round-off (the oracle's own counts vary between runs by 5 %): the
+    # tensors are compared there, not the counts
+    if name != "fluid_2d":
+        _its_close(log, logref)
 
 
 CASES = [
     # name, analysis, shape (y, x), nmat, flags
     ("t2_pcg", 0, (37, 45), 3, []),
     ("t2_cg", 0, (20, 33), 2, ["-j", "0"]),
-    ("t2_minres", 0, (16, 40), 4, ["-s", "1"]),
+    ("t2_minres", 0, (16, 40), 4, ["-s", "1", "-j", "0"]),
     ("t2_cg3_inf", 0, (24, 24), 2, ["-s", "2", "-c", "1"]),
     ("t2_thin", 0, (1, 50), 2, []),
     ("e2_pcg", 1, (33, 29), 2, []),
-    ("e2_minres", 1, (18, 22), 3, ["-s", "1"]),
+    ("e2_minres", 1, (18, 22), 3, ["-s", "1", "-j", "0"]),
     ("e2_cg3_err", 1, (26, 20), 2, ["-s", "2", "-c", "2"]),
     ("e2_many", 1, (30, 31), 12, []),
     ("e2_ebe", 1, (21, 17), 3, ["-p", "1"]),
@@ -92,6 +97,17 @@ def test_2d_refinement_and_solution_files(tmp_path):
     assert all(i <= 1 for i in H.parse_iterations(log))
 
 
+@pytest.mark.parametrize("analysis", [0, 1])
+def test_2d_pminres_equals_pcg(tmp_path, analysis):
+    """PMINRES with Jacobi (-s 1 -j 1), whose reference version iterates on an unscaled residual
+    for thermal / elastic models (its inverse Jacobi is a stub, wrappers.cu:635-648), runs the
+    intended recurrence here: the tensor equals the PCG one."""
+    nf, raw = _case(tmp_path, f"pm2_{analysis}", analysis, (19, 23), 3)
+    Cp, _ = H.run_exec(H.CHFEM_EXEC, nf, raw)
+    Cm, _ = H.run_exec(H.CHFEM_EXEC, nf, raw, "-s", "1")
+    assert H.rel_to_max(Cm, Cp) < 1e-6
+
+
 def test_2d_compute_property():
     """The Python API on a 2D array: tensors of the 2D shapes, symmetric stiffness."""
     from chfem_b200 import compute_property
@@ -102,3 +118,34 @@ def test_2d_compute_property():
     assert Ce.shape == (3, 3)
     assert np.allclose(Ce, Ce.T, rtol=1e-5, atol=1e-7 * np.abs(Ce).max())
     assert Kt[0, 0] > 1.0 and Kt[1, 1] > 1.0
+
+
+FLUID_CASES = [
+    # name, shape (y, x), pore fraction, flags
+    ("f2_cg", (30, 26), 0.65, ["-s", "0"]),
+    ("f2_pminres", (22, 35), 0.6, ["-s", "1"]),
+    ("f2_minres_nopre", (18, 18), 0.7, ["-s", "1", "-j", "0"]),
+    ("f2_minres3_inf", (25, 21), 0.6, ["-s", "3", "-c", "1"]),
+]
+
+
+@pytest.mark.parametrize("name,shape,porosity,flags", FLUID_CASES)
+def test_2d_stokes(tmp_path, name, shape, porosity, flags):
+    rng = np.random.default_rng(zlib.crc32(name.encode()) % 10000)
+    img = np.where(rng.random(shape) < porosity, 0, 255).astype(np.uint8)
+    nf, raw = H.write_small_case(str(tmp_path), name, img, 2, tol=1e-8, maxit=20000)
+    Cref, logref = H.run_exec(H.ORACLE_EXEC, nf, raw, *flags)
+    C, log = H.run_exec(H.CHFEM_EXEC, nf, raw, *flags)
+    assert C.shape == (2, 2)
+    assert H.rel_to_max(C, Cref) < 1e-6
+    if flags[1] != "0":  # CG on the indefinite system stops at round-off-dependent iterations
+        its, its_ref = H.parse_iterations(log), H.parse_iterations(logref)
+        # MINRES without Jacobi plateaus near the tolerance: within 2 %, as for 3D Stokes
+        assert all(abs(a - b) <= max(1, 0.02 * b) for a, b in zip(its, its_ref)), (its, its_ref)
+
+
+def test_2d_stokes_rejects_two_vector(tmp_path):
+    img = np.where(np.random.default_rng(3).random((12, 12)) < 0.6, 0, 255).astype(np.uint8)
+    nf, raw = H.write_small_case(str(tmp_path), "f2_tv", img, 2, tol=1e-8, maxit=20000)
+    with pytest.raises(RuntimeError):
+        H.run_exec(H.CHFEM_EXEC, nf, raw, "-s", "5")

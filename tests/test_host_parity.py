@@ -120,6 +120,25 @@ def test_fluid_maps_rhs_updateC(tmp_path):
         assert H.rel_to_max(C[:9].reshape(3, 3)[:, d], ref["C"][:9].reshape(3, 3)[:, d]) < 1e-12
 
 
+def test_fluid_2d_maps_rhs_updateC(tmp_path):
+    """2D Stokes (femhmg_fluid_2D.c): fluid keys, DOF numbering (pore nodes first, then interface
+    nodes), DOF->node map and interface keys bit-exact; the 12 x 12 element matrix, right-hand
+    sides and permeability column equal the reference's host code."""
+    rng = np.random.default_rng(21)
+    img = np.where(rng.random((14, 17)) < 0.3, 255, 0).astype(np.uint8)
+    nf, raw = H.write_small_case(str(tmp_path), "fl2d", img, 2, tol=1e-6, maxit=50)
+    for d in [0, 1]:
+        ref = H.oracle_capture(nf, raw, d)
+        lib, mine = host_arrays(nf, raw, d)
+        assert np.array_equal(mine[1], ref["1"]), "node->DOF map differs"
+        assert np.array_equal(mine[2], ref["2"]), "DOF->node map differs"
+        assert np.array_equal(mine[3], ref["3"]), "interface fluid keys differ"
+        np.testing.assert_allclose(mine[4], ref["4"], rtol=1e-12, atol=1e-14)
+        np.testing.assert_allclose(mine["rhs"], ref["5"], rtol=1e-12, atol=1e-14)
+        C = updateC(lib, d, ref["6"])
+        assert H.rel_to_max(C[:4].reshape(2, 2)[:, d], ref["C"][:4].reshape(2, 2)[:, d]) < 1e-12
+
+
 def test_refinement_and_transpose(tmp_path):
     """%refinement replicates each voxel and the x-fastest file order is transposed."""
     img = H.small_image((3, 4, 5), 2, seed=3)

@@ -19,10 +19,11 @@ def test_oracle_matches_golden(tmp_path, name):
     assert H.rel_to_max(col, meta["column"]) < meta["reference_tolerance"]
 
 
-@pytest.mark.parametrize("name", ["thermal_2d", "elastic_2d"])
-@pytest.mark.parametrize("par", ["0", "1"])
+@pytest.mark.parametrize("name,par", [("thermal_2d", "0"), ("thermal_2d", "1"), ("elastic_2d", "0"), ("elastic_2d", "1"),
+                                      ("fluid_2d", "0")])
 def test_oracle_matches_golden_2d(tmp_path, name, par):
-    """2D pixel models (test/input/2D): every load case, node-by-node and element-by-element."""
+    """2D pixel models (test/input/2D): every load case, node-by-node and (thermal, elastic)
+    element-by-element."""
     nf, raw, meta = H.golden_case_files(name, str(tmp_path))
     C, out = H.run_exec(H.ORACLE_EXEC, nf, raw, "-p", par, env={"OMP_NUM_THREADS": str(os.cpu_count() or 4)})
     assert H.rel_to_max(C, meta["tensor"]) < meta["reference_tolerance"]
