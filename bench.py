@@ -771,6 +771,10 @@ def dominant_kernel_roofline(model, w, block, workload):
                      f"+ directions + dots, {nr} load cases)" if asm else
                      f"k_blk_apply<{nd},{tn},{nr}> (block operator + directions + dots, {nr} load cases)")
             per_unit = nr * 4 * nd * es + 2  # per load case s, d_old in; d_new, q out; one 16-bit key
+        elif nd == 1 and model.nmat <= 4 and os.environ.get("CHFEM_B200_THERMAL_OP") != "generic":
+            kern_which = 1
+            kname = f"k_th_apply<{tn},TE_PCG> (thermal operator for cubic-symmetric conduction matrices + direction + dot)"
+            per_unit = 4 * es + 2
         else:
             kern_which, kname = 1, f"k_te_apply<{nd},{tn},TE_PCG> (operator + direction + dot)"
             per_unit = 4 * nd * es + 2  # s, d_old in; d_new, q out (nd comps); 16-bit key

@@ -24,6 +24,7 @@
 #include "stencil_block.cuh"
 #include "stencil_asm.cuh"
 #include "asm_apply.h"
+#include "th_apply.h"
 #include "stencil_2d.cuh"
 #include "pore_maps.h"
 #include "stencil_fluid_block.cuh"
@@ -112,6 +113,11 @@ struct Solver {
   // assembled neighbour blocks of a two-material model (stencil_asm.cuh), per precision
   double* d_tab64 = nullptr;
   float* d_tab32 = nullptr;
+  // thermal models with cubic-symmetric element matrices: the table of the thermal pass
+  // (stencil_th.cuh), per precision; th_state 0 not checked yet, 1 applies, -1 does not
+  double* d_th64 = nullptr;
+  float* d_th32 = nullptr;
+  int th_state = 0;
   // scalar density field (cudapcgSetParametricDensityField): 16-bit code per voxel and its
   // range; the inverse Jacobi diagonal it implies, per unknown (FP64, built at solve set-up)
   uint16_t* d_sdf = nullptr;
@@ -204,9 +210,11 @@ static void free_model_dev() {
   if (!S) return;
   free_ptr(S->d_keys); free_ptr(S->d_dof_of_node); free_ptr(S->d_node_of_dof); free_ptr(S->d_bkeys);
   free_ptr(S->d_K64); free_ptr(S->d_K32); free_ptr(S->d_tab64); free_ptr(S->d_tab32);
+  free_ptr(S->d_th64); free_ptr(S->d_th32);
   free_ptr(S->d_sdf); free_ptr(S->d_invd);
   S->d_keys = nullptr; S->d_dof_of_node = S->d_node_of_dof = nullptr; S->d_bkeys = nullptr;
   S->d_K64 = nullptr; S->d_K32 = nullptr; S->d_tab64 = nullptr; S->d_tab32 = nullptr;
+  S->d_th64 = nullptr; S->d_th32 = nullptr; S->th_state = 0;
   S->d_sdf = nullptr; S->d_invd = nullptr;
   S->have_K = S->have_keys = S->have_maps = false;
 }
@@ -303,6 +311,35 @@ static bool ensure_tab() {
   return true;
 }
 
+// The thermal pass of stencil_th.cuh: 3D thermal models without a density field whose element
+// matrices have the cubic structure it relies on (checked once per model);
+// CHFEM_B200_THERMAL_OP=generic keeps the generic pass.
+static bool th_applies() {
+  if (S->analysis != CUDAPCG_THERMAL_3D || S->d_sdf || S->nmat > 4 || !S->have_K) return false;
+  const char* e = getenv("CHFEM_B200_THERMAL_OP");
+  if (e && !strcmp(e, "generic")) return false;
+  if (S->th_state == 0) {
+    std::vector<double> t((size_t)th_table_words());
+    S->th_state = th_build_table((int)S->nmat, S->Kd.data(), t.data()) ? 1 : -1;
+  }
+  return S->th_state == 1;
+}
+template <typename T> static T*& thdev();
+template <> double*& thdev<double>() { return S->d_th64; }
+template <> float*& thdev<float>() { return S->d_th32; }
+template <typename T>
+static bool ensure_th() {
+  if (thdev<T>()) return true;
+  std::vector<double> t64((size_t)th_table_words());
+  if (!th_build_table((int)S->nmat, S->Kd.data(), t64.data())) { set_err("solve", "thermal table"); return false; }
+  std::vector<T> t(t64.begin(), t64.end());
+  T* d = nullptr;
+  CKV(cudaMalloc(&d, t.size() * sizeof(T)));
+  CKV(cudaMemcpy(d, t.data(), t.size() * sizeof(T), cudaMemcpyHostToDevice));
+  thdev<T>() = d;
+  return true;
+}
+
 // Inverse Jacobi diagonal under a scalar density field: sum over the node's 8 voxels of the
 // scaled diagonal of its element matrix (matrix_free.cu:2270-2306 and the elastic counterpart
 // compute it per application; here once per model).
@@ -358,6 +395,7 @@ template <> float* Kdev<float>() { return S->d_K32; }
 template <typename T>
 static bool ensure_K() {
   if (Kdev<T>()) {  // the derived tables may have been dropped since (new density field, new model)
+    if (th_applies() && !ensure_th<T>()) return false;
     if (asm_applies() && !ensure_tab<T>()) return false;
     if ((S->d_sdf || S->dim2) && !ensure_invd()) return false;
     return true;
@@ -369,6 +407,7 @@ static bool ensure_K() {
   CKV(cudaMalloc(&dk, kt.size() * sizeof(T)));
   CKV(cudaMemcpy(dk, kt.data(), kt.size() * sizeof(T), cudaMemcpyHostToDevice));
   if (sizeof(T) == 8) S->d_K64 = (double*)dk; else S->d_K32 = (float*)dk;
+  if (th_applies() && !ensure_th<T>()) return false;
   if (asm_applies() && !ensure_tab<T>()) return false;
   if ((S->d_sdf || S->dim2) && !ensure_invd()) return false;
   if (S->fluid) {
@@ -472,6 +511,14 @@ static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, i
       if (fuse) k_2d_apply<2, T, TE_PCG><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<2, T>(), S->stream>>>(a);
       else k_2d_apply<2, T, TE_PLAIN><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<2, T>(), S->stream>>>(a);
     }
+  } else if (th_applies()) {
+    const int nb = fuse ? th_ctas<T, TE_PCG>(S->R, S->C, S->L, num_sms()) : th_ctas<T, TE_PLAIN>(S->R, S->C, S->L, num_sms());
+    if (nb < 1 || !ensure_reduction(nb)) return false;
+    TeArgs<1, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->cur_sc, redctl(nb), finish, skip_if_done, MrCfg{S->tol, 0, S->resnorm, S->precond, 0}};
+    const cudaError_t e = fuse ? th_launch<T, TE_PCG>(a, thdev<T>(), nb, S->stream) : th_launch<T, TE_PLAIN>(a, thdev<T>(), nb, S->stream);
+    S->launches++;
+    if (e != cudaSuccess) { set_err("operator pass", cudaGetErrorString(e)); return false; }
+    return true;
   } else if (asm_applies()) {
     int nb;
     cudaError_t e;
@@ -577,6 +624,11 @@ static bool launch_te_mode(const T* in0, const T* in1, T* vout, double* x, int f
       k_2d_apply<2, T, MODE><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<2, T>(), S->stream>>>(a);
     }
     e = cudaGetLastError();
+  } else if (th_applies()) {
+    const int nb = th_ctas<T, MODE>(S->R, S->C, S->L, num_sms());
+    if (nb < 1 || !ensure_reduction(nb)) return false;
+    TeArgs<1, T> a{in0, in1, vout, nullptr, x, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->cur_sc, redctl(nb), finish, 1, cfg};
+    e = th_launch<T, MODE>(a, thdev<T>(), nb, S->stream);
   } else if (asm_applies()) {
     if (S->nd == 1) {
       const int nb = asm_te_ctas<1, T, MODE>(S->R, S->C, S->L, num_sms());
@@ -1281,6 +1333,7 @@ cudapcgFlag_t cudapcgSetParametricDensityField(parametricScalarField_t* field, d
   }
   free_ptr(S->d_invd); S->d_invd = nullptr;
   free_ptr(S->d_tab64); free_ptr(S->d_tab32); S->d_tab64 = nullptr; S->d_tab32 = nullptr;
+  free_ptr(S->d_th64); free_ptr(S->d_th32); S->d_th64 = nullptr; S->d_th32 = nullptr; S->th_state = 0;
   invalidate_graphs();
   return CUDAPCG_TRUE;
 }
@@ -1340,6 +1393,7 @@ cudapcgFlag_t cudapcgSetLclMtxs(cudapcgVar_t* Lm) {
   S->have_K = true;
   free_ptr(S->d_K64); free_ptr(S->d_K32); S->d_K64 = nullptr; S->d_K32 = nullptr;
   free_ptr(S->d_tab64); free_ptr(S->d_tab32); S->d_tab64 = nullptr; S->d_tab32 = nullptr;
+  free_ptr(S->d_th64); free_ptr(S->d_th32); S->d_th64 = nullptr; S->d_th32 = nullptr; S->th_state = 0;
   free_ptr(S->d_invd); S->d_invd = nullptr;
   invalidate_graphs();  // captured launches hold the old matrix pointers
   if (S->fluid && !set_fluid_diag()) return CUDAPCG_FALSE;

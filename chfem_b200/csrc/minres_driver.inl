@@ -39,6 +39,14 @@ static bool launch_mr_op_buf(const T* rin, T* rout, const T* q, T* s, double* x,
       a.invd = S->d_invd;
       k_2d_apply<2, T, TE_MR><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<2, T>(), S->stream>>>(a);
     }
+  } else if (th_applies()) {
+    const int nb = th_ctas<T, TE_MR>(S->R, S->C, S->L, num_sms());
+    if (nb < 1 || !ensure_reduction(nb)) return false;
+    TeArgs<1, T> a{rin, q, rout, s, x, d, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->cur_sc, redctl(nb), fin, skip_if_done, cfg};
+    const cudaError_t e = th_launch<T, TE_MR>(a, thdev<T>(), nb, S->stream);
+    S->launches++;
+    if (e != cudaSuccess) { set_err("operator pass", cudaGetErrorString(e)); return false; }
+    return true;
   } else if (asm_applies()) {
     int nb;
     cudaError_t e;

@@ -157,7 +157,7 @@ __global__ void k_2d_invdiag(const uint16_t* keys, const double* Kd, long N, dou
 }
 
 // 2D node keys from the per-pixel material map (EBE input, femhmg_2D.c:14-46)
-__global__ inline void k_keys_from_elements_2d(const uint16_t* em, uint16_t* keys, int R, int C) {
+__global__ void k_keys_from_elements_2d(const uint16_t* em, uint16_t* keys, int R, int C) {
   const long N = (long)R * C;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
     const int r = (int)(i % R), c = (int)(i / R);

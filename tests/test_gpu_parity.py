@@ -238,6 +238,39 @@ def test_operator_and_jacobi(tmp_path, name, analysis, spec, precision):
     assert H.rel_to_max(z, zref) < tol
 
 
+@pytest.mark.parametrize("spec", [("img", (13, 35, 17), 4), ("img", (40, 9, 66), 2), ("img", (1, 2, 3), 3)])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_thermal_pass_equals_generic(tmp_path, spec, precision, monkeypatch):
+    """The thermal pass written for cubic-symmetric conduction matrices (stencil_th.cuh) against
+    the oracle and against the generic thermal pass (CHFEM_B200_THERMAL_OP=generic), 2 to 4
+    materials, thin and ragged shapes."""
+    import pickle
+    from chfem_b200 import _native
+    nf, raw = build_small(tmp_path, "thp", 0, spec)
+    a = host_arrays(nf, raw)
+    a["x"] = np.random.default_rng(7).standard_normal(a["ndof"])
+    pk = str(tmp_path / "a.pkl")
+    pickle.dump(a, open(pk, "wb"))
+    p = subprocess.run([sys.executable, "-c", _ORACLE_APPLY, pk, os.path.join(H.ROOT, "oracle", "liboracle_cudapcg.so"), H.ROOT],
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    yref = np.load(pk + ".y.npy")
+    lib = _native.cudapcg()
+    ys = []
+    for op in ("", "generic"):
+        monkeypatch.setenv("CHFEM_B200_THERMAL_OP", op)
+        setup_model(lib, a)
+        assert lib.cudapcgB200SetPrecision(precision)
+        y = np.zeros(a["ndof"])
+        assert lib.cudapcgB200ApplyOperator(a["x"].ctypes.data_as(ctypes.c_void_p), y.ctypes.data_as(ctypes.c_void_p)), lib.cudapcgB200LastError()
+        lib.cudapcgEnd()
+        ys.append(y)
+    tol = 1e-12 if precision == 0 else 1e-5
+    assert H.rel_to_max(ys[0], yref) < tol
+    assert H.rel_to_max(ys[1], yref) < tol
+    assert H.rel_to_max(ys[0], ys[1]) < (1e-13 if precision == 0 else 1e-5)
+
+
 _ORACLE_APPLY_MANY = r'''
 import ctypes, sys, pickle, numpy as np
 sys.path.insert(0, sys.argv[3])
