@@ -28,6 +28,13 @@ __host__ __device__ constexpr bool shares_edge(int a, int b) {
 
 __host__ __device__ inline int wrap(int v, int n) { v %= n; return v < 0 ? v + n : v; }
 
+// L2 prefetch of [p, p + bytes) rounded out to 16-byte boundaries (sm_90+ bulk prefetch); the
+// rounded range stays inside the 16-byte granules of the buffer it starts in
+__device__ __forceinline__ void asm_prefetch_l2(const void* p, size_t bytes) {
+  const size_t a0 = (size_t)p & ~(size_t)15, a1 = ((size_t)p + bytes + 15) & ~(size_t)15;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a0), "r"((unsigned)(a1 - a0)) : "memory");
+}
+
 // ---- solver scalars living on the device (one record per right-hand side) -----------
 struct DevScalars {
   double delta;      // current r^T M^-1 r (PCG) or (M^-1 r)^T A (M^-1 r) (PMINRES)

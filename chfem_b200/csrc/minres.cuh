@@ -77,7 +77,10 @@ struct MrDirFl {
 template <typename T, int DIM = 3>
 __global__ void __launch_bounds__(PW_NT) k_fl_mr_dir(MrDirFl<T> a) {
   __shared__ double sred[PW_NT / 32];
+  __shared__ double sbd[256];  // interface-node inverse diagonals by fluid key
   if (a.sc->done) return;
+  for (int i = threadIdx.x; i < 256; i += PW_NT) sbd[i] = c_fldiag.border[i];
+  __syncthreads();
   const T b = T(a.sc->beta);
   const long nV = a.nV, nT = a.nV + a.nB;
   double sum = 0.0;
@@ -87,7 +90,7 @@ __global__ void __launch_bounds__(PW_NT) k_fl_mr_dir(MrDirFl<T> a) {
     for (int k = 0; k < cnt; k++) {
       const long j = pore ? (k < DIM ? DIM * t + k : DIM * nV + t) : DIM * nV + t;
       T inv = T(1);
-      if (a.precond) inv = pore ? T(c_fldiag.pore[k]) : T(c_fldiag.border[a.bkeys[t - nV]]);
+      if (a.precond) inv = pore ? T(c_fldiag.pore[k]) : T(sbd[a.bkeys[t - nV]]);
       const T z = a.r[j] * inv;
       a.d[j] = fma(b, a.d[j], z);
       const T qn = fma(b, a.q[j], a.s[j]);

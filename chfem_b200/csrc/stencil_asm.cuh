@@ -22,11 +22,6 @@ inline size_t asm_smem_bytes() {
   return ((size_t)asm_table_words(ND, Lo::BS) + (size_t)(ZB + 2) * pp * Lo::PS) * sizeof(T);
 }
 
-// L2 prefetch of [p, p + bytes) rounded out to 16-byte boundaries (sm_90+ bulk prefetch)
-__device__ __forceinline__ void asm_prefetch_l2(const void* p, size_t bytes) {
-  const size_t a0 = (size_t)p & ~(size_t)15, a1 = ((size_t)p + bytes + 15) & ~(size_t)15;
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a0), "r"((unsigned)(a1 - a0)) : "memory");
-}
 
 // does any of the ZB nodes use the neighbour position (Q plane, DR row, DC column)?
 template <int ND, int ZB>

@@ -75,7 +75,10 @@ __global__ void __launch_bounds__(FL_NT) k_fl_apply(FlArgs<T> a) {
   constexpr int NE = 1 << DIM, ED = (DIM + 1) * NE, PC = DIM * NE, NO = DIM == 3 ? 27 : 9;
   constexpr unsigned FULL = (1u << NE) - 1u;
   __shared__ double sred[FL_NT / 32];
+  __shared__ T sbd[256];  // interface-node inverse diagonals by fluid key (per-thread keys: shared, not constant, memory)
   if (a.skip_if_done && a.sc->done) return;
+  for (int i = threadIdx.x; i < 256; i += FL_NT) sbd[i] = T(c_fldiag.border[i]);
+  __syncthreads();
   const long nV = a.nV, nT = a.nV + a.nB;
   const int R = a.R, C = a.C, L = a.L;
   const T beta = (MODE == TE_PCG) ? T(a.sc->beta) : T(0);
@@ -119,7 +122,7 @@ __global__ void __launch_bounds__(FL_NT) k_fl_apply(FlArgs<T> a) {
         for (int k = 0; k < DIM; k++) vv[k] = fl_in<T, MODE>(a, DIM * (size_t)dof + k, beta, alpha, ivv[k]);
       }
       T ip = ivp;
-      if (MODE == TE_MR && pre && !vel) ip = T(c_fldiag.border[a.bkeys[dof - (uint32_t)nV]]);
+      if (MODE == TE_MR && pre && !vel) ip = sbd[a.bkeys[dof - (uint32_t)nV]];
       const T vp = fl_in<T, MODE>(a, DIM * (size_t)nV + dof, beta, alpha, ip);
 #pragma unroll
       for (int e = 0; e < NE; e++) {
@@ -155,7 +158,7 @@ __global__ void __launch_bounds__(FL_NT) k_fl_apply(FlArgs<T> a) {
     for (int k = 0; k < cnt; k++) {
       const size_t j = offs[k];
       T iv = T(1);
-      if (MODE == TE_MR && pre) iv = pore ? (k == DIM ? ivp : ivv[k < DIM ? k : 0]) : T(c_fldiag.border[fk]);
+      if (MODE == TE_MR && pre) iv = pore ? (k == DIM ? ivp : ivv[k < DIM ? k : 0]) : sbd[fk];
       const T v = fl_in<T, MODE>(a, j, beta, alpha, iv);
       a.y[j] = outv[k];
       if (MODE == TE_PCG) a.vout[j] = v;
@@ -205,7 +208,10 @@ struct FlPw {
 template <typename T, int MODE, int DIM = 3>
 __global__ void __launch_bounds__(PW_NT) k_fl_point(FlPw<T> a) {
   __shared__ double sred[PW_NT / 32];
+  __shared__ double sbd[256];  // interface-node inverse diagonals by fluid key
   if (MODE != PW_INIT && MODE != PW_CHECK && a.sc->done) return;
+  for (int i = threadIdx.x; i < 256; i += PW_NT) sbd[i] = c_fldiag.border[i];
+  __syncthreads();
   const long nV = a.nV, nT = a.nV + a.nB;
   const double alpha64 = (MODE == PW_PCG) ? a.sc->alpha : 0.0;
   const T alpha = T(alpha64);
@@ -223,7 +229,7 @@ __global__ void __launch_bounds__(PW_NT) k_fl_point(FlPw<T> a) {
       for (int k = 0; k <= DIM; k++) inv[k] = c_fldiag.pore[k];
     } else {
       idx[0] = DIM * nV + t; cnt = 1;
-      inv[0] = c_fldiag.border[a.bkeys[t - nV]];
+      inv[0] = sbd[a.bkeys[t - nV]];
     }
     for (int k = 0; k < cnt; k++) {
       const long j = idx[k];
