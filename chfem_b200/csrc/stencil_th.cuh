@@ -18,11 +18,9 @@
 // B200 design: a CTA owns a 32 x TC column of nodes and marches through a run of layers.  Each
 // layer's plane of the formed input (with its one-node halo) goes through a 3-slot shared-memory
 // ring; the global loads of the plane after it are issued before the current node is computed
-// and held in registers until their slot is free, and the tile's rows of the layers TH_PD
-// further on are prefetched into L2 (bulk prefetch), so that enough DRAM reads are in flight.
-// Each thread reads the 9 values around its column of a plane once into registers and adds them
-// into the node below (th_finish), at and above (th_start) them, so a node costs 9
-// shared-memory loads and two planes live in registers.
+// and held in registers until their slot is free.  Each thread reads the 9 values around its
+// column of a plane once into registers and adds them into the node below (th_finish), at and
+// above (th_start) them, so a node costs 9 shared-memory loads and two planes live in registers.
 // All per-node index arithmetic is incremental (no division in the layer loop).  Modes, outputs
 // and finishers are those of k_te_apply (stencil_te.cuh).
 #pragma once
@@ -58,8 +56,6 @@ struct ThGeom {
   static constexpr int PR = TE_TR + 2, PC = TC + 2, PP = PR * PC, NT = TE_TR * TC;
   static constexpr int PER = (PP + NT - 1) / NT;  // staged points per thread
 };
-
-constexpr int TH_PD = 4;  // L2 prefetch distance in layers
 
 template <typename T, int TC>
 inline size_t th_smem_bytes() {
@@ -180,23 +176,6 @@ __global__ void __launch_bounds__(TE_TR * TC, sizeof(T) == 8 ? 2 : 3) k_th_apply
     const int r = r0 + threadIdx.x, c = c0 + threadIdx.y;
     const bool active = (r < R) && (c < C);
     const size_t col = active ? (size_t)r + (size_t)c * R : 0;
-    // L2 prefetch of the tile's own rows of a layer (one column per lane of the first warp), so
-    // that the DRAM reads of the layers ahead are in flight while this layer is computed
-    const int prow = min(TE_TR, R - r0);
-    auto prefetch = [&](size_t lofs) {
-      if (tid < TC && c0 + tid < C) {
-        const size_t base = (size_t)r0 + (size_t)(c0 + tid) * R + lofs;
-        asm_prefetch_l2(a.in0 + base, (size_t)prow * sizeof(T));
-        if (TWO_IN) asm_prefetch_l2(a.in1 + base, (size_t)prow * sizeof(T));
-        asm_prefetch_l2(a.keys + base, (size_t)prow * sizeof(uint16_t));
-      }
-    };
-    size_t lofs_pf = layer_ofs(l0 + 1);
-    for (int q = 1; q <= TH_PD && l0 + 1 + q <= l1; q++) {  // layers l0 + 2 .. l0 + 1 + TH_PD
-      lofs_pf += RC;
-      if (lofs_pf >= (size_t)L * RC) lofs_pf -= (size_t)L * RC;
-      prefetch(lofs_pf);
-    }
     // ring slots of the planes below, at and above the current node
     T* s_m = sV;
     T* s_0 = sV + PP;
@@ -225,11 +204,6 @@ __global__ void __launch_bounds__(TE_TR * TC, sizeof(T) == 8 ? 2 : 3) k_th_apply
         lofs_next += RC;
         if (lofs_next >= (size_t)L * RC) lofs_next -= (size_t)L * RC;
         load(lofs_next);
-      }
-      if (l + 1 + TH_PD < l1) {  // layer l + 2 + TH_PD: TH_PD after the one just loaded
-        lofs_pf += RC;
-        if (lofs_pf >= (size_t)L * RC) lofs_pf -= (size_t)L * RC;
-        prefetch(lofs_pf);
       }
       __syncthreads();
       gather(s_p, vn);
