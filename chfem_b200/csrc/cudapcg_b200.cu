@@ -372,8 +372,9 @@ static bool ensure_invd() {
   CKV(cudaMalloc(&S->d_invd, sizeof(double) * S->N * S->nd));
   const long g = std::max(1L, std::min<long>((S->N + 255) / 256, 8L * num_sms()));
   if (S->dim2) {
-    if (S->nd == 1) k_2d_invdiag<1><<<(int)g, 256, 0, S->stream>>>(S->d_keys, S->d_K64, S->N, S->d_invd);
-    else k_2d_invdiag<2><<<(int)g, 256, 0, S->stream>>>(S->d_keys, S->d_K64, S->N, S->d_invd);
+    const double fr = S->sdf_max - S->sdf_min;
+    if (S->nd == 1) k_2d_invdiag<1><<<(int)g, 256, 0, S->stream>>>(S->d_keys, S->d_K64, S->R, S->C, S->d_sdf, S->sdf_min, fr, S->d_invd);
+    else k_2d_invdiag<2><<<(int)g, 256, 0, S->stream>>>(S->d_keys, S->d_K64, S->R, S->C, S->d_sdf, S->sdf_min, fr, S->d_invd);
   } else if (S->nd == 1) k_sdf_invdiag<1><<<(int)g, 256, 0, S->stream>>>(S->d_keys, S->d_sdf, S->sdf_min, S->sdf_max - S->sdf_min, S->d_K64, S->R, S->C, S->L, S->d_invd);
   else k_sdf_invdiag<3><<<(int)g, 256, 0, S->stream>>>(S->d_keys, S->d_sdf, S->sdf_min, S->sdf_max - S->sdf_min, S->d_K64, S->R, S->C, S->L, S->d_invd);
   CKV(cudaGetLastError());
@@ -502,12 +503,12 @@ static bool launch_apply(const T* in0, const T* in1, T* vout, T* y, bool fuse, i
     const MrCfg cfg{S->tol, 0, S->resnorm, S->precond, 0};
     if (S->nd == 1) {
       TeArgs<1, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, 1, S->cur_sc, redctl(nb), finish, skip_if_done, cfg};
-      a.invd = S->d_invd;
+      sdf_args(a);
       if (fuse) k_2d_apply<1, T, TE_PCG><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<1, T>(), S->stream>>>(a);
       else k_2d_apply<1, T, TE_PLAIN><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<1, T>(), S->stream>>>(a);
     } else {
       TeArgs<2, T> a{in0, in1, vout, y, nullptr, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, 1, S->cur_sc, redctl(nb), finish, skip_if_done, cfg};
-      a.invd = S->d_invd;
+      sdf_args(a);
       if (fuse) k_2d_apply<2, T, TE_PCG><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<2, T>(), S->stream>>>(a);
       else k_2d_apply<2, T, TE_PLAIN><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<2, T>(), S->stream>>>(a);
     }
@@ -616,11 +617,11 @@ static bool launch_te_mode(const T* in0, const T* in1, T* vout, double* x, int f
     if (!ensure_reduction(nb)) return false;
     if (S->nd == 1) {
       TeArgs<1, T> a{in0, in1, vout, nullptr, x, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, 1, S->cur_sc, redctl(nb), finish, 1, cfg};
-      a.invd = S->d_invd;
+      sdf_args(a);
       k_2d_apply<1, T, MODE><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<1, T>(), S->stream>>>(a);
     } else {
       TeArgs<2, T> a{in0, in1, vout, nullptr, x, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, 1, S->cur_sc, redctl(nb), finish, 1, cfg};
-      a.invd = S->d_invd;
+      sdf_args(a);
       k_2d_apply<2, T, MODE><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<2, T>(), S->stream>>>(a);
     }
     e = cudaGetLastError();

@@ -63,16 +63,71 @@ void write_bin(const std::string& fn, const double* v, size_t n) {
   fwrite(v, sizeof(double), n, f);
   fclose(f);
 }
+// 2D exported field (flux k grad T, 2 per node; stress D eps, 3 per node: xx, yy, xy, with D the
+// plane-strain or plane-stress matrix of the element matrices): at each node the mean over its 4
+// pixels of the pixel's field at the node's corner, each pixel on the cell's +axis side seeing
+// the load case's jump on its +axis side nodes (a node gathers its 4 corner values: no
+// accumulation race).  Under plane stress the reference's stress helper takes E / (1 - nu) for
+// the factor of D (femhmg_elastic_2D.c:815-847), not its element matrices' E / (1 - nu^2).
+std::vector<double> fields_2d(const Model& m, int dir, const double* x) {
+  const long R = m.ny, C = m.nx, N = m.N;
+  const int nd = m.nd, nf = m.analysis == THERMAL ? 2 : 3;
+  int axis, comp;
+  case_axis(m, dir, axis, comp);
+  const double jump = (double)(axis == 0 ? m.nx : m.ny);
+  static const int FACE[2][2] = {{1, 2}, {2, 3}};
+  auto dr = [](int k) { return -((k & 3) >> 1); };
+  auto dc = [](int k) { return ((k & 3) == 1 || (k & 3) == 2) ? 1 : 0; };
+  std::vector<double> out((size_t)nf * N, 0.0);
+#pragma omp parallel for schedule(static)
+  for (long n = 0; n < N; n++) {
+    const long r = n % R, c = n / R;
+    double f[3] = {0, 0, 0};
+    for (int k = 0; k < 4; k++) {
+      const long er = ((r - dr(k) - 1) % R + R) % R, ec = ((c - dc(k)) % C + C) % C;
+      const bool boundary = axis == 0 ? ec == C - 1 : er == 0;
+      const double px = dc(k), py = -dr(k);  // the node's corner in the pixel
+      double g[2][2] = {{0, 0}, {0, 0}};       // [component][d/dx, d/dy]
+      for (int j = 0; j < 4; j++) {
+        const long node = ((er + 1 + dr(j)) % R + R) % R + ((ec + dc(j)) % C + C) % C * R;
+        const int xj = dc(j), yj = -dr(j);
+        const double dx = (xj ? 1.0 : -1.0) * (yj ? py : 1.0 - py), dy = (xj ? px : 1.0 - px) * (yj ? 1.0 : -1.0);
+        const bool on_face = boundary && (FACE[axis][0] == j || FACE[axis][1] == j);
+        for (int ci = 0; ci < nd; ci++) {
+          const double v = x[node * nd + ci] + ((on_face && ci == comp) ? jump : 0.0);
+          g[ci][0] += dx * v;
+          g[ci][1] += dy * v;
+        }
+      }
+      const int mat = m.elem_mat[er + ec * R];
+      if (m.analysis == THERMAL) {
+        f[0] += 0.25 * m.props[mat] * g[0][0];
+        f[1] += 0.25 * m.props[mat] * g[0][1];
+      } else {
+        double D[3][3];
+        plane_D(m, mat, D);
+        const double exx = g[0][0], eyy = g[1][1], gxy = g[0][1] + g[1][0];
+        for (int t = 0; t < 3; t++) f[t] += 0.25 * (D[t][0] * exx + D[t][1] * eyy + D[t][2] * gxy);
+      }
+    }
+    for (int t = 0; t < nf; t++) out[(size_t)n * nf + t] = f[t];
+  }
+  return out;
+}
+
 void export_fields(const Model& m, int dir, const double* x, int block_index) {
   const std::string pre = m.nf_noext + "_";
   const std::string suf = "_" + std::to_string(dir) + ".bin";
-  if (m.analysis == FLUID) {  // femhmg_fluid_3D.c:312-360
-    std::vector<double> u(3 * (size_t)m.N, 0.0), p(m.N, 0.0);
+  if (m.analysis == FLUID) {  // femhmg_fluid_3D.c:312-360, femhmg_fluid_2D.c:314-350
+    const int D = m.dim2 ? 2 : 3;
+    const uint8_t full = m.dim2 ? 15 : 255;
+    std::vector<double> u(D * (size_t)m.N, 0.0), p(m.N, 0.0);
     for (long n = 0; n < m.N; n++) {
       const uint32_t id = m.dof_of_node[n];
       const uint8_t fk = m.fluid_keys[n];
-      if (fk == 255) { u[3 * n] = x[3 * (size_t)id]; u[3 * n + 1] = x[3 * (size_t)id + 1]; u[3 * n + 2] = x[3 * (size_t)id + 2]; }
-      if (fk) p[n] = x[3 * (size_t)m.nV + id];
+      if (fk == full)
+        for (int c = 0; c < D; c++) u[D * n + c] = x[D * (size_t)id + c];
+      if (fk) p[n] = x[D * (size_t)m.nV + id];
     }
     write_bin(pre + "velocity" + suf, u.data(), u.size());
     write_bin(pre + "pressure" + suf, p.data(), p.size());
@@ -81,6 +136,11 @@ void export_fields(const Model& m, int dir, const double* x, int block_index) {
   write_bin(pre + (m.analysis == THERMAL ? "temperature" : "displacement") + suf, x, m.ndof);
   int axis, comp;
   case_axis(m, dir, axis, comp);
+  if (m.dim2) {  // femhmg_thermal_2D.c:423-596, femhmg_elastic_2D.c:908-1170
+    const std::vector<double> f = fields_2d(m, dir, x);
+    write_bin(pre + (m.analysis == THERMAL ? "flux" : "stress") + suf, f.data(), f.size());
+    return;
+  }
   const int nf = m.analysis == THERMAL ? 3 : 6;
   std::vector<double> field((size_t)nf * m.N);
   if (!cudapcgB200ComputeFields(block_index, axis, comp, (double)axis_len(m, axis), m.props, field.data())) {
@@ -224,6 +284,7 @@ bool read_density_field(Model& m, const char* fn) {
   const unsigned ref = m.refinement, rows = m.frows, cols = m.fcols, slices = m.fslices;
   const size_t R = m.ny, C = m.nx, N = (size_t)m.N, nfile = (size_t)rows * cols * slices;
   const size_t sz = m.data_type ? 8 : 4;
+  const size_t lref = m.dim2 ? 1 : ref;  // a 2D image has one layer
   std::vector<unsigned char> raw(sz * N);
   FILE* f = fopen(fn, "rb");
   if (!f) { fail(std::string("failed to open ") + fn); return false; }
@@ -252,7 +313,7 @@ bool read_density_field(Model& m, const char* fn) {
       for (size_t j = 0; j < cols; j++) {
         const double v = value(j + i * cols + k * rows * cols) * m.props[m.elem_mat[(i + j * R + k * R * C) * ref] * stride];
         const uint16_t q = (uint16_t)(65535 * (v - vmin) / dv);
-        for (size_t kk = ref * k; kk < ref * (k + 1); kk++)
+        for (size_t kk = lref * k; kk < lref * (k + 1); kk++)
           for (size_t ii = ref * i; ii < ref * (i + 1); ii++)
             for (size_t jj = ref * j; jj < ref * (j + 1); jj++) m.sdf[ii + jj * R + kk * R * C] = q;
       }
@@ -411,7 +472,7 @@ logical hmgInit(char* data_filename, char* elem_filename, char* sdf_filename, ui
   if (!read_colors(*m, data, elem_filename)) { delete m; return 0; }
   if (m->dim2) {
     // 2D: the node keys (4 bits per pixel) or the Stokes DOF numbering are built on the host
-    if (sdf_filename && m->analysis != FLUID) { fail("a scalar density field is not provided for 2D images"); delete m; return 0; }
+    if (sdf_filename && m->analysis != FLUID && !read_density_field(*m, sdf_filename)) { delete m; return 0; }
     if (!ensure_host_maps(*m)) { delete m; return 0; }
   } else if (m->analysis == FLUID) {
     // the sizes of the DOF numbering here; the numbering itself on the device at upload
@@ -550,10 +611,6 @@ void hmgSolveHomogenization(void) {
   Model& m = *g_m;
   if (!m.sdf.empty() && (g_export_fields || m.has_thermal_expansion)) {
     fail("field export and thermal expansion are not provided with a scalar density field");
-    return;
-  }
-  if (m.dim2 && (g_export_fields || m.has_thermal_expansion)) {
-    fail("field export and thermal expansion are not provided for 2D images");
     return;
   }
   const auto t_all = std::chrono::steady_clock::now();
@@ -754,11 +811,14 @@ void hmgSolveHomogenization(void) {
     std::vector<double> rhs(m.ndof);
     assemble_rhs_thermal_expansion(m, rhs.data());
     double volume[6];
-    const bool ok = cudapcgSetRHS(rhs.data()) && cudapcgSetX0(nullptr, 0) && (cudapcgSolve(nullptr), true) &&
-                    cudapcgB200VolumeTerm(m.CB.data(), 6, volume);
+    std::vector<double> xs(m.dim2 ? m.ndof : 0);  // 2D: the stress sums are taken on the host
+    const bool ok = cudapcgSetRHS(rhs.data()) && cudapcgSetX0(nullptr, 0) &&
+                    (cudapcgSolve(m.dim2 ? xs.data() : nullptr), true) &&
+                    (m.dim2 || cudapcgB200VolumeTerm(m.CB.data(), 6, volume));
     if (!ok) { fail(std::string("thermal expansion: ") + cudapcgB200LastError()); cudapcgEnd(); return; }
     if (!g_quiet) cudapcgPrintSolverMetrics();
-    update_thermal_expansion(m, volume);
+    if (m.dim2) update_thermal_expansion_2d(m, xs.data());
+    else update_thermal_expansion(m, volume);
   }
   cudapcgSetX0(nullptr, 0);
   cudapcgFreeArrays();
@@ -794,23 +854,24 @@ void hmgPrintConstitutiveMtx(void) {
     printf("\n");
   }
   printf("-------------------------------------------------------\n");
-  if (m.analysis == ELASTIC && m.has_thermal_expansion) {  // femhmg_elastic_3D.c:1625-1631
+  if (m.analysis == ELASTIC && m.has_thermal_expansion) {  // femhmg_elastic_3D.c:1625-1631, femhmg_elastic_2D.c:754-759
     const double* a = m.thermal_expansion;
     printf("Effective thermal expansion:\n");
-    printf("  %.8e  %.8e  %.8e\n  %.8e  %.8e  %.8e\n  %.8e  %.8e  %.8e\n", a[0], a[5], a[4], a[5], a[1], a[3], a[4], a[3], a[2]);
+    if (m.dim2) printf("  %.8e  %.8e\n  %.8e  %.8e\n", a[0], a[2], a[2], a[1]);
+    else printf("  %.8e  %.8e  %.8e\n  %.8e  %.8e  %.8e\n  %.8e  %.8e  %.8e\n", a[0], a[5], a[4], a[5], a[1], a[3], a[4], a[3], a[2]);
     printf("-------------------------------------------------------\n");
   }
 }
 var* hmgGetConstitutiveMtx(void) { return g_m ? g_m->C : nullptr; }
 unsigned int hmgGetConstitutiveMtxDim(void) { return g_m ? g_m->C_dim : 0; }
 var* hmgGetThermalExpansion(void) { return (g_m && g_m->analysis == ELASTIC && g_m->has_thermal_expansion) ? g_m->thermal_expansion : nullptr; }
-unsigned int hmgGetThermalExpansionDim(void) { return hmgGetThermalExpansion() ? 6 : 0; }
+unsigned int hmgGetThermalExpansionDim(void) { return hmgGetThermalExpansion() ? (g_m->dim2 ? 3 : 6) : 0; }  // femhmg.c:1341-1345
 logical hmgSaveConstitutiveMtx(const char* filename) {
   if (!g_m) return 0;
   FILE* f = fopen(filename, "wb");
   if (!f) return 0;
   fwrite(g_m->C, sizeof(double), g_m->C_dim, f);
-  if (hmgGetThermalExpansionDim()) fwrite(g_m->thermal_expansion, sizeof(double), 6, f);  // femhmg.c:1362-1363
+  if (hmgGetThermalExpansionDim()) fwrite(g_m->thermal_expansion, sizeof(double), hmgGetThermalExpansionDim(), f);  // femhmg.c:1362-1363
   fclose(f);
   return 1;
 }

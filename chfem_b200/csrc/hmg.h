@@ -81,6 +81,10 @@ void update_C(Model& m, int direction, const double* x);
 // effective expansion from the tensor C and the volume term of its solution
 void assemble_rhs_thermal_expansion(const Model& m, double* rhs);
 void update_thermal_expansion(Model& m, const double* volume);
+// 2D: from the solution itself (xx, yy, xy into thermal_expansion[0..2])
+void update_thermal_expansion_2d(Model& m, const double* x);
+// 2D elastic: plane constitutive matrix of material k (xx, yy, xy) used by the element matrices
+void plane_D(const Model& m, int k, double D[3][3]);
 // material index of model voxel (r, c, l) (refined grid), from elem_mat or from the colours
 int voxel_material(const Model& m, long r, long c, long l);
 void update_C_from_volume(Model& m, int direction, const double* volume);

@@ -103,6 +103,7 @@ static bool build_maps_2d(Model& m, std::string& err);
 static void build_local_matrices_2d(Model& m);
 static void assemble_rhs_2d(const Model& m, int dir, double* rhs);
 static void update_C_2d(Model& m, int dir, const double* x);
+static void assemble_rhs_thermal_expansion_2d(const Model& m, double* rhs);
 
 bool build_maps(Model& m, std::string& err) {
   if (m.dim2) return build_maps_2d(m, err);
@@ -377,12 +378,37 @@ void update_C(Model& m, int dir, const double* x) {
 // sigma_m = D_m alpha_m (1,1,1,0,0,0) = alpha_m E_m / (1 - 2 nu_m) on the normal components.
 // The reference evaluates the element load B^T sigma at the voxel centre, where every shape
 // gradient is 1/4 (+-1, +-1, +-1), with the sign + where the node sits at coordinate 1.
+// effective expansion: C alpha = beta, n = 6 (3D) or 3 (2D), elimination with partial pivoting
+static void solve_expansion(Model& m, const double* beta, int n) {
+  double M[6][7];
+  for (int i = 0; i < n; i++) {
+    for (int j = 0; j < n; j++) M[i][j] = m.C[n * i + j];
+    M[i][n] = beta[i];
+  }
+  for (int i = 0; i < n; i++) {
+    int p = i;
+    for (int j = i + 1; j < n; j++) if (std::fabs(M[j][i]) > std::fabs(M[p][i])) p = j;
+    if (p != i) for (int k = 0; k <= n; k++) std::swap(M[i][k], M[p][k]);
+    for (int j = i + 1; j < n; j++) {
+      const double s = M[j][i] / M[i][i];
+      for (int k = i; k <= n; k++) M[j][k] -= s * M[i][k];
+    }
+  }
+  for (int i = n - 1; i >= 0; i--) {
+    double v = M[i][n];
+    for (int j = i + 1; j < n; j++) v -= M[i][j] * m.thermal_expansion[j];
+    m.thermal_expansion[i] = v / M[i][i];
+  }
+  for (int i = n; i < 6; i++) m.thermal_expansion[i] = 0.0;
+}
+
 static double thermal_stress(const Model& m, int mat) {
   const double E = m.props[2 * mat], nu = m.props[2 * mat + 1];
   return m.alpha[mat] * E / (1.0 - 2.0 * nu);
 }
 
 void assemble_rhs_thermal_expansion(const Model& m, double* rhs) {
+  if (m.dim2) { assemble_rhs_thermal_expansion_2d(m, rhs); return; }
   std::memset(rhs, 0, sizeof(double) * m.ndof);
   const long R = m.ny, C = m.nx, L = m.nz, N = m.N;
   double f[4][24];
@@ -417,26 +443,7 @@ void update_thermal_expansion(Model& m, const double* volume) {
   for (unsigned mat = 0; mat < m.nmat && mat < 4; mat++)
     for (int k = 0; k < 3; k++) stress[k] -= count[mat] * thermal_stress(m, (int)mat);
   for (int k = 0; k < 6; k++) beta[k] = -stress[k] / (double)m.N;
-  // effective expansion: C alpha = beta (6x6 elimination with partial pivoting)
-  double M[6][7];
-  for (int i = 0; i < 6; i++) {
-    for (int j = 0; j < 6; j++) M[i][j] = m.C[6 * i + j];
-    M[i][6] = beta[i];
-  }
-  for (int i = 0; i < 6; i++) {
-    int p = i;
-    for (int j = i + 1; j < 6; j++) if (std::fabs(M[j][i]) > std::fabs(M[p][i])) p = j;
-    if (p != i) for (int k = 0; k < 7; k++) std::swap(M[i][k], M[p][k]);
-    for (int j = i + 1; j < 6; j++) {
-      const double s = M[j][i] / M[i][i];
-      for (int k = i; k < 7; k++) M[j][k] -= s * M[i][k];
-    }
-  }
-  for (int i = 5; i >= 0; i--) {
-    double v = M[i][6];
-    for (int j = i + 1; j < 6; j++) v -= M[i][j] * m.thermal_expansion[j];
-    m.thermal_expansion[i] = v / M[i][i];
-  }
+  solve_expansion(m, beta, 6);
 }
 
 int voxel_material(const Model& m, long r, long c, long l) {
@@ -537,6 +544,22 @@ static bool count_pore_nodes_2d(Model& m, std::string& err) {
   return true;
 }
 
+// Plane constitutive matrix of material k (xx, yy, xy): plane strain, or plane stress under
+// CHFEM_B200_PLANE_STRESS=1 (femhmg_elastic_2D.c:56-200)
+void plane_D(const Model& m, int k, double D[3][3]) {
+  const char* ps = getenv("CHFEM_B200_PLANE_STRESS");
+  const double E = m.props[2 * k], nu = m.props[2 * k + 1];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) D[i][j] = 0.0;
+  if (ps && ps[0] == '1') {
+    const double f = E / (1.0 - nu * nu);
+    D[0][0] = D[1][1] = f; D[0][1] = D[1][0] = f * nu; D[2][2] = f * 0.5 * (1.0 - nu);
+  } else {
+    const double lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), mu = E / (2.0 * (1.0 + nu));
+    D[0][0] = D[1][1] = lam + 2.0 * mu; D[0][1] = D[1][0] = lam; D[2][2] = mu;
+  }
+}
+
 static void build_local_matrices_2d(Model& m) {
   const double g[2] = {0.5 - 0.5 / std::sqrt(3.0), 0.5 + 0.5 / std::sqrt(3.0)};
   double grad[4][4][2];  // [qp][node][x, y]
@@ -589,19 +612,10 @@ static void build_local_matrices_2d(Model& m) {
         }
     }
   } else {
-    const char* ps = getenv("CHFEM_B200_PLANE_STRESS");
-    const bool stress = ps && ps[0] == '1';
     m.CB.assign((size_t)24 * m.nmat, 0.0);  // [mat][stress s (xx, yy, xy)][dof]
     for (unsigned k = 0; k < m.nmat; k++) {
-      const double E = m.props[2 * k], nu = m.props[2 * k + 1];
-      double D[3][3] = {{0}};
-      if (stress) {
-        const double f = E / (1.0 - nu * nu);
-        D[0][0] = D[1][1] = f; D[0][1] = D[1][0] = f * nu; D[2][2] = f * 0.5 * (1.0 - nu);
-      } else {
-        const double lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), mu = E / (2.0 * (1.0 + nu));
-        D[0][0] = D[1][1] = lam + 2.0 * mu; D[0][1] = D[1][0] = lam; D[2][2] = mu;
-      }
+      double D[3][3];
+      plane_D(m, (int)k, D);
       for (int q = 0; q < 4; q++) {
         double B[3][8] = {{0}};
         for (int a = 0; a < 4; a++) {
@@ -651,15 +665,43 @@ static void assemble_rhs_2d(const Model& m, int dir, double* rhs) {
   const int nd = m.nd, ed = 4 * nd;
   for_boundary_pixels(m, axis, [&](long r, long c) {
     const double* K = m.Kdense.data() + (size_t)m.elem_mat[r + c * R] * ed * ed;
+    const double f_e = sdf_scale(m, r + c * R);
     for (int a = 0; a < 4; a++) {
       const long n = elem_node_2d(r, c, a, R, C);
       for (int ci = 0; ci < nd; ci++) {
         double s = 0.0;
         for (int f = 0; f < 2; f++) s += K[(a * nd + ci) * ed + FACE2D[axis][f] * nd + comp];
-        rhs[n * nd + ci] -= s * jump;
+        rhs[n * nd + ci] -= f_e * s * jump;
       }
     }
   });
+}
+
+// sum_e f_e CB_e x_e over all pixels (flux or stress components; f_e the pixel's density scale,
+// 1 without a density field; femhmg_thermal_2D.c:293-372, femhmg_elastic_2D.c:638-742)
+static void volume_term_2d(const Model& m, const double* x, double* acc) {
+  const long R = m.ny, C = m.nx, N = m.N;
+  const int nd = m.nd, ns = tensor_dim(m), ec = 4 * nd;
+  for (int s = 0; s < 3; s++) acc[s] = 0.0;
+#pragma omp parallel
+  {
+    double loc[3] = {0, 0, 0};
+#pragma omp for schedule(static)
+    for (long e = 0; e < N; e++) {
+      const long r = e % R, c = e / R;
+      const double* CB = m.CB.data() + (size_t)m.elem_mat[e] * ns * ec;
+      double le[3] = {0, 0, 0};
+      for (int a = 0; a < 4; a++) {
+        const long n = elem_node_2d(r, c, a, R, C);
+        for (int ci = 0; ci < nd; ci++)
+          for (int s = 0; s < ns; s++) le[s] += CB[s * ec + a * nd + ci] * x[n * nd + ci];
+      }
+      const double f_e = sdf_scale(m, e);
+      for (int s = 0; s < ns; s++) loc[s] += f_e * le[s];
+    }
+#pragma omp critical
+    for (int s = 0; s < ns; s++) acc[s] += loc[s];
+  }
 }
 
 static void update_C_2d(Model& m, int dir, const double* x) {
@@ -686,29 +728,74 @@ static void update_C_2d(Model& m, int dir, const double* x) {
   case_axis(m, dir, axis, comp);
   const double jump = (double)(axis == 0 ? m.nx : m.ny);
   const int nd = m.nd, ns = tensor_dim(m), ec = 4 * nd, col = tensor_column(m, dir);
-  double acc[3] = {0, 0, 0};
-#pragma omp parallel
-  {
-    double loc[3] = {0, 0, 0};
-#pragma omp for schedule(static)
-    for (long e = 0; e < N; e++) {
-      const long r = e % R, c = e / R;
-      const double* CB = m.CB.data() + (size_t)m.elem_mat[e] * ns * ec;
-      for (int a = 0; a < 4; a++) {
-        const long n = elem_node_2d(r, c, a, R, C);
-        for (int ci = 0; ci < nd; ci++)
-          for (int s = 0; s < ns; s++) loc[s] += CB[s * ec + a * nd + ci] * x[n * nd + ci];
-      }
-    }
-#pragma omp critical
-    for (int s = 0; s < ns; s++) acc[s] += loc[s];
-  }
+  double acc[3];
+  volume_term_2d(m, x, acc);
   for_boundary_pixels(m, axis, [&](long r, long c) {
     const double* CB = m.CB.data() + (size_t)m.elem_mat[r + c * R] * ns * ec;
+    const double f_e = sdf_scale(m, r + c * R);
     for (int f = 0; f < 2; f++)
-      for (int s = 0; s < ns; s++) acc[s] += CB[s * ec + FACE2D[axis][f] * nd + comp] * jump;
+      for (int s = 0; s < ns; s++) acc[s] += f_e * CB[s * ec + FACE2D[axis][f] * nd + comp] * jump;
   });
   for (int s = 0; s < ns; s++) m.C[s * ns + col] = acc[s] / (double)N;
+}
+
+// ---- 2D thermal expansion (femhmg_elastic_2D.c:277-300 RHS, :388-528 effective expansion) ----
+// A unit temperature rise gives material m the in-plane eigenstrain alpha_m (1, 1, 0) and the
+// stress D_m alpha_m (1, 1, 0), D_m the plane matrix of the element matrices (plane strain:
+// alpha E / ((1 + nu)(1 - 2 nu)) on both normal components).  The element load is B^T sigma at
+// the pixel centre, where every shape gradient is +-1/2 (+ where the node sits at coordinate 1).
+// Under plane stress the reference's helpers (femhmg_elastic_2D.c:849-866, :868-906) take
+// E / (1 - nu) for the factor of D, which is not the plane-stress matrix of its own element
+// matrices (E / (1 - nu^2), :148-200): a homogeneous image would not return its own alpha.  Here
+// both use the element matrices' D.
+static void thermal_stress_2d(const Model& m, int mat, double s[2]) {
+  double D[3][3];
+  plane_D(m, mat, D);
+  s[0] = m.alpha[mat] * (D[0][0] + D[0][1]);
+  s[1] = m.alpha[mat] * (D[1][0] + D[1][1]);
+}
+
+static void assemble_rhs_thermal_expansion_2d(const Model& m, double* rhs) {
+  std::memset(rhs, 0, sizeof(double) * m.ndof);
+  const long R = m.ny, C = m.nx, N = m.N;
+  std::vector<double> f((size_t)8 * m.nmat);
+  for (unsigned mat = 0; mat < m.nmat; mat++) {
+    double sn[2];
+    thermal_stress_2d(m, (int)mat, sn);
+    for (int a = 0; a < 4; a++) {
+      f[8 * mat + 2 * a] = 0.5 * sn[0] * (nxi(a) ? 1.0 : -1.0);
+      f[8 * mat + 2 * a + 1] = 0.5 * sn[1] * (neta(a) ? 1.0 : -1.0);
+    }
+  }
+  for (long e = 0; e < N; e++) {
+    const long r = e % R, c = e / R;
+    const double* fe = f.data() + 8 * (size_t)m.elem_mat[e];
+    for (int a = 0; a < 4; a++) {
+      const long n = elem_node_2d(r, c, a, R, C);
+      rhs[2 * n] += fe[2 * a];
+      rhs[2 * n + 1] += fe[2 * a + 1];
+    }
+  }
+}
+
+// The effective expansion from the solution x of the unit-temperature load: mean stress
+// sum_e (CB_e x_e - sigma_e) / N, and alpha_eff = C^-1 (-mean stress).  The mean strain of the
+// periodic fluctuation, which the reference also multiplies by C and adds, is zero: the centre
+// gradients of the 4 shape functions sum to zero and every node enters once per local index.
+void update_thermal_expansion_2d(Model& m, const double* x) {
+  double stress[3];
+  volume_term_2d(m, x, stress);
+  std::vector<double> count(m.nmat, 0.0);
+  for (long e = 0; e < m.N; e++) count[m.elem_mat[e]] += 1.0;
+  for (unsigned mat = 0; mat < m.nmat; mat++) {
+    double sn[2];
+    thermal_stress_2d(m, (int)mat, sn);
+    stress[0] -= count[mat] * sn[0];
+    stress[1] -= count[mat] * sn[1];
+  }
+  double beta[3];
+  for (int k = 0; k < 3; k++) beta[k] = -stress[k] / (double)m.N;
+  solve_expansion(m, beta, 3);
 }
 
 }  // namespace chfem_host

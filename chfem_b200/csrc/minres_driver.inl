@@ -32,11 +32,11 @@ static bool launch_mr_op_buf(const T* rin, T* rout, const T* q, T* s, double* x,
     if (!ensure_reduction(nb)) return false;
     if (S->nd == 1) {
       TeArgs<1, T> a{rin, q, rout, s, x, d, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, 1, S->cur_sc, redctl(nb), fin, skip_if_done, cfg};
-      a.invd = S->d_invd;
+      sdf_args(a);
       k_2d_apply<1, T, TE_MR><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<1, T>(), S->stream>>>(a);
     } else {
       TeArgs<2, T> a{rin, q, rout, s, x, d, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, 1, S->cur_sc, redctl(nb), fin, skip_if_done, cfg};
-      a.invd = S->d_invd;
+      sdf_args(a);
       k_2d_apply<2, T, TE_MR><<<nb, dim3(T2_TR, T2_TC), t2_smem_bytes<2, T>(), S->stream>>>(a);
     }
   } else if (th_applies()) {

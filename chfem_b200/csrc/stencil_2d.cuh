@@ -8,7 +8,10 @@
 // B200 design: a CTA owns tiles of 32 (rows) x 8 (cols) nodes in turn (persistent grid); the
 // tile's formed input with its one-node periodic halo is staged in shared memory once, next to
 // the element matrices of up to 16 materials.  The Jacobi diagonal comes precomputed (a.invd,
-// FP64 per unknown).  Modes, outputs and finishers are those of k_te_apply (stencil_te.cuh).
+// FP64 per unknown).  Under a scalar density field (a.sdf) each pixel's row block is scaled by
+// the pixel's density (the reference's element-by-element density operators,
+// matrix_free.cu:1832-1880, :2788-2850).  Modes, outputs and finishers are those of k_te_apply
+// (stencil_te.cuh).
 #pragma once
 #include "common.cuh"
 #include "stencil_te.cuh"
@@ -71,13 +74,25 @@ __global__ void __launch_bounds__(T2_NT) k_2d_apply(TeArgs<ND, T> a) {
 #pragma unroll
     for (int e = 0; e < 4; e++) {
       const T* K = sK + ((key >> (4 * e)) & 15u) * ED * ED + e * ND * ED;
+      T pe[ND];  // the row block of pixel e times the pixel's nodal values
+#pragma unroll
+      for (int ci = 0; ci < ND; ci++) pe[ci] = T(0);
 #pragma unroll
       for (int b = 0; b < 4; b++) {
         const T* v = sP + (ctr + (drow(b) - drow(e)) + (dcol(b) - dcol(e)) * T2_PR) * ND;
 #pragma unroll
         for (int ci = 0; ci < ND; ci++)
 #pragma unroll
-          for (int cj = 0; cj < ND; cj++) out[ci] = fma(K[ci * ED + b * ND + cj], v[cj], out[ci]);
+          for (int cj = 0; cj < ND; cj++) pe[ci] = fma(K[ci * ED + b * ND + cj], v[cj], pe[ci]);
+      }
+      if (a.sdf) {  // scalar density field: pixel e's matrix scaled by its density
+        const size_t pix = (size_t)wrap(r - drow(e) - 1, R) + (size_t)wrap(c - dcol(e), C) * R;
+        const T f = T(a.sdf_min + a.sdf_rng * (double)a.sdf[pix] * (1.0 / 65535.0));
+#pragma unroll
+        for (int ci = 0; ci < ND; ci++) out[ci] = fma(f, pe[ci], out[ci]);
+      } else {
+#pragma unroll
+        for (int ci = 0; ci < ND; ci++) out[ci] += pe[ci];
       }
     }
 #pragma unroll
@@ -140,17 +155,28 @@ __global__ void __launch_bounds__(T2_NT) k_2d_apply(TeArgs<ND, T> a) {
   }
 }
 
-// Inverse Jacobi diagonal of a 2D model, per unknown, FP64 (matrix_free.cu:51-68, :325-346)
+// Inverse Jacobi diagonal of a 2D model, per unknown, FP64 (matrix_free.cu:51-68, :325-346);
+// under a scalar density field (sdf non-null) each pixel's diagonal term is scaled by its
+// density (matrix_free.cu:1350-1365, :1398-1416)
 template <int ND>
-__global__ void k_2d_invdiag(const uint16_t* keys, const double* Kd, long N, double* invd) {
+__global__ void k_2d_invdiag(const uint16_t* keys, const double* Kd, int R, int C, const uint16_t* sdf, double fmin,
+                             double frng, double* invd) {
   constexpr int ED = 4 * ND;
+  const long N = (long)R * C;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
     const unsigned key = keys[i];
+    const int r = (int)(i % R), cc = (int)(i / R);
+    double f[4] = {1.0, 1.0, 1.0, 1.0};
+    if (sdf) {
+#pragma unroll
+      for (int e = 0; e < 4; e++)
+        f[e] = fmin + frng * (double)sdf[(size_t)wrap(r - drow(e) - 1, R) + (size_t)wrap(cc - dcol(e), C) * R] * (1.0 / 65535.0);
+    }
 #pragma unroll
     for (int c = 0; c < ND; c++) {
       double s = 0.0;
 #pragma unroll
-      for (int e = 0; e < 4; e++) s += Kd[(size_t)((key >> (4 * e)) & 15u) * ED * ED + (e * ND + c) * ED + e * ND + c];
+      for (int e = 0; e < 4; e++) s += f[e] * Kd[(size_t)((key >> (4 * e)) & 15u) * ED * ED + (e * ND + c) * ED + e * ND + c];
       invd[i * ND + c] = 1.0 / s;
     }
   }

@@ -11,7 +11,7 @@
  * Each function cites the reference file:line it follows (paths inside cortezpedro/chfem).
  * Scope: 3D thermal (1 DOF/node), 3D elastic (3 DOF/node), 3D Stokes with the DOF-number
  * pore map (CUDAPCG_POREMAP_NUM), including the 2-vector solvers with on-the-fly reduction of
- * the solution (CG2/PCG2/MINRES2/PMINRES2, Stokes); the scalar density field (3D); 2D thermal
+ * the solution (CG2/PCG2/MINRES2/PMINRES2, Stokes); the scalar density field; 2D thermal
  * (1 DOF/node), 2D elastic (2 DOF/node) and 2D Stokes (2 velocities + pressure) on pixel images.
  *
  * Operator restatement.  The reference applies A node-by-node: for node i and each of the
@@ -270,6 +270,15 @@ static void apply_fluid(const double *v, double *y) {
    the pixel (row - DROW[e] - 1, col - DCOL[e]) and that pixel's local node b sits at
    (row - DROW[e] + DROW[b], col - DCOL[e] + DCOL[b]); the key holds the pixel's material in bits
    [4e, 4e + 4) (femhmg_2D.c:14-46); element matrices are dense (4 nd) x (4 nd), row-major. */
+/* Density scale of the pixel in which node (r, c) is local node e, the pixel at
+   (r - DROW[e] - 1, c - DCOL[e]); 1 without a density field (matrix_free.cu:1800-1880 and
+   :2748-2850: each pixel's element matrix, of its own material, scaled by its density) */
+static double sdf_scale_2d(int r, int c, int e, unsigned int R, unsigned int C) {
+  if (!S->sdf) return 1.0;
+  const unsigned int v = wrapi(r - DROW[e] - 1, R) + wrapi(c - DCOL[e], C) * R;
+  return S->sdf_min + (S->sdf_max - S->sdf_min) * (double)S->sdf[v] * (1.0 / 65535.0);
+}
+
 static void apply_2d(const double *v, double *y) {
   cudapcgModel_t *m = S->model;
   const unsigned int R = m->nrows, C = m->ncols, N = R * C;
@@ -281,26 +290,34 @@ static void apply_2d(const double *v, double *y) {
     double acc[2] = {0, 0};
     for (int e = 0; e < 4; e++) {
       const double *K = S->Kd + (size_t)((key >> (4 * e)) & 15u) * ed * ed;
+      const double f = sdf_scale_2d(r, c, e, R, C);
       for (int b = 0; b < 4; b++) {
         const unsigned int j = wrapi(r - DROW[e] + DROW[b], R) + wrapi(c - DCOL[e] + DCOL[b], C) * R;
-        for (unsigned int ci = 0; ci < nd; ci++)
-          for (unsigned int cj = 0; cj < nd; cj++) acc[ci] += K[(e * nd + ci) * ed + b * nd + cj] * v[(size_t)j * nd + cj];
+        for (unsigned int ci = 0; ci < nd; ci++) {
+          double s = 0.0;
+          for (unsigned int cj = 0; cj < nd; cj++) s += K[(e * nd + ci) * ed + b * nd + cj] * v[(size_t)j * nd + cj];
+          acc[ci] += f * s;
+        }
       }
     }
     for (unsigned int ci = 0; ci < nd; ci++) y[(size_t)i * nd + ci] = acc[ci];
   }
 }
-/* 2D Jacobi (matrix_free.cu:51-68, :325-346): the node's diagonal entries over its 4 pixels */
+/* 2D Jacobi (matrix_free.cu:51-68, :325-346): the node's diagonal entries over its 4 pixels,
+   each scaled by the pixel's density under a density field (matrix_free.cu:1350-1365,
+   :1398-1416) */
 static void inv_diag_2d(double *dinv) {
   cudapcgModel_t *m = S->model;
-  const unsigned int N = m->nrows * m->ncols;
+  const unsigned int R = m->nrows, C = m->ncols, N = R * C;
   const unsigned int nd = (S->analysis == CUDAPCG_ELASTIC_2D) ? 2 : 1, ed = 4 * nd;
 #pragma omp parallel for schedule(static)
   for (long i = 0; i < (long)N; i++) {
+    const int r = (int)(i % R), c = (int)(i / R);
     const unsigned int key = S->keys[i];
     for (unsigned int ci = 0; ci < nd; ci++) {
       double s = 0.0;
-      for (int e = 0; e < 4; e++) s += S->Kd[(size_t)((key >> (4 * e)) & 15u) * ed * ed + (e * nd + ci) * ed + e * nd + ci];
+      for (int e = 0; e < 4; e++)
+        s += sdf_scale_2d(r, c, e, R, C) * S->Kd[(size_t)((key >> (4 * e)) & 15u) * ed * ed + (e * nd + ci) * ed + e * nd + ci];
       dinv[(size_t)i * nd + ci] = 1.0 / s;
     }
   }
@@ -696,7 +713,7 @@ cudapcgFlag_t cudapcgSetImage(cudapcgMap_t *img) {
 /* cudapcg.cu:327-334: the density codes of every voxel and their range; a thermal model has one
    material (femhmg.c:256-262 normalises it), whose key is zero everywhere. */
 cudapcgFlag_t cudapcgSetParametricDensityField(parametricScalarField_t *f, double fmin, double fmax) {
-  if (!S || !S->model || !f || S->dim2) return 0;
+  if (!S || !S->model || !f) return 0;
   cudapcgModel_t *m = S->model;
   free(S->sdf);
   S->sdf = (parametricScalarField_t *)malloc(sizeof(parametricScalarField_t) * m->nelem);

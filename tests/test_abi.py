@@ -44,8 +44,8 @@ def test_errors_are_reported_not_fatal(tmp_path):
     raw = tmp_path / "bad.raw"
     raw.write_bytes(bytes(16))
     sdf = str(tmp_path / "field.bin").encode()
-    assert lib.hmgInit(str(nf).encode(), str(raw).encode(), sdf, None) == 0  # density field on a 2D image
-    assert b"2D" in lib.chfemB200LastError()
+    assert lib.hmgInit(str(nf).encode(), str(raw).encode(), sdf, None) == 0  # density field file missing
+    assert b"field.bin" in lib.chfemB200LastError()
     # 2D with more than 16 materials for 16-bit keys of 4 bits per pixel
     mats = "".join(f"{i} {i + 1}\n" for i in range(17))
     nf.write_text(f"%type_of_analysis\n0\n%image_dimensions\n4 4 0\n%number_of_materials\n17\n%properties_of_materials\n{mats}")

@@ -52,7 +52,7 @@ def make_case(tmp_path, analysis, shape, refinement, dtype, seed=5, field=None):
                      solver_tolerance=1e-10, solver_maxiter=20000)
     with open(prefix + ".nf", "a") as f:
         f.write(f"\n%data_type {dtype}\n")
-    n = img.size * refinement ** 3  # the reference reads as many values as the refined model has voxels
+    n = img.size * refinement ** img.ndim  # the reference reads as many values as the refined model has voxels
     vals = field if field is not None else 0.5 + rng.random(n)
     vals = np.resize(np.asarray(vals, float), n)
     vals.astype(np.float32 if dtype == "float32" else np.float64).tofile(prefix + ".bin")
@@ -60,10 +60,13 @@ def make_case(tmp_path, analysis, shape, refinement, dtype, seed=5, field=None):
 
 
 @pytest.mark.skipif(not H.oracle_available(), reason="oracle not built")
-@pytest.mark.parametrize("analysis,refinement,dtype", [(0, 1, "float32"), (1, 1, "float64"), (0, 2, "float64"), (1, 2, "float32")])
-def test_density_codes_equal_reference(tmp_path, analysis, refinement, dtype):
+@pytest.mark.parametrize("analysis,refinement,dtype,shape", [(0, 1, "float32", (5, 6, 7)), (1, 1, "float64", (5, 6, 7)),
+                                                             (0, 2, "float64", (5, 6, 7)), (1, 2, "float32", (5, 6, 7)),
+                                                             (0, 1, "float64", (9, 11)), (1, 2, "float32", (7, 6)),
+                                                             (0, 3, "float32", (4, 5))])
+def test_density_codes_equal_reference(tmp_path, analysis, refinement, dtype, shape):
     from chfem_b200 import _native
-    nf, raw, fb = make_case(tmp_path, analysis, (5, 6, 7), refinement, dtype)
+    nf, raw, fb = make_case(tmp_path, analysis, shape, refinement, dtype)
     out = str(tmp_path / "cap.npz")
     p = subprocess.run([sys.executable, "-c", _CAPTURE, H.ORACLE_REF_LIB, nf, raw, fb, out], capture_output=True, text=True,
                        timeout=600)
@@ -83,12 +86,15 @@ def test_density_codes_equal_reference(tmp_path, analysis, refinement, dtype):
     assert np.array_equal(rg, ref["rg"])
 
 
-def _x_of(exe, nf, raw, fb, extra=()):
+def _x_of(exe, nf, raw, fb, extra=(), dim=3):
     C, log = H.run_exec(exe, nf, raw, "-f", fb, "-xo", *extra)
-    k = C.shape[0] if C.shape[0] == 3 else 6
+    if dim == 2:  # 2D load cases: thermal X, Y; elastic X, Y, XY (files _0, _1, _5)
+        dirs = [0, 1] if C.shape[0] == 2 else [0, 1, 5]
+    else:
+        dirs = list(range(C.shape[0] if C.shape[0] == 3 else 6))
     base = nf[:-3] + "_X"
-    xs = [np.fromfile(f"{base}_{d}.bin") for d in range(k)]
-    for d in range(k):
+    xs = [np.fromfile(f"{base}_{d}.bin") for d in dirs]
+    for d in dirs:
         os.remove(f"{base}_{d}.bin")
     return C, xs, log
 
@@ -136,3 +142,42 @@ def test_density_field_minres(tmp_path, analysis):
     Cp, _ = H.run_exec(H.CHFEM_EXEC, nf, raw, "-f", fb)
     Cm, _ = H.run_exec(H.CHFEM_EXEC, nf, raw, "-f", fb, "-s", "1")
     assert H.rel_to_max(Cm, Cp) < 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("analysis,refinement,extra", [(0, 1, []), (1, 1, []), (0, 2, []), (1, 1, ["-s", "2"]),
+                                                       (1, 1, ["-j", "0"]), (1, 1, ["--precision", "mixed"])])
+def test_density_2d_equal_oracle(tmp_path, analysis, refinement, extra):
+    """2D images (femhmg_thermal_2D.c / femhmg_elastic_2D.c *_ScalarDensityField,
+    matrix_free.cu:1800-1880, :2748-2850): solutions of every load case and the whole tensor
+    (the reference's 2D updates scale each pixel by its own density) against the oracle."""
+    nf, raw, fb = make_case(tmp_path, analysis, (23, 19), refinement, "float32")
+    flags = [f for f in extra if f not in ("--precision", "mixed")]
+    Cref, xref, logref = _x_of(H.ORACLE_EXEC, nf, raw, fb, flags, dim=2)
+    C, xs, log = _x_of(H.CHFEM_EXEC, nf, raw, fb, extra, dim=2)
+    tol = 1e-4 if "mixed" in extra else 1e-6
+    for a, b in zip(xs, xref):
+        assert H.rel_to_max(a, b) < tol
+    assert H.rel_to_max(C, Cref) < tol
+    if "mixed" not in extra:
+        its, its_ref = H.parse_iterations(log), H.parse_iterations(logref)
+        assert all(abs(a - b) <= 1 for a, b in zip(its, its_ref)), (its, its_ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("analysis", [0, 1])
+def test_density_2d_minres_and_ones(tmp_path, analysis):
+    """2D: MINRES without Jacobi equals the oracle's; a field of ones gives the two-phase
+    tensor; PMINRES gives the PCG tensor."""
+    nf, raw, fb = make_case(tmp_path, analysis, (17, 21), 1, "float32")
+    Cref, xref, _ = _x_of(H.ORACLE_EXEC, nf, raw, fb, ["-s", "1", "-j", "0"], dim=2)
+    C, xs, _ = _x_of(H.CHFEM_EXEC, nf, raw, fb, ["-s", "1", "-j", "0"], dim=2)
+    for a, b in zip(xs, xref):
+        assert H.rel_to_max(a, b) < 1e-6
+    Cp, _ = H.run_exec(H.CHFEM_EXEC, nf, raw, "-f", fb)
+    Cm, _ = H.run_exec(H.CHFEM_EXEC, nf, raw, "-f", fb, "-s", "1")
+    assert H.rel_to_max(Cm, Cp) < 1e-6
+    nf1, raw1, fb1 = make_case(tmp_path, analysis, (17, 21), 1, "float32", field=np.ones(1))
+    Cplain, _ = H.run_exec(H.CHFEM_EXEC, nf1, raw1)
+    Cf, _ = H.run_exec(H.CHFEM_EXEC, nf1, raw1, "-f", fb1)
+    assert H.rel_to_max(Cf, Cplain) < 1e-6

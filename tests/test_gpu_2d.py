@@ -8,6 +8,8 @@ of its 2D operators) on the same inputs: tensors 1e-6 in FP64 and 1e-4 in mixed 
 iteration counts within one, across the solvers, stopping norms, Jacobi on/off, node-by-node
 and element-by-element input, %refinement, thin images and 12 materials.
 """
+import glob
+import os
 import zlib
 
 import numpy as np
@@ -149,3 +151,48 @@ def test_2d_stokes_rejects_two_vector(tmp_path):
     nf, raw = H.write_small_case(str(tmp_path), "f2_tv", img, 2, tol=1e-8, maxit=20000)
     with pytest.raises(RuntimeError):
         H.run_exec(H.CHFEM_EXEC, nf, raw, "-s", "5")
+
+
+@pytest.mark.parametrize("analysis", [0, 1, 2])
+def test_2d_fields(tmp_path, analysis):
+    """-e on 2D models: the solution and field files (temperature / flux 2 per node, displacement /
+    plane-strain stress 3 per node, velocity 2 per node / pressure) equal those the reference's
+    own saveFields code writes from the oracle's solution (run with one OpenMP thread: its field
+    loops add into shared nodes without synchronisation)."""
+    rng = np.random.default_rng(40 + analysis)
+    if analysis == 2:
+        img = np.where(rng.random((15, 18)) < 0.6, 0, 255).astype(np.uint8)
+    else:
+        img = H.small_image((15, 18), 2, seed=40 + analysis)
+    files = {}
+    for who, exe, env in [("ref", H.ORACLE_EXEC, {"OMP_NUM_THREADS": "1"}), ("b200", H.CHFEM_EXEC, None)]:
+        d = tmp_path / who
+        d.mkdir()
+        nf, raw = H.write_small_case(str(d), "f2", img, analysis, tol=1e-12, maxit=50000, solver=1 if analysis == 2 else 0)
+        H.run_exec(exe, nf, raw, "-e", env=env)
+        files[who] = {os.path.basename(f): np.fromfile(f) for f in glob.glob(str(d / "f2_*_*.bin"))}
+    assert sorted(files["ref"]) == sorted(files["b200"]) and files["ref"]
+    for name, ref in files["ref"].items():
+        got = files["b200"][name]
+        assert got.size == ref.size, name
+        if "temperature" in name or "displacement" in name or "pressure" in name:
+            # the periodic solution is defined up to a constant per component
+            k = 2 if "displacement" in name else 1
+            got, ref = got.reshape(-1, k), ref.reshape(-1, k)
+            got, ref = got - got.mean(axis=0), ref - ref.mean(axis=0)
+        assert H.rel_to_max(got, ref) < 1e-6, name
+
+
+def test_2d_plane_stress_fields(tmp_path):
+    """-e under plane stress (CHFEM_B200_PLANE_STRESS=1): on a homogeneous image the X load case
+    is the uniform strain xx = 1, so every node's stress is the first column of the element
+    matrices' plane-stress matrix, E / (1 - nu^2) (1, nu, 0)."""
+    img = np.full((8, 10), 255, np.uint8)
+    img[3, 4] = 0
+    E, nu = 2.0, 0.3
+    nf, raw = H.write_small_case(str(tmp_path), "ps", img, 1, tol=1e-12, maxit=20000,
+                                 props={0: (E, nu), 255: (E, nu)})
+    H.run_exec(H.CHFEM_EXEC, nf, raw, "-e", env={"CHFEM_B200_PLANE_STRESS": "1"})
+    s = np.fromfile(str(tmp_path / "ps_stress_0.bin")).reshape(-1, 3)
+    f = E / (1 - nu * nu)
+    np.testing.assert_allclose(s, np.tile([f, f * nu, 0.0], (s.shape[0], 1)), atol=1e-9 * f)
