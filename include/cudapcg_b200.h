@@ -11,8 +11,8 @@
  *     calls exit() or cudaDeviceReset() (reference: error_handling.h:6-14, cudapcg.cu:201);
  *   - 2D analyses (CUDAPCG_THERMAL_2D, CUDAPCG_ELASTIC_2D, CUDAPCG_FLUID_2D) run with the
  *     reference's 2D formats (4-bit key fields, dense 4x4 / 8x8 / 12x12 element matrices, up
- *     to 16 materials); the 2-vector solvers and the scalar density field
- *     (cudapcgSetParametricDensityField) apply to 3D models;
+ *     to 16 materials); the scalar density field (cudapcgSetParametricDensityField)
+ *     applies to thermal and elastic models, 3D and 2D; the 2-vector solvers to 3D Stokes;
  *   - the 2-vector solvers (CG2/MINRES2, solvers/cg2.cu, pcg2.cu, minres2.cu, pminres2.cu)
  *     run for Stokes: cudapcgSolve then writes the 3 reduced velocity sums of the solution
  *     (x[0..2], scaled by cudapcgSetXReduceScale) and <model name>_xreduce_metrics_<n>.bin;
