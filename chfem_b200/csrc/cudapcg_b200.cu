@@ -104,6 +104,10 @@ struct Solver {
   int nmat = 0, nd = 1;
   std::vector<double> Kd;   // dense element matrices (host copy)
   bool have_K = false, have_keys = false, have_maps = false;
+  // image pore map (CUDAPCG_POREMAP_IMG): the per-node fluid keys handed over by
+  // cudapcgSetPoreMap, kept until the node->DOF map is there too
+  bool poremap_img = false, have_img_keys = false;
+  uint8_t* d_img_fkeys = nullptr;
   uint16_t* d_keys = nullptr;
   uint32_t* d_dof_of_node = nullptr;
   uint32_t* d_node_of_dof = nullptr;
@@ -211,7 +215,8 @@ static void free_model_dev() {
   free_ptr(S->d_keys); free_ptr(S->d_dof_of_node); free_ptr(S->d_node_of_dof); free_ptr(S->d_bkeys);
   free_ptr(S->d_K64); free_ptr(S->d_K32); free_ptr(S->d_tab64); free_ptr(S->d_tab32);
   free_ptr(S->d_th64); free_ptr(S->d_th32);
-  free_ptr(S->d_sdf); free_ptr(S->d_invd);
+  free_ptr(S->d_sdf); free_ptr(S->d_invd); free_ptr(S->d_img_fkeys);
+  S->d_img_fkeys = nullptr; S->have_img_keys = false;
   S->d_keys = nullptr; S->d_dof_of_node = S->d_node_of_dof = nullptr; S->d_bkeys = nullptr;
   S->d_K64 = nullptr; S->d_K32 = nullptr; S->d_tab64 = nullptr; S->d_tab32 = nullptr;
   S->d_th64 = nullptr; S->d_th32 = nullptr; S->th_state = 0;
@@ -936,12 +941,13 @@ cudapcgModel_t* cudapcgNewModel(void) {
 
 static cudapcgFlag_t adopt_model() {
   cudapcgModel_t* m = S->model;
-  if (S->fluid && m->poremap_flag != CUDAPCG_POREMAP_NUM) {
-    set_err("model", "only the DOF-number pore map (-pm 1) is provided by chfem_b200");
+  if (S->fluid && m->poremap_flag != CUDAPCG_POREMAP_NUM && m->poremap_flag != CUDAPCG_POREMAP_IMG) {
+    set_err("model", "unknown pore map flag");
     return CUDAPCG_FALSE;
   }
   free_vectors();
   free_model_dev();
+  S->poremap_img = S->fluid && m->poremap_flag == CUDAPCG_POREMAP_IMG;
   block_free();
   S->R = (int)m->nrows; S->C = (int)m->ncols; S->L = std::max(1, (int)m->nlayers);  // 2D: one layer
   S->N = (long)S->R * S->C * S->L;
@@ -1338,9 +1344,42 @@ cudapcgFlag_t cudapcgSetParametricDensityField(parametricScalarField_t* field, d
   invalidate_graphs();
   return CUDAPCG_TRUE;
 }
+// Image pore map (CUDAPCG_POREMAP_IMG; femhmg.c:962-965, cudapcg.cu:336-355): the host hands
+// over the node->DOF map and every node's fluid key (bit e set when the node's local voxel e is
+// pore; 0 for a node in the solid) instead of the DOF->node map and the interface keys.  The
+// reference runs dedicated image-walking kernels on it (matrix_free.cu:4707-4958); here the two
+// DOF-number maps are scattered from it once, on the device, and the same Stokes passes run:
+// node i with a non-zero key and DOF id d < nV + nB is the node of DOF d, and an interface DOF
+// (d >= nV) takes the node's key.
+__global__ void k_maps_from_pore_image(const uint8_t* fk, const uint32_t* dof_of_node, long N, uint32_t nV, uint32_t nVB,
+                                       uint32_t* node_of_dof, uint8_t* bkeys) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const uint8_t k = fk[i];
+    if (!k) continue;
+    const uint32_t d = dof_of_node[i];
+    if (d >= nVB) continue;
+    node_of_dof[d] = (uint32_t)i;
+    if (d >= nV) bkeys[d - nV] = k;
+  }
+}
+static bool maps_from_pore_image() {
+  if (!S->poremap_img || !S->have_img_keys || !S->have_maps) return true;
+  const long g = std::max(1L, std::min<long>((S->N + 255) / 256, 8L * num_sms()));
+  k_maps_from_pore_image<<<(int)g, 256, 0, S->stream>>>(S->d_img_fkeys, S->d_dof_of_node, S->N, (uint32_t)S->nV,
+                                                        (uint32_t)(S->nV + S->nB), S->d_node_of_dof, S->d_bkeys);
+  CKV(cudaGetLastError());
+  CKV(cudaStreamSynchronize(S->stream));
+  return true;
+}
 cudapcgFlag_t cudapcgSetPoreMap(cudapcgFlag_t* pores) {
   if (!S || !S->model || !pores) return CUDAPCG_FALSE;
   if (!S->fluid) return CUDAPCG_FALSE;
+  if (S->poremap_img) {  // one fluid key per node
+    if (!S->d_img_fkeys) CK(cudaMalloc(&S->d_img_fkeys, S->N));
+    CK(cudaMemcpy(S->d_img_fkeys, pores, S->N, cudaMemcpyHostToDevice));
+    S->have_img_keys = true;
+    return maps_from_pore_image() ? CUDAPCG_TRUE : CUDAPCG_FALSE;
+  }
   if (S->nB) CK(cudaMemcpy(S->d_bkeys, pores, S->nB, cudaMemcpyHostToDevice));
   return CUDAPCG_TRUE;
 }
@@ -1348,10 +1387,11 @@ cudapcgFlag_t cudapcgSetPeriodic2DOFMap(cudapcgIdMap_t* vars) {
   if (!S || !S->model || !vars || !S->fluid) return CUDAPCG_FALSE;
   CK(cudaMemcpy(S->d_dof_of_node, vars, sizeof(uint32_t) * S->N, cudaMemcpyHostToDevice));
   S->have_maps = true;
-  return CUDAPCG_TRUE;
+  return maps_from_pore_image() ? CUDAPCG_TRUE : CUDAPCG_FALSE;
 }
 cudapcgFlag_t cudapcgSetDOF2PeriodicMap(cudapcgIdMap_t* nodes) {
   if (!S || !S->model || !nodes || !S->fluid) return CUDAPCG_FALSE;
+  if (S->poremap_img) { set_err("cudapcgSetDOF2PeriodicMap", "not used with the image pore map"); return CUDAPCG_FALSE; }  // cudapcg.cu:360
   CK(cudaMemcpy(S->d_node_of_dof, nodes, sizeof(uint32_t) * (S->nV + S->nB), cudaMemcpyHostToDevice));
   return CUDAPCG_TRUE;
 }

@@ -370,12 +370,13 @@ int pcg_flag_of(const Model& m) {
 const char* DIR_STR[6] = {"X", "Y", "Z", "YZ (shear)", "XZ (shear)", "XY (shear)"};
 
 // The model coarsened by 2 per axis for the recursive initial-guess search
-// (femhmg.c:1844-1916): floor(n/2) voxels per axis, voxel (r,c,l) takes the material of fine
-// voxel (2r,2c,2l); same voxel size, materials and local matrices.  nullptr when an axis
-// would vanish.
+// (femhmg.c:1844-1916): floor(n/2) voxels per axis (a 2D image keeps its one layer), voxel
+// (r,c,l) takes the material of fine voxel (2r,2c,2l); same voxel size, materials and local
+// matrices.  nullptr when an axis would vanish.
 Model* coarse_copy(const Model& f) {
-  if (f.nx < 2 || f.ny < 2 || f.nz < 2) return nullptr;
+  if (f.nx < 2 || f.ny < 2 || (!f.dim2 && f.nz < 2)) return nullptr;
   Model* c = new Model();
+  c->dim2 = f.dim2;
   c->analysis = f.analysis; c->solver_flag = f.solver_flag; c->voxel = f.voxel; c->tol = f.tol; c->maxit = f.maxit;
   c->refinement = f.refinement; c->nmat = f.nmat;
   memcpy(c->props, f.props, sizeof(f.props));
@@ -384,7 +385,7 @@ Model* coarse_copy(const Model& f) {
   c->has_thermal_expansion = f.has_thermal_expansion;
   c->nf = f.nf; c->nf_noext = f.nf_noext; c->raw = f.raw;
   c->nd = f.nd; c->C_dim = f.C_dim;
-  c->nx = f.nx / 2; c->ny = f.ny / 2; c->nz = f.nz / 2;
+  c->nx = f.nx / 2; c->ny = f.ny / 2; c->nz = f.dim2 ? 1u : f.nz / 2;
   c->N = (long)c->nx * c->ny * c->nz;
   c->elem_mat.assign(c->N, 0);
   const long fR = f.ny, fRC = (long)f.ny * f.nx, R = c->ny, RC = (long)c->ny * c->nx;
@@ -427,6 +428,9 @@ bool setup_solver(Model& m, bool coarse = false) {
     } else {
       ok = ensure_host_maps(m) && cudapcgSetImage(g_par == CUDAPCG_EBE ? m.elem_mat.data() : m.keys.data());
     }
+  } else if (g_poremap == CUDAPCG_POREMAP_IMG) {
+    // femhmg.c:962-965: the node->DOF map and every node's fluid key (image pore map)
+    ok = ensure_host_maps(m) && cudapcgSetPeriodic2DOFMap(m.dof_of_node.data()) && cudapcgSetPoreMap(m.fluid_keys.data());
   } else if (!m.host_maps) {
     int lut[256];
     for (int c = 0; c < 256; c++) lut[c] = m.props_keys[c];
@@ -513,10 +517,6 @@ void hmgSetPreConditionerFlag(uint8_t flag) { g_precond = flag > 0; }
 void hmgSetStoppingCriteria(uint8_t flag) { g_stopcrit = flag; }
 logical hmgSetPoreMappingStrategy(uint8_t flag) {
   if (flag > CUDAPCG_POREMAP_NUM) return 1;  // femhmg.c:484: out-of-range flags are ignored
-  if (flag == CUDAPCG_POREMAP_IMG && g_m && g_m->analysis == FLUID) {
-    fail("the image pore map (-pm 0) is not provided by chfem_b200; use the DOF-number map (-pm 1)");
-    return 0;
-  }
   g_poremap = flag;
   return 1;
 }
@@ -534,11 +534,6 @@ void hmgFindInitialGuesses(unsigned int nlevels) {
   Model& fine = *g_m;
   if (!fine.sdf.empty()) {  // a coarse level would need a coarsened density field
     fail("recursive initial guesses (-r) are not provided with a scalar density field");
-    return;
-  }
-  if (fine.dim2) {
-    SAY("WARNING: Initial guess estimation is not provided by chfem_b200 for 2D images.\n");
-    SAY("         Null initial guess will be considered (x0 = [0]).\n");
     return;
   }
   if (fine.analysis == FLUID) {  // femhmg.c:565-570

@@ -611,6 +611,26 @@ static void alloc_model_arrays(void) {
     if (!m->periodic2DOF_map) m->periodic2DOF_map = (cudapcgIdMap_t *)calloc(m->nelem, sizeof(cudapcgIdMap_t));
     if (!m->border_pore_map) m->border_pore_map = (cudapcgFlag_t *)calloc(m->nbordernodes + 1, 1);
     if (!m->DOF2periodic_map) m->DOF2periodic_map = (cudapcgIdMap_t *)calloc(m->nporenodes + m->nbordernodes + 1, sizeof(cudapcgIdMap_t));
+    if (m->poremap_flag == CUDAPCG_POREMAP_IMG && !m->pore_map) m->pore_map = (cudapcgFlag_t *)calloc(m->nelem, 1);
+  }
+}
+
+/* Image pore map (CUDAPCG_POREMAP_IMG, femhmg.c:962-965): the host hands over every node's
+   fluid key (bit e set when the node's local voxel e is pore) with the node->DOF map, and the
+   reference's image kernels walk the nodes with them (matrix_free.cu:4707-4958).  The operator
+   is the same; here the DOF->node map and the interface keys are scattered from the two maps
+   (node i with a non-zero key and DOF id d is the node of DOF d; an interface DOF d >= nV
+   takes the node's key) and the DOF-number restatement runs. */
+static void maps_from_pore_image(void) {
+  cudapcgModel_t *m = S->model;
+  const unsigned int nV = m->nporenodes, nVB = m->nporenodes + m->nbordernodes;
+  for (unsigned int i = 0; i < m->nelem; i++) {
+    const unsigned int k = m->pore_map[i];
+    if (!k) continue;
+    const unsigned int d = m->periodic2DOF_map[i];
+    if (d >= nVB) continue;
+    m->DOF2periodic_map[d] = i;
+    if (d >= nV) m->border_pore_map[d - nV] = (cudapcgFlag_t)k;
   }
 }
 
@@ -619,8 +639,8 @@ cudapcgFlag_t cudapcgBuildModel(const void *data) {
   if (!S->model) S->model = cudapcgNewModel();
   else if (S->model->freeAllowed_flag) { free_model(S->model); S->model = cudapcgNewModel(); }
   if (!model_ctor(&S->model, data)) return CUDAPCG_FALSE;
-  if (is_fluid() && S->model->poremap_flag != CUDAPCG_POREMAP_NUM) {
-    fprintf(stderr, "oracle: only the DOF-number pore map is supported\n");
+  if (is_fluid() && S->model->poremap_flag != CUDAPCG_POREMAP_NUM && S->model->poremap_flag != CUDAPCG_POREMAP_IMG) {
+    fprintf(stderr, "oracle: unknown pore map flag\n");
     return CUDAPCG_FALSE;
   }
   free_arrays();
@@ -728,6 +748,11 @@ cudapcgFlag_t cudapcgSetParametricDensityField(parametricScalarField_t *f, doubl
 }
 cudapcgFlag_t cudapcgSetPoreMap(cudapcgFlag_t *pores) {
   if (!S || !S->model) return 0;
+  if (S->model->poremap_flag == CUDAPCG_POREMAP_IMG) {  /* cudapcg.cu:339-341: one key per node */
+    memcpy(S->model->pore_map, pores, S->model->nelem);
+    capture(3, pores, S->model->nelem);
+    return 1;
+  }
   memcpy(S->model->border_pore_map, pores, S->model->nbordernodes);
   capture(3, pores, S->model->nbordernodes);
   return 1;
@@ -740,6 +765,7 @@ cudapcgFlag_t cudapcgSetPeriodic2DOFMap(cudapcgIdMap_t *vars) {
 }
 cudapcgFlag_t cudapcgSetDOF2PeriodicMap(cudapcgIdMap_t *nodes) {
   if (!S || !S->model) return 0;
+  if (S->model->poremap_flag != CUDAPCG_POREMAP_NUM) return 0;  /* cudapcg.cu:360 */
   unsigned int n = S->model->nporenodes + S->model->nbordernodes;
   memcpy(S->model->DOF2periodic_map, nodes, sizeof(cudapcgIdMap_t) * n);
   capture(2, nodes, n);
@@ -1231,6 +1257,7 @@ cudapcgFlag_t cudapcgSolve(cudapcgVar_t *res_x) {
   double t0 = omp_get_wtime();
   int must_free = (S->d == NULL);
   cudapcgAllocateArrays();
+  if (is_fluid() && S->model->poremap_flag == CUDAPCG_POREMAP_IMG) maps_from_pore_image();
   inv_diag(g_dinv);
   S->found = 0;
   S->count++;

@@ -6,7 +6,7 @@ The B200 path (k_2d_apply; k_fl_apply<.., 2> for Stokes) against the reference's
 reference's bar 1e-4) and against the oracle (the reference's host code with the CPU restatement
 of its 2D operators) on the same inputs: tensors 1e-6 in FP64 and 1e-4 in mixed precision,
 iteration counts within one, across the solvers, stopping norms, Jacobi on/off, node-by-node
-and element-by-element input, %refinement, thin images and 12 materials.
+and element-by-element input, %refinement, thin images, 12 materials and recursive coarse guesses.
 """
 import glob
 import os
@@ -196,3 +196,22 @@ def test_2d_plane_stress_fields(tmp_path):
     s = np.fromfile(str(tmp_path / "ps_stress_0.bin")).reshape(-1, 3)
     f = E / (1 - nu * nu)
     np.testing.assert_allclose(s, np.tile([f, f * nu, 0.0], (s.shape[0], 1)), atol=1e-9 * f)
+
+
+@pytest.mark.parametrize("name,analysis,shape,flags", [("r2_t1", 0, (36, 44), ["-r", "1"]), ("r2_t2_odd", 0, (37, 41), ["-r", "2"]),
+                                                       ("r2_e1", 1, (30, 34), ["-r", "1"]),
+                                                       ("r2_e1_minres", 1, (28, 26), ["-r", "1", "-s", "1", "-j", "0"])])
+def test_2d_recursive_initial_guess(tmp_path, name, analysis, shape, flags):
+    """-r N on 2D images (femhmg.c:561-846, interpl2 with no layer pass, wrappers.cu:290-303):
+    the tensor and every level's iteration count equal the oracle's (+-1), and the fine level
+    needs no more iterations than from the zero guess."""
+    nf, raw = _case(tmp_path, name, analysis, shape, 3)
+    Cref, logref = H.run_exec(H.ORACLE_EXEC, nf, raw, *flags)
+    C, log = H.run_exec(H.CHFEM_EXEC, nf, raw, *flags)
+    assert H.rel_to_max(C, Cref) < 1e-6
+    _its_close(log, logref)
+    i = flags.index("-r")
+    C0, log0 = H.run_exec(H.CHFEM_EXEC, nf, raw, *(flags[:i] + flags[i + 2:]))
+    assert H.rel_to_max(C0, C) < 1e-6
+    its, its0 = H.parse_iterations(log), H.parse_iterations(log0)
+    assert sum(its[-len(its0):]) <= sum(its0) + 2 * len(its0), (its, its0)
