@@ -1007,7 +1007,6 @@ cudapcgFlag_t cudapcgSetReduceStabFactor(double) { return S ? CUDAPCG_TRUE : CUD
 cudapcgFlag_t cudapcgSetSolver(cudapcgFlag_t flag) {
   if (!S) return CUDAPCG_FALSE;
   if (flag > CUDAPCG_MINRES2_SOLVER) { printf("ERROR: Invalid \"solverFlag\" (%d).\n", flag); return CUDAPCG_FALSE; }
-  if (flag >= CUDAPCG_CG2_SOLVER && is2d()) { set_err("cudapcgSetSolver", "the 2-vector solvers are provided for 3D Stokes models"); return CUDAPCG_FALSE; }
   // the 2-vector solvers keep another set of device vectors: a switch drops the old set
   if ((flag >= CUDAPCG_CG2_SOLVER) != (S->solver_flag >= CUDAPCG_CG2_SOLVER) && S->r) {
     free_vectors();

@@ -621,7 +621,6 @@ void hmgSolveHomogenization(void) {
   }
   // the 2-vector solvers never form the solution: its exports have nothing to write
   const bool two_vector = g_solver >= CUDAPCG_CG2_SOLVER;
-  if (two_vector && m.dim2) { fail("the 2-vector solvers (CG2/MINRES2) are provided for 3D Stokes models"); return; }
   if (two_vector && (g_export_fields || g_export_x))
     SAY("WARNING: the 2-vector solvers (CG2/MINRES2) reduce the solution on the fly; fields and x are not exported.\n");
   SAY("Running homogenization...\n");
@@ -761,9 +760,10 @@ void hmgSolveHomogenization(void) {
     g_stats.kernel_launches += st.kernel_launches;
     if (two_vector) {  // femhmg.c:1087-1094: the reduced sums are the column of C
       SAY("    Effective fields:\n");
-      for (int jj = 0; jj < 3; jj++) {
+      const int D = tensor_dim(m);  // 3, or 2 on a 2D image
+      for (int jj = 0; jj < D; jj++) {
         SAY("        %.8e\n", x[jj]);
-        m.C[jj * 3 + dir] = x[jj];
+        m.C[jj * D + dir] = x[jj];
       }
       if (g_report) {
         char buf[512];

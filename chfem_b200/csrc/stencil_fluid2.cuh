@@ -18,7 +18,9 @@
 // another thread of the same pass reads as a neighbour value, so r and d are updated in place.
 //
 // Rows follow the Stokes operator of stencil_fluid.cuh (one thread per pore or interface
-// node; the 27 neighbours gathered once through the node -> DOF map).
+// node; the 27 neighbours -- 9 on a 2D image -- gathered once through the node -> DOF map).
+// DIM = 2: pixel images, 2 velocities + pressure per pore node; the reference's 2-vector
+// solvers are generic over its 2D and 3D Stokes operators (nvarspernode = 2 or 3).
 #pragma once
 #include "common.cuh"
 #include "stencil_fluid.cuh"
@@ -56,18 +58,83 @@ struct Fl2Args {
   Fl2Cfg cfg;
 };
 
-// Jacobi inverse of the row at vector offset j (velocity rows 3 id + c, pressure rows 3 nV + id)
+// Jacobi inverse of the row at vector offset j (velocity rows DIM id + c, pressure rows
+// DIM nV + id)
+template <int DIM>
 __device__ __forceinline__ double fl2_inv(long j, long nV, const uint8_t* bkeys) {
-  if (j < 3 * nV) return c_fldiag.pore[j % 3];
-  const long id = j - 3 * nV;
-  return id < nV ? c_fldiag.pore[3] : c_fldiag.border[bkeys[id - nV]];
+  if (j < DIM * nV) return c_fldiag.pore[j % DIM];
+  const long id = j - DIM * nV;
+  return id < nV ? c_fldiag.pore[DIM] : c_fldiag.border[bkeys[id - nV]];
+}
+
+// 2D rows (pixels: 4 elements, 9 neighbours, 12 x 12 element matrix, 2 velocities + pressure
+// per node; matrix_free.cu:484-518, :628-660), in the order of the 3D statement below
+template <bool FORM_Z>
+__device__ __forceinline__ void fl2_rows_2d(const Fl2Args& a, long t, bool pre, double (&out)[4], unsigned& fk_out) {
+  constexpr int NE = 4, ED = 12, PC = 8;
+  const long nV = a.nV;
+  const int R = a.R, C = a.C;
+  const uint32_t node = a.node_of_dof[t];
+  const int r = (int)(node % (uint32_t)R), c = (int)((node / (uint32_t)R) % (uint32_t)C);
+  const bool pore = t < nV;
+  const unsigned fk = pore ? 15u : a.bkeys[t - nV];
+  fk_out = fk;
+  const int rr[3] = {wrap(r - 1, R), r, wrap(r + 1, R)};
+  const int cc[3] = {wrap(c - 1, C), c, wrap(c + 1, C)};
+  double ov0 = 0, ov1 = 0, op = 0;
+  const double ivv0 = (FORM_Z && pre) ? c_fldiag.pore[0] : 1.0, ivv1 = (FORM_Z && pre) ? c_fldiag.pore[1] : 1.0;
+  const double ivp = (FORM_Z && pre) ? c_fldiag.pore[2] : 1.0;
+#pragma unroll
+  for (int o = 0; o < 9; o++) {
+    const int orr = o % 3 - 1, occ = o / 3 - 1;
+    unsigned emask = 0;
+#pragma unroll
+    for (int e = 0; e < NE; e++)
+#pragma unroll
+      for (int b = 0; b < NE; b++)
+        if (drow(b) - drow(e) == orr && dcol(b) - dcol(e) == occ) emask |= 1u << e;
+    if (!(fk & emask)) continue;
+    const uint32_t nb = (uint32_t)rr[orr + 1] + (uint32_t)cc[occ + 1] * (uint32_t)R;
+    const uint32_t dof = a.dof_of_node[nb];
+    double vx = 0, vy = 0;
+    const bool vel = dof < (uint32_t)nV;
+    if (vel) {
+      vx = a.in[2 * (size_t)dof] * ivv0;
+      vy = a.in[2 * (size_t)dof + 1] * ivv1;
+    }
+    double ip = ivp;
+    if (FORM_Z && pre && !vel) ip = c_fldiag.border[a.bkeys[dof - (uint32_t)nV]];
+    const double vp = a.in[2 * (size_t)nV + dof] * ip;
+#pragma unroll
+    for (int e = 0; e < NE; e++) {
+#pragma unroll
+      for (int b = 0; b < NE; b++) {
+        if (!(drow(b) - drow(e) == orr && dcol(b) - dcol(e) == occ)) continue;
+        if (!((fk >> e) & 1u)) continue;
+        if (pore) {
+          ov0 += c_flK64[(2 * e + 0) * ED + 2 * b] * vx + c_flK64[(2 * e + 0) * ED + 2 * b + 1] * vy + c_flK64[(2 * e + 0) * ED + PC + b] * vp;
+          ov1 += c_flK64[(2 * e + 1) * ED + 2 * b] * vx + c_flK64[(2 * e + 1) * ED + 2 * b + 1] * vy + c_flK64[(2 * e + 1) * ED + PC + b] * vp;
+        }
+        op += c_flK64[(PC + e) * ED + 2 * b] * vx + c_flK64[(PC + e) * ED + 2 * b + 1] * vy - c_flK64[(PC + e) * ED + PC + b] * vp;
+      }
+    }
+  }
+  out[0] = pore ? ov0 : op;
+  out[1] = ov1;
+  out[2] = op;
+  out[3] = op;
 }
 
 // Operator rows of row set t (pore node: 3 velocities + pressure; interface node: pressure)
 // applied to the vector `in`, formed as in * M^-1 when FORM_Z.  The dropped velocity columns
-// of non-pore neighbours and the voxel mask of interface rows follow k_fl_apply.
-template <bool FORM_Z>
+// of non-pore neighbours and the voxel mask of interface rows follow k_fl_apply.  out holds
+// the DIM velocity rows then the pressure row (out[0] the pressure row of an interface node).
+template <bool FORM_Z, int DIM = 3>
 __device__ __forceinline__ void fl2_rows(const Fl2Args& a, long t, bool pre, double (&out)[4], unsigned& fk_out) {
+  if constexpr (DIM == 2) {
+    fl2_rows_2d<FORM_Z>(a, t, pre, out, fk_out);
+    return;
+  }
   const long nV = a.nV;
   const int R = a.R, C = a.C, L = a.L;
   const uint32_t node = a.node_of_dof[t];
@@ -172,7 +239,7 @@ __device__ inline void fl2_step_finish(const double* s, const Fl2Args& a) {
   if (!cont || it >= cfg.maxit) sc->done = 1;
 }
 
-template <int MODE>
+template <int MODE, int DIM = 3>
 __global__ void __launch_bounds__(FL_NT) k_fl2_apply(Fl2Args a) {
   __shared__ double sred[FL_NT / 32];
   if (a.sc->done) return;
@@ -184,11 +251,11 @@ __global__ void __launch_bounds__(FL_NT) k_fl2_apply(Fl2Args a) {
   for (long t = blockIdx.x * (long)FL_NT + threadIdx.x; t < nT; t += (long)gridDim.x * FL_NT) {
     double out[4];
     unsigned fk;
-    fl2_rows<MODE == F2_ZAZ>(a, t, pre, out, fk);
+    fl2_rows<MODE == F2_ZAZ, DIM>(a, t, pre, out, fk);
     const bool pore = t < nV;
-    const int cnt = pore ? 4 : 1;
+    const int cnt = pore ? DIM + 1 : 1;
     for (int k = 0; k < cnt; k++) {
-      const long j = pore ? (k < 3 ? 3 * t + k : 3 * nV + t) : 3 * nV + t;
+      const long j = pore ? (k < DIM ? DIM * t + k : DIM * nV + t) : DIM * nV + t;
       const double y = pore ? out[k] : out[0];
       const double iv = pre ? (pore ? c_fldiag.pore[k] : c_fldiag.border[fk]) : 1.0;
       if (MODE == F2_DAD) acc += a.in[j] * y;
@@ -199,7 +266,7 @@ __global__ void __launch_bounds__(FL_NT) k_fl2_apply(Fl2Args a) {
         a.r[j] = rn;
         acc += rn * rn * iv;
         mr = fmax(mr, fabs(rn));
-        if (pore && k < 3) {  // velocity rows: the reduced solution
+        if (pore && k < DIM) {  // velocity rows: the reduced solution
           const double dv = a.d[j];
           if (MODE == F2_UPD) md = fmax(md, fabs(dv));
           double xv = dv;  // F2_X0: the guess itself
@@ -274,17 +341,17 @@ __global__ void __launch_bounds__(FL_NT) k_fl2_apply(Fl2Args a) {
 // (d = M^-1 r + beta d in place; d = M^-1 r in the first step, where d is not read).
 enum Fl2Pw : int { P2_INIT = 0, P2_DIR = 1 };
 
-template <int MODE>
+template <int MODE, int DIM = 3>
 __global__ void __launch_bounds__(PW_NT) k_fl2_point(Fl2Args a, double* d) {
   __shared__ double sred[PW_NT / 32];
   if (MODE == P2_DIR && a.sc->done) return;
-  const long nV = a.nV, n = 4 * a.nV + a.nB;
+  const long nV = a.nV, n = (DIM + 1) * a.nV + a.nB;
   const bool pre = a.cfg.precond != 0;
   const bool first = (MODE == P2_DIR) && a.sc->iteration == 0;
   const double beta = (MODE == P2_DIR && !first) ? a.sc->beta : 0.0;
   double s = 0.0, mr = 0.0;
   for (long j = blockIdx.x * (long)PW_NT + threadIdx.x; j < n; j += (long)gridDim.x * PW_NT) {
-    const double iv = pre ? fl2_inv(j, nV, a.bkeys) : 1.0;
+    const double iv = pre ? fl2_inv<DIM>(j, nV, a.bkeys) : 1.0;
     const double rv = a.r[j];
     if (MODE == P2_DIR) {
       d[j] = first ? rv * iv : fma(beta, d[j], rv * iv);

@@ -2,12 +2,13 @@
 // stencil_fluid2.cuh), included by cudapcg_b200.cu.
 //
 // Device memory of a solve: r and d (FP64, the two vectors), the reduction accumulator of the
-// solution's velocity part (FULL: 3 nV values, ONLYDIR: nV, NONE: none) and the per-step sums
-// (3 x (max iterations + 1)), as in chfem/src/femhmg/cudapcg/solvers/pcg2.cu:37-56.  The
-// steps run as CUDA-graph chunks like the other solvers; the host reads one scalar record per
-// chunk.  The result is the three velocity sums of the solution scaled by the x-reduce scale
-// (the permeability column), and the per-step sums go to <model name>_xreduce_metrics_<n>.bin
-// (xreduce.cu:29-48, pcg2.cu:258-280).
+// solution's velocity part (FULL: D nV values, ONLYDIR: nV, NONE: none; D = 3, or 2 on a 2D
+// image) and the per-step sums (3 x (max iterations + 1)), as in
+// chfem/src/femhmg/cudapcg/solvers/pcg2.cu:37-56.  The steps run as CUDA-graph chunks like the
+// other solvers; the host reads one scalar record per chunk.  The result is the D velocity sums
+// of the solution scaled by the x-reduce scale (the permeability column), and the per-step sums
+// of the D components go to <model name>_xreduce_metrics_<n>.bin (xreduce.cu:29-48,
+// pcg2.cu:258-280).
 
 static constexpr int VEC_LEAN = 7;  // vec_prec marker of the 2-vector allocation
 
@@ -28,7 +29,7 @@ static bool ensure_lean_vectors() {
 }
 
 static bool ensure_lean_work() {
-  const size_t nxa = S->xr_mode == CUDAPCG_XREDUCE_FULL ? 3 * (size_t)S->nV : (S->xr_mode == CUDAPCG_XREDUCE_ONLYDIR ? (size_t)S->nV : 0);
+  const size_t nxa = S->xr_mode == CUDAPCG_XREDUCE_FULL ? (size_t)S->fdim * S->nV : (S->xr_mode == CUDAPCG_XREDUCE_ONLYDIR ? (size_t)S->nV : 0);
   const size_t nh = 3 * ((size_t)S->maxit + 1);
   if (nxa > S->xa_cap) {
     free_ptr(S->d_xa);
@@ -57,7 +58,7 @@ static Fl2Args fl2_args(const double* in, int finish) {
   a.sc = S->d_sc;
   a.finish = finish;
   a.cfg = Fl2Cfg{S->tol, (int)std::min<unsigned>(S->maxit, 0x7fffffffu), S->resnorm, S->precond,
-                 S->solver_flag == CUDAPCG_MINRES2_SOLVER ? 1 : 0, (int)S->xr_mode, (int)std::min(S->xr_shift, 2u)};
+                 S->solver_flag == CUDAPCG_MINRES2_SOLVER ? 1 : 0, (int)S->xr_mode, (int)std::min(S->xr_shift, (unsigned)S->fdim - 1)};
   return a;
 }
 
@@ -66,12 +67,22 @@ static bool launch_fl2(int mode, const double* in, int finish) {
   const int g = pw_grid(S->nV + S->nB);
   if (!ensure_reduction(g)) return false;
   a.rc = redctl(g);
-  switch (mode) {
-    case F2_DAD: k_fl2_apply<F2_DAD><<<g, FL_NT, 0, S->stream>>>(a); break;
-    case F2_AMA: k_fl2_apply<F2_AMA><<<g, FL_NT, 0, S->stream>>>(a); break;
-    case F2_UPD: k_fl2_apply<F2_UPD><<<g, FL_NT, 0, S->stream>>>(a); break;
-    case F2_ZAZ: k_fl2_apply<F2_ZAZ><<<g, FL_NT, 0, S->stream>>>(a); break;
-    default: k_fl2_apply<F2_X0><<<g, FL_NT, 0, S->stream>>>(a); break;
+  if (S->fdim == 2) {
+    switch (mode) {
+      case F2_DAD: k_fl2_apply<F2_DAD, 2><<<g, FL_NT, 0, S->stream>>>(a); break;
+      case F2_AMA: k_fl2_apply<F2_AMA, 2><<<g, FL_NT, 0, S->stream>>>(a); break;
+      case F2_UPD: k_fl2_apply<F2_UPD, 2><<<g, FL_NT, 0, S->stream>>>(a); break;
+      case F2_ZAZ: k_fl2_apply<F2_ZAZ, 2><<<g, FL_NT, 0, S->stream>>>(a); break;
+      default: k_fl2_apply<F2_X0, 2><<<g, FL_NT, 0, S->stream>>>(a); break;
+    }
+  } else {
+    switch (mode) {
+      case F2_DAD: k_fl2_apply<F2_DAD><<<g, FL_NT, 0, S->stream>>>(a); break;
+      case F2_AMA: k_fl2_apply<F2_AMA><<<g, FL_NT, 0, S->stream>>>(a); break;
+      case F2_UPD: k_fl2_apply<F2_UPD><<<g, FL_NT, 0, S->stream>>>(a); break;
+      case F2_ZAZ: k_fl2_apply<F2_ZAZ><<<g, FL_NT, 0, S->stream>>>(a); break;
+      default: k_fl2_apply<F2_X0><<<g, FL_NT, 0, S->stream>>>(a); break;
+    }
   }
   S->launches++;
   return cudaPeekAtLastError() == cudaSuccess;
@@ -79,11 +90,16 @@ static bool launch_fl2(int mode, const double* in, int finish) {
 
 static bool launch_fl2_point(int mode) {
   Fl2Args a = fl2_args((const double*)S->r, F2F_NONE);
-  const int g = pw_grid(4 * S->nV + S->nB);
+  const int g = pw_grid((S->fdim + 1) * S->nV + S->nB);
   if (!ensure_reduction(g)) return false;
   a.rc = redctl(g);
-  if (mode == P2_INIT) k_fl2_point<P2_INIT><<<g, PW_NT, 0, S->stream>>>(a, (double*)S->d0);
-  else k_fl2_point<P2_DIR><<<g, PW_NT, 0, S->stream>>>(a, (double*)S->d0);
+  if (S->fdim == 2) {
+    if (mode == P2_INIT) k_fl2_point<P2_INIT, 2><<<g, PW_NT, 0, S->stream>>>(a, (double*)S->d0);
+    else k_fl2_point<P2_DIR, 2><<<g, PW_NT, 0, S->stream>>>(a, (double*)S->d0);
+  } else {
+    if (mode == P2_INIT) k_fl2_point<P2_INIT><<<g, PW_NT, 0, S->stream>>>(a, (double*)S->d0);
+    else k_fl2_point<P2_DIR><<<g, PW_NT, 0, S->stream>>>(a, (double*)S->d0);
+  }
   S->launches++;
   return cudaPeekAtLastError() == cudaSuccess;
 }
@@ -122,12 +138,13 @@ static bool build_two_vector_graph(int key, int chunk, bool minres) {
 static bool finish_two_vector(double* res_x, bool write_metrics) {
   const unsigned it = (unsigned)S->h_sc->iteration;
   const size_t stride = (size_t)S->maxit + 1;
-  std::vector<double> h(3 * (size_t)(it + 1));
-  for (int c = 0; c < 3; c++)
+  const int D = S->fdim;
+  std::vector<double> h((size_t)D * (it + 1));
+  for (int c = 0; c < D; c++)
     CKV(cudaMemcpyAsync(h.data() + (size_t)c * (it + 1), S->d_hist + c * stride, (it + 1) * 8, cudaMemcpyDeviceToHost, S->stream));
   CKV(cudaStreamSynchronize(S->stream));
   for (double& v : h) v *= S->xr_scale;
-  const unsigned shift = std::min(S->xr_shift, 2u);
+  const unsigned shift = std::min(S->xr_shift, (unsigned)D - 1);
   if (write_metrics) {
     const std::string fn = std::string(S->model->name ? S->model->name : "") + "_xreduce_metrics_" + std::to_string(S->count) + ".bin";
     FILE* f = fopen(fn.c_str(), "wb");
@@ -137,7 +154,7 @@ static bool finish_two_vector(double* res_x, bool write_metrics) {
       fclose(f);
     }
   }
-  for (int c = 0; c < 3; c++) {
+  for (int c = 0; c < D; c++) {
     const double* p = h.data() + (size_t)c * (it + 1);
     if (S->xr_mode == CUDAPCG_XREDUCE_NONE) {
       double s = 0.0;
@@ -174,7 +191,7 @@ static bool solve_two_vector(double* res_x) {
   CKV(cudaEventRecord(S->ev1, S->stream));
   const int chunk = std::max(2u, S->iters_per_launch & ~1u);
   const int key = 0x40000000 | (minres ? 0x80 : 0) | (chunk & 0x7f) | (S->resnorm << 16) | (S->precond << 20) | ((int)S->xr_mode << 22) |
-                  ((int)std::min(S->xr_shift, 2u) << 24);
+                  ((int)std::min(S->xr_shift, (unsigned)S->fdim - 1) << 24) | (S->fdim << 26);
   if (!build_two_vector_graph(key, chunk, minres)) return false;
   const bool trace = getenv("CHFEM_B200_TRACE") != nullptr;
   for (;;) {

@@ -12,10 +12,11 @@
  *   - 2D analyses (CUDAPCG_THERMAL_2D, CUDAPCG_ELASTIC_2D, CUDAPCG_FLUID_2D) run with the
  *     reference's 2D formats (4-bit key fields, dense 4x4 / 8x8 / 12x12 element matrices, up
  *     to 16 materials); the scalar density field (cudapcgSetParametricDensityField)
- *     applies to thermal and elastic models, 3D and 2D; the 2-vector solvers to 3D Stokes;
+ *     applies to thermal and elastic models, 3D and 2D;
  *   - the 2-vector solvers (CG2/MINRES2, solvers/cg2.cu, pcg2.cu, minres2.cu, pminres2.cu)
- *     run for Stokes: cudapcgSolve then writes the 3 reduced velocity sums of the solution
- *     (x[0..2], scaled by cudapcgSetXReduceScale) and <model name>_xreduce_metrics_<n>.bin;
+ *     run for Stokes, 3D and 2D: cudapcgSolve then writes the 3 (2D: 2) reduced velocity sums
+ *     of the solution (x[0..2], scaled by cudapcgSetXReduceScale) and
+ *     <model name>_xreduce_metrics_<n>.bin;
  *     for thermal / elastic models they return an error (the reference's host never runs them
  *     there, femhmg.c:852-856).
  *

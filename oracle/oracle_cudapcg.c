@@ -10,9 +10,10 @@
  *
  * Each function cites the reference file:line it follows (paths inside cortezpedro/chfem).
  * Scope: 3D thermal (1 DOF/node), 3D elastic (3 DOF/node), 3D Stokes with the DOF-number
- * pore map (CUDAPCG_POREMAP_NUM), including the 2-vector solvers with on-the-fly reduction of
- * the solution (CG2/PCG2/MINRES2/PMINRES2, Stokes); the scalar density field; 2D thermal
- * (1 DOF/node), 2D elastic (2 DOF/node) and 2D Stokes (2 velocities + pressure) on pixel images.
+ * pore map (CUDAPCG_POREMAP_NUM; the image pore map is turned into it), including the 2-vector
+ * solvers with on-the-fly reduction of the solution (CG2/PCG2/MINRES2/PMINRES2, Stokes); the
+ * scalar density field; 2D thermal (1 DOF/node), 2D elastic (2 DOF/node) and 2D Stokes (2
+ * velocities + pressure, the 2-vector solvers included) on pixel images.
  *
  * Operator restatement.  The reference applies A node-by-node: for node i and each of the
  * 8 voxels (elements) around it, i is local node e of element e, and the row block of the
@@ -665,7 +666,7 @@ cudapcgFlag_t cudapcgSetXReduceMode(cudapcgFlag_t f) { if (!S) return 0; S->xr_m
 cudapcgFlag_t cudapcgSetXReduceShift(unsigned int s) { if (!S) return 0; S->xr_shift = s; return 1; }
 cudapcgFlag_t cudapcgSetXReduceScale(double s) { if (!S) return 0; S->xr_scale = s; return 1; }
 cudapcgFlag_t cudapcgSetReduceStabFactor(double s) { (void)s; return S ? 1 : 0; }
-/* cudapcg.cu:597-671: 3-vector variants run the same iterates; 2-vector variants are out of scope. */
+/* cudapcg.cu:597-671: 3-vector variants run the same iterates; the 2-vector variants run the restatements below. */
 cudapcgFlag_t cudapcgSetSolver(cudapcgFlag_t flag) {
   if (!S) return 0;
   if (flag > CUDAPCG_MINRES2_SOLVER) { printf("ERROR: Invalid \"solverFlag\" (%d).\n", flag); return 0; }
@@ -1034,13 +1035,15 @@ static void solve_minres(void) {
 /* 2-vector solvers (solvers/cg2.cu, pcg2.cu, minres2.cu, pminres2.cu): only r and d are   */
 /* kept; the solution is never stored, only reduced on the fly into the per-component sums */
 /* of its velocity part (xreduce.cu:4-27), which are the effective-permeability column.    */
-/*   NONE    res[c][it] = a * sum_j d[3j+c]   (the sums are accumulated at the end)        */
-/*   ONLYDIR x[j] += a d[3j+shift];  res[shift][it] = sum_j x[j]                           */
-/*   FULL    x[i] += a d[i] (velocity DOFs);  res[c][it] = sum_j x[3j+c]                    */
+/*   NONE    res[c][it] = a * sum_j d[Dj+c]   (the sums are accumulated at the end)        */
+/*   ONLYDIR x[j] += a d[Dj+shift];  res[shift][it] = sum_j x[j]                           */
+/*   FULL    x[i] += a d[i] (velocity DOFs);  res[c][it] = sum_j x[Dj+c]                    */
+/* with D = nvarspernode = 3 velocities per node, 2 on a 2D image (femhmg.c:75, :82).       */
 typedef struct {
   double *res[3];
-  double *xa;          /* reduction accumulator (ONLYDIR: nV values, FULL: 3 nV, NONE: none) */
+  double *xa;          /* reduction accumulator (ONLYDIR: nV values, FULL: D nV, NONE: none) */
   unsigned int nv;     /* velocity nodes */
+  unsigned int D;      /* velocity components per node */
 } xred_t;
 
 static double sum_stride(const double *v, unsigned int nv, unsigned int stride, unsigned int c) {
@@ -1053,16 +1056,16 @@ static void xred_update(xred_t *X, unsigned int it, double a, const double *d) {
   const unsigned int nv = X->nv;
   switch (S->xr_mode) {
     case CUDAPCG_XREDUCE_NONE:
-      for (unsigned int c = 0; c < 3; c++) X->res[c][it] = a * sum_stride(d, nv, 3, c);
+      for (unsigned int c = 0; c < X->D; c++) X->res[c][it] = a * sum_stride(d, nv, X->D, c);
       break;
     case CUDAPCG_XREDUCE_ONLYDIR:
 #pragma omp parallel for schedule(static)
-      for (long j = 0; j < (long)nv; j++) X->xa[j] += a * d[3 * (size_t)j + S->xr_shift];
+      for (long j = 0; j < (long)nv; j++) X->xa[j] += a * d[X->D * (size_t)j + S->xr_shift];
       X->res[S->xr_shift][it] = sum_stride(X->xa, nv, 1, 0);
       break;
     default:
-      axpy_iny(X->xa, d, a, 3 * nv);
-      for (unsigned int c = 0; c < 3; c++) X->res[c][it] = sum_stride(X->xa, nv, 3, c);
+      axpy_iny(X->xa, d, a, X->D * nv);
+      for (unsigned int c = 0; c < X->D; c++) X->res[c][it] = sum_stride(X->xa, nv, X->D, c);
   }
 }
 /* the x0 stored in d enters the accumulator and the first sums (cg2.cu:131-146) */
@@ -1070,32 +1073,32 @@ static void xred_x0(xred_t *X, const double *d) {
   const unsigned int nv = X->nv;
   if (S->xr_mode == CUDAPCG_XREDUCE_ONLYDIR) {
 #pragma omp parallel for schedule(static)
-    for (long j = 0; j < (long)nv; j++) X->xa[j] += d[3 * (size_t)j + S->xr_shift];
+    for (long j = 0; j < (long)nv; j++) X->xa[j] += d[X->D * (size_t)j + S->xr_shift];
   } else if (S->xr_mode == CUDAPCG_XREDUCE_FULL) {
-    memcpy(X->xa, d, sizeof(double) * 3 * nv);
+    memcpy(X->xa, d, sizeof(double) * X->D * nv);
   }
-  for (unsigned int c = 0; c < 3; c++) X->res[c][0] = sum_stride(d, nv, 3, c);
+  for (unsigned int c = 0; c < X->D; c++) X->res[c][0] = sum_stride(d, nv, X->D, c);
 }
 /* the largest |x| the solver holds, for the error norm of CG2/PCG2 (cg2.cu:181); without */
 /* an accumulator (NONE) the denominator is 1, as in (P)MINRES2                            */
 static double xred_absmax(const xred_t *X) {
   if (S->xr_mode == CUDAPCG_XREDUCE_NONE) return 1.0;
-  return absmax(X->xa, S->xr_mode == CUDAPCG_XREDUCE_ONLYDIR ? X->nv : 3 * X->nv);
+  return absmax(X->xa, S->xr_mode == CUDAPCG_XREDUCE_ONLYDIR ? X->nv : X->D * X->nv);
 }
 /* save_xreduce (xreduce.cu:29-48) and the result (pcg2.cu:262-280) */
 static void xred_finish(xred_t *X, unsigned int it, double *res_x) {
   const double scl = S->xr_scale;
-  for (unsigned int c = 0; c < 3; c++)
+  for (unsigned int c = 0; c < X->D; c++)
     for (unsigned int j = 0; j <= it; j++) X->res[c][j] *= scl;
   char fn[2048];
   snprintf(fn, sizeof fn, "%s_xreduce_metrics_%lu.bin", S->model->name ? S->model->name : "", S->count);
   FILE *f = fopen(fn, "wb");
   if (f) {
-    if (S->xr_mode != CUDAPCG_XREDUCE_ONLYDIR) for (unsigned int c = 0; c < 3; c++) fwrite(X->res[c], sizeof(double), it + 1, f);
+    if (S->xr_mode != CUDAPCG_XREDUCE_ONLYDIR) for (unsigned int c = 0; c < X->D; c++) fwrite(X->res[c], sizeof(double), it + 1, f);
     else fwrite(X->res[S->xr_shift], sizeof(double), it + 1, f);
     fclose(f);
   }
-  for (unsigned int c = 0; c < 3; c++) {
+  for (unsigned int c = 0; c < X->D; c++) {
     double *p = X->res[c];
     switch (S->xr_mode) {
       case CUDAPCG_XREDUCE_NONE:
@@ -1237,13 +1240,14 @@ static void solve_two_vector(double *res_x) {
   cudapcgModel_t *m = S->model;
   xred_t X;
   X.nv = m->nporenodes;
+  X.D = S->analysis == CUDAPCG_FLUID_2D ? 2 : 3;
   double *buf = (double *)calloc((size_t)3 * (S->maxit + 1), sizeof(double));
   for (int c = 0; c < 3; c++) X.res[c] = buf + (size_t)c * (S->maxit + 1);
   X.xa = (S->xr_mode == CUDAPCG_XREDUCE_NONE) ? NULL
-       : (double *)calloc(S->xr_mode == CUDAPCG_XREDUCE_ONLYDIR ? X.nv : 3 * (size_t)X.nv, sizeof(double));
+       : (double *)calloc(S->xr_mode == CUDAPCG_XREDUCE_ONLYDIR ? X.nv : X.D * (size_t)X.nv, sizeof(double));
   /* the x0 lives in d (cudapcg.cu:302) */
   if (S->x0_set) memcpy(S->d, S->x, sizeof(double) * m->nvars);
-  res_x[0] = res_x[1] = res_x[2] = 0.0;
+  for (unsigned int c = 0; c < X.D; c++) res_x[c] = 0.0;
   const int minres = S->solver_flag == CUDAPCG_MINRES2_SOLVER;
   if (minres) solve_minres2_family(S->precond, &X, res_x);
   else solve_cg2_family(S->precond, &X, res_x);
@@ -1262,13 +1266,13 @@ cudapcgFlag_t cudapcgSolve(cudapcgVar_t *res_x) {
   S->found = 0;
   S->count++;
   if (S->solver_flag >= CUDAPCG_CG2_SOLVER) {
-    if (S->analysis != CUDAPCG_FLUID_3D) {
-      printf("ERROR: the 2-vector solvers are restated for 3D Stokes; use CG3/MINRES3.\n");
+    if (!is_fluid()) {
+      printf("ERROR: the 2-vector solvers are restated for Stokes; use CG3/MINRES3.\n");
       if (must_free) free_arrays();
       return 0;
     }
     solve_two_vector(res_x);
-    capture(6, res_x, 3);
+    capture(6, res_x, S->analysis == CUDAPCG_FLUID_2D ? 2 : 3);
   } else {
     int minres = (S->solver_flag == CUDAPCG_MINRES_SOLVER || S->solver_flag == CUDAPCG_MINRES3_SOLVER);
     if (minres) { if (S->precond) solve_pminres(); else solve_minres(); }

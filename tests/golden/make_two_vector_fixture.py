@@ -1,10 +1,11 @@
 """Generate tests/golden/two_vector_ref.json: the reference's own CUDA build run with the
 2-vector Stokes solvers (CG2 / MINRES2, every x-reduce mode, with and without Jacobi, the three
-stopping norms, an imported initial guess) on two small seeded pore images.
+stopping norms, an imported initial guess) on two small seeded pore images; with --2d,
+tests/golden/two_vector_2d_ref.json from two seeded 2D pore images (pixels).
 
 Needs a GPU and oracle/_ref/chfem_exec_ref (make -C oracle refgpu):
 
-    python tests/golden/make_two_vector_fixture.py [out.json]
+    python tests/golden/make_two_vector_fixture.py [--2d] [out.json]
 
 For each run the fixture keeps the effective permeability tensor, the per-load-case iteration
 counts and, for some runs, the per-step reductions the reference writes to
@@ -36,13 +37,25 @@ FLAGS = [
     ["-s", "4"], ["-s", "4", "-u", "0"], ["-s", "4", "-u", "1"], ["-s", "4", "-j", "0"], ["-s", "4", "-c", "1"],
     ["-s", "4", "-c", "2"],
 ]
+CASES_2D = {
+    "pix30x26": dict(shape=(30, 26), porosity=0.6, seed=5, voxel=1.0, tol=1e-8),
+    "pix22x35_h05": dict(shape=(22, 35), porosity=0.65, seed=17, voxel=0.5, tol=1e-9),
+}
 KEEP_METRICS = [["-s", "5"], ["-s", "5", "-u", "0"], ["-s", "4", "-u", "1"]]
+
+
+def image(spec):
+    """3D: a percolating Gaussian-random-field pore space; 2D: seeded uniform pixels."""
+    if len(spec["shape"]) == 2:
+        rng = np.random.default_rng(spec["seed"])
+        return np.where(rng.random(spec["shape"]) < spec["porosity"], 0, 255).astype(np.uint8)
+    from chfem_b200.synthetic import pore_grf
+    return pore_grf(spec["shape"], corr=spec["corr"], porosity=spec["porosity"], seed=spec["seed"])
 
 
 def make_case(workdir, name, spec):
     from chfem_b200.io import export_for_chfem
-    from chfem_b200.synthetic import pore_grf
-    img = pore_grf(spec["shape"], corr=spec["corr"], porosity=spec["porosity"], seed=spec["seed"])
+    img = image(spec)
     prefix = os.path.join(workdir, name)
     export_for_chfem(prefix + ".raw", img, 2, mat_props=None, voxel_size=spec["voxel"], solver_type=1, refinement=1,
                      export_raw=True, export_nf=True, solver_tolerance=spec["tol"], solver_maxiter=20000)
@@ -52,8 +65,7 @@ def make_case(workdir, name, spec):
 def guess_settings(workdir, name, spec):
     """Same model, 20 iterations at most: the .nf file of the initial-guess run."""
     from chfem_b200.io import export_for_chfem
-    from chfem_b200.synthetic import pore_grf
-    img = pore_grf(spec["shape"], corr=spec["corr"], porosity=spec["porosity"], seed=spec["seed"])
+    img = image(spec)
     prefix = os.path.join(workdir, name + "_guess")
     export_for_chfem(prefix + ".raw", img, 2, mat_props=None, voxel_size=spec["voxel"], solver_type=1, refinement=1,
                      export_raw=False, export_nf=True, solver_tolerance=spec["tol"], solver_maxiter=20)
@@ -65,17 +77,22 @@ def run(nf, raw, flags):
     p = subprocess.run([REF_EXEC, nf, raw, "-b", out, *flags], capture_output=True, text=True, timeout=600)
     if p.returncode != 0 or not os.path.exists(out):
         raise RuntimeError(p.stdout[-2000:] + p.stderr[-2000:])
-    C = np.fromfile(out)[:9].reshape(3, 3)
+    v = np.fromfile(out)
+    k = 2 if v.size == 4 else 3
+    C = v[:k * k].reshape(k, k)
     os.remove(out)
     its = [int(m) for m in re.findall(r"iteration: (\d+), residual", p.stdout)]
     return C, its
 
 
 def main():
-    out_path = sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden", "two_vector_ref.json")
+    args = [a for a in sys.argv[1:] if a != "--2d"]
+    dim2 = "--2d" in sys.argv[1:]
+    default = "two_vector_2d_ref.json" if dim2 else "two_vector_ref.json"
+    out_path = args[0] if args else os.path.join(ROOT, "tests", "golden", default)
     work = tempfile.mkdtemp()
-    fixture = {"generator": "tests/golden/make_two_vector_fixture.py", "cases": {}}
-    for name, spec in CASES.items():
+    fixture = {"generator": "tests/golden/make_two_vector_fixture.py" + (" --2d" if dim2 else ""), "cases": {}}
+    for name, spec in (CASES_2D if dim2 else CASES).items():
         nf, raw = make_case(work, name, spec)
         runs = []
         for flags in FLAGS:
@@ -85,7 +102,9 @@ def main():
             C, its = run(nf, raw, flags)
             entry = {"flags": flags, "C": C.tolist(), "iterations": its}
             if flags in KEEP_METRICS:
-                entry["metrics"] = [np.fromfile(os.path.join(work, f"{name}_xreduce_metrics_{k}.bin")).tolist() for k in (1, 2, 3)]
+                ncase = C.shape[0]  # load cases of the run: one metrics file each
+                entry["metrics"] = [np.fromfile(os.path.join(work, f"{name}_xreduce_metrics_{k}.bin")).tolist()
+                                    for k in range(1, ncase + 1)]
             runs.append(entry)
             print(name, flags, its, np.diag(C).tolist(), flush=True)
         # an imported initial guess: 20 MINRES steps (-xo, a settings file capped at 20

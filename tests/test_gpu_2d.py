@@ -136,7 +136,9 @@ def test_2d_stokes(tmp_path, name, shape, porosity, flags):
     rng = np.random.default_rng(zlib.crc32(name.encode()) % 10000)
     img = np.where(rng.random(shape) < porosity, 0, 255).astype(np.uint8)
     nf, raw = H.write_small_case(str(tmp_path), name, img, 2, tol=1e-8, maxit=20000)
-    Cref, logref = H.run_exec(H.ORACLE_EXEC, nf, raw, *flags)
+    # one oracle thread: its threaded sums combine in run-dependent order, and on this
+    # indefinite system the stopping step moves with them (148 to 156 steps across thread counts)
+    Cref, logref = H.run_exec(H.ORACLE_EXEC, nf, raw, *flags, env={"OMP_NUM_THREADS": "1"})
     C, log = H.run_exec(H.CHFEM_EXEC, nf, raw, *flags)
     assert C.shape == (2, 2)
     assert H.rel_to_max(C, Cref) < 1e-6
@@ -146,11 +148,17 @@ def test_2d_stokes(tmp_path, name, shape, porosity, flags):
         assert all(abs(a - b) <= max(1, 0.02 * b) for a, b in zip(its, its_ref)), (its, its_ref)
 
 
-def test_2d_stokes_rejects_two_vector(tmp_path):
-    img = np.where(np.random.default_rng(3).random((12, 12)) < 0.6, 0, 255).astype(np.uint8)
-    nf, raw = H.write_small_case(str(tmp_path), "f2_tv", img, 2, tol=1e-8, maxit=20000)
-    with pytest.raises(RuntimeError):
-        H.run_exec(H.CHFEM_EXEC, nf, raw, "-s", "5")
+def test_2d_stokes_two_vector_equals_full(tmp_path):
+    """PMINRES2 / PCG2 on a 2D image (2 velocity sums per load case) give the PMINRES / PCG
+    permeability; the runs against the oracle and the reference's own build are in
+    test_two_vector.py."""
+    img = np.where(np.random.default_rng(3).random((24, 20)) < 0.6, 0, 255).astype(np.uint8)
+    nf, raw = H.write_small_case(str(tmp_path), "f2_tv", img, 2, tol=1e-9, maxit=20000)
+    C1, _ = H.run_exec(H.CHFEM_EXEC, nf, raw, "-s", "1")
+    C5, log = H.run_exec(H.CHFEM_EXEC, nf, raw, "-s", "5")
+    C4, _ = H.run_exec(H.CHFEM_EXEC, nf, raw, "-s", "4")
+    assert C5.shape == (2, 2) and "Effective fields" in log
+    assert H.rel_to_max(C5, C1) < 1e-6 and H.rel_to_max(C4, C1) < 1e-6
 
 
 @pytest.mark.parametrize("analysis", [0, 1, 2])

@@ -2,8 +2,9 @@
 the solution (chfem_exec -s 4 / -s 5, -u 0/1/2).
 
 CPU: the oracle's restatement of these solvers is pinned on the reference's own CUDA build
-(tests/golden/two_vector_ref.json, made by tests/golden/make_two_vector_fixture.py): tensors,
-iteration counts and the per-step reductions it writes to <nf>_xreduce_metrics_<n>.bin.
+(tests/golden/two_vector_ref.json for 3D images and two_vector_2d_ref.json for 2D images, made
+by tests/golden/make_two_vector_fixture.py): tensors, iteration counts and the per-step
+reductions it writes to <nf>_xreduce_metrics_<n>.bin.
 GPU: the B200 library against the oracle on the same runs, its device memory, and the Python
 entry point.
 """
@@ -18,26 +19,35 @@ import pytest
 from tests import helpers as H
 
 FIXTURE = os.path.join(H.GOLDEN, "two_vector_ref.json")
+FIXTURE_2D = os.path.join(H.GOLDEN, "two_vector_2d_ref.json")
 needs_oracle = pytest.mark.skipif(not H.oracle_available(), reason="oracle executable not built")
 
 
-def fixture():
-    with open(FIXTURE) as f:
+def fixture(path=FIXTURE):
+    with open(path) as f:
         return json.load(f)
+
+
+def _image(spec):
+    """The generator's images: a percolating GRF pore space (3D), seeded uniform pixels (2D)."""
+    if len(spec["shape"]) == 2:
+        rng = np.random.default_rng(spec["seed"])
+        return np.where(rng.random(tuple(spec["shape"])) < spec["porosity"], 0, 255).astype(np.uint8)
+    from chfem_b200.synthetic import pore_grf
+    return pore_grf(tuple(spec["shape"]), corr=spec["corr"], porosity=spec["porosity"], seed=spec["seed"])
 
 
 def make_case(workdir, name, spec, maxit=20000, suffix=""):
     from chfem_b200.io import export_for_chfem
-    from chfem_b200.synthetic import pore_grf
-    img = pore_grf(tuple(spec["shape"]), corr=spec["corr"], porosity=spec["porosity"], seed=spec["seed"])
+    img = _image(spec)
     prefix = os.path.join(str(workdir), name + suffix)
     export_for_chfem(prefix + ".raw", img, 2, mat_props=None, voxel_size=spec["voxel"], solver_type=1, refinement=1,
                      export_raw=True, export_nf=True, solver_tolerance=spec["tol"], solver_maxiter=maxit)
     return prefix + ".nf", prefix + ".raw"
 
 
-def read_metrics(prefix):
-    return [np.fromfile(f"{prefix}_xreduce_metrics_{k}.bin") for k in (1, 2, 3)]
+def read_metrics(prefix, ncases=3):
+    return [np.fromfile(f"{prefix}_xreduce_metrics_{k}.bin") for k in range(1, ncases + 1)]
 
 
 def clear_metrics(workdir):
@@ -46,12 +56,21 @@ def clear_metrics(workdir):
             os.remove(os.path.join(workdir, f))
 
 
-def iterations_close(its, ref, flags):
+def iterations_close(its, ref, flags, dim=3):
     """Same counts (+-1) with Jacobi and the residual norms.  The error norm is a step-size test
     and the unpreconditioned recurrences amplify rounding, so there the summation order (the
     reference's GPU reductions, the oracle's threaded sums, the B200 passes) moves the stop by
-    a few steps."""
+    a few steps.  On the 2D pixel images the stopping step is dominated by rounding: the
+    reference's own MINRES and MINRES2 stop 7 steps apart on pix22x35_h05, and the oracle's
+    counts there move between 141 and 160 from run to run (its threaded sums combine in
+    run-dependent order); MINRES-family counts are held to 10 %, CG-family ones not at all."""
     assert len(its) == len(ref)
+    if dim == 2:
+        if flags[flags.index("-s") + 1] in ("0", "4"):
+            return
+        for a, b in zip(its, ref):
+            assert abs(a - b) <= max(2, int(0.10 * b)) + (max(3, int(0.03 * b)) if "-j" in flags else 0), (its, ref)
+        return
     slack = 1
     if "-c" in flags and flags[flags.index("-c") + 1] == "2":
         slack = 3
@@ -69,19 +88,27 @@ def run_with_guess(exe, tmp_path, name, spec, nf, raw, flags):
 
 # ---- CPU: the oracle on the reference's own runs ----------------------------------------
 def _fixture_runs():
-    if not os.path.exists(FIXTURE):
-        return []
-    return [(name, i) for name, case in fixture()["cases"].items() for i in range(len(case["runs"]))]
+    out = []
+    for path in (FIXTURE, FIXTURE_2D):
+        if os.path.exists(path):
+            out += [(os.path.basename(path), name, i) for name, case in fixture(path)["cases"].items() for i in range(len(case["runs"]))]
+    return out
 
 
 @needs_oracle
-@pytest.mark.parametrize("name,i", _fixture_runs())
-def test_oracle_matches_reference_two_vector_runs(tmp_path, name, i):
-    case = fixture()["cases"][name]
+@pytest.mark.parametrize("fname,name,i", _fixture_runs())
+def test_oracle_matches_reference_two_vector_runs(tmp_path, fname, name, i):
+    case = fixture(os.path.join(H.GOLDEN, fname))["cases"][name]
     spec, run = case["spec"], case["runs"][i]
+    ncases = len(spec["shape"])  # load cases: 3 on a 3D image, 2 on a 2D one
     flags = run["flags"]
-    if flags == ["-s", "4", "-c", "2"]:
+    if flags == ["-s", "4", "-c", "2"] and ncases == 3:
         pytest.skip("reference defect: see test_reference_pcg2_error_norm_defect")
+    if ncases == 2 and flags[:2] == ["-s", "4"] and not ("-u" in flags and flags[flags.index("-u") + 1] != "2"):
+        cg = {tuple(r["flags"]): r for r in case["runs"]}[("-s", "0")]
+        if H.rel_to_max(run["C"], cg["C"]) > 1e-7:
+            pytest.skip("reference defect: its PCG2 FULL-mode tensor departs from its own PCG tensor "
+                        "(test_reference_pcg2_2d_full_defect)")
     nf, raw = make_case(tmp_path, name, spec)
     if "-xi" in flags:
         C, log = run_with_guess(H.ORACLE_EXEC, tmp_path, name, spec, nf, raw, flags)
@@ -89,11 +116,11 @@ def test_oracle_matches_reference_two_vector_runs(tmp_path, name, i):
         C, log = H.run_exec(H.ORACLE_EXEC, nf, raw, *flags)
     assert H.rel_to_max(C, np.array(run["C"])) < 1e-7, (flags, H.rel_to_max(C, np.array(run["C"])))
     its = H.parse_iterations(log)
-    iterations_close(its, run["iterations"], flags)
+    iterations_close(its, run["iterations"], flags, ncases)
     if "metrics" in run:
         full = "-u" not in flags or flags[flags.index("-u") + 1] == "2"
-        ncomp = 1 if ("-u" in flags and flags[flags.index("-u") + 1] == "1") else 3
-        for k, (got, ref) in enumerate(zip(read_metrics(nf[:-3]), run["metrics"])):
+        ncomp = 1 if ("-u" in flags and flags[flags.index("-u") + 1] == "1") else ncases
+        for k, (got, ref) in enumerate(zip(read_metrics(nf[:-3], ncases), run["metrics"])):
             ref = np.asarray(ref)
             if its[k] != run["iterations"][k]:
                 continue  # a step more or less (threaded sums): the tensor column is checked above
@@ -124,12 +151,30 @@ def test_reference_pcg2_error_norm_defect():
 
 def test_fixture_two_vector_equals_full_solvers():
     """In the reference, CG2 / MINRES2 reproduce CG / MINRES's tensor (the reduced sums are the
-    velocity averages the full solvers' tensor update forms)."""
+    velocity averages the full solvers' tensor update forms), on 3D and 2D images (2D: PCG2
+    without an accumulator, -u 0, and MINRES2; see test_reference_pcg2_2d_full_defect)."""
     for name, case in fixture()["cases"].items():
         runs = {tuple(r["flags"]): r for r in case["runs"]}
         assert H.rel_to_max(runs[("-s", "5")]["C"], runs[("-s", "1")]["C"]) < 1e-7
         assert H.rel_to_max(runs[("-s", "4")]["C"], runs[("-s", "0")]["C"]) < 1e-7
         assert runs[("-s", "5")]["iterations"] == runs[("-s", "1")]["iterations"]
+    for name, case in fixture(FIXTURE_2D)["cases"].items():
+        runs = {tuple(r["flags"]): r for r in case["runs"]}
+        assert H.rel_to_max(runs[("-s", "5")]["C"], runs[("-s", "1")]["C"]) < 1e-7
+        assert H.rel_to_max(runs[("-s", "4", "-u", "0")]["C"], runs[("-s", "0")]["C"]) < 1e-7
+
+
+def test_reference_pcg2_2d_full_defect():
+    """On the 2D image pix30x26 the reference's PCG2 with the accumulator (FULL, -u 2: the
+    default and -c 2) stops where its PCG does but returns a tensor 1.9e-5 away from it, while
+    its PCG2 without an accumulator (-u 0) agrees to 1e-10: the FULL-mode sums pick up leftovers
+    of an earlier reduction (as in test_reference_pcg2_error_norm_defect).  chfem_b200 and the
+    oracle return the PCG tensor there; this records the reference's behaviour."""
+    runs = {tuple(r["flags"]): r for r in fixture(FIXTURE_2D)["cases"]["pix30x26"]["runs"]}
+    for bad in (("-s", "4"), ("-s", "4", "-c", "2")):
+        assert runs[bad]["iterations"] == runs[("-s", "0")]["iterations"]
+        assert H.rel_to_max(runs[bad]["C"], runs[("-s", "0")]["C"]) > 1e-6
+    assert H.rel_to_max(runs[("-s", "4", "-u", "0")]["C"], runs[("-s", "0")]["C"]) < 1e-9
 
 
 # ---- GPU: the B200 library ---------------------------------------------------------------
@@ -139,21 +184,23 @@ GPU_FLAGS = [["-s", "5"], ["-s", "5", "-u", "0"], ["-s", "5", "-u", "1"], ["-s",
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["pore16", "pore12_h05"])
+@pytest.mark.parametrize("fname,name", [("two_vector_ref.json", "pore16"), ("two_vector_ref.json", "pore12_h05"),
+                                        ("two_vector_2d_ref.json", "pix30x26"), ("two_vector_2d_ref.json", "pix22x35_h05")])
 @pytest.mark.parametrize("flags", GPU_FLAGS)
-def test_gpu_two_vector_vs_oracle(tmp_path, name, flags):
-    spec = fixture()["cases"][name]["spec"]
+def test_gpu_two_vector_vs_oracle(tmp_path, fname, name, flags):
+    spec = fixture(os.path.join(H.GOLDEN, fname))["cases"][name]["spec"]
+    ncases = len(spec["shape"])
     nf, raw = make_case(tmp_path, name, spec)
     Cref, logref = H.run_exec(H.ORACLE_EXEC, nf, raw, *flags)
-    mref = read_metrics(nf[:-3])
+    mref = read_metrics(nf[:-3], ncases)
     clear_metrics(str(tmp_path))
     C, log = H.run_exec(H.CHFEM_EXEC, nf, raw, *flags)
     assert "Effective fields" in log
     assert H.rel_to_max(C, Cref) < 1e-7, H.rel_to_max(C, Cref)
     its, itsref = H.parse_iterations(log), H.parse_iterations(logref)
-    iterations_close(its, itsref, flags)
-    m = read_metrics(nf[:-3])
-    for k in range(3):
+    iterations_close(its, itsref, flags, ncases)
+    m = read_metrics(nf[:-3], ncases)
+    for k in range(ncases):
         n = its[k] + 1
         assert m[k].size % n == 0
         if its[k] == itsref[k] and "-j" not in flags:
