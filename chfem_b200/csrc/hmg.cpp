@@ -116,6 +116,10 @@ std::vector<double> fields_2d(const Model& m, int dir, const double* x) {
 }
 
 void export_fields(const Model& m, int dir, const double* x, int block_index) {
+  if (!m.sdf.empty()) {  // femhmg_thermal_3D.c:1113-1116 and its elastic / 2D counterparts
+    SAY("WARNING: Field exportation not supported for scalar field input (.bin) yet.\n");
+    return;
+  }
   const std::string pre = m.nf_noext + "_";
   const std::string suf = "_" + std::to_string(dir) + ".bin";
   if (m.analysis == FLUID) {  // femhmg_fluid_3D.c:312-360, femhmg_fluid_2D.c:314-350
@@ -532,12 +536,13 @@ void hmgFindInitialGuesses(unsigned int nlevels) {
   g_have_coarse = false;
   if (!nlevels || !g_m) return;
   Model& fine = *g_m;
-  if (!fine.sdf.empty()) {  // a coarse level would need a coarsened density field
-    fail("recursive initial guesses (-r) are not provided with a scalar density field");
-    return;
-  }
   if (fine.analysis == FLUID) {  // femhmg.c:565-570
     SAY("WARNING: Initial guess estimation is not yet available for permeability analysis.\n");
+    SAY("         Null initial guess will be considered (x0 = [0]).\n");
+    return;
+  }
+  if (!fine.sdf.empty()) {  // femhmg.c:572-577 (a coarse level would need a coarsened field)
+    SAY("WARNING: Initial guess estimation is not yet available for analyses with a scalar field input (.bin).\n");
     SAY("         Null initial guess will be considered (x0 = [0]).\n");
     return;
   }
@@ -604,8 +609,8 @@ void hmgSetHomogenizationFlag(hmgFlag_t flag) {
 void hmgSolveHomogenization(void) {
   if (!g_m) return;
   Model& m = *g_m;
-  if (!m.sdf.empty() && (g_export_fields || m.has_thermal_expansion)) {
-    fail("field export and thermal expansion are not provided with a scalar density field");
+  if (!m.sdf.empty() && m.has_thermal_expansion) {
+    fail("thermal expansion is not provided with a scalar density field");
     return;
   }
   const auto t_all = std::chrono::steady_clock::now();

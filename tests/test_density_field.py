@@ -181,3 +181,18 @@ def test_density_2d_minres_and_ones(tmp_path, analysis):
     Cplain, _ = H.run_exec(H.CHFEM_EXEC, nf1, raw1)
     Cf, _ = H.run_exec(H.CHFEM_EXEC, nf1, raw1, "-f", fb1)
     assert H.rel_to_max(Cf, Cplain) < 1e-6
+
+
+@pytest.mark.gpu
+def test_density_field_warnings_as_reference(tmp_path):
+    """-e and -r with a density field print the reference's warnings and carry on (no field
+    files, zero guess), with the tensor of the plain run."""
+    import glob
+    nf, raw, fb = make_case(tmp_path, 0, (6, 7, 8), 1, "float32")
+    C, _ = H.run_exec(H.CHFEM_EXEC, nf, raw, "-f", fb)
+    Ce, loge = H.run_exec(H.CHFEM_EXEC, nf, raw, "-f", fb, "-e")
+    assert "Field exportation not supported for scalar field input" in loge
+    assert not glob.glob(str(tmp_path / "*_flux_*.bin"))
+    Cr, logr = H.run_exec(H.CHFEM_EXEC, nf, raw, "-f", fb, "-r", "1")
+    assert "Initial guess estimation is not yet available for analyses with a scalar field input" in logr
+    assert H.rel_to_max(Ce, C) < 1e-12 and H.rel_to_max(Cr, C) < 1e-12
