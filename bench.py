@@ -669,11 +669,12 @@ def main():
         t, C, st = e2e_step(img, nf, w)
         ncs = max(1, st.n_cases)
         breakdowns.append([t - st.total_seconds, st.rhs_seconds, float(sum(st.solve_seconds[i] for i in range(ncs))),
-                           st.update_seconds, st.setup_seconds, st.total_seconds])
+                           st.update_seconds, st.setup_seconds, st.total_seconds, st.solve_call_seconds, st.teardown_seconds])
         e2e_times.append(t)
     bm = np.mean(np.array(breakdowns), axis=0)
     breakdown = {"model_build_and_upload_s": bm[0], "rhs_assembly_s": bm[1], "solve_device_s": bm[2],
-                 "tensor_update_s": bm[3], "solver_setup_s": bm[4], "solver_call_total_s": bm[5]}
+                 "tensor_update_s": bm[3], "solver_setup_s": bm[4], "solver_call_total_s": bm[5],
+                 "solve_calls_wall_s": bm[6], "teardown_s": bm[7]}
     e2e = allmax(float(np.mean(e2e_times)))
     # the plain method end to end (FP64, one load case at a time, zero guess): its tensor is the
     # FP64 reference of the mixed / block / learned one

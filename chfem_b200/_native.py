@@ -101,7 +101,8 @@ class SolveStats(ctypes.Structure):
                 ("iterations", ctypes.c_uint * 6), ("residual", ctypes.c_double * 6),
                 ("solve_seconds", ctypes.c_double * 6), ("rhs_seconds", ctypes.c_double),
                 ("update_seconds", ctypes.c_double), ("total_seconds", ctypes.c_double),
-                ("kernel_launches", ctypes.c_ulonglong), ("ndof", ctypes.c_uint), ("setup_seconds", ctypes.c_double)]
+                ("kernel_launches", ctypes.c_ulonglong), ("ndof", ctypes.c_uint), ("setup_seconds", ctypes.c_double),
+                ("solve_call_seconds", ctypes.c_double), ("teardown_seconds", ctypes.c_double)]
 
 
 class CudapcgStats(ctypes.Structure):

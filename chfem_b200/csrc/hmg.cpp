@@ -681,8 +681,10 @@ void hmgSolveHomogenization(void) {
     SAY(")...\n");
     unsigned its[6] = {0};
     double res[6] = {0};
-    if (!cudapcgB200SolveLoadCases((unsigned)nd, axis, comp, jump, m.CB.data(), ns, px0.data(), interp, volume, px.data(), its, res) &&
-        cudapcgB200LastError()[0]) {
+    const auto tc = std::chrono::steady_clock::now();
+    const bool solved = cudapcgB200SolveLoadCases((unsigned)nd, axis, comp, jump, m.CB.data(), ns, px0.data(), interp, volume, px.data(), its, res);
+    g_stats.solve_call_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - tc).count();
+    if (!solved && cudapcgB200LastError()[0]) {
       fail(std::string("block solve: ") + cudapcgB200LastError());
       cudapcgEnd();
       return;
@@ -754,7 +756,9 @@ void hmgSolveHomogenization(void) {
     }
     SAY("    Solving system of equations...\n");
     if (two_vector) cudapcgSetXReduceShift(dir <= 2 ? dir : 0);  // femhmg.c:1068
+    const auto tc = std::chrono::steady_clock::now();
     cudapcgSolve(on_device && !two_vector ? nullptr : x.data());
+    g_stats.solve_call_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - tc).count();
     if (!g_quiet) cudapcgPrintSolverMetrics();
     cudapcgB200Stats st;
     cudapcgB200GetStats(&st);
@@ -820,9 +824,13 @@ void hmgSolveHomogenization(void) {
     if (m.dim2) update_thermal_expansion_2d(m, xs.data());
     else update_thermal_expansion(m, volume);
   }
-  cudapcgSetX0(nullptr, 0);
-  cudapcgFreeArrays();
-  cudapcgEnd();
+  {
+    const auto tt = std::chrono::steady_clock::now();
+    cudapcgSetX0(nullptr, 0);
+    cudapcgFreeArrays();
+    cudapcgEnd();
+    g_stats.teardown_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tt).count();
+  }
   for (auto& p : g_x0_user) p = nullptr;  // used once
   g_stats.total_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_all).count();
   SAY("    ------------------------------------------------------\nDone.(%.2e s)\n", g_stats.total_seconds);

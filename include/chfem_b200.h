@@ -77,6 +77,9 @@ typedef struct {
   unsigned long long kernel_launches;
   unsigned int ndof;
   double setup_seconds;      /* host wall time of the solver set-up (context, uploads, allocations) */
+  double solve_call_seconds; /* host wall time of the solve calls (work-vector allocation, device
+                                solve, result readout) */
+  double teardown_seconds;   /* host wall time of releasing the solver's device memory */
 } chfemB200SolveStats;
 int chfemB200GetSolveStats(chfemB200SolveStats *out);
 
