@@ -1050,6 +1050,11 @@ int chfemB200AssembleRHS(int direction, double* dst) {
   assemble_rhs(*g_m, direction, dst);
   return 1;
 }
+int chfemB200AssembleThermalExpansionRHS(double* dst) {
+  if (!g_m || !dst || g_m->analysis != ELASTIC || !ensure_host_maps(*g_m)) return 0;
+  assemble_rhs_thermal_expansion(*g_m, dst);
+  return 1;
+}
 int chfemB200UpdateC(int direction, const double* x, double* C_out) {
   if (!g_m || !x || !ensure_host_maps(*g_m)) return 0;
   update_C(*g_m, direction, x);

@@ -121,6 +121,10 @@ int chfemB200CopyModelArray(int which, void *dst, unsigned long long bytes);
 int chfemB200AssembleRHS(int direction, double *dst);
 /* Effective-tensor column of load case `direction` from a solution x (ndof doubles). */
 int chfemB200UpdateC(int direction, const double *x, double *C_out);
+/* Right-hand side of the thermal-expansion load (a unit temperature rise; elastic models with
+   %thermal_expansion) into dst (ndof doubles): femhmg_elastic_3D.c:464-505,
+   femhmg_elastic_2D.c:277-300. */
+int chfemB200AssembleThermalExpansionRHS(double *dst);
 /* Export the solution and its field for every load case of the next solve (as hmgSaveFields
    does; for the one-call chfemB200Run, which re-initializes the model). */
 void chfemB200SetExportFields(int on);

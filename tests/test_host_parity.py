@@ -148,3 +148,20 @@ def test_refinement_and_transpose(tmp_path):
     assert mine["info"][:3] == [10, 8, 6]
     assert np.array_equal(mine[0], ref["0"])
     np.testing.assert_allclose(mine["rhs"], ref["5"], rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("name,shape", [("te3d", (5, 6, 7)), ("te2d", (9, 12))])
+def test_thermal_expansion_rhs(tmp_path, name, shape):
+    """The thermal-expansion load (a unit temperature rise; femhmg_elastic_3D.c:464-505,
+    femhmg_elastic_2D.c:277-300): the reference's host code hands it over last (after the load
+    case), chfem_b200's host layer assembles the same vector."""
+    from chfem_b200 import _native
+    from tests.test_thermal_expansion import write_case
+    img = H.small_image(shape, 2, seed=zlib.crc32(name.encode()) % 1000)
+    nf, raw = write_case(tmp_path, name, img, {0: (1.0, 0.3, 2e-5), 255: (10.0, 0.2, -1e-5)})
+    ref = H.oracle_capture(nf, raw, 0)
+    lib, mine = host_arrays(nf, raw, 0)
+    rhs = np.zeros(mine["info"][4])
+    assert lib.chfemB200AssembleThermalExpansionRHS(rhs.ctypes.data_as(ctypes.c_void_p))
+    np.testing.assert_allclose(rhs, ref["5"], rtol=1e-11, atol=1e-11 * np.abs(ref["5"]).max())
+    assert np.abs(rhs).max() > 0
