@@ -566,7 +566,7 @@ def main():
     ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-check", action="store_true", help="skip the untimed reference run (tensor error, same-precision ratio)")
-    ap.add_argument("--no-north-star", action="store_true", help="skip the 256^3 north-star sub-record of the default workload")
+    ap.add_argument("--no-elastic256", action="store_true", help="skip the 256^3 elastic sub-record of the default workload")
     ap.add_argument("--kernel", type=int, default=None,
                     help="only time one kernel of the workload's resident model, 10 launches (for ncu captures): "
                          "0 plain operator pass, 1 operator pass (PCG), 2 pointwise pass (PCG), 3 operator pass "
@@ -736,8 +736,8 @@ def main():
         if learned_run:
             line["learned_guess"] = {"network_s": float(np.mean(net_times[-args.steps:])), "zero_guess_block": zero_guess,
                                      "weights": "chfem_b200/weights/elastic_unet.bin"}
-        if rank == 0 and world == 1 and not args.no_north_star and args.workload == DEFAULT:
-            line["north_star_256"] = north_star_256()
+        if rank == 0 and world == 1 and not args.no_elastic256 and args.workload == DEFAULT:
+            line["elastic256"] = elastic256_record()
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
@@ -812,8 +812,8 @@ def reference_once(wd, w, img):
             "build": "reference CUDA build, stock FP64 PCG one load case at a time, zero guess"}
 
 
-def north_star_256():
-    """The 256^3 elastic job of the north star, once: mixed + block + learned guess against the
+def elastic256_record():
+    """The 256^3 elastic GRF job (50 M DOF, 6 load cases), once: mixed + block + learned guess against the
     plain FP64 PCG (one load case at a time), end to end through the public API, with the device
     time, iterations and tensor error of each, and the block operator's roofline at that size."""
     from chfem_b200 import _native, compute_property
