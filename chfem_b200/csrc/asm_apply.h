@@ -7,8 +7,10 @@
 
 namespace chfem {
 
-// Tile of the FP32 elastic six-case pass: column tile of 32 x TC nodes, ZB layers per thread.
-enum AsmTile : int { ASM_TILE_8x1 = 0, ASM_TILE_6x2 = 1, ASM_TILE_8x2 = 2, ASM_TILE_4x2 = 3 };
+// Tile of the FP32 elastic six-case pass: column tile of 32 x TC nodes, ZB layers per thread;
+// _RING4: a 4-slot plane ring (the next plane staged during the arithmetic, one barrier a layer).
+enum AsmTile : int { ASM_TILE_8x1 = 0, ASM_TILE_6x2 = 1, ASM_TILE_8x2 = 2, ASM_TILE_4x2 = 3, ASM_TILE_6x1_RING4 = 4,
+                     ASM_TILE_7x1_RING4 = 5 };
 
 // CTAs of one pass on an R x C x L model: as many as fit on the GPU at once, at least
 // TE_MIN_RUN layers of work each.

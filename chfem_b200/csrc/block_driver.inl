@@ -60,8 +60,8 @@ static bool blk_prepare() {
   return true;
 }
 
-// tile of the FP32 elastic assembled operator: CHFEM_B200_ASM_TILE = "8x1", "6x2", "8x2" or "4x2"
-// (columns x layers per thread)
+// tile of the FP32 elastic assembled operator: CHFEM_B200_ASM_TILE = "8x1", "6x2", "8x2", "4x2"
+// (columns x layers per thread), "6x1r" or "7x1r" (one layer per thread, 4-slot plane ring)
 static int asm_tile_choice() {
   static int choice = -1;
   if (choice < 0) {
@@ -70,6 +70,8 @@ static int asm_tile_choice() {
     if (e && !strcmp(e, "6x2")) choice = ASM_TILE_6x2;
     if (e && !strcmp(e, "8x2")) choice = ASM_TILE_8x2;
     if (e && !strcmp(e, "4x2")) choice = ASM_TILE_4x2;
+    if (e && !strcmp(e, "6x1r")) choice = ASM_TILE_6x1_RING4;
+    if (e && !strcmp(e, "7x1r")) choice = ASM_TILE_7x1_RING4;
   }
   return choice;
 }

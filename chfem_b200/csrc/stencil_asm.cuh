@@ -15,11 +15,13 @@
 
 namespace chfem {
 
-template <int ND, typename T, int NR, int TC, int ZB>
+// RING: staged planes in the shared-memory ring, ZB + 2 (the planes one step reads) or 2 ZB + 2
+// (those plus the ZB planes the next step needs, staged while this step computes)
+template <int ND, typename T, int NR, int TC, int ZB, int RING = ZB + 2>
 inline size_t asm_smem_bytes() {
   using Lo = AsmLayout<ND, T, NR>;
   const size_t pp = (size_t)(TE_TR + 2) * (TC + 2);
-  return ((size_t)asm_table_words(ND, Lo::BS) + (size_t)(ZB + 2) * pp * Lo::PS) * sizeof(T);
+  return ((size_t)asm_table_words(ND, Lo::BS) + (size_t)RING * pp * Lo::PS) * sizeof(T);
 }
 
 
@@ -80,10 +82,15 @@ __device__ __forceinline__ void asm_positions(std::integer_sequence<int, Ps...>,
 // halo'd planes of d_new staged in shared memory (d_new is formed while staging).  At the start
 // of a step the CTA asks L2 to prefetch (bulk prefetch, one request per contiguous column
 // segment of every input vector) the planes it stages after the step, so that those loads find
-// them in L2.  MINB: CTAs per SM the registers are capped for.  Requires node keys of materials
-// 0 and 1 only.
-template <int ND, typename T, int NR, int TC, int ZB, int MINB = 1>
+// them in L2.  MINB: CTAs per SM the registers are capped for.  RING = 2 ZB + 2: the ring also
+// holds the next step's planes, which are staged before this step's arithmetic (into slots
+// that step does not read), so a step ends with one barrier instead of two and a warp's
+// staging loads overlap the other warps' arithmetic.  Requires node keys of materials 0 and 1
+// only.
+template <int ND, typename T, int NR, int TC, int ZB, int MINB = 1, int RING = ZB + 2>
 __global__ void __launch_bounds__(TE_TR * TC, MINB) k_asm_apply(BlkArgs<ND, T> a, const T* __restrict__ tab) {
+  static_assert(RING == ZB + 2 || RING == 2 * ZB + 2, "plane ring: ZB + 2 or 2 ZB + 2 slots");
+  constexpr bool AHEAD = RING == 2 * ZB + 2;
   using Lo = AsmLayout<ND, T, NR>;
   using V = typename Lo::V;
   constexpr int NW = Lo::NW;
@@ -117,7 +124,7 @@ __global__ void __launch_bounds__(TE_TR * TC, MINB) k_asm_apply(BlkArgs<ND, T> a
   for (int k = 0; k < NR; k++) beta[k] = sbeta[k];
   int r0 = 0, c0 = 0;
   size_t poff[PPT];  // in-layer node index of this thread's staged points (for the current tile)
-  auto slot_of = [&](int l) { return ((l % NPL) + NPL) % NPL; };
+  auto slot_of = [&](int l) { return ((l % RING) + RING) % RING; };
   auto load_plane = [&](int l) {
     const size_t lo = (size_t)wrap(l, L) * RC;
     T* dst = sP + slot_of(l) * PP * PS;
@@ -192,6 +199,14 @@ __global__ void __launch_bounds__(TE_TR * TC, MINB) k_asm_apply(BlkArgs<ND, T> a
       unsigned kn[ZB];
 #pragma unroll
       for (int z = 0; z < ZB; z++) kn[z] = a.keys[col + (size_t)(l + ZB + z < l1 ? l + ZB + z : l) * RC];
+      if constexpr (AHEAD) {
+        // planes l + ZB + 1 .. l + 2 ZB into the slots of l - ZB - 1 .. l - 2, read by the
+        // previous step only (done before its closing barrier)
+        if (l + ZB < l1) {
+#pragma unroll
+          for (int q = 1; q <= ZB; q++) load_plane(l + ZB + q);
+        }
+      }
       if (active) {
         const T* pl[NPL];
 #pragma unroll
@@ -233,10 +248,14 @@ __global__ void __launch_bounds__(TE_TR * TC, MINB) k_asm_apply(BlkArgs<ND, T> a
 #pragma unroll
       for (int z = 0; z < ZB; z++) kc[z] = kn[z];
       if (l + ZB < l1) {
-        __syncthreads();  // planes l - 1 .. l + ZB - 2 are no longer read
+        if constexpr (AHEAD) {
+          __syncthreads();  // the next step's planes are in place; this step's are no longer read
+        } else {
+          __syncthreads();  // planes l - 1 .. l + ZB - 2 are no longer read
 #pragma unroll
-        for (int q = 1; q <= ZB; q++) load_plane(l + ZB + q);
-        __syncthreads();
+          for (int q = 1; q <= ZB; q++) load_plane(l + ZB + q);
+          __syncthreads();
+        }
       }
     }
     w += l1 - l0;
