@@ -1055,6 +1055,13 @@ int chfemB200AssembleThermalExpansionRHS(double* dst) {
   assemble_rhs_thermal_expansion(*g_m, dst);
   return 1;
 }
+int chfemB200UpdateThermalExpansion(const double* x, const double* C, double* alpha_out) {
+  if (!g_m || !x || !C || !alpha_out || g_m->analysis != ELASTIC || !ensure_host_maps(*g_m)) return 0;
+  memcpy(g_m->C, C, sizeof(double) * g_m->C_dim);
+  thermal_expansion_from_solution(*g_m, x);
+  memcpy(alpha_out, g_m->thermal_expansion, sizeof(double) * (g_m->dim2 ? 3 : 6));
+  return 1;
+}
 int chfemB200UpdateC(int direction, const double* x, double* C_out) {
   if (!g_m || !x || !ensure_host_maps(*g_m)) return 0;
   update_C(*g_m, direction, x);

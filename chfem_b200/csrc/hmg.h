@@ -83,6 +83,8 @@ void assemble_rhs_thermal_expansion(const Model& m, double* rhs);
 void update_thermal_expansion(Model& m, const double* volume);
 // 2D: from the solution itself (xx, yy, xy into thermal_expansion[0..2])
 void update_thermal_expansion_2d(Model& m, const double* x);
+// 3D or 2D, from the solution itself (the stress sums on the host)
+void thermal_expansion_from_solution(Model& m, const double* x);
 // 2D elastic: plane constitutive matrix of material k (xx, yy, xy) used by the element matrices
 void plane_D(const Model& m, int k, double D[3][3]);
 // material index of model voxel (r, c, l) (refined grid), from elem_mat or from the colours

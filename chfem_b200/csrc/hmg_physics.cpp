@@ -317,6 +317,33 @@ void assemble_rhs(const Model& m, int dir, double* rhs) {
   });
 }
 
+// sum_e f_e CB_e x_e over all voxels (flux or stress components; f_e the voxel's density
+// scale, 1 without a density field)
+static void volume_term_3d(const Model& m, const double* x, double* acc) {
+  const long R = m.ny, C = m.nx, L = m.nz, N = m.N;
+  const int nd = m.nd, ns = (m.analysis == ELASTIC) ? 6 : 3, ec = 8 * nd;
+  for (int s = 0; s < 6; s++) acc[s] = 0.0;
+#pragma omp parallel
+  {
+    double loc[6] = {0, 0, 0, 0, 0, 0};
+#pragma omp for schedule(static)
+    for (long e = 0; e < N; e++) {
+      const long r = e % R, c = (e / R) % C, l = e / (R * C);
+      const double* CB = m.CB.data() + (size_t)m.elem_mat[e] * ns * ec;
+      const double f_e = sdf_scale(m, e);
+      for (int a = 0; a < 8; a++) {
+        const long n = elem_node(r, c, l, a, R, C, L);
+        for (int ci = 0; ci < nd; ci++) {
+          const double v = f_e * x[n * nd + ci];
+          for (int s = 0; s < ns; s++) loc[s] += CB[s * ec + a * nd + ci] * v;
+        }
+      }
+    }
+#pragma omp critical
+    for (int s = 0; s < ns; s++) acc[s] += loc[s];
+  }
+}
+
 void update_C(Model& m, int dir, const double* x) {
   if (m.dim2) { update_C_2d(m, dir, x); return; }
   const long R = m.ny, C = m.nx, L = m.nz, N = m.N;
@@ -343,26 +370,8 @@ void update_C(Model& m, int dir, const double* x) {
   case_axis(m, dir, axis, comp);
   const double jump = (double)axis_len(m, axis);
   const int nd = m.nd, ns = (m.analysis == ELASTIC) ? 6 : 3, ec = 8 * nd;
-  double acc[6] = {0, 0, 0, 0, 0, 0};
-#pragma omp parallel
-  {
-    double loc[6] = {0, 0, 0, 0, 0, 0};
-#pragma omp for schedule(static)
-    for (long e = 0; e < N; e++) {
-      const long r = e % R, c = (e / R) % C, l = e / (R * C);
-      const double* CB = m.CB.data() + (size_t)m.elem_mat[e] * ns * ec;
-      const double f_e = sdf_scale(m, e);
-      for (int a = 0; a < 8; a++) {
-        const long n = elem_node(r, c, l, a, R, C, L);
-        for (int ci = 0; ci < nd; ci++) {
-          const double v = f_e * x[n * nd + ci];
-          for (int s = 0; s < ns; s++) loc[s] += CB[s * ec + a * nd + ci] * v;
-        }
-      }
-    }
-#pragma omp critical
-    for (int s = 0; s < ns; s++) acc[s] += loc[s];
-  }
+  double acc[6];
+  volume_term_3d(m, x, acc);
   for_boundary_voxels(m, axis, [&](long r, long c, long l) {
     const long e = r + c * R + l * R * C;
     const double* CB = m.CB.data() + (size_t)m.elem_mat[e] * ns * ec;
@@ -796,6 +805,15 @@ void update_thermal_expansion_2d(Model& m, const double* x) {
   double beta[3];
   for (int k = 0; k < 3; k++) beta[k] = -stress[k] / (double)m.N;
   solve_expansion(m, beta, 3);
+}
+
+// The effective thermal expansion from the solution x of the unit-temperature load, with the
+// stress sums taken on the host (the device path reduces the 3D volume term on the GPU)
+void thermal_expansion_from_solution(Model& m, const double* x) {
+  if (m.dim2) { update_thermal_expansion_2d(m, x); return; }
+  double volume[6];
+  volume_term_3d(m, x, volume);
+  update_thermal_expansion(m, volume);
 }
 
 }  // namespace chfem_host

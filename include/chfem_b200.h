@@ -125,6 +125,10 @@ int chfemB200UpdateC(int direction, const double *x, double *C_out);
    %thermal_expansion) into dst (ndof doubles): femhmg_elastic_3D.c:464-505,
    femhmg_elastic_2D.c:277-300. */
 int chfemB200AssembleThermalExpansionRHS(double *dst);
+/* The effective thermal expansion (6 values, 3 in 2D, into alpha_out) from that load's solution
+   x (ndof doubles) and the effective tensor C (C_dim doubles), the stress sums taken on the host:
+   femhmg_elastic_3D.c:863-1074, femhmg_elastic_2D.c:388-528. */
+int chfemB200UpdateThermalExpansion(const double *x, const double *C, double *alpha_out);
 /* Export the solution and its field for every load case of the next solve (as hmgSaveFields
    does; for the one-call chfemB200Run, which re-initializes the model). */
 void chfemB200SetExportFields(int on);

@@ -90,6 +90,11 @@ lib.hmgGetConstitutiveMtxDim.restype = ctypes.c_uint
 d = lib.hmgGetConstitutiveMtxDim()
 C = np.ctypeslib.as_array(lib.hmgGetConstitutiveMtx(), shape=(d,)).copy()
 arrs["C"] = C
+lib.hmgGetThermalExpansion.restype = ctypes.POINTER(ctypes.c_double)
+lib.hmgGetThermalExpansionDim.restype = ctypes.c_uint
+na = lib.hmgGetThermalExpansionDim()
+if na:
+    arrs["alpha"] = np.ctypeslib.as_array(lib.hmgGetThermalExpansion(), shape=(na,)).copy()
 np.savez(out, **arrs)
 '''
 

@@ -165,3 +165,23 @@ def test_thermal_expansion_rhs(tmp_path, name, shape):
     assert lib.chfemB200AssembleThermalExpansionRHS(rhs.ctypes.data_as(ctypes.c_void_p))
     np.testing.assert_allclose(rhs, ref["5"], rtol=1e-11, atol=1e-11 * np.abs(ref["5"]).max())
     assert np.abs(rhs).max() > 0
+
+
+@pytest.mark.parametrize("name,shape", [("tu3d", (5, 6, 7)), ("tu2d", (9, 12))])
+def test_thermal_expansion_update(tmp_path, name, shape):
+    """The effective thermal expansion from the reference's own solution of the unit-temperature
+    load and its own tensor (all load cases, femhmg_elastic_3D.c:863-1074,
+    femhmg_elastic_2D.c:388-528): chfem_b200's host layer returns the reference's coefficients."""
+    from tests.test_thermal_expansion import write_case
+    img = H.small_image(shape, 2, seed=zlib.crc32(name.encode()) % 1000)
+    nf, raw = write_case(tmp_path, name, img, {0: (1.0, 0.3, 2e-5), 255: (10.0, 0.2, -1e-5)})
+    ref = H.oracle_capture(nf, raw, 6)  # every load case, then the thermal-expansion solve
+    lib, mine = host_arrays(nf, raw, 0)
+    na = 3 if len(shape) == 2 else 6
+    alpha = np.zeros(na)
+    x = np.ascontiguousarray(ref["6"])
+    C = np.ascontiguousarray(ref["C"])
+    assert lib.chfemB200UpdateThermalExpansion(x.ctypes.data_as(ctypes.c_void_p), C.ctypes.data_as(ctypes.c_void_p),
+                                               alpha.ctypes.data_as(ctypes.c_void_p))
+    assert ref["alpha"].size == na
+    assert H.rel_to_max(alpha, ref["alpha"]) < 1e-9, (alpha, ref["alpha"])
