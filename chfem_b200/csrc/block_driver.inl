@@ -42,10 +42,10 @@ static bool block_alloc(int nr) {
   // operator pass); Stokes (P)MINRES also keeps s
   std::vector<void**> vs = {&B->r, &B->d0, &B->d1, &B->q};
   if (S->fluid) vs.push_back(&B->s);
-  for (void** v : vs) { CKV(cudaMalloc(v, tot * sizeof(T))); CKV(cudaMemset(*v, 0, tot * sizeof(T))); }
-  CKV(cudaMalloc(&B->x, tot * 8));
-  CKV(cudaMalloc(&B->b64, tot * 8));
-  CKV(cudaMalloc(&B->sc, nr * sizeof(DevScalars)));
+  for (void** v : vs) { CKV(dev_malloc(v, tot * sizeof(T))); CKV(cudaMemset(*v, 0, tot * sizeof(T))); }
+  CKV(dev_malloc(&B->x, tot * 8));
+  CKV(dev_malloc(&B->b64, tot * 8));
+  CKV(dev_malloc(&B->sc, nr * sizeof(DevScalars)));
   CKV(cudaMallocHost(&B->h_sc, nr * sizeof(DevScalars)));
   return true;
 }
@@ -76,47 +76,55 @@ static int asm_tile_choice() {
   return choice;
 }
 
-// The assembled-stencil block operator pass (stencil_asm.cuh, launched from asm_apply.cu).
+// The assembled-stencil block operator pass (stencil_asm.cuh, launched from asm_apply.cu), on
+// the NR right-hand sides from k0 on (dold / dnew: the direction buffers of right-hand side 0).
 template <int ND, typename T, int NR>
-static bool launch_asm_block(T* dold, T* dnew, int precond) {
+static bool launch_asm_block(T* dold, T* dnew, int precond, int k0 = 0) {
   const int tile = asm_tile_choice();
   const int nb = asm_block_ctas<ND, T, NR>(S->R, S->C, S->L, num_sms(), tile);
   if (nb < 1) { set_err("assembled block operator", "launch configuration"); return false; }
   if (!ensure_reduction(nb)) return false;
-  BlkArgs<ND, T> a{(const T*)B->r, dold, dnew, (T*)B->q, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, S->nvars, B->sc, redctl(nb), precond};
+  const size_t off = (size_t)k0 * S->nvars;
+  BlkArgs<ND, T> a{(const T*)B->r + off, dold + off, dnew + off, (T*)B->q + off, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L,
+                   S->nvars, B->sc + k0, redctl(nb), precond};
   const cudaError_t e = asm_block_launch<ND, T, NR>(a, tabdev<T>(), nb, tile, S->stream);
   S->launches++;
   if (e != cudaSuccess) { set_err("assembled block operator", cudaGetErrorString(e)); return false; }
   return true;
 }
 
-// plain: the bare operator (M = I in the direction), for cudapcgB200ApplyBlockOperator
+// plain: the bare operator (M = I in the direction), for cudapcgB200ApplyBlockOperator.  k0:
+// the first of the NR right-hand sides the pass works on.
 template <int ND, typename T, int NR>
-static bool launch_blk_apply(int parity, bool plain = false) {
+static bool launch_blk_apply(int parity, bool plain = false, int k0 = 0) {
   const long n = S->nvars;
   T* dold = (T*)(parity ? B->d1 : B->d0);
   T* dnew = (T*)(parity ? B->d0 : B->d1);
   const int precond = plain ? 0 : S->precond;
-  if (asm_applies()) return launch_asm_block<ND, T, NR>(dold, dnew, precond);
+  if (asm_applies()) return launch_asm_block<ND, T, NR>(dold, dnew, precond, k0);
   const dim3 block(TE_TR, TE_TC);
   if (!blk_prepare<ND, T, NR>()) return false;
   const int nb = te_ctas(k_blk_apply<ND, T, NR>, blk_smem_bytes<ND, T, NR>());
   if (!ensure_reduction(nb)) return false;
-  BlkArgs<ND, T> a{(const T*)B->r, dold, dnew, (T*)B->q, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, n, B->sc, redctl(nb), precond};
+  const size_t off = (size_t)k0 * n;
+  BlkArgs<ND, T> a{(const T*)B->r + off, dold + off, dnew + off, (T*)B->q + off, S->d_keys, Kdev<T>(), S->nmat, S->R, S->C, S->L, n,
+                   B->sc + k0, redctl(nb), precond};
   k_blk_apply<ND, T, NR><<<nb, block, blk_smem_bytes<ND, T, NR>(), S->stream>>>(a);
   S->launches++;
   return cudaPeekAtLastError() == cudaSuccess;
 }
 
 template <int ND, typename T, int NR>
-static bool launch_blk_point(int parity) {
+static bool launch_blk_point(int parity, int k0 = 0) {
   const long n = S->nvars;
   T* dnew = (T*)(parity ? B->d0 : B->d1);
   // whole 16-byte chunks per thread when every right-hand side's vectors start aligned
   const bool chunks = n % 4 == 0;
   const int g = pw_grid(chunks ? n / 4 : S->N);
   if (!ensure_reduction(g)) return false;
-  BlkPw<ND, T> p{B->x, dnew, (T*)B->r, (const T*)B->q, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->N, n, B->sc, redctl(g), solvecfg()};
+  const size_t off = (size_t)k0 * n;
+  BlkPw<ND, T> p{B->x + off, dnew + off, (T*)B->r + off, (const T*)B->q + off, nullptr, S->d_keys, Kdev<T>(), S->nmat, S->N, n,
+                 B->sc + k0, redctl(g), solvecfg()};
   if (chunks) {
     if (S->resnorm == CUDAPCG_L2_NORM) k_blk_point4<ND, T, NR, false><<<g, PW_NT, 0, S->stream>>>(p);
     else k_blk_point4<ND, T, NR, true><<<g, PW_NT, 0, S->stream>>>(p);
@@ -127,8 +135,8 @@ static bool launch_blk_point(int parity) {
 }
 
 template <int ND, typename T, int NR>
-static bool enqueue_blk_iteration(int parity) {
-  return launch_blk_apply<ND, T, NR>(parity) && launch_blk_point<ND, T, NR>(parity);
+static bool enqueue_blk_iteration(int parity, int k0 = 0) {
+  return launch_blk_apply<ND, T, NR>(parity, false, k0) && launch_blk_point<ND, T, NR>(parity, k0);
 }
 
 // Device time of one block operator pass (which 5) or one block vector pass (which 6), for the
@@ -161,15 +169,15 @@ static double time_block_kernel_T(int which, unsigned reps) {
 }
 
 template <int ND, typename T, int NR>
-static bool blk_build_graph(int chunk) {
-  const int key = (prec_of<T>() << 12) | (ND << 8) | (NR << 4) | (S->resnorm << 2) | S->precond | (chunk << 16);
+static bool blk_build_graph(int chunk, int k0 = 0) {
+  const int key = (prec_of<T>() << 12) | (ND << 8) | (NR << 4) | (S->resnorm << 2) | S->precond | (chunk << 16) | (k0 << 28);
   if (B->gexec && B->graph_key == key) return true;
   if (B->gexec) { cudaGraphExecDestroy(B->gexec); B->gexec = nullptr; }
   cudaGraph_t g;
   CKV(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
   bool ok = true;
   const unsigned long long l0 = S->launches;
-  for (int it = 0; it < chunk && ok; it++) ok = enqueue_blk_iteration<ND, T, NR>(it & 1);
+  for (int it = 0; it < chunk && ok; it++) ok = enqueue_blk_iteration<ND, T, NR>(it & 1, k0);
   S->launches = l0;
   cudaError_t e = cudaStreamEndCapture(S->stream, &g);
   if (!ok || e != cudaSuccess) { set_err("block graph capture", cudaGetErrorString(e)); return false; }
@@ -213,6 +221,7 @@ static bool solve_block_device(const bool* has_x0) {
   CKV(cudaEventRecord(S->ev1, S->stream));
   const int chunk = std::max(2u, S->iters_per_launch & ~1u);
   if (!blk_build_graph<ND, T, NR>(chunk)) return false;
+  int cur_k0 = 0;  // first right-hand side of the captured passes
   const bool mixed = sizeof(T) == 4 && S->replace_every > 0;
   unsigned next_replace[NR];
   double repl_delta[NR];
@@ -270,6 +279,19 @@ static bool solve_block_device(const bool* has_x0) {
     bool any = false;
     for (int k = 0; k < NR; k++) any = any || !B->h_sc[k].done;
     if (!any) break;
+    if constexpr (NR == 6) {
+      // once the first three cases (the normal strains, which converge first) are done, the
+      // passes run on the last three only (the converged cases' lanes are no longer computed);
+      // a true-residual check that reopens one of the first three brings all six back
+      bool head_done = true;
+      for (int k = 0; k < 3; k++) head_done = head_done && B->h_sc[k].done;
+      const int want = head_done ? 3 : 0;
+      if (want != cur_k0) {
+        if (!(want ? blk_build_graph<ND, T, 3>(chunk, 3) : blk_build_graph<ND, T, NR>(chunk, 0))) return false;
+        cur_k0 = want;
+        if (trace) fprintf(stderr, "[block] passes on right-hand sides %d..%d\n", want, NR - 1);
+      }
+    }
     CKV(cudaGraphLaunch(B->gexec, S->stream));
     S->launches += (unsigned long long)chunk * 2;
   }
@@ -454,7 +476,7 @@ static bool rhs_on_device(const LoadCases& lc, int k) {
 
 // volume term of the effective tensor for every right-hand side into lc.moments (host)
 static bool moments_on_device(const LoadCases& lc, int nr) {
-  if (!B->d_mom) CKV(cudaMalloc(&B->d_mom, (size_t)BLK_MAX * 8 * sizeof(double) + 4 * 6 * 24 * sizeof(double)));
+  if (!B->d_mom) CKV(dev_malloc(&B->d_mom, (size_t)BLK_MAX * 8 * sizeof(double) + 4 * 6 * 24 * sizeof(double)));
   double* d_cb = B->d_mom + BLK_MAX * 8;
   const int g = pw_grid(S->fluid ? S->nV : S->N);
   if (!ensure_reduction(g)) return false;

@@ -19,8 +19,8 @@ static bool ensure_lean_vectors() {
   if (S->vec_prec == VEC_LEAN && S->r && S->d0) return true;
   free_vectors();
   const size_t n = std::max<size_t>((size_t)S->nvars, 1);
-  CKV(cudaMalloc(&S->r, n * 8));
-  CKV(cudaMalloc(&S->d0, n * 8));
+  CKV(dev_malloc(&S->r, n * 8));
+  CKV(dev_malloc(&S->d0, n * 8));
   CKV(cudaMemsetAsync(S->r, 0, n * 8, S->stream));
   CKV(cudaMemsetAsync(S->d0, 0, n * 8, S->stream));
   S->vec_prec = VEC_LEAN;
@@ -34,14 +34,14 @@ static bool ensure_lean_work() {
   if (nxa > S->xa_cap) {
     free_ptr(S->d_xa);
     S->d_xa = nullptr;
-    CKV(cudaMalloc(&S->d_xa, nxa * 8));
+    CKV(dev_malloc(&S->d_xa, nxa * 8));
     S->xa_cap = nxa;
     invalidate_graphs();
   }
   if (nh > S->hist_cap) {
     free_ptr(S->d_hist);
     S->d_hist = nullptr;
-    CKV(cudaMalloc(&S->d_hist, nh * 8));
+    CKV(dev_malloc(&S->d_hist, nh * 8));
     S->hist_cap = nh;
     invalidate_graphs();
   }
