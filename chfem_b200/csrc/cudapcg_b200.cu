@@ -182,7 +182,8 @@ static cudapcgFlag_t ctor_simple(cudapcgModel_t** ptr, const void* data) {
 template <typename T> static int prec_of() { return sizeof(T) == 8 ? CHFEM_B200_FP64 : CHFEM_B200_MIXED; }
 
 // Device memory of the solver comes from the device's default stream-ordered pool, whose
-// release threshold is raised so that what one model frees stays mapped for the next: repeated
+// release threshold is raised (to a quarter of the device's memory) so that what one model
+// frees stays mapped for the next: repeated
 // solves (one compute_property call after another) then skip the driver's unmapping and
 // mapping, which cost 0.006 to 0.47 s per 128^3 elastic call on different B200 boxes.
 // cudapcgB200TrimMemory hands the kept blocks back.  Allocations are made on the legacy stream
@@ -193,8 +194,11 @@ static void pool_keep() {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || kept[dev]) return;
   cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-    uint64_t threshold = UINT64_MAX;
+  size_t free_b = 0, total_b = 0;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+    // kept at most: a quarter of the device's memory, or CHFEM_B200_POOL_KEEP_BYTES
+    uint64_t threshold = total_b / 4;
+    if (const char* e = getenv("CHFEM_B200_POOL_KEEP_BYTES")) threshold = strtoull(e, nullptr, 10);
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
   }
   kept[dev] = true;
@@ -914,17 +918,51 @@ extern "C" {
 
 const char* cudapcgB200LastError(void) { return g_err.c_str(); }
 
-cudapcgFlag_t cudapcgEnd(void) {
-  if (!S) return CUDAPCG_FALSE;
-  block_free();
-  free_vectors();
-  free_model_dev();
-  free_ptr(S->d_sc); free_ptr(S->d_part); free_ptr(S->d_ticket); free_ptr(S->d_vt);
+// The stream, its three events and the pinned scalar record outlive a solver: cudapcgEnd keeps
+// them for the next cudapcgInit on the same device (destroying and re-creating them cost up to
+// 0.7 s per model on some B200 boxes).  A solver on another device gets new ones.
+struct KeptHandles {
+  int dev = -1;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  DevScalars* h_sc = nullptr;
+};
+static KeptHandles g_kept;
+static void keep_handles() {
+  int dev = -1;
+  if (S->stream) cudaStreamSynchronize(S->stream);
+  if (cudaGetDevice(&dev) == cudaSuccess && S->stream && S->ev0 && S->ev1 && S->ev2 && S->h_sc && !g_kept.stream) {
+    g_kept.dev = dev; g_kept.stream = S->stream; g_kept.ev[0] = S->ev0; g_kept.ev[1] = S->ev1; g_kept.ev[2] = S->ev2;
+    g_kept.h_sc = S->h_sc;
+    return;
+  }
   if (S->h_sc) cudaFreeHost(S->h_sc);
   if (S->ev0) cudaEventDestroy(S->ev0);
   if (S->ev1) cudaEventDestroy(S->ev1);
   if (S->ev2) cudaEventDestroy(S->ev2);
   if (S->stream) cudaStreamDestroy(S->stream);
+}
+static bool take_kept_handles() {
+  int dev = -1;
+  if (!g_kept.stream || cudaGetDevice(&dev) != cudaSuccess || dev != g_kept.dev) return false;
+  S->stream = g_kept.stream; S->ev0 = g_kept.ev[0]; S->ev1 = g_kept.ev[1]; S->ev2 = g_kept.ev[2]; S->h_sc = g_kept.h_sc;
+  g_kept = KeptHandles();
+  return true;
+}
+
+cudapcgFlag_t cudapcgEnd(void) {
+  if (!S) return CUDAPCG_FALSE;
+  const bool trace = getenv("CHFEM_B200_TRACE") != nullptr;
+  const auto t0 = std::chrono::steady_clock::now();
+  auto since = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
+  block_free();
+  const double t_block = since();
+  free_vectors();
+  free_model_dev();
+  free_ptr(S->d_sc); free_ptr(S->d_part); free_ptr(S->d_ticket); free_ptr(S->d_vt);
+  const double t_dev = since();
+  keep_handles();
+  if (trace) fprintf(stderr, "[end] block buffers %.4f s, other device buffers %.4f s, stream and events %.4f s\n", t_block, t_dev - t_block, since() - t_dev);
   if (S->model && S->model->freeAllowed_flag) { free(S->model->name); free(S->model); }
   delete S;
   S = nullptr;
@@ -949,11 +987,13 @@ cudapcgFlag_t cudapcgInit(cudapcgFlag_t analysis_flag, cudapcgFlag_t parStrategy
   S->nd = (analysis_flag == CUDAPCG_ELASTIC_3D) ? 3 : (analysis_flag == CUDAPCG_ELASTIC_2D ? 2 : 1);
   if (const char* e = getenv("CHFEM_B200_PRECISION")) cudapcgB200SetPrecision((!strcmp(e, "mixed") || !strcmp(e, "fp32")) ? CHFEM_B200_MIXED : CHFEM_B200_FP64);
   if (!g_ctor) g_ctor = ctor_simple;
-  CK(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
-  CK(cudaEventCreate(&S->ev0)); CK(cudaEventCreate(&S->ev1)); CK(cudaEventCreate(&S->ev2));
+  if (!take_kept_handles()) {
+    CK(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&S->ev0)); CK(cudaEventCreate(&S->ev1)); CK(cudaEventCreate(&S->ev2));
+    CK(cudaMallocHost(&S->h_sc, sizeof(DevScalars)));
+  }
   CK(dev_malloc(&S->d_sc, sizeof(DevScalars)));
   S->cur_sc = S->d_sc;
-  CK(cudaMallocHost(&S->h_sc, sizeof(DevScalars)));
   CK(dev_malloc(&S->d_ticket, sizeof(unsigned)));
   CK(cudaMemset(S->d_ticket, 0, sizeof(unsigned)));
   memset(S->h_sc, 0, sizeof(DevScalars));

@@ -295,8 +295,8 @@ int cudapcgB200ApplyOperatorNoAlloc(int analysis_flag, unsigned int nrows, unsig
 /* Number of bytes the library holds on the device for the current model and arrays. */
 unsigned long long cudapcgB200DeviceBytes(void);
 /* The solver's device blocks come from the current device's default stream-ordered memory pool,
-   which keeps freed blocks mapped for the next model (cudapcgEnd returns them to the pool, not
-   to the driver).  This hands every kept block of the pool back to the driver.  Returns 1, or 0
+   which keeps freed blocks (up to a quarter of the device's memory) mapped for the next model
+   (cudapcgEnd returns them to the pool, not to the driver).  This hands every kept block of the pool back to the driver.  Returns 1, or 0
    with cudapcgB200LastError() set. */
 int cudapcgB200TrimMemory(void);
 
